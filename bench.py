@@ -1,0 +1,383 @@
+"""Benchmark: batched 512^2 ocean updates per second on B200.
+
+Workload (one "step" = one frame of every ocean in the batch): the 512^2
+foam patch - 250 m, 22 m/s wind, choppiness 1.5, orbital velocity on and
+persistent advected foam (1 substep of 1/60 s per frame) - replicated over
+`--batch` independent sea states (seeds 7, 8, ...), frames at t = k/60 s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One JSON line on stdout (rank 0). `value` is device-timed (CUDA events on
+the launching stream, inputs resident in HBM); `e2e` is the same metric
+through ocean_batch_update_host with pinned host buffers, the copies of every
+output inside the timed region. Under torchrun every rank runs its own batch
+(no data-path collective: the oceans are independent), and the time is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "512^2 ocean updates/s (batched, exact FP32 FFT)"
+UNIT = "updates/s"
+N = 512
+CELLS = N * N
+# Algorithmic bytes per 512^2 update with velocity and persistent foam:
+# read h0 (8 B/cell), write displacement + normal + velocity RGBA32F
+# (48 B/cell), read + write the foam plane (8 B/cell) = 64 B/cell.
+ALG_BYTES_PER_CELL = 64
+# Split between the passes: the row pass reads h0 (8 B/cell); the column pass
+# writes the three RGBA32F outputs and reads/writes foam (56 B/cell).
+COL_ALG_BYTES_PER_CELL = 56
+ROW_ALG_BYTES_PER_CELL = 8
+L2_BYTES = 126 * 2 ** 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=64, help="oceans per GPU")
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        j = json.loads(p.read_text())
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def smi_id(local: int) -> str:
+    """nvidia-smi --id for the CUDA device (PCI bus id, so CUDA_VISIBLE_DEVICES
+    remapping cannot point the sampler at another GPU)."""
+    import torch
+
+    p = torch.cuda.get_device_properties(local)
+    try:
+        return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+    except AttributeError:
+        return str(local)
+
+
+def profile_traffic():
+    """ncu DRAM bytes per column-pass launch from the committed profile summary."""
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# Reference CPU implementation (the reference compiled from its own sources)
+# ---------------------------------------------------------------------------
+def reference_rate(seconds: float, warm: int = 2):
+    """Updates/s of the reference's own Ocean + FoamField on this host's cores
+    for the same workload, sequential frames of one ocean with its built-in
+    thread pool over all hardware threads (the reference's threaded path)."""
+    import oracle as O
+    from oceanlib_b200 import workloads as W
+
+    desc = W.foam_patch_512()
+    ro = O.RefOcean(desc)
+    rf = O.RefFoam(ro, W.foam_desc())
+    cores = int(O.ref().oref_hardware_concurrency())
+    dt = W.FOAM_DT
+    frame = 0
+    for _ in range(warm):
+        frame += 1
+        ro.update(frame * dt)
+        rf.update(dt)
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        frame += 1
+        ro.update(frame * dt)
+        rf.update(dt)
+        done += 1
+        el = time.perf_counter() - t0
+        if el >= seconds and done >= 3:
+            break
+    return done / el, cores, done
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    import oracle as O
+    from oceanlib_b200 import workloads as W
+
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference library not built"}))
+        return
+    desc = W.foam_patch_512()
+    ro = O.RefOcean(desc)
+    rf = O.RefFoam(ro, W.foam_desc())
+    cores = int(O.ref().oref_hardware_concurrency())
+    dt = W.FOAM_DT
+    per_step = 4  # frames of one ocean per step: a bounded sample of the batch frame
+    frame = 0
+    for _ in range(args.warmup * per_step):
+        frame += 1
+        ro.update(frame * dt)
+        rf.update(dt)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        for _ in range(per_step):
+            frame += 1
+            ro.update(frame * dt)
+            rf.update(dt)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = per_step * args.steps / total
+    ms = [1000.0 * t for t in times]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "foam_patch_512 (N=512, L=250 m, U=22 m/s, choppiness 1.5, "
+                               "velocity + persistent foam, dt=1/60 s)",
+                   "sample": f"{per_step} frames of one ocean per step"},
+        "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{per_step * args.steps} sequential frames of one 512^2 ocean, "
+                                   f"reference thread pool over {cores} hardware threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    import oceanlib_b200 as ob
+    from oceanlib_b200 import workloads as W
+
+    B = args.batch
+    descs = [W.foam_patch_512(seed=7 + rank * B + b) for b in range(B)]
+    batch = ob.OceanBatch(descs, foam=W.foam_desc(), chunk=args.chunk)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    dt = W.FOAM_DT
+    frame = 0
+
+    def step():
+        nonlocal frame
+        frame += 1
+        batch.update([frame * dt], foam_dt=dt, stream=sh)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- device-timed region ----
+    batch.set_profiling(True)
+    batch.read_profile()  # reset
+    launches0 = batch.launch_count
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    clocks = ClockSampler(smi_id(local))
+    clocks.start()
+    time.sleep(0.4)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    evs[0].record(stream)
+    for i in range(args.steps):
+        step()
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    total_ms = evs[0].elapsed_time(evs[-1])
+    prof = batch.read_profile()
+    batch.set_profiling(False)
+    launches = batch.launch_count - launches0
+
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    updates = B * args.steps * world
+    value = updates / (total_ms / 1000.0)
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    pinned = [torch.empty((B, CELLS, 4), dtype=torch.float32, pin_memory=True) for _ in range(3)]
+    pinned.append(torch.empty((B, CELLS), dtype=torch.float32, pin_memory=True))
+    disp, nrm, vel, foam = (t.numpy() for t in pinned)
+    e2e_steps = max(3, args.steps // 3)
+    for _ in range(2):
+        frame += 1
+        batch.update_host([frame * dt], dt, disp, nrm, vel, foam)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        frame += 1
+        batch.update_host([frame * dt], dt, disp, nrm, vel, foam)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = B * e2e_steps * world / e2e_s
+    d2h = B * CELLS * (3 * 16 + 4)
+    h2d = 8  # one absolute time per frame (double)
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        col_launch_ms = prof["col_ms"] / max(1, prof["col_launches"])
+        row_launch_ms = prof["row_ms"] / max(1, prof["row_launches"])
+        oceans_per_col_launch = B * args.steps / max(1, prof["col_launches"])
+        col_alg = COL_ALG_BYTES_PER_CELL * CELLS * oceans_per_col_launch
+        row_alg = ROW_ALG_BYTES_PER_CELL * CELLS * oceans_per_col_launch
+        col_achieved = col_alg / (col_launch_ms / 1000.0) / 1e9
+        frame_achieved = ALG_BYTES_PER_CELL * CELLS * (value / world) / 1e9
+        traffic = profile_traffic()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "foam_patch_512 (N=512, L=250 m, U=22 m/s, choppiness 1.5, "
+                                   "velocity + persistent foam, dt=1/60 s)",
+                       "oceans_per_gpu": B, "grid": N, "fft_form": "exact",
+                       "chunk_oceans": int(round(oceans_per_col_launch)),
+                       "l2": f"inputs larger than L2 (per-step working set "
+                             f"{B * CELLS * 72 / 2**30:.2f} GiB > 126 MB)",
+                       "parallelism": f"replicas x{world}"},
+            "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
+                           "p99": float(np.percentile(step_ms, 99))},
+            "roofline": {"bound": "hbm", "kernel": "col_pass (column FFT + finalize + foam)",
+                         "achieved": col_achieved, "peak": peak, "unit": "GB/s",
+                         "frac": col_achieved / peak, "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": col_alg,
+                         "avg_launch_ms": col_launch_ms,
+                         "traffic": None if traffic is None else traffic.get("col_bytes_per_launch_scaled"),
+                         "row_pass": {"avg_launch_ms": row_launch_ms, "alg_bytes_per_launch": row_alg,
+                                      "achieved": row_alg / (row_launch_ms / 1000.0) / 1e9},
+                         "frame": {"achieved": frame_achieved, "frac": frame_achieved / peak,
+                                   "alg_bytes_per_update": ALG_BYTES_PER_CELL * CELLS},
+                         "share": {"row": prof["row_ms"] / max(1e-9, prof["row_ms"] + prof["col_ms"]),
+                                   "col": prof["col_ms"] / max(1e-9, prof["row_ms"] + prof["col_ms"])}},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "api": "ocean_batch_update_host (pinned host buffers)"},
+        }
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                rate, cores, frames = reference_rate(args.cpu_seconds)
+                line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
+                                        "sample": f"{frames} sequential frames of one 512^2 ocean "
+                                                  f"(reference Ocean + FoamField, its thread pool "
+                                                  f"over {cores} hardware threads)"}
+            except Exception as e:  # the checker is optional on a box without it
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
+                                        "sample": f"unavailable: {e}"}
+        print(json.dumps(line))
+    batch.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,310 @@
+/* oceanlib-b200 - C ABI of the B200 (sm_100a) ocean library.
+ *
+ * Part 1 re-declares the reference oceanlib C ABI (include/ocean/ocean.h of
+ * DarshanVShah/oceanlib) with identical names, struct layouts, status codes
+ * and NULL-handle behaviour, so a binding written against the reference binds
+ * this library unchanged. Each declaration cites the reference line it
+ * replaces. Part 2 adds entry points that only a GPU library needs: device
+ * buffer access, asynchronous updates on a caller's stream, batched updates
+ * of many oceans in one launch, batched world queries, and persistent foam.
+ *
+ * All compute runs on the GPU; there is no CPU fallback. A handle is created
+ * on the CUDA device that is current on the calling thread.
+ */
+#ifndef OCEAN_B200_H
+#define OCEAN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__cplusplus)
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define OCEAN_API __declspec(dllexport)
+#else
+#define OCEAN_API __attribute__((visibility("default")))
+#endif
+
+/* =========================================================================
+ * Part 1: the reference C ABI (drop-in)
+ * ========================================================================= */
+
+/* Opaque handle. include/ocean/ocean.h:35 */
+typedef struct ocean_sim ocean_sim;
+
+/* include/ocean/ocean.h:37-42. Values are part of the ABI; new codes are only
+ * ever appended. */
+typedef enum ocean_status {
+    OCEAN_OK                  = 0,
+    OCEAN_ERROR_INVALID_ARG   = 1,
+    OCEAN_ERROR_OUT_OF_MEMORY = 2,
+    OCEAN_ERROR_UNKNOWN       = 3,
+    OCEAN_ERROR_DEVICE        = 4, /* a CUDA call failed (appended)          */
+    OCEAN_ERROR_TIMEOUT       = 5  /* a bounded device wait gave up          */
+} ocean_status;
+
+/* include/ocean/ocean.h:46 */
+OCEAN_API const char* ocean_status_string(ocean_status status);
+
+/* include/ocean/ocean.h:53-63. The hook is called exactly four times per
+ * ocean_update, each with count == 1, and every call launches and completes
+ * one device stage (row pass, column pass, displacement copy-back, normal
+ * copy-back). */
+typedef void (*ocean_task_fn)(void* ctx, uint32_t index);
+typedef void (*ocean_parallel_for_fn)(void* user, ocean_task_fn task, void* ctx,
+                                      uint32_t count);
+
+/* include/ocean/ocean.h:75-83. Never grows (embedded by value below). */
+typedef struct ocean_spectrum_desc {
+    float wind_speed;
+    float fetch;
+    float wind_direction;
+    float peak_enhancement;
+    float swell;
+    float small_wave_cutoff;
+    float gravity;
+} ocean_spectrum_desc;
+
+/* include/ocean/ocean.h:85-134. 88 bytes on LP64; struct_size prefix
+ * versioning: a smaller struct_size takes defaults for the missing tail, zero
+ * or a larger one is OCEAN_ERROR_INVALID_ARG. thread_count is accepted and
+ * ignored (the GPU does the work). */
+typedef struct ocean_desc {
+    size_t struct_size;
+    uint32_t size;
+    float    patch_length;
+    ocean_spectrum_desc spectrum;
+    float    choppiness;
+    float    foam_threshold;
+    uint64_t seed;
+    ocean_parallel_for_fn parallel_for;
+    void*                 parallel_for_user;
+    uint32_t              thread_count;
+    float    water_depth;
+    int32_t  compute_velocity;
+} ocean_desc;
+
+/* include/ocean/ocean.h:139 */
+OCEAN_API void ocean_desc_init(ocean_desc* desc);
+
+/* include/ocean/ocean.h:155-160. Host pointers into a pinned mirror that
+ * ocean_update refreshes before it returns. */
+typedef struct ocean_buffers {
+    const float* displacement;
+    const float* normal;
+    uint32_t     size;
+    float        patch_length;
+} ocean_buffers;
+
+/* include/ocean/ocean.h:162-170 */
+typedef struct ocean_surface {
+    float height;
+    float offset_x;
+    float offset_z;
+    float normal_x;
+    float normal_y;
+    float normal_z;
+    float foam;
+} ocean_surface;
+
+/* include/ocean/ocean.h:181. Allocates device memory, builds h0(k) on the
+ * device and evaluates t = 0. NULL + status on failure. */
+OCEAN_API ocean_sim* ocean_create(const ocean_desc* desc, ocean_status* out_status);
+
+/* include/ocean/ocean.h:184. NULL tolerated. */
+OCEAN_API void ocean_destroy(ocean_sim* sim);
+
+/* include/ocean/ocean.h:193. Absolute time; a pure function of
+ * (seed, desc, time). Runs the device frame and refreshes the host mirror
+ * synchronously. No allocation. */
+OCEAN_API void ocean_update(ocean_sim* sim, double time);
+
+/* include/ocean/ocean.h:195 */
+OCEAN_API ocean_buffers ocean_get_buffers(const ocean_sim* sim);
+
+/* include/ocean/ocean.h:197 */
+OCEAN_API double ocean_get_time(const ocean_sim* sim);
+
+/* include/ocean/ocean.h:205. Runs the reference's 4-step fixed-point
+ * inversion on the host mirror (one query is latency-bound; use
+ * ocean_sample_many for many). */
+OCEAN_API float ocean_height_at(const ocean_sim* sim, float world_x, float world_z);
+
+/* include/ocean/ocean.h:215 (frozen: returned by value). */
+OCEAN_API ocean_surface ocean_sample_at(const ocean_sim* sim, float world_x, float world_z);
+
+/* include/ocean/ocean.h:223-234 */
+typedef struct ocean_surface_ex {
+    float height;
+    float offset_x;
+    float offset_z;
+    float normal_x;
+    float normal_y;
+    float normal_z;
+    float foam;
+    float velocity_x;
+    float velocity_y;
+    float velocity_z;
+} ocean_surface_ex;
+
+/* include/ocean/ocean.h:234 */
+OCEAN_API void ocean_sample_ex(const ocean_sim* sim, float world_x, float world_z,
+                               ocean_surface_ex* out);
+
+/* include/ocean/ocean.h:240 */
+OCEAN_API const float* ocean_get_velocity(const ocean_sim* sim);
+
+/* include/ocean/ocean.h:249. Reports "CUDA sm_100a (exact)" or
+ * "CUDA sm_100a (fast)". */
+OCEAN_API const char* ocean_simd_level(void);
+
+/* include/ocean/ocean.h:262. "scalar" (and "sse2", "avx2", "neon", "exact")
+ * select the exact FFT form, whose results are bit-identical to the
+ * reference's scalar kernels; "fast" selects the FMA form. Affects handles
+ * created after the call. Returns the reference's spelling of the level for
+ * the reference names, so "scalar" returns "scalar". */
+OCEAN_API const char* ocean_force_simd_level(const char* name);
+
+/* include/ocean/ocean.h:265. Reports 1.0.0, the reference ABI version this
+ * library implements. */
+OCEAN_API void ocean_version(uint32_t* major, uint32_t* minor, uint32_t* patch);
+
+/* =========================================================================
+ * Part 2: GPU entry points (no reference counterpart; new symbols only)
+ * ========================================================================= */
+
+/* Device pointers (valid until destroy). RGBA32F layouts as in ocean_buffers;
+ * foam is N*N floats. Members are NULL when the feature is off. */
+typedef struct ocean_device_buffers {
+    float*   displacement;
+    float*   normal;
+    float*   velocity;
+    float*   foam;
+    uint32_t size;
+    float    patch_length;
+} ocean_device_buffers;
+
+/* FFT arithmetic forms. */
+typedef enum ocean_fft_form {
+    OCEAN_FFT_EXACT = 0, /* radix-2 Stockham in the reference's operation order,
+                            no FMA: bit-identical to the reference           */
+    OCEAN_FFT_FAST  = 1  /* same dataflow with fused multiply-adds           */
+} ocean_fft_form;
+
+/* Device pointers of a single ocean. */
+OCEAN_API ocean_status ocean_get_device_buffers(const ocean_sim* sim, ocean_device_buffers* out);
+
+/* Run the frame on `stream` (a cudaStream_t; NULL = the handle's own stream)
+ * and return without waiting or refreshing the host mirror. */
+OCEAN_API ocean_status ocean_update_async(ocean_sim* sim, double time, void* stream);
+
+/* Copy the current device outputs into the host mirror (synchronous). */
+OCEAN_API ocean_status ocean_refresh_host(ocean_sim* sim);
+
+/* Batched world queries on the device: `xz` holds count (x, z) pairs and
+ * `out` count ocean_surface_ex records. Both are HOST arrays here; the call
+ * copies them across and waits. Results are bit-identical to ocean_sample_ex
+ * point by point. */
+OCEAN_API ocean_status ocean_sample_many(const ocean_sim* sim, const float* xz, uint64_t count,
+                                         ocean_surface_ex* out);
+
+/* --- Persistent advected foam (reference: include/ocean/foam.hpp:38-142) - */
+
+/* Mirrors ocean::FoamDesc (include/ocean/foam.hpp:38-74). */
+typedef struct ocean_foam_desc {
+    size_t   struct_size;
+    float    decay;
+    float    source_gain;
+    float    advect_scale;
+    float    wind_drift_x;
+    float    wind_drift_z;
+    float    fixed_dt;
+    uint32_t max_substeps;
+} ocean_foam_desc;
+
+OCEAN_API void ocean_foam_desc_init(ocean_foam_desc* desc);
+
+/* --- Batches: many independent oceans advanced by one launch per pass ---- */
+
+typedef struct ocean_batch ocean_batch;
+
+typedef struct ocean_batch_desc {
+    size_t            struct_size;
+    const ocean_desc* oceans;          /* `count` descriptors, all the same size N */
+    uint32_t          count;
+    int32_t           fft_form;        /* ocean_fft_form                          */
+    int32_t           persistent_foam; /* non-zero: a FoamField per ocean (needs
+                                          compute_velocity on every ocean)        */
+    ocean_foam_desc   foam;
+    uint32_t          chunk;           /* oceans per row/column pass pair; 0 = auto
+                                          (sized so the intermediate stays in L2) */
+} ocean_batch_desc;
+
+OCEAN_API void ocean_batch_desc_init(ocean_batch_desc* desc);
+OCEAN_API ocean_batch* ocean_batch_create(const ocean_batch_desc* desc, ocean_status* out_status);
+OCEAN_API void ocean_batch_destroy(ocean_batch* batch);
+OCEAN_API uint32_t ocean_batch_count(const ocean_batch* batch);
+
+/* Advance every ocean to its absolute time (times[i], or times[0] for all
+ * when `per_ocean_times` is zero) and, when persistent foam is on, run the
+ * foam accumulator by foam_dt. Asynchronous on `stream` (NULL = the batch's
+ * own stream). No allocation. */
+OCEAN_API ocean_status ocean_batch_update(ocean_batch* batch, const double* times,
+                                          int32_t per_ocean_times, float foam_dt, void* stream);
+
+/* The same frame, end to end for host callers: times come from host memory
+ * and every ocean's outputs are copied into the caller's host arrays
+ * (displacement, normal, and velocity / foam when present; each array holds
+ * count * N*N*4 floats, foam count * N*N). Pinned host memory gives full
+ * copy bandwidth. Returns when the copies are complete. */
+OCEAN_API ocean_status ocean_batch_update_host(ocean_batch* batch, const double* times,
+                                               int32_t per_ocean_times, float foam_dt,
+                                               float* displacement, float* normal,
+                                               float* velocity, float* foam);
+
+OCEAN_API ocean_status ocean_batch_get_device_buffers(const ocean_batch* batch, uint32_t index,
+                                                      ocean_device_buffers* out);
+
+/* Number of foam substeps the last update ran (0..max_substeps). */
+OCEAN_API uint32_t ocean_batch_last_foam_substeps(const ocean_batch* batch);
+
+/* Waits for all work queued on the batch's own stream. */
+OCEAN_API ocean_status ocean_batch_synchronize(ocean_batch* batch);
+
+/* Device spectrum tables of ocean `index`, written to HOST memory as
+ * n*n float2 h0(k) (re, im) followed by n*n float2 (omega, 1/|k|). For
+ * parity checks of the device h0 generation. */
+OCEAN_API ocean_status ocean_batch_read_spectrum(const ocean_batch* batch, uint32_t index,
+                                                 float* h0, float* omega_kinv);
+
+/* Per-kernel device time of the frame passes, from CUDA events recorded on
+ * the launching stream around every launch while profiling is on. */
+typedef struct ocean_pass_profile {
+    uint64_t row_launches;
+    uint64_t col_launches;
+    uint64_t foam_launches;
+    double   row_ms;   /* summed launch durations */
+    double   col_ms;
+    double   foam_ms;
+} ocean_pass_profile;
+
+/* Turn per-launch event timing on or off (allocates its event pool when
+ * turned on, so do it outside any timed region). */
+OCEAN_API ocean_status ocean_batch_set_profiling(ocean_batch* batch, int32_t enable);
+
+/* Waits for the batch's work, returns the accumulated profile and resets it. */
+OCEAN_API ocean_status ocean_batch_read_profile(ocean_batch* batch, ocean_pass_profile* out);
+
+/* Kernels this batch has launched (all kinds) since it was created. */
+OCEAN_API uint64_t ocean_batch_launch_count(const ocean_batch* batch);
+
+/* Name of the device the library was built for ("sm_100a"). */
+OCEAN_API const char* ocean_device_arch(void);
+
+#if defined(__cplusplus)
+} /* extern "C" */
+#endif
+
+#endif /* OCEAN_B200_H */

@@ -1,0 +1,338 @@
+"""oceanlib_b200 - the B200 (sm_100a) ocean library, Python host side.
+
+Mirrors the reference's ocean::Ocean / OceanDesc interface (include/ocean/
+ocean.hpp of DarshanVShah/oceanlib) over the C ABI in include/ocean_b200.h:
+
+    desc = OceanDesc(size=256, patch_length=200.0, wind_speed=12.0)
+    ocean = Ocean(desc)            # ValueError on a malformed descriptor
+    ocean.update(10.0)             # absolute time; pure function of (seed, desc, t)
+    b = ocean.buffers()            # numpy views of the RGBA32F host mirror
+    ocean.height_at(3.0, 4.0)      # fixed-point inversion, on the GPU
+
+and adds OceanBatch for many oceans per launch. All compute runs in
+libocean_b200.so on the GPU; importing this package without the built library
+raises, there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .abi import OceanDescC, FoamDescC, BatchDescC, SurfaceEx, DeviceBuffers
+
+_LIB_PATH = Path(__file__).resolve().parent / "libocean_b200.so"
+_lib: Optional[C.CDLL] = None
+
+
+class OceanError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {status_string(status)} ({status})")
+
+
+def lib() -> C.CDLL:
+    """The loaded C-ABI library (loaded once, with every signature bound)."""
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            raise ImportError(
+                f"{_LIB_PATH} is missing: build it with `python -m oceanlib_b200.build`")
+        l = C.CDLL(str(_LIB_PATH))
+        for name, (res, args) in abi.SIGNATURES.items():
+            fn = getattr(l, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = l
+    return _lib
+
+
+def library_path() -> Path:
+    return _LIB_PATH
+
+
+def status_string(status: int) -> str:
+    return lib().ocean_status_string(status).decode()
+
+
+def _check(status: int, what: str) -> None:
+    if status != abi.OCEAN_OK:
+        raise OceanError(status, what)
+
+
+# ---------------------------------------------------------------------------
+# Descriptors
+# ---------------------------------------------------------------------------
+@dataclass
+class OceanDesc:
+    """ocean::OceanDesc (include/ocean/ocean.hpp:39-130) flattened: the
+    SpectrumDesc fields sit beside the grid fields."""
+
+    size: int = 256
+    patch_length: float = 200.0
+    wind_speed: float = 10.0
+    fetch: float = 100000.0
+    wind_direction: float = 0.0
+    peak_enhancement: float = 3.3
+    swell: float = 0.0
+    small_wave_cutoff: float = 0.5
+    gravity: float = 9.81
+    depth: float = 0.0
+    choppiness: float = 1.0
+    foam_threshold: float = 0.5
+    seed: int = 1337
+    compute_velocity: bool = False
+    thread_count: int = 0
+
+    def to_c(self) -> OceanDescC:
+        d = OceanDescC()
+        lib().ocean_desc_init(C.byref(d))
+        d.size = self.size
+        d.patch_length = self.patch_length
+        s = d.spectrum
+        s.wind_speed = self.wind_speed
+        s.fetch = self.fetch
+        s.wind_direction = self.wind_direction
+        s.peak_enhancement = self.peak_enhancement
+        s.swell = self.swell
+        s.small_wave_cutoff = self.small_wave_cutoff
+        s.gravity = self.gravity
+        d.water_depth = self.depth
+        d.choppiness = self.choppiness
+        d.foam_threshold = self.foam_threshold
+        d.seed = self.seed
+        d.compute_velocity = 1 if self.compute_velocity else 0
+        d.thread_count = self.thread_count
+        return d
+
+
+@dataclass
+class FoamDesc:
+    """ocean::FoamDesc (include/ocean/foam.hpp:38-74)."""
+
+    decay: float = 0.35
+    source_gain: float = 4.0
+    advect_scale: float = 1.0
+    wind_drift_x: float = 0.0
+    wind_drift_z: float = 0.0
+    fixed_dt: float = 1.0 / 60.0
+    max_substeps: int = 4
+
+    def to_c(self) -> FoamDescC:
+        f = FoamDescC()
+        lib().ocean_foam_desc_init(C.byref(f))
+        f.decay = self.decay
+        f.source_gain = self.source_gain
+        f.advect_scale = self.advect_scale
+        f.wind_drift_x = self.wind_drift_x
+        f.wind_drift_z = self.wind_drift_z
+        f.fixed_dt = self.fixed_dt
+        f.max_substeps = self.max_substeps
+        return f
+
+
+SURFACE_FIELDS = ("height", "offset_x", "offset_z", "normal_x", "normal_y", "normal_z", "foam",
+                  "velocity_x", "velocity_y", "velocity_z")
+
+
+def _host_view(ptr, count: int) -> np.ndarray:
+    return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_float)), shape=(count,))
+
+
+# ---------------------------------------------------------------------------
+# Single ocean (the reference-shaped handle)
+# ---------------------------------------------------------------------------
+class Ocean:
+    """One ocean patch on the current CUDA device; see ocean::Ocean."""
+
+    def __init__(self, desc: OceanDesc | OceanDescC):
+        cd = desc.to_c() if isinstance(desc, OceanDesc) else desc
+        st = C.c_int(-1)
+        h = lib().ocean_create(C.byref(cd), C.byref(st))
+        if not h:
+            if st.value == abi.OCEAN_ERROR_INVALID_ARG:
+                raise ValueError(f"invalid ocean descriptor ({status_string(st.value)})")
+            raise OceanError(st.value, "ocean_create")
+        self._h = h
+        self.size = cd.size
+        self.patch_length = cd.patch_length
+        self.velocity_on = bool(cd.compute_velocity)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().ocean_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def update(self, time: float) -> None:
+        lib().ocean_update(self._h, float(time))
+
+    def update_async(self, time: float, stream: int = 0) -> None:
+        _check(lib().ocean_update_async(self._h, float(time), C.c_void_p(stream)), "ocean_update_async")
+
+    def refresh_host(self) -> None:
+        _check(lib().ocean_refresh_host(self._h), "ocean_refresh_host")
+
+    @property
+    def time(self) -> float:
+        return lib().ocean_get_time(self._h)
+
+    def buffers(self) -> dict:
+        """Numpy views (N*N, 4) of the host mirror; rewritten by update()."""
+        b = lib().ocean_get_buffers(self._h)
+        n = b.size * b.size
+        out = {"displacement": _host_view(b.displacement, 4 * n).reshape(n, 4),
+               "normal": _host_view(b.normal, 4 * n).reshape(n, 4),
+               "size": b.size, "patch_length": b.patch_length}
+        v = lib().ocean_get_velocity(self._h)
+        out["velocity"] = _host_view(v, 4 * n).reshape(n, 4) if v else None
+        return out
+
+    def device_buffers(self) -> DeviceBuffers:
+        d = DeviceBuffers()
+        _check(lib().ocean_get_device_buffers(self._h, C.byref(d)), "ocean_get_device_buffers")
+        return d
+
+    def height_at(self, x: float, z: float) -> float:
+        return lib().ocean_height_at(self._h, x, z)
+
+    def sample_at(self, x: float, z: float) -> dict:
+        s = SurfaceEx()
+        lib().ocean_sample_ex(self._h, x, z, C.byref(s))
+        return {k: getattr(s, k) for k in SURFACE_FIELDS}
+
+    def sample_many(self, xz: np.ndarray) -> np.ndarray:
+        """(count, 2) float32 world positions -> (count, 10) float32 records in
+        SURFACE_FIELDS order, computed on the GPU."""
+        xz = np.ascontiguousarray(xz, dtype=np.float32)
+        out = np.empty((xz.shape[0], 10), dtype=np.float32)
+        _check(lib().ocean_sample_many(self._h, xz.ctypes.data, xz.shape[0], out.ctypes.data),
+               "ocean_sample_many")
+        return out
+
+
+# ---------------------------------------------------------------------------
+# Batches
+# ---------------------------------------------------------------------------
+class OceanBatch:
+    """Many same-size oceans advanced together (one row and one column launch
+    per chunk of oceans)."""
+
+    def __init__(self, descs: Sequence[OceanDesc], *, form: int = abi.OCEAN_FFT_EXACT,
+                 foam: Optional[FoamDesc] = None, chunk: int = 0):
+        arr = (OceanDescC * len(descs))(*[d.to_c() for d in descs])
+        bd = BatchDescC()
+        lib().ocean_batch_desc_init(C.byref(bd))
+        bd.oceans = arr
+        bd.count = len(descs)
+        bd.fft_form = form
+        bd.persistent_foam = 1 if foam is not None else 0
+        if foam is not None:
+            bd.foam = foam.to_c()
+        bd.chunk = chunk
+        st = C.c_int(-1)
+        h = lib().ocean_batch_create(C.byref(bd), C.byref(st))
+        if not h:
+            if st.value == abi.OCEAN_ERROR_INVALID_ARG:
+                raise ValueError(f"invalid batch descriptor ({status_string(st.value)})")
+            raise OceanError(st.value, "ocean_batch_create")
+        self._h = h
+        self._keep = arr
+        self.count = len(descs)
+        self.size = descs[0].size
+        self.velocity_on = bool(descs[0].compute_velocity)
+        self.foam_on = foam is not None
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().ocean_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def update(self, times, foam_dt: float = 0.0, stream: int = 0) -> None:
+        t = np.ascontiguousarray(np.atleast_1d(np.asarray(times, dtype=np.float64)))
+        per = 1 if t.size > 1 else 0
+        if per and t.size != self.count:
+            raise ValueError("times must hold one value or one per ocean")
+        _check(lib().ocean_batch_update(self._h, t.ctypes.data, per, float(foam_dt),
+                                        C.c_void_p(stream)), "ocean_batch_update")
+
+    def update_host(self, times, foam_dt: float, disp: np.ndarray, normal: np.ndarray,
+                    velocity: Optional[np.ndarray] = None, foam: Optional[np.ndarray] = None) -> None:
+        t = np.ascontiguousarray(np.atleast_1d(np.asarray(times, dtype=np.float64)))
+        per = 1 if t.size > 1 else 0
+        ptr = lambda a: None if a is None else a.ctypes.data
+        _check(lib().ocean_batch_update_host(self._h, t.ctypes.data, per, float(foam_dt),
+                                             ptr(disp), ptr(normal), ptr(velocity), ptr(foam)),
+               "ocean_batch_update_host")
+
+    def synchronize(self) -> None:
+        _check(lib().ocean_batch_synchronize(self._h), "ocean_batch_synchronize")
+
+    def device_buffers(self, index: int) -> DeviceBuffers:
+        d = DeviceBuffers()
+        _check(lib().ocean_batch_get_device_buffers(self._h, index, C.byref(d)),
+               "ocean_batch_get_device_buffers")
+        return d
+
+    @property
+    def last_foam_substeps(self) -> int:
+        return lib().ocean_batch_last_foam_substeps(self._h)
+
+    def set_profiling(self, on: bool) -> None:
+        _check(lib().ocean_batch_set_profiling(self._h, 1 if on else 0), "ocean_batch_set_profiling")
+
+    def read_profile(self) -> dict:
+        p = abi.PassProfile()
+        _check(lib().ocean_batch_read_profile(self._h, C.byref(p)), "ocean_batch_read_profile")
+        return {k: getattr(p, k) for k, _ in abi.PassProfile._fields_}
+
+    @property
+    def launch_count(self) -> int:
+        return lib().ocean_batch_launch_count(self._h)
+
+    def read_spectrum(self, index: int):
+        n = self.size
+        h0 = np.empty((n * n, 2), dtype=np.float32)
+        wk = np.empty((n * n, 2), dtype=np.float32)
+        _check(lib().ocean_batch_read_spectrum(self._h, index, h0.ctypes.data, wk.ctypes.data),
+               "ocean_batch_read_spectrum")
+        return h0, wk
+
+
+def force_simd_level(name: Optional[str]) -> str:
+    r = lib().ocean_force_simd_level(None if name is None else name.encode())
+    return r.decode()
+
+
+def simd_level() -> str:
+    return lib().ocean_simd_level().decode()
+
+
+def version() -> tuple:
+    a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    lib().ocean_version(C.byref(a), C.byref(b), C.byref(c))
+    return (a.value, b.value, c.value)

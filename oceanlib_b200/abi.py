@@ -1,0 +1,157 @@
+"""ctypes mirror of include/ocean_b200.h (the reference C ABI's structs plus the
+GPU extensions). Pure layout: importing this module touches no library."""
+from __future__ import annotations
+
+import ctypes as C
+
+OCEAN_OK = 0
+OCEAN_ERROR_INVALID_ARG = 1
+OCEAN_ERROR_OUT_OF_MEMORY = 2
+OCEAN_ERROR_UNKNOWN = 3
+OCEAN_ERROR_DEVICE = 4
+OCEAN_ERROR_TIMEOUT = 5
+
+OCEAN_FFT_EXACT = 0
+OCEAN_FFT_FAST = 1
+
+TASK_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32)
+PARALLEL_FOR_FN = C.CFUNCTYPE(None, C.c_void_p, TASK_FN, C.c_void_p, C.c_uint32)
+
+
+class SpectrumDesc(C.Structure):
+    _fields_ = [
+        ("wind_speed", C.c_float),
+        ("fetch", C.c_float),
+        ("wind_direction", C.c_float),
+        ("peak_enhancement", C.c_float),
+        ("swell", C.c_float),
+        ("small_wave_cutoff", C.c_float),
+        ("gravity", C.c_float),
+    ]
+
+
+class OceanDescC(C.Structure):
+    """`ocean_desc` (include/ocean/ocean.h:85-134 in the reference)."""
+
+    _fields_ = [
+        ("struct_size", C.c_size_t),
+        ("size", C.c_uint32),
+        ("patch_length", C.c_float),
+        ("spectrum", SpectrumDesc),
+        ("choppiness", C.c_float),
+        ("foam_threshold", C.c_float),
+        ("seed", C.c_uint64),
+        ("parallel_for", C.c_void_p),
+        ("parallel_for_user", C.c_void_p),
+        ("thread_count", C.c_uint32),
+        ("water_depth", C.c_float),
+        ("compute_velocity", C.c_int32),
+    ]
+
+
+class Buffers(C.Structure):
+    _fields_ = [
+        ("displacement", C.POINTER(C.c_float)),
+        ("normal", C.POINTER(C.c_float)),
+        ("size", C.c_uint32),
+        ("patch_length", C.c_float),
+    ]
+
+
+class Surface(C.Structure):
+    _fields_ = [(n, C.c_float) for n in
+                ("height", "offset_x", "offset_z", "normal_x", "normal_y", "normal_z", "foam")]
+
+
+class SurfaceEx(C.Structure):
+    _fields_ = [(n, C.c_float) for n in
+                ("height", "offset_x", "offset_z", "normal_x", "normal_y", "normal_z", "foam",
+                 "velocity_x", "velocity_y", "velocity_z")]
+
+
+class DeviceBuffers(C.Structure):
+    _fields_ = [
+        ("displacement", C.c_void_p),
+        ("normal", C.c_void_p),
+        ("velocity", C.c_void_p),
+        ("foam", C.c_void_p),
+        ("size", C.c_uint32),
+        ("patch_length", C.c_float),
+    ]
+
+
+class FoamDescC(C.Structure):
+    """Mirrors ocean::FoamDesc (include/ocean/foam.hpp:38-74)."""
+
+    _fields_ = [
+        ("struct_size", C.c_size_t),
+        ("decay", C.c_float),
+        ("source_gain", C.c_float),
+        ("advect_scale", C.c_float),
+        ("wind_drift_x", C.c_float),
+        ("wind_drift_z", C.c_float),
+        ("fixed_dt", C.c_float),
+        ("max_substeps", C.c_uint32),
+    ]
+
+
+class BatchDescC(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_size_t),
+        ("oceans", C.POINTER(OceanDescC)),
+        ("count", C.c_uint32),
+        ("fft_form", C.c_int32),
+        ("persistent_foam", C.c_int32),
+        ("foam", FoamDescC),
+        ("chunk", C.c_uint32),
+    ]
+
+
+class PassProfile(C.Structure):
+    _fields_ = [
+        ("row_launches", C.c_uint64),
+        ("col_launches", C.c_uint64),
+        ("foam_launches", C.c_uint64),
+        ("row_ms", C.c_double),
+        ("col_ms", C.c_double),
+        ("foam_ms", C.c_double),
+    ]
+
+
+# Every function include/ocean_b200.h declares, with its ctypes signature.
+SIGNATURES = {
+    "ocean_status_string": (C.c_char_p, [C.c_int]),
+    "ocean_desc_init": (None, [C.POINTER(OceanDescC)]),
+    "ocean_create": (C.c_void_p, [C.POINTER(OceanDescC), C.POINTER(C.c_int)]),
+    "ocean_destroy": (None, [C.c_void_p]),
+    "ocean_update": (None, [C.c_void_p, C.c_double]),
+    "ocean_get_buffers": (Buffers, [C.c_void_p]),
+    "ocean_get_time": (C.c_double, [C.c_void_p]),
+    "ocean_height_at": (C.c_float, [C.c_void_p, C.c_float, C.c_float]),
+    "ocean_sample_at": (Surface, [C.c_void_p, C.c_float, C.c_float]),
+    "ocean_sample_ex": (None, [C.c_void_p, C.c_float, C.c_float, C.POINTER(SurfaceEx)]),
+    "ocean_get_velocity": (C.POINTER(C.c_float), [C.c_void_p]),
+    "ocean_simd_level": (C.c_char_p, []),
+    "ocean_force_simd_level": (C.c_char_p, [C.c_char_p]),
+    "ocean_version": (None, [C.POINTER(C.c_uint32)] * 3),
+    "ocean_get_device_buffers": (C.c_int, [C.c_void_p, C.POINTER(DeviceBuffers)]),
+    "ocean_update_async": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
+    "ocean_refresh_host": (C.c_int, [C.c_void_p]),
+    "ocean_sample_many": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
+    "ocean_foam_desc_init": (None, [C.POINTER(FoamDescC)]),
+    "ocean_batch_desc_init": (None, [C.POINTER(BatchDescC)]),
+    "ocean_batch_create": (C.c_void_p, [C.POINTER(BatchDescC), C.POINTER(C.c_int)]),
+    "ocean_batch_destroy": (None, [C.c_void_p]),
+    "ocean_batch_count": (C.c_uint32, [C.c_void_p]),
+    "ocean_batch_update": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_void_p]),
+    "ocean_batch_update_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_float,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ocean_batch_get_device_buffers": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(DeviceBuffers)]),
+    "ocean_batch_last_foam_substeps": (C.c_uint32, [C.c_void_p]),
+    "ocean_batch_synchronize": (C.c_int, [C.c_void_p]),
+    "ocean_batch_read_spectrum": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "ocean_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
+    "ocean_batch_read_profile": (C.c_int, [C.c_void_p, C.POINTER(PassProfile)]),
+    "ocean_batch_launch_count": (C.c_uint64, [C.c_void_p]),
+    "ocean_device_arch": (C.c_char_p, []),
+}

@@ -1,0 +1,543 @@
+// oceanlib-b200: the per-frame kernels.
+//
+// One frame of N x N oceans is two passes over HBM/L2:
+//
+//   row pass   (grid: row-pair groups x oceans)
+//     h0 rows y and N-y -> shared memory; evolve every cell of both rows into
+//     NF packed complex fields (src/core/evolve.cpp:28-184); 2*NF row FFTs in
+//     shared memory, one lane group per sequence; write the rows to the
+//     intermediate, cell-major [y][x][field] so the column pass reads whole
+//     128-byte lines.
+//
+//   column pass (grid: W-column strips x oceans)
+//     gather the strip's NF*W columns; column FFTs; finalize every cell
+//     (src/core/evolve.cpp:238-327 and :186-203) straight into the RGBA32F
+//     displacement / normal / velocity outputs; optionally the first
+//     persistent-foam substep (src/foam.cpp:89-139) for the same cell, reading
+//     only the previous foam state.
+//
+// Pairing rows y and N-y means h0(-k) - the conjugate-mirror table the
+// reference stores separately (src/core/spectrum.cpp:329-338) - is read from
+// the other row already in shared memory, so h0 is read from HBM once.
+#include "ocean_device.cuh"
+#include "spectrum.h"
+
+namespace ocean_b200 {
+namespace {
+
+constexpr int kPad = 4;  // float2 padding between sequences in shared memory
+
+template <int LOG_N>
+struct Shape {
+    static constexpr int N = 1 << LOG_N;
+    static constexpr int G = lanes_for(LOG_N);                       // lanes / sequence
+    static constexpr int SEQ = N + kPad;                             // sequence stride
+    static constexpr int RP = cmin(N / 2, 32 / G > 1 ? 32 / G : 1); // row pairs / CTA
+    // columns / CTA: 4 at N = 512 (128-byte rows of the intermediate); 2 at
+    // N = 1024, where 32 values per lane leave room for fewer threads only.
+    static constexpr int W = LOG_N >= 10 ? 2 : cmin(N, (128 / G) > 4 ? 128 / G : 4);
+};
+
+// ---------------------------------------------------------------------------
+// Row pass
+// ---------------------------------------------------------------------------
+template <int LOG_N, int NF, bool FAST>
+__global__ void __launch_bounds__(Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G)
+row_pass_kernel(FrameArgs a)
+{
+    using S = Shape<LOG_N>;
+    constexpr int N = S::N, G = S::G, SEQ = S::SEQ, RP = S::RP;
+    constexpr int NT = RP * 2 * NF * G;
+
+    extern __shared__ float4 smem4[];
+    float2* data = reinterpret_cast<float2*>(smem4);  // [RP*2*NF][SEQ]
+    float2* h0s = data + RP * 2 * NF * SEQ;           // [RP*2][N]
+    float2* tws = h0s + RP * 2 * N;                   // [N-1]
+
+    const int tid = threadIdx.x;
+    const int o = blockIdx.y;
+    const int ocean = a.ocean_base + o;
+    const OceanConsts cst = a.consts[ocean];
+    const double top = a.t_over_2pi[ocean];
+    const float2* geom = a.omega_kinv + static_cast<size_t>(cst.geom) * N * N;
+    const float* kvec = a.kvec + static_cast<size_t>(cst.geom) * N;
+    const float2* h0 = a.h0 + static_cast<size_t>(ocean) * N * N;
+
+    // Rows handled by pair slot j of this CTA: (p, N-p), or (0, N/2) for p = 0.
+    auto row_of = [&](int j, int r) -> int {
+        const int p = blockIdx.x * RP + j;
+        if (p == 0) return r ? N / 2 : 0;
+        return r ? N - p : p;
+    };
+
+    // Stage the 2*RP h0 rows and the twiddles.
+    for (int i = tid; i < RP * 2 * (N / 2); i += NT) {
+        const int jr = i / (N / 2);
+        const int c = i % (N / 2);
+        const int row = row_of(jr >> 1, jr & 1);
+        reinterpret_cast<float4*>(h0s + jr * N)[c] =
+            reinterpret_cast<const float4*>(h0 + static_cast<size_t>(row) * N)[c];
+    }
+    for (int i = tid; i < N - 1; i += NT) tws[i] = a.twiddles[i];
+    __syncthreads();
+
+    // Evolve (src/core/evolve.cpp:28-121 and :123-184), one cell at a time.
+    for (int cell = tid; cell < RP * 2 * N; cell += NT) {
+        const int jr = cell >> LOG_N;  // j*2 + r
+        const int x = cell & (N - 1);
+        const int j = jr >> 1, r = jr & 1;
+        const int p = blockIdx.x * RP + j;
+        const int row = row_of(j, r);
+        const int mr = (p == 0) ? r : 1 - r;  // row holding h0 at -kz
+        const float2 av = h0s[jr * N + x];
+        const float2 bm = h0s[(j * 2 + mr) * N + ((N - x) & (N - 1))];
+        const float b_re = bm.x, b_im = -bm.y;
+        const float2 wk = geom[static_cast<size_t>(row) * N + x];
+
+        float s, c;
+        sincos_poly(fold_phase(wk.x, top), s, c);
+        const float fwd_re = av.x * c - av.y * s;
+        const float fwd_im = av.x * s + av.y * c;
+        const float bwd_re = b_re * c + b_im * s;
+        const float bwd_im = b_im * c - b_re * s;
+        const float hr = fwd_re + bwd_re;
+        const float hi = fwd_im + bwd_im;
+        const float kx = kvec[x];
+        const float kz = kvec[row];
+        const float ki = wk.y;
+        const float sx = kx * ki;
+        const float sz = kz * ki;
+        const float dx_re = sx * hi, dx_im = -sx * hr;
+        const float dz_re = sz * hi, dz_im = -sz * hr;
+        const float hx_re = -kx * hi, hx_im = kx * hr;
+        const float hz_re = -kz * hi, hz_im = kz * hr;
+        const float jxx = kx * sx, jzz = kz * sz, jxz = kx * sz;
+        const float jxx_re = jxx * hr, jxx_im = jxx * hi;
+        const float jzz_re = jzz * hr, jzz_im = jzz * hi;
+        const float jxz_re = jxz * hr, jxz_im = jxz * hi;
+
+        float2* base = data + (jr * NF) * SEQ + swz(x);
+        base[0 * SEQ] = make_float2(hr - dx_im, hi + dx_re);
+        base[1 * SEQ] = make_float2(dz_re - hx_im, dz_im + hx_re);
+        base[2 * SEQ] = make_float2(hz_re - jxx_im, hz_im + jxx_re);
+        base[3 * SEQ] = make_float2(jzz_re - jxz_im, jzz_im + jxz_re);
+        if constexpr (NF == 6) {
+            const float dr = fwd_re - bwd_re;
+            const float di = fwd_im - bwd_im;
+            const float w = wk.x;
+            const float wsx = w * sx, wsz = w * sz;
+            const float ux_re = -wsx * dr, ux_im = -wsx * di;
+            const float uz_re = -wsz * dr, uz_im = -wsz * di;
+            const float uy_re = -w * di, uy_im = w * dr;
+            base[4 * SEQ] = make_float2(ux_re - uy_im, ux_im + uy_re);
+            base[5 * SEQ] = make_float2(uz_re, uz_im);
+        }
+    }
+    __syncthreads();
+
+    fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);
+    __syncthreads();
+
+    // Write both rows cell-major: inter[o][row][x][f], NF/2 float4 per cell.
+    constexpr int Q = NF / 2;
+    float4* inter = reinterpret_cast<float4*>(a.inter + static_cast<size_t>(o) * N * N * NF);
+    for (int i = tid; i < RP * 2 * N * Q; i += NT) {
+        const int jr = i / (N * Q);
+        const int rem = i % (N * Q);
+        const int x = rem / Q;
+        const int fp = rem % Q;
+        const int row = row_of(jr >> 1, jr & 1);
+        const float2 v0 = data[(jr * NF + 2 * fp) * SEQ + swz(x)];
+        const float2 v1 = data[(jr * NF + 2 * fp + 1) * SEQ + swz(x)];
+        inter[(static_cast<size_t>(row) * N + x) * Q + fp] = make_float4(v0.x, v0.y, v1.x, v1.y);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Column pass
+// ---------------------------------------------------------------------------
+
+// Periodic bilinear fetch from one channel grid (src/foam.cpp:22-41).
+__device__ __forceinline__ float foam_sample_wrap(const float* f, float u, float v, int n)
+{
+    const float fu = floorf(u), fv = floorf(v);
+    const float tu = u - fu, tv = v - fv;
+    int x0 = __float2int_rz(fu) % n;
+    if (x0 < 0) x0 += n;
+    int z0 = __float2int_rz(fv) % n;
+    if (z0 < 0) z0 += n;
+    const int x1 = (x0 + 1) % n;
+    const int z1 = (z0 + 1) % n;
+    const float fa = f[static_cast<size_t>(z0) * n + x0];
+    const float fb = f[static_cast<size_t>(z0) * n + x1];
+    const float fc = f[static_cast<size_t>(z1) * n + x0];
+    const float fd = f[static_cast<size_t>(z1) * n + x1];
+    return fa * (1.0f - tu) * (1.0f - tv) + fb * tu * (1.0f - tv) + fc * (1.0f - tu) * tv +
+           fd * tu * tv;
+}
+
+// One persistent-foam substep for cell (x, z) (src/foam.cpp:89-139).
+__device__ __forceinline__ float foam_cell(const float* cur, int n, int x, int z, float velx,
+                                           float velz, float src, float dt, float decay,
+                                           float gain, float scale, float drift_x,
+                                           float drift_z, float inv_cell)
+{
+    const float vx = velx * scale + drift_x;
+    const float vz = velz * scale + drift_z;
+    const float su = static_cast<float>(x) - vx * dt * inv_cell;
+    const float sv = static_cast<float>(z) - vz * dt * inv_cell;
+    float f = foam_sample_wrap(cur, su, sv, n);
+    f = f * decay + src * gain;
+    if (f > 1.0f) f = 1.0f;
+    if (f < 0.0f) f = 0.0f;
+    return f;
+}
+
+template <int LOG_N, int NF, bool FAST, bool FOAM>
+__global__ void __launch_bounds__(NF * Shape<LOG_N>::W * Shape<LOG_N>::G)
+col_pass_kernel(FrameArgs a)
+{
+    using S = Shape<LOG_N>;
+    constexpr int N = S::N, G = S::G, SEQ = S::SEQ, W = S::W;
+    constexpr int NT = NF * W * G;
+    constexpr int Q = NF / 2;
+
+    extern __shared__ float4 smem4[];
+    float2* data = reinterpret_cast<float2*>(smem4);  // [NF*W][SEQ], sequence = f*W + w
+    float2* tws = data + NF * W * SEQ;
+
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * W;
+    const int o = blockIdx.y;
+    const int ocean = a.ocean_base + o;
+
+    const float4* inter =
+        reinterpret_cast<const float4*>(a.inter + static_cast<size_t>(o) * N * N * NF);
+    for (int i = tid; i < N * W * Q; i += NT) {
+        const int y = i / (W * Q);
+        const int rem = i % (W * Q);
+        const int w = rem / Q;
+        const int fp = rem % Q;
+        const float4 v = inter[(static_cast<size_t>(y) * N + x0 + w) * Q + fp];
+        data[((2 * fp) * W + w) * SEQ + swz(y)] = make_float2(v.x, v.y);
+        data[((2 * fp + 1) * W + w) * SEQ + swz(y)] = make_float2(v.z, v.w);
+    }
+    for (int i = tid; i < N - 1; i += NT) tws[i] = a.twiddles[i];
+    __syncthreads();
+
+    fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);
+    __syncthreads();
+
+    const OceanConsts cst = a.consts[ocean];
+    const float lambda = cst.lambda;
+    const size_t base = static_cast<size_t>(ocean) * N * N;
+    for (int i = tid; i < N * W; i += NT) {
+        const int y = i / W;
+        const int w = i % W;
+        const int x = x0 + w;
+        const int sy = swz(y);
+        const float2 f0 = data[(0 * W + w) * SEQ + sy];
+        const float2 f1 = data[(1 * W + w) * SEQ + sy];
+        const float2 f2 = data[(2 * W + w) * SEQ + sy];
+        const float2 f3 = data[(3 * W + w) * SEQ + sy];
+        const float h = f0.x, d_x = f0.y, d_z = f1.x, hx = f1.y;
+        const float hz = f2.x, jxx = f2.y, jzz = f3.x, jxz = f3.y;
+
+        const float disp_x = lambda * d_x;
+        const float disp_z = lambda * d_z;
+        const float axx = 1.0f + lambda * jxx;
+        const float azz = 1.0f + lambda * jzz;
+        const float axz = lambda * jxz;
+        const float jac = axx * azz - axz * axz;
+        float nx = -(hx * azz - axz * hz);
+        float ny = jac;
+        float nz = -(axx * hz - hx * axz);
+        const float len2 = nx * nx + ny * ny + nz * nz;
+        const float inv_len = (len2 > 0.0f) ? 1.0f / sqrtf(len2) : 0.0f;
+        nx *= inv_len;
+        ny *= inv_len;
+        nz *= inv_len;
+        float foam = (cst.foam_threshold - jac) * cst.inv_threshold;
+        if (foam < 0.0f) foam = 0.0f;
+        if (foam > 1.0f) foam = 1.0f;
+
+        const size_t idx = base + static_cast<size_t>(y) * N + x;
+        __stcs(&a.disp[idx], make_float4(disp_x, h, disp_z, foam));
+        __stcs(&a.normal[idx], make_float4(nx, ny, nz, jac));
+        if constexpr (NF == 6) {
+            const float2 f4 = data[(4 * W + w) * SEQ + sy];
+            const float2 f5 = data[(5 * W + w) * SEQ + sy];
+            __stcs(&a.velocity[idx], make_float4(f4.x, f4.y, f5.x, 0.0f));
+            if constexpr (FOAM) {
+                const float* cur = a.foam_cur + base;
+                a.foam_next[idx] = foam_cell(cur, N, x, y, f4.x, f5.x, foam, a.foam_dt,
+                                             a.foam_decay, a.foam_gain, a.foam_scale,
+                                             a.foam_drift_x, a.foam_drift_z, a.foam_inv_cell);
+            }
+        }
+    }
+}
+
+__global__ void foam_step_kernel(int n, int count, const float4* __restrict__ disp,
+                                 const float4* __restrict__ vel, const float* __restrict__ cur,
+                                 float* __restrict__ next, float dt, float decay, float gain,
+                                 float scale, float drift_x, float drift_z, float inv_cell)
+{
+    const uint64_t cells = static_cast<uint64_t>(n) * n;
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= cells * count) return;
+    const uint64_t o = i / cells;
+    const uint64_t c = i % cells;
+    const int z = static_cast<int>(c / n), x = static_cast<int>(c % n);
+    const float4 v = vel[i];
+    const float src = disp[i].w;
+    next[i] = foam_cell(cur + o * cells, n, x, z, v.x, v.z, src, dt, decay, gain, scale, drift_x,
+                        drift_z, inv_cell);
+}
+
+// ---------------------------------------------------------------------------
+// World queries (src/ocean.cpp:322-452)
+// ---------------------------------------------------------------------------
+struct Tap {
+    uint32_t i00, i10, i01, i11;
+    float w00, w10, w01, w11;
+};
+
+__device__ __forceinline__ uint32_t wrap_index(int i, int n)
+{
+    i %= n;
+    if (i < 0) i += n;
+    return static_cast<uint32_t>(i);
+}
+
+__device__ __forceinline__ Tap make_tap(float u, float v, int n, float inv_cell)
+{
+    const float gu = u * inv_cell;
+    const float gv = v * inv_cell;
+    const float fu = floorf(gu);
+    const float fv = floorf(gv);
+    const uint32_t x0 = wrap_index(__float2int_rz(fu), n);
+    const uint32_t z0 = wrap_index(__float2int_rz(fv), n);
+    const uint32_t x1 = (x0 + 1u) % static_cast<uint32_t>(n);
+    const uint32_t z1 = (z0 + 1u) % static_cast<uint32_t>(n);
+    const float tu = gu - fu;
+    const float tv = gv - fv;
+    Tap t;
+    t.i00 = z0 * n + x0;
+    t.i10 = z0 * n + x1;
+    t.i01 = z1 * n + x0;
+    t.i11 = z1 * n + x1;
+    t.w00 = (1.0f - tu) * (1.0f - tv);
+    t.w10 = tu * (1.0f - tv);
+    t.w01 = (1.0f - tu) * tv;
+    t.w11 = tu * tv;
+    return t;
+}
+
+struct Texels {
+    float4 a, b, c, d;
+};
+
+__device__ __forceinline__ Texels load_texels(const float4* __restrict__ buf, const Tap& t)
+{
+    return Texels{__ldg(&buf[t.i00]), __ldg(&buf[t.i10]), __ldg(&buf[t.i01]), __ldg(&buf[t.i11])};
+}
+
+// buf[i00+c]*w00 + buf[i10+c]*w10 + buf[i01+c]*w01 + buf[i11+c]*w11, in that order.
+#define OCEAN_FETCH(T, t, C) ((T).a.C * (t).w00 + (T).b.C * (t).w10 + (T).c.C * (t).w01 + (T).d.C * (t).w11)
+
+__global__ void sample_kernel(int n, float inv_cell, const float4* __restrict__ disp,
+                              const float4* __restrict__ normal, const float4* __restrict__ vel,
+                              const float2* __restrict__ xz, uint64_t count,
+                              SurfaceEx* __restrict__ out)
+{
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float2 p = xz[i];
+    float u = p.x, v = p.y;
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+        const Tap t = make_tap(u, v, n, inv_cell);
+        const Texels d = load_texels(disp, t);
+        u = p.x - OCEAN_FETCH(d, t, x);
+        v = p.y - OCEAN_FETCH(d, t, z);
+    }
+    const Tap t = make_tap(u, v, n, inv_cell);
+    const Texels d = load_texels(disp, t);
+    SurfaceEx s;
+    s.offset_x = OCEAN_FETCH(d, t, x);
+    s.height = OCEAN_FETCH(d, t, y);
+    s.offset_z = OCEAN_FETCH(d, t, z);
+    s.foam = OCEAN_FETCH(d, t, w);
+    const Texels nm = load_texels(normal, t);
+    float nx = OCEAN_FETCH(nm, t, x);
+    float ny = OCEAN_FETCH(nm, t, y);
+    float nz = OCEAN_FETCH(nm, t, z);
+    const float len2 = nx * nx + ny * ny + nz * nz;
+    if (len2 > 0.0f) {
+        const float inv = 1.0f / sqrtf(len2);
+        nx *= inv;
+        ny *= inv;
+        nz *= inv;
+    } else {
+        nx = 0.0f;
+        ny = 1.0f;
+        nz = 0.0f;
+    }
+    s.normal_x = nx;
+    s.normal_y = ny;
+    s.normal_z = nz;
+    if (vel != nullptr) {
+        const Texels vv = load_texels(vel, t);
+        s.velocity_x = OCEAN_FETCH(vv, t, x);
+        s.velocity_y = OCEAN_FETCH(vv, t, y);
+        s.velocity_z = OCEAN_FETCH(vv, t, z);
+    } else {
+        s.velocity_x = s.velocity_y = s.velocity_z = 0.0f;
+    }
+    out[i] = s;
+}
+
+// ---------------------------------------------------------------------------
+// Launch helpers: compile-time dispatch over (log N, fields, form, foam).
+// ---------------------------------------------------------------------------
+template <int LOG_N, int NF>
+constexpr size_t row_smem_bytes()
+{
+    using S = Shape<LOG_N>;
+    return sizeof(float2) * (S::RP * 2 * NF * S::SEQ + S::RP * 2 * S::N + (S::N - 1));
+}
+template <int LOG_N, int NF>
+constexpr size_t col_smem_bytes()
+{
+    using S = Shape<LOG_N>;
+    return sizeof(float2) * (NF * S::W * S::SEQ + (S::N - 1));
+}
+
+template <int LOG_N, int NF, bool FAST>
+cudaError_t row_launch(const FrameArgs& a, cudaStream_t st)
+{
+    using S = Shape<LOG_N>;
+    constexpr size_t smem = row_smem_bytes<LOG_N, NF>();
+    auto k = row_pass_kernel<LOG_N, NF, FAST>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    dim3 grid((S::N / 2) / S::RP, a.chunk);
+    k<<<grid, S::RP * 2 * NF * S::G, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int LOG_N, int NF, bool FAST, bool FOAM>
+cudaError_t col_launch(const FrameArgs& a, cudaStream_t st)
+{
+    using S = Shape<LOG_N>;
+    constexpr size_t smem = col_smem_bytes<LOG_N, NF>();
+    auto k = col_pass_kernel<LOG_N, NF, FAST, FOAM>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    dim3 grid(S::N / S::W, a.chunk);
+    k<<<grid, NF * S::W * S::G, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int LOG_N>
+cudaError_t row_dispatch_n(int nf, bool fast, const FrameArgs& a, cudaStream_t st)
+{
+    if (nf == 4) return fast ? row_launch<LOG_N, 4, true>(a, st) : row_launch<LOG_N, 4, false>(a, st);
+    return fast ? row_launch<LOG_N, 6, true>(a, st) : row_launch<LOG_N, 6, false>(a, st);
+}
+
+template <int LOG_N>
+cudaError_t col_dispatch_n(int nf, bool fast, bool foam, const FrameArgs& a, cudaStream_t st)
+{
+    if (nf == 4) return fast ? col_launch<LOG_N, 4, true, false>(a, st)
+                             : col_launch<LOG_N, 4, false, false>(a, st);
+    if (foam) return fast ? col_launch<LOG_N, 6, true, true>(a, st)
+                          : col_launch<LOG_N, 6, false, true>(a, st);
+    return fast ? col_launch<LOG_N, 6, true, false>(a, st) : col_launch<LOG_N, 6, false, false>(a, st);
+}
+
+}  // namespace
+
+cudaError_t launch_row_pass(int log_n, int nf, bool fast, const FrameArgs& a, cudaStream_t st)
+{
+    switch (log_n) {
+        case 4: return row_dispatch_n<4>(nf, fast, a, st);
+        case 5: return row_dispatch_n<5>(nf, fast, a, st);
+        case 6: return row_dispatch_n<6>(nf, fast, a, st);
+        case 7: return row_dispatch_n<7>(nf, fast, a, st);
+        case 8: return row_dispatch_n<8>(nf, fast, a, st);
+        case 9: return row_dispatch_n<9>(nf, fast, a, st);
+        case 10: return row_dispatch_n<10>(nf, fast, a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_col_pass(int log_n, int nf, bool fast, bool fuse_foam, const FrameArgs& a,
+                            cudaStream_t st)
+{
+    switch (log_n) {
+        case 4: return col_dispatch_n<4>(nf, fast, fuse_foam, a, st);
+        case 5: return col_dispatch_n<5>(nf, fast, fuse_foam, a, st);
+        case 6: return col_dispatch_n<6>(nf, fast, fuse_foam, a, st);
+        case 7: return col_dispatch_n<7>(nf, fast, fuse_foam, a, st);
+        case 8: return col_dispatch_n<8>(nf, fast, fuse_foam, a, st);
+        case 9: return col_dispatch_n<9>(nf, fast, fuse_foam, a, st);
+        case 10: return col_dispatch_n<10>(nf, fast, fuse_foam, a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+size_t row_pass_smem(int log_n, int nf)
+{
+    switch (log_n) {
+        case 4: return nf == 4 ? row_smem_bytes<4, 4>() : row_smem_bytes<4, 6>();
+        case 5: return nf == 4 ? row_smem_bytes<5, 4>() : row_smem_bytes<5, 6>();
+        case 6: return nf == 4 ? row_smem_bytes<6, 4>() : row_smem_bytes<6, 6>();
+        case 7: return nf == 4 ? row_smem_bytes<7, 4>() : row_smem_bytes<7, 6>();
+        case 8: return nf == 4 ? row_smem_bytes<8, 4>() : row_smem_bytes<8, 6>();
+        case 9: return nf == 4 ? row_smem_bytes<9, 4>() : row_smem_bytes<9, 6>();
+        case 10: return nf == 4 ? row_smem_bytes<10, 4>() : row_smem_bytes<10, 6>();
+        default: return 0;
+    }
+}
+
+size_t col_pass_smem(int log_n, int nf)
+{
+    switch (log_n) {
+        case 4: return nf == 4 ? col_smem_bytes<4, 4>() : col_smem_bytes<4, 6>();
+        case 5: return nf == 4 ? col_smem_bytes<5, 4>() : col_smem_bytes<5, 6>();
+        case 6: return nf == 4 ? col_smem_bytes<6, 4>() : col_smem_bytes<6, 6>();
+        case 7: return nf == 4 ? col_smem_bytes<7, 4>() : col_smem_bytes<7, 6>();
+        case 8: return nf == 4 ? col_smem_bytes<8, 4>() : col_smem_bytes<8, 6>();
+        case 9: return nf == 4 ? col_smem_bytes<9, 4>() : col_smem_bytes<9, 6>();
+        case 10: return nf == 4 ? col_smem_bytes<10, 4>() : col_smem_bytes<10, 6>();
+        default: return 0;
+    }
+}
+
+cudaError_t launch_foam_step(int n, int count, const float4* disp, const float4* velocity,
+                             const float* cur, float* next, float dt, float decay, float gain,
+                             float scale, float drift_x, float drift_z, float inv_cell,
+                             cudaStream_t stream)
+{
+    const uint64_t total = static_cast<uint64_t>(n) * n * count;
+    const unsigned blocks = static_cast<unsigned>((total + 255) / 256);
+    foam_step_kernel<<<blocks, 256, 0, stream>>>(n, count, disp, velocity, cur, next, dt, decay,
+                                                 gain, scale, drift_x, drift_z, inv_cell);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sample(int n, float inv_cell, const float4* disp, const float4* normal,
+                          const float4* velocity, const float2* xz, uint64_t count,
+                          SurfaceEx* out, cudaStream_t stream)
+{
+    if (count == 0) return cudaSuccess;
+    const unsigned blocks = static_cast<unsigned>((count + 255) / 256);
+    sample_kernel<<<blocks, 256, 0, stream>>>(n, inv_cell, disp, normal, velocity, xz, count, out);
+    return cudaGetLastError();
+}
+
+}  // namespace ocean_b200

@@ -1,0 +1,1191 @@
+// oceanlib-b200: C++ host layer and the C ABI.
+//
+// The handle types are C++ objects, as in the reference (src/c_api.cpp:22-37):
+//   Batch     - N same-size oceans on one device: spectrum tables, the
+//               row-pass intermediate, outputs, persistent foam, a stream.
+//   ocean_sim - a Batch of one plus the pinned host mirror that the
+//               reference-shaped calls (ocean_get_buffers, ...) hand out.
+// No exception crosses the C boundary; failures are NULL + ocean_status.
+// Every compute step is a CUDA launch; there is no host compute path.
+
+#include "../../include/ocean_b200.h"
+#include "spectrum.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cctype>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace ocean_b200 {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+struct DeviceError : std::runtime_error {
+    cudaError_t code;
+    DeviceError(cudaError_t c, const char* what) : std::runtime_error(what), code(c) {}
+};
+
+void check(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess) throw DeviceError(e, what);
+}
+
+ocean_status status_of(const DeviceError& e)
+{
+    return e.code == cudaErrorMemoryAllocation ? OCEAN_ERROR_OUT_OF_MEMORY : OCEAN_ERROR_DEVICE;
+}
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    explicit DevBuf(size_t count) : n(count)
+    {
+        if (count) check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+    }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept
+    {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+        return *this;
+    }
+    ~DevBuf() { if (p) cudaFree(p); }
+};
+
+template <typename T>
+struct HostBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    HostBuf() = default;
+    explicit HostBuf(size_t count) : n(count)
+    {
+        if (count) check(cudaMallocHost(&p, count * sizeof(T)), "cudaMallocHost");
+        if (p) std::memset(p, 0, count * sizeof(T));
+    }
+    HostBuf(const HostBuf&) = delete;
+    HostBuf& operator=(const HostBuf&) = delete;
+    HostBuf(HostBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    HostBuf& operator=(HostBuf&& o) noexcept
+    {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+        return *this;
+    }
+    ~HostBuf() { if (p) cudaFreeHost(p); }
+};
+
+// ---------------------------------------------------------------------------
+// Global kernel-form selection (ocean_force_simd_level)
+// ---------------------------------------------------------------------------
+std::mutex g_level_mutex;
+std::string g_level_name = "sm_100a";
+std::atomic<int> g_form{OCEAN_FFT_EXACT};
+
+// ---------------------------------------------------------------------------
+// Descriptor handling (src/c_api.cpp:46-60, src/ocean.cpp:28-59)
+// ---------------------------------------------------------------------------
+void desc_defaults(ocean_desc* d)
+{
+    // The reference's defaults (include/ocean/ocean.hpp:39-130).
+    std::memset(d, 0, sizeof(*d));
+    d->struct_size = sizeof(ocean_desc);
+    d->size = 256;
+    d->patch_length = 200.0f;
+    d->spectrum.wind_speed = 10.0f;
+    d->spectrum.fetch = 100000.0f;
+    d->spectrum.wind_direction = 0.0f;
+    d->spectrum.peak_enhancement = 3.3f;
+    d->spectrum.swell = 0.0f;
+    d->spectrum.small_wave_cutoff = 0.5f;
+    d->spectrum.gravity = 9.81f;
+    d->choppiness = 1.0f;
+    d->foam_threshold = 0.5f;
+    d->seed = 1337;
+    d->thread_count = 0;
+    d->water_depth = 0.0f;
+    d->compute_velocity = 0;
+}
+
+bool copy_desc(const ocean_desc* src, ocean_desc& dst)
+{
+    if (src == nullptr) return false;
+    if (src->struct_size == 0 || src->struct_size > sizeof(ocean_desc)) return false;
+    desc_defaults(&dst);
+    std::memcpy(&dst, src, src->struct_size);
+    dst.struct_size = sizeof(ocean_desc);
+    return true;
+}
+
+constexpr uint32_t kMaxSize = 1024;  // largest N the frame kernels are built for
+
+void validate(const ocean_desc& d)
+{
+    const uint32_t n = d.size;
+    const bool pow2 = n != 0 && (n & (n - 1)) == 0;
+    if (!pow2 || n < 16 || n > 4096) throw std::invalid_argument("size");
+    if (n > kMaxSize) throw std::invalid_argument("size above the built kernel range");
+    if (!(d.patch_length > 0.0f)) throw std::invalid_argument("patch_length");
+    if (!(d.spectrum.gravity > 0.0f)) throw std::invalid_argument("gravity");
+    if (!(d.spectrum.fetch > 0.0f)) throw std::invalid_argument("fetch");
+    if (!(d.spectrum.wind_speed >= 0.0f)) throw std::invalid_argument("wind_speed");
+    if (!(d.spectrum.peak_enhancement >= 1.0f)) throw std::invalid_argument("peak_enhancement");
+    if (!(d.choppiness >= 0.0f)) throw std::invalid_argument("choppiness");
+}
+
+void foam_desc_defaults(ocean_foam_desc* f)
+{
+    // include/ocean/foam.hpp:38-74
+    std::memset(f, 0, sizeof(*f));
+    f->struct_size = sizeof(ocean_foam_desc);
+    f->decay = 0.35f;
+    f->source_gain = 4.0f;
+    f->advect_scale = 1.0f;
+    f->wind_drift_x = 0.0f;
+    f->wind_drift_z = 0.0f;
+    f->fixed_dt = 1.0f / 60.0f;
+    f->max_substeps = 4;
+}
+
+void validate_foam(const ocean_foam_desc& d)
+{
+    // src/foam.cpp:145-164
+    if (!(d.decay >= 0.0f)) throw std::invalid_argument("foam decay");
+    if (!(d.source_gain >= 0.0f)) throw std::invalid_argument("foam source_gain");
+    if (!(d.fixed_dt > 0.0f)) throw std::invalid_argument("foam fixed_dt");
+    if (d.max_substeps < 1) throw std::invalid_argument("foam max_substeps");
+    if (!std::isfinite(d.advect_scale) || !std::isfinite(d.wind_drift_x) ||
+        !std::isfinite(d.wind_drift_z))
+        throw std::invalid_argument("foam drift");
+}
+
+int ilog2u(uint32_t v)
+{
+    int l = 0;
+    while ((1u << l) < v) ++l;
+    return l;
+}
+
+// Per-stage inverse twiddle tables: for stage l the entries W^(p << l),
+// p < N >> (l+1), contiguously from N - (N >> l); W^j = (cos, sin)(2 pi j / N)
+// evaluated in double and narrowed, exactly as src/core/fft.cpp:24-33 builds
+// its table (same literal, same operation order).
+std::vector<float2> stage_twiddles(uint32_t n)
+{
+    std::vector<float2> w(n > 1 ? n - 1 : 1);
+    std::vector<float2> base(n / 2 > 0 ? n / 2 : 1);
+    constexpr double kTwoPi = 6.283185307179586476925286766559;
+    for (uint32_t j = 0; j < n / 2; ++j) {
+        const double angle = kTwoPi * static_cast<double>(j) / static_cast<double>(n);
+        base[j] = make_float2(static_cast<float>(std::cos(angle)), static_cast<float>(std::sin(angle)));
+    }
+    const int log_n = ilog2u(n);
+    for (int l = 0; l < log_n; ++l) {
+        const uint32_t off = n - (n >> l);
+        for (uint32_t p = 0; p < (n >> (l + 1)); ++p) w[off + p] = base[static_cast<size_t>(p) << l];
+    }
+    return w;
+}
+
+SpectrumParams spectrum_params(const ocean_desc& d)
+{
+    SpectrumParams p;
+    p.n = d.size;
+    p.patch_length = d.patch_length;
+    p.wind_speed = d.spectrum.wind_speed;
+    p.fetch = d.spectrum.fetch;
+    p.wind_direction = d.spectrum.wind_direction;
+    p.peak_enhancement = d.spectrum.peak_enhancement;
+    p.swell = d.spectrum.swell;
+    p.small_wave_cutoff = d.spectrum.small_wave_cutoff;
+    p.gravity = d.spectrum.gravity;
+    p.depth = d.water_depth;
+    p.seed = d.seed;
+    return p;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Batch: `count` oceans of one size on one device.
+// ---------------------------------------------------------------------------
+class Batch {
+public:
+    Batch(const ocean_desc* descs, uint32_t count, int form, bool foam_on,
+          const ocean_foam_desc& foam, uint32_t chunk_hint)
+    {
+        if (descs == nullptr || count == 0) throw std::invalid_argument("no oceans");
+        descs_.resize(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            if (!copy_desc(&descs[i], descs_[i])) throw std::invalid_argument("desc");
+            validate(descs_[i]);
+        }
+        n_ = descs_[0].size;
+        velocity_ = descs_[0].compute_velocity != 0;
+        for (const ocean_desc& d : descs_) {
+            if (d.size != n_) throw std::invalid_argument("mixed sizes");
+            if ((d.compute_velocity != 0) != velocity_) throw std::invalid_argument("mixed velocity");
+            if (d.patch_length != descs_[0].patch_length)
+                throw std::invalid_argument("mixed patch lengths");
+        }
+        foam_on_ = foam_on;
+        if (foam_on_) {
+            foam_ = foam;
+            validate_foam(foam_);
+            // FoamField requires the velocity field (src/foam.cpp:171-179).
+            if (!velocity_) throw std::invalid_argument("foam needs compute_velocity");
+        }
+        form_ = form;
+        count_ = count;
+        log_n_ = ilog2u(n_);
+        nf_ = velocity_ ? 6 : 4;
+        cells_ = static_cast<size_t>(n_) * n_;
+
+        check(cudaGetDevice(&device_), "cudaGetDevice");
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+
+        // Chunk: enough oceans per pass pair to fill the GPU, few enough that
+        // the row-pass intermediate (cells * NF * 8 B each) stays L2-resident.
+        const size_t inter_bytes = cells_ * nf_ * sizeof(float2);
+        uint32_t chunk = chunk_hint;
+        if (chunk == 0) {
+            const size_t budget = 40ull << 20;
+            chunk = static_cast<uint32_t>(std::max<size_t>(1, budget / inter_bytes));
+        }
+        chunk_ = std::min(chunk, count_);
+
+        // Geometry tables are shared by oceans with equal (N, L, g, depth).
+        std::vector<int32_t> geom_of(count_);
+        std::vector<uint32_t> geom_rep;
+        for (uint32_t i = 0; i < count_; ++i) {
+            int32_t g = -1;
+            for (size_t k = 0; k < geom_rep.size(); ++k) {
+                const ocean_desc& a = descs_[geom_rep[k]];
+                const ocean_desc& b = descs_[i];
+                if (a.patch_length == b.patch_length && a.spectrum.gravity == b.spectrum.gravity &&
+                    a.water_depth == b.water_depth) {
+                    g = static_cast<int32_t>(k);
+                    break;
+                }
+            }
+            if (g < 0) {
+                g = static_cast<int32_t>(geom_rep.size());
+                geom_rep.push_back(i);
+            }
+            geom_of[i] = g;
+        }
+
+        h0_ = DevBuf<float2>(cells_ * count_);
+        geom_ = DevBuf<float2>(cells_ * geom_rep.size());
+        kvec_ = DevBuf<float>(static_cast<size_t>(n_) * geom_rep.size());
+        tw_ = DevBuf<float2>(n_ - 1);
+        consts_ = DevBuf<OceanConsts>(count_);
+        top_ = DevBuf<double>(count_ * kTimeSlots);
+        top_host_ = HostBuf<double>(count_ * kTimeSlots);
+        inter_ = DevBuf<float2>(cells_ * nf_ * chunk_);
+        disp_ = DevBuf<float4>(cells_ * count_);
+        normal_ = DevBuf<float4>(cells_ * count_);
+        if (velocity_) velocity_buf_ = DevBuf<float4>(cells_ * count_);
+        if (foam_on_) {
+            foam_a_ = DevBuf<float>(cells_ * count_);
+            foam_b_ = DevBuf<float>(cells_ * count_);
+            check(cudaMemsetAsync(foam_a_.p, 0, cells_ * count_ * sizeof(float), stream_), "memset");
+            check(cudaMemsetAsync(foam_b_.p, 0, cells_ * count_ * sizeof(float), stream_), "memset");
+        }
+        for (int s = 0; s < kTimeSlots; ++s) {
+            check(cudaEventCreateWithFlags(&slot_done_[s], cudaEventDisableTiming), "event");
+        }
+        for (uint32_t c = 0; c * chunk_ < count_; ++c) chunk_events_.emplace_back();
+        for (auto& e : chunk_events_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+
+        const std::vector<float2> tw = stage_twiddles(n_);
+        check(cudaMemcpyAsync(tw_.p, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice,
+                              stream_), "upload twiddles");
+        std::vector<OceanConsts> consts(count_);
+        for (uint32_t i = 0; i < count_; ++i) {
+            const ocean_desc& d = descs_[i];
+            consts[i].lambda = d.choppiness;
+            consts[i].foam_threshold = d.foam_threshold;
+            // src/core/evolve.cpp:251-252
+            consts[i].inv_threshold = (d.foam_threshold > 1e-6f) ? (1.0f / d.foam_threshold) : 0.0f;
+            consts[i].geom = geom_of[i];
+        }
+        check(cudaMemcpyAsync(consts_.p, consts.data(), consts.size() * sizeof(OceanConsts),
+                              cudaMemcpyHostToDevice, stream_), "upload consts");
+        for (size_t g = 0; g < geom_rep.size(); ++g) {
+            check(launch_geometry(spectrum_params(descs_[geom_rep[g]]), geom_.p + g * cells_,
+                                  kvec_.p + g * n_, stream_), "geometry kernel");
+        }
+        for (uint32_t i = 0; i < count_; ++i) {
+            check(launch_h0(spectrum_params(descs_[i]), h0_.p + i * cells_, stream_), "h0 kernel");
+        }
+        check(cudaStreamSynchronize(stream_), "spectrum build");
+    }
+
+    ~Batch()
+    {
+        if (stream_) cudaStreamSynchronize(stream_);
+        if (copy_stream_) cudaStreamSynchronize(copy_stream_);
+        for (auto& e : slot_done_) if (e) cudaEventDestroy(e);
+        for (auto& e : chunk_events_) if (e) cudaEventDestroy(e);
+        for (auto& e : prof_events_) if (e) cudaEventDestroy(e);
+        if (copy_stream_) cudaStreamDestroy(copy_stream_);
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+
+    uint32_t count() const { return count_; }
+    uint32_t size() const { return n_; }
+    bool velocity() const { return velocity_; }
+    bool foam_on() const { return foam_on_; }
+    const ocean_desc& desc(uint32_t i) const { return descs_[i]; }
+    cudaStream_t stream() const { return stream_; }
+    uint32_t last_foam_substeps() const { return foam_last_; }
+    size_t cells() const { return cells_; }
+
+    float4* disp(uint32_t i) const { return disp_.p + i * cells_; }
+    float4* normal(uint32_t i) const { return normal_.p + i * cells_; }
+    float4* velocity_ptr(uint32_t i) const { return velocity_ ? velocity_buf_.p + i * cells_ : nullptr; }
+    float* foam_ptr(uint32_t i) const
+    {
+        if (!foam_on_) return nullptr;
+        return (foam_cur_ == 0 ? foam_a_.p : foam_b_.p) + i * cells_;
+    }
+
+    // The whole frame for every ocean, queued on `st`. Optional per-stage
+    // hook points let ocean_sim drive the reference's four dispatches.
+    void update(const double* times, bool per_ocean, float foam_dt, cudaStream_t st)
+    {
+        if (st == nullptr) st = stream_;
+        // Per-ocean t/(2pi), hoisted exactly as src/core/evolve.cpp:33 does.
+        const int slot = slot_next_;
+        slot_next_ = (slot_next_ + 1) % kTimeSlots;
+        check(cudaEventSynchronize(slot_done_[slot]), "time slot");
+        double* host = top_host_.p + static_cast<size_t>(slot) * count_;
+        for (uint32_t i = 0; i < count_; ++i) {
+            const double t = per_ocean ? times[i] : times[0];
+            host[i] = t * kInvTwoPi;
+        }
+        double* dev = top_.p + static_cast<size_t>(slot) * count_;
+        check(cudaMemcpyAsync(dev, host, count_ * sizeof(double), cudaMemcpyHostToDevice, st),
+              "upload times");
+        check(cudaEventRecord(slot_done_[slot], st), "event");
+
+        const uint32_t steps = foam_on_ ? foam_accumulate(foam_dt) : 0u;
+        FrameArgs a = frame_args(dev);
+        if (steps > 0) set_foam_args(a);
+        for (uint32_t base = 0, c = 0; base < count_; base += chunk_, ++c) {
+            a.ocean_base = static_cast<int32_t>(base);
+            a.chunk = static_cast<int32_t>(std::min(chunk_, count_ - base));
+            run_row(a, st);
+            run_col(a, st, steps > 0);
+        }
+        if (steps > 0) {
+            foam_cur_ ^= 1;
+            for (uint32_t s = 1; s < steps; ++s) {
+                foam_substep(st);
+                foam_cur_ ^= 1;
+            }
+        }
+    }
+
+    // Stage-by-stage form for the parallel_for compatibility path: stage 0 is
+    // the row pass of every chunk, stage 1 the column pass (plus foam).
+    void update_stage(int stage, const double* times, cudaStream_t st)
+    {
+        if (stage == 0) {
+            const int slot = slot_next_;
+            slot_next_ = (slot_next_ + 1) % kTimeSlots;
+            check(cudaEventSynchronize(slot_done_[slot]), "time slot");
+            double* host = top_host_.p + static_cast<size_t>(slot) * count_;
+            for (uint32_t i = 0; i < count_; ++i) host[i] = times[0] * kInvTwoPi;
+            staged_top_ = top_.p + static_cast<size_t>(slot) * count_;
+            check(cudaMemcpyAsync(staged_top_, host, count_ * sizeof(double),
+                                  cudaMemcpyHostToDevice, st), "upload times");
+            check(cudaEventRecord(slot_done_[slot], st), "event");
+            // One chunk only on this path (a single ocean).
+            FrameArgs a = frame_args(staged_top_);
+            a.ocean_base = 0;
+            a.chunk = static_cast<int32_t>(count_);
+            run_row(a, st);
+        } else {
+            FrameArgs a = frame_args(staged_top_);
+            a.ocean_base = 0;
+            a.chunk = static_cast<int32_t>(count_);
+            run_col(a, st, false);
+        }
+    }
+
+    // End-to-end frame for host callers: per chunk, the copies of the
+    // chunk's outputs run on a second stream while later chunks compute.
+    void update_host(const double* times, bool per_ocean, float foam_dt, float* h_disp,
+                     float* h_normal, float* h_vel, float* h_foam)
+    {
+        const int slot = slot_next_;
+        slot_next_ = (slot_next_ + 1) % kTimeSlots;
+        check(cudaEventSynchronize(slot_done_[slot]), "time slot");
+        double* host = top_host_.p + static_cast<size_t>(slot) * count_;
+        for (uint32_t i = 0; i < count_; ++i) host[i] = (per_ocean ? times[i] : times[0]) * kInvTwoPi;
+        double* dev = top_.p + static_cast<size_t>(slot) * count_;
+        check(cudaMemcpyAsync(dev, host, count_ * sizeof(double), cudaMemcpyHostToDevice, stream_),
+              "upload times");
+        check(cudaEventRecord(slot_done_[slot], stream_), "event");
+        const uint32_t steps = foam_on_ ? foam_accumulate(foam_dt) : 0u;
+        FrameArgs a = frame_args(dev);
+        if (steps > 0) set_foam_args(a);
+        // Foam beyond the first substep needs every ocean's previous state,
+        // so copies start per chunk only when the frame has one substep.
+        const bool pipelined = steps <= 1;
+        const size_t bytes4 = cells_ * sizeof(float4);
+        uint32_t c = 0;
+        for (uint32_t base = 0; base < count_; base += chunk_, ++c) {
+            const uint32_t k = std::min(chunk_, count_ - base);
+            a.ocean_base = static_cast<int32_t>(base);
+            a.chunk = static_cast<int32_t>(k);
+            run_row(a, stream_);
+            run_col(a, stream_, steps > 0);
+            if (pipelined) {
+                check(cudaEventRecord(chunk_events_[c], stream_), "event");
+                check(cudaStreamWaitEvent(copy_stream_, chunk_events_[c], 0), "wait");
+                copy_out(base, k, bytes4, h_disp, h_normal, h_vel, h_foam, steps > 0);
+            }
+        }
+        if (steps > 0) {
+            foam_cur_ ^= 1;
+            for (uint32_t s = 1; s < steps; ++s) {
+                foam_substep(stream_);
+                foam_cur_ ^= 1;
+            }
+        }
+        if (!pipelined) {
+            check(cudaEventRecord(chunk_events_[0], stream_), "event");
+            check(cudaStreamWaitEvent(copy_stream_, chunk_events_[0], 0), "wait");
+            copy_out(0, count_, bytes4, h_disp, h_normal, h_vel, h_foam, false);
+            if (h_foam) {
+                check(cudaMemcpyAsync(h_foam, foam_ptr(0), cells_ * count_ * sizeof(float),
+                                      cudaMemcpyDeviceToHost, copy_stream_), "copy foam");
+            }
+        }
+        check(cudaStreamSynchronize(copy_stream_), "copy back");
+        check(cudaStreamSynchronize(stream_), "frame");
+    }
+
+    void read_spectrum(uint32_t i, float* h0, float* omega_kinv) const
+    {
+        if (h0) check(cudaMemcpy(h0, h0_.p + i * cells_, cells_ * sizeof(float2),
+                                 cudaMemcpyDeviceToHost), "read h0");
+        if (omega_kinv) {
+            std::vector<OceanConsts> c(1);
+            check(cudaMemcpy(c.data(), consts_.p + i, sizeof(OceanConsts), cudaMemcpyDeviceToHost),
+                  "read consts");
+            check(cudaMemcpy(omega_kinv, geom_.p + static_cast<size_t>(c[0].geom) * cells_,
+                             cells_ * sizeof(float2), cudaMemcpyDeviceToHost), "read geometry");
+        }
+    }
+
+    // ---- profiling (ocean_batch_set_profiling / read_profile) ----
+    void set_profiling(bool on)
+    {
+        if (on && prof_events_.empty()) {
+            prof_events_.resize(2 * kProfilePairs);
+            for (auto& e : prof_events_) check(cudaEventCreate(&e), "event");
+            prof_kind_.resize(kProfilePairs);
+        }
+        prof_on_ = on;
+    }
+
+    ocean_pass_profile read_profile()
+    {
+        flush_profile();
+        ocean_pass_profile p{};
+        p.row_launches = prof_n_[0];
+        p.col_launches = prof_n_[1];
+        p.foam_launches = prof_n_[2];
+        p.row_ms = prof_ms_[0];
+        p.col_ms = prof_ms_[1];
+        p.foam_ms = prof_ms_[2];
+        for (int k = 0; k < 3; ++k) {
+            prof_n_[k] = 0;
+            prof_ms_[k] = 0.0;
+        }
+        return p;
+    }
+
+    uint64_t launch_count() const { return launches_; }
+
+private:
+    static constexpr int kTimeSlots = 4;
+    static constexpr size_t kProfilePairs = 8192;
+
+    template <typename F>
+    void timed(int kind, cudaStream_t st, F&& f)
+    {
+        if (prof_on_) {
+            if (prof_used_ == kProfilePairs) flush_profile();
+            check(cudaEventRecord(prof_events_[2 * prof_used_], st), "event");
+        }
+        f();
+        ++launches_;
+        if (prof_on_) {
+            check(cudaEventRecord(prof_events_[2 * prof_used_ + 1], st), "event");
+            prof_kind_[prof_used_] = kind;
+            ++prof_used_;
+        }
+    }
+
+    void flush_profile()
+    {
+        for (size_t i = 0; i < prof_used_; ++i) {
+            check(cudaEventSynchronize(prof_events_[2 * i + 1]), "event");
+            float ms = 0.0f;
+            check(cudaEventElapsedTime(&ms, prof_events_[2 * i], prof_events_[2 * i + 1]), "elapsed");
+            prof_ms_[prof_kind_[i]] += ms;
+            ++prof_n_[prof_kind_[i]];
+        }
+        prof_used_ = 0;
+    }
+
+    void run_row(const FrameArgs& a, cudaStream_t st)
+    {
+        timed(0, st, [&] { check(launch_row_pass(log_n_, nf_, form_ == OCEAN_FFT_FAST, a, st), "row pass"); });
+    }
+
+    void run_col(const FrameArgs& a, cudaStream_t st, bool foam)
+    {
+        timed(1, st, [&] {
+            check(launch_col_pass(log_n_, nf_, form_ == OCEAN_FFT_FAST, foam, a, st), "column pass");
+        });
+    }
+    static constexpr double kInvTwoPi = 0.159154943091895335769;
+
+    FrameArgs frame_args(const double* top) const
+    {
+        FrameArgs a{};
+        a.h0 = h0_.p;
+        a.omega_kinv = geom_.p;
+        a.kvec = kvec_.p;
+        a.twiddles = tw_.p;
+        a.consts = consts_.p;
+        a.t_over_2pi = top;
+        a.inter = inter_.p;
+        a.disp = disp_.p;
+        a.normal = normal_.p;
+        a.velocity = velocity_buf_.p;
+        return a;
+    }
+
+    void set_foam_args(FrameArgs& a) const
+    {
+        const float dt = foam_.fixed_dt;
+        a.foam_cur = foam_cur_ == 0 ? foam_a_.p : foam_b_.p;
+        a.foam_next = foam_cur_ == 0 ? foam_b_.p : foam_a_.p;
+        a.foam_dt = dt;
+        a.foam_decay = std::exp(-foam_.decay * dt);  // src/foam.cpp:94
+        a.foam_gain = foam_.source_gain * dt;
+        a.foam_scale = foam_.advect_scale;
+        a.foam_drift_x = foam_.wind_drift_x;
+        a.foam_drift_z = foam_.wind_drift_z;
+        const float cell = descs_[0].patch_length / static_cast<float>(n_);
+        a.foam_inv_cell = 1.0f / cell;
+    }
+
+    void foam_substep(cudaStream_t st)
+    {
+        FrameArgs a = frame_args(nullptr);
+        set_foam_args(a);
+        timed(2, st, [&] {
+            check(launch_foam_step(static_cast<int>(n_), static_cast<int>(count_), disp_.p,
+                                   velocity_buf_.p, a.foam_cur, a.foam_next, a.foam_dt,
+                                   a.foam_decay, a.foam_gain, a.foam_scale, a.foam_drift_x,
+                                   a.foam_drift_z, a.foam_inv_cell, st), "foam step");
+        });
+    }
+
+    // FoamField::update's fixed-step accumulator (src/foam.cpp:218-252).
+    uint32_t foam_accumulate(float dt)
+    {
+        if (!(dt > 0.0f)) dt = 0.0f;
+        foam_accum_ += static_cast<double>(dt);
+        const double step = static_cast<double>(foam_.fixed_dt);
+        const double eps = step * 1e-6;
+        uint32_t steps = 0;
+        if (foam_accum_ + eps >= step) steps = static_cast<uint32_t>((foam_accum_ + eps) / step);
+        if (steps > foam_.max_substeps) {
+            steps = foam_.max_substeps;
+            foam_accum_ = 0.0;
+        } else {
+            foam_accum_ -= static_cast<double>(steps) * step;
+            if (foam_accum_ < 0.0) foam_accum_ = 0.0;
+        }
+        foam_last_ = steps;
+        return steps;
+    }
+
+    void copy_out(uint32_t base, uint32_t k, size_t bytes4, float* h_disp, float* h_normal,
+                  float* h_vel, float* h_foam, bool foam_written)
+    {
+        if (h_disp)
+            check(cudaMemcpyAsync(h_disp + base * cells_ * 4, disp(base), bytes4 * k,
+                                  cudaMemcpyDeviceToHost, copy_stream_), "copy displacement");
+        if (h_normal)
+            check(cudaMemcpyAsync(h_normal + base * cells_ * 4, normal(base), bytes4 * k,
+                                  cudaMemcpyDeviceToHost, copy_stream_), "copy normal");
+        if (h_vel && velocity_)
+            check(cudaMemcpyAsync(h_vel + base * cells_ * 4, velocity_ptr(base), bytes4 * k,
+                                  cudaMemcpyDeviceToHost, copy_stream_), "copy velocity");
+        if (h_foam && foam_on_ && foam_written) {
+            // The fused substep wrote the buffer that becomes current.
+            const float* src = (foam_cur_ == 0 ? foam_b_.p : foam_a_.p) + base * cells_;
+            check(cudaMemcpyAsync(h_foam + base * cells_, src, cells_ * k * sizeof(float),
+                                  cudaMemcpyDeviceToHost, copy_stream_), "copy foam");
+        } else if (h_foam && foam_on_) {
+            check(cudaMemcpyAsync(h_foam + base * cells_, foam_ptr(base), cells_ * k * sizeof(float),
+                                  cudaMemcpyDeviceToHost, copy_stream_), "copy foam");
+        }
+    }
+
+    std::vector<ocean_desc> descs_;
+    uint32_t n_ = 0, count_ = 0, chunk_ = 1;
+    int log_n_ = 0, nf_ = 4, form_ = OCEAN_FFT_EXACT;
+    bool velocity_ = false, foam_on_ = false;
+    size_t cells_ = 0;
+    int device_ = 0;
+    cudaStream_t stream_ = nullptr, copy_stream_ = nullptr;
+    cudaEvent_t slot_done_[kTimeSlots] = {};
+    std::vector<cudaEvent_t> chunk_events_;
+    bool prof_on_ = false;
+    std::vector<cudaEvent_t> prof_events_;
+    std::vector<int> prof_kind_;
+    size_t prof_used_ = 0;
+    uint64_t prof_n_[3] = {0, 0, 0};
+    double prof_ms_[3] = {0.0, 0.0, 0.0};
+    uint64_t launches_ = 0;
+    int slot_next_ = 0;
+    double* staged_top_ = nullptr;
+
+    DevBuf<float2> h0_, geom_, tw_, inter_;
+    DevBuf<float> kvec_;
+    DevBuf<OceanConsts> consts_;
+    DevBuf<double> top_;
+    HostBuf<double> top_host_;
+    DevBuf<float4> disp_, normal_, velocity_buf_;
+    DevBuf<float> foam_a_, foam_b_;
+    int foam_cur_ = 0;
+    ocean_foam_desc foam_{};
+    double foam_accum_ = 0.0;
+    uint32_t foam_last_ = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Single ocean with a host mirror (the reference-shaped handle).
+// ---------------------------------------------------------------------------
+class Sim {
+public:
+    explicit Sim(const ocean_desc& d)
+        : desc_(d), batch_(&desc_, 1, g_form.load(), false, foam_defaults(), 1)
+    {
+        const size_t cells = batch_.cells();
+        disp_ = HostBuf<float>(cells * 4);
+        normal_ = HostBuf<float>(cells * 4);
+        if (batch_.velocity()) vel_ = HostBuf<float>(cells * 4);
+        q_in_ = DevBuf<float2>(1);
+        q_out_ = DevBuf<SurfaceEx>(1);
+        q_host_in_ = HostBuf<float2>(1);
+        q_host_out_ = HostBuf<SurfaceEx>(1);
+        // The reference constructor leaves the ocean evaluated at t = 0
+        // (src/ocean.cpp:275-277).
+        update(0.0);
+    }
+
+    void update(double t)
+    {
+        if (desc_.parallel_for != nullptr) {
+            // Four blocking dispatches per frame, as the reference makes
+            // (src/ocean.cpp:251-268); each runs one device stage to completion.
+            StageCtx ctx{this, t, 0};
+            for (int s = 0; s < 4; ++s) {
+                ctx.stage = s;
+                desc_.parallel_for(desc_.parallel_for_user, &Sim::run_stage, &ctx, 1u);
+            }
+            if (ctx.failed) last_error_ = OCEAN_ERROR_DEVICE;
+        } else {
+            batch_.update(&t, false, 0.0f, nullptr);
+            refresh();
+        }
+        time_ = t;
+    }
+
+    void update_async(double t, cudaStream_t st)
+    {
+        batch_.update(&t, false, 0.0f, st);
+        time_ = t;
+    }
+
+    void refresh()
+    {
+        const size_t bytes = batch_.cells() * sizeof(float4);
+        cudaStream_t st = batch_.stream();
+        check(cudaMemcpyAsync(disp_.p, batch_.disp(0), bytes, cudaMemcpyDeviceToHost, st), "copy");
+        check(cudaMemcpyAsync(normal_.p, batch_.normal(0), bytes, cudaMemcpyDeviceToHost, st), "copy");
+        if (vel_.p)
+            check(cudaMemcpyAsync(vel_.p, batch_.velocity_ptr(0), bytes, cudaMemcpyDeviceToHost, st),
+                  "copy");
+        check(cudaStreamSynchronize(st), "refresh");
+    }
+
+    void sample(float x, float z, SurfaceEx* out) const
+    {
+        std::lock_guard<std::mutex> lock(query_mutex_);
+        cudaStream_t st = batch_.stream();
+        q_host_in_.p[0] = make_float2(x, z);
+        check(cudaMemcpyAsync(q_in_.p, q_host_in_.p, sizeof(float2), cudaMemcpyHostToDevice, st), "query");
+        check(launch_sample(static_cast<int>(desc_.size), inv_cell(), batch_.disp(0), batch_.normal(0),
+                            batch_.velocity_ptr(0), q_in_.p, 1, q_out_.p, st), "query kernel");
+        check(cudaMemcpyAsync(q_host_out_.p, q_out_.p, sizeof(SurfaceEx), cudaMemcpyDeviceToHost, st),
+              "query");
+        check(cudaStreamSynchronize(st), "query");
+        *out = q_host_out_.p[0];
+    }
+
+    void sample_many(const float* xz, uint64_t count, SurfaceEx* out) const
+    {
+        std::lock_guard<std::mutex> lock(query_mutex_);
+        if (count == 0) return;
+        cudaStream_t st = batch_.stream();
+        if (many_in_.n < count) {
+            many_in_ = DevBuf<float2>(count);
+            many_out_ = DevBuf<SurfaceEx>(count);
+        }
+        check(cudaMemcpyAsync(many_in_.p, xz, count * sizeof(float2), cudaMemcpyHostToDevice, st), "query");
+        check(launch_sample(static_cast<int>(desc_.size), inv_cell(), batch_.disp(0), batch_.normal(0),
+                            batch_.velocity_ptr(0), many_in_.p, count, many_out_.p, st), "query kernel");
+        check(cudaMemcpyAsync(out, many_out_.p, count * sizeof(SurfaceEx), cudaMemcpyDeviceToHost, st),
+              "query");
+        check(cudaStreamSynchronize(st), "query");
+    }
+
+    const ocean_desc& desc() const { return desc_; }
+    double time() const { return time_; }
+    const float* host_disp() const { return disp_.p; }
+    const float* host_normal() const { return normal_.p; }
+    const float* host_velocity() const { return vel_.p; }
+    Batch& batch() { return batch_; }
+    const Batch& batch() const { return batch_; }
+
+private:
+    struct StageCtx {
+        Sim* self;
+        double t;
+        int stage;
+        bool failed = false;
+    };
+
+    static ocean_foam_desc foam_defaults()
+    {
+        ocean_foam_desc f;
+        foam_desc_defaults(&f);
+        return f;
+    }
+
+    static void run_stage(void* ctx, uint32_t)
+    {
+        auto* c = static_cast<StageCtx*>(ctx);
+        Sim& m = *c->self;
+        try {
+            cudaStream_t st = m.batch_.stream();
+            const size_t bytes = m.batch_.cells() * sizeof(float4);
+            switch (c->stage) {
+                case 0: m.batch_.update_stage(0, &c->t, st); break;
+                case 1: m.batch_.update_stage(1, &c->t, st); break;
+                case 2:
+                    check(cudaMemcpyAsync(m.disp_.p, m.batch_.disp(0), bytes, cudaMemcpyDeviceToHost, st),
+                          "copy");
+                    break;
+                default:
+                    check(cudaMemcpyAsync(m.normal_.p, m.batch_.normal(0), bytes,
+                                          cudaMemcpyDeviceToHost, st), "copy");
+                    if (m.vel_.p)
+                        check(cudaMemcpyAsync(m.vel_.p, m.batch_.velocity_ptr(0), bytes,
+                                              cudaMemcpyDeviceToHost, st), "copy");
+                    break;
+            }
+            check(cudaStreamSynchronize(st), "stage");
+        } catch (...) {
+            c->failed = true;
+        }
+    }
+
+    float inv_cell() const { return static_cast<float>(desc_.size) / desc_.patch_length; }
+
+    ocean_desc desc_;
+    Batch batch_;
+    double time_ = 0.0;
+    HostBuf<float> disp_, normal_, vel_;
+    mutable std::mutex query_mutex_;
+    mutable DevBuf<float2> q_in_, many_in_;
+    mutable DevBuf<SurfaceEx> q_out_, many_out_;
+    mutable HostBuf<float2> q_host_in_;
+    mutable HostBuf<SurfaceEx> q_host_out_;
+    ocean_status last_error_ = OCEAN_OK;
+};
+
+}  // namespace ocean_b200
+
+using ocean_b200::Batch;
+using ocean_b200::DeviceError;
+using ocean_b200::Sim;
+
+struct ocean_sim {
+    Sim impl;
+    explicit ocean_sim(const ocean_desc& d) : impl(d) {}
+};
+struct ocean_batch {
+    Batch impl;
+    ocean_batch(const ocean_desc* d, uint32_t n, int form, bool foam, const ocean_foam_desc& f,
+                uint32_t chunk)
+        : impl(d, n, form, foam, f, chunk) {}
+};
+
+namespace {
+
+template <typename Fn>
+ocean_status guarded(Fn&& fn)
+{
+    try {
+        fn();
+        return OCEAN_OK;
+    } catch (const std::invalid_argument&) {
+        return OCEAN_ERROR_INVALID_ARG;
+    } catch (const DeviceError& e) {
+        return ocean_b200::status_of(e);
+    } catch (const std::bad_alloc&) {
+        return OCEAN_ERROR_OUT_OF_MEMORY;
+    } catch (...) {
+        return OCEAN_ERROR_UNKNOWN;
+    }
+}
+
+void fill_device_buffers(const Batch& b, uint32_t index, ocean_device_buffers* out)
+{
+    out->displacement = reinterpret_cast<float*>(b.disp(index));
+    out->normal = reinterpret_cast<float*>(b.normal(index));
+    out->velocity = reinterpret_cast<float*>(b.velocity_ptr(index));
+    out->foam = b.foam_ptr(index);
+    out->size = b.size();
+    out->patch_length = b.desc(index).patch_length;
+}
+
+void to_surface(const ocean_b200::SurfaceEx& s, ocean_surface_ex* o)
+{
+    static_assert(sizeof(ocean_b200::SurfaceEx) == sizeof(ocean_surface_ex), "layout");
+    std::memcpy(o, &s, sizeof(*o));
+}
+
+}  // namespace
+
+// Layout checks against the reference ABI (include/ocean/ocean.h). On LP64 the
+// descriptor is 96 bytes: water_depth sits in what was the 88-byte struct's
+// tail padding (tests/test_c_api.cpp:282-300) and compute_velocity follows.
+static_assert(sizeof(ocean_desc) == 96, "ocean_desc layout changed");
+static_assert(offsetof(ocean_desc, compute_velocity) == 88, "layout");
+static_assert(offsetof(ocean_desc, size) == 8, "layout");
+static_assert(offsetof(ocean_desc, spectrum) == 16, "layout");
+static_assert(offsetof(ocean_desc, choppiness) == 44, "layout");
+static_assert(offsetof(ocean_desc, seed) == 56, "layout");
+static_assert(offsetof(ocean_desc, parallel_for) == 64, "layout");
+static_assert(offsetof(ocean_desc, thread_count) == 80, "layout");
+static_assert(offsetof(ocean_desc, water_depth) == 84, "layout");
+static_assert(sizeof(ocean_spectrum_desc) == 28, "layout");
+static_assert(sizeof(ocean_surface) == 28, "layout");
+static_assert(sizeof(ocean_surface_ex) == 40, "layout");
+static_assert(sizeof(ocean_buffers) == 24, "layout");
+
+extern "C" {
+
+const char* ocean_status_string(ocean_status status)
+{
+    switch (status) {
+        case OCEAN_OK: return "ok";
+        case OCEAN_ERROR_INVALID_ARG: return "invalid argument";
+        case OCEAN_ERROR_OUT_OF_MEMORY: return "out of memory";
+        case OCEAN_ERROR_UNKNOWN: return "unknown error";
+        case OCEAN_ERROR_DEVICE: return "device error";
+        case OCEAN_ERROR_TIMEOUT: return "device wait timed out";
+    }
+    return "unrecognised status";
+}
+
+void ocean_desc_init(ocean_desc* desc)
+{
+    if (desc == nullptr) return;
+    ocean_b200::desc_defaults(desc);
+}
+
+ocean_sim* ocean_create(const ocean_desc* desc, ocean_status* out_status)
+{
+    ocean_sim* sim = nullptr;
+    ocean_desc resolved;
+    ocean_status st = OCEAN_OK;
+    if (!ocean_b200::copy_desc(desc, resolved)) {
+        st = OCEAN_ERROR_INVALID_ARG;
+    } else {
+        st = guarded([&] { sim = new ocean_sim(resolved); });
+    }
+    if (out_status != nullptr) *out_status = st;
+    return st == OCEAN_OK ? sim : nullptr;
+}
+
+void ocean_destroy(ocean_sim* sim) { delete sim; }
+
+void ocean_update(ocean_sim* sim, double time)
+{
+    if (sim == nullptr) return;
+    guarded([&] { sim->impl.update(time); });
+}
+
+ocean_buffers ocean_get_buffers(const ocean_sim* sim)
+{
+    ocean_buffers out;
+    std::memset(&out, 0, sizeof(out));
+    if (sim == nullptr) return out;
+    out.displacement = sim->impl.host_disp();
+    out.normal = sim->impl.host_normal();
+    out.size = sim->impl.desc().size;
+    out.patch_length = sim->impl.desc().patch_length;
+    return out;
+}
+
+double ocean_get_time(const ocean_sim* sim) { return sim == nullptr ? 0.0 : sim->impl.time(); }
+
+void ocean_sample_ex(const ocean_sim* sim, float world_x, float world_z, ocean_surface_ex* out)
+{
+    if (out == nullptr) return;
+    std::memset(out, 0, sizeof(*out));
+    out->normal_y = 1.0f;
+    if (sim == nullptr) return;
+    ocean_b200::SurfaceEx s{};
+    if (guarded([&] { sim->impl.sample(world_x, world_z, &s); }) == OCEAN_OK) to_surface(s, out);
+}
+
+float ocean_height_at(const ocean_sim* sim, float world_x, float world_z)
+{
+    if (sim == nullptr) return 0.0f;
+    ocean_surface_ex s;
+    ocean_sample_ex(sim, world_x, world_z, &s);
+    return s.height;
+}
+
+ocean_surface ocean_sample_at(const ocean_sim* sim, float world_x, float world_z)
+{
+    ocean_surface out;
+    std::memset(&out, 0, sizeof(out));
+    out.normal_y = 1.0f;
+    if (sim == nullptr) return out;
+    ocean_surface_ex s;
+    ocean_sample_ex(sim, world_x, world_z, &s);
+    out.height = s.height;
+    out.offset_x = s.offset_x;
+    out.offset_z = s.offset_z;
+    out.normal_x = s.normal_x;
+    out.normal_y = s.normal_y;
+    out.normal_z = s.normal_z;
+    out.foam = s.foam;
+    return out;
+}
+
+const float* ocean_get_velocity(const ocean_sim* sim)
+{
+    return sim == nullptr ? nullptr : sim->impl.host_velocity();
+}
+
+const char* ocean_simd_level(void)
+{
+    std::lock_guard<std::mutex> lock(ocean_b200::g_level_mutex);
+    return ocean_b200::g_level_name.c_str();
+}
+
+const char* ocean_force_simd_level(const char* name)
+{
+    {
+        std::lock_guard<std::mutex> lock(ocean_b200::g_level_mutex);
+        if (name == nullptr) {
+            ocean_b200::g_level_name = "sm_100a";
+            ocean_b200::g_form = OCEAN_FFT_EXACT;
+        } else {
+            std::string s(name);
+            for (char& ch : s) ch = static_cast<char>(std::tolower(static_cast<unsigned char>(ch)));
+            if (s == "scalar" || s == "sse2" || s == "avx2" || s == "neon" || s == "exact") {
+                ocean_b200::g_level_name = s;
+                ocean_b200::g_form = OCEAN_FFT_EXACT;
+            } else if (s == "fast") {
+                ocean_b200::g_level_name = s;
+                ocean_b200::g_form = OCEAN_FFT_FAST;
+            }
+        }
+    }
+    return ocean_simd_level();
+}
+
+void ocean_version(uint32_t* major, uint32_t* minor, uint32_t* patch)
+{
+    if (major != nullptr) *major = 1;
+    if (minor != nullptr) *minor = 0;
+    if (patch != nullptr) *patch = 0;
+}
+
+ocean_status ocean_get_device_buffers(const ocean_sim* sim, ocean_device_buffers* out)
+{
+    if (sim == nullptr || out == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    fill_device_buffers(sim->impl.batch(), 0, out);
+    return OCEAN_OK;
+}
+
+ocean_status ocean_update_async(ocean_sim* sim, double time, void* stream)
+{
+    if (sim == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { sim->impl.update_async(time, static_cast<cudaStream_t>(stream)); });
+}
+
+ocean_status ocean_refresh_host(ocean_sim* sim)
+{
+    if (sim == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { sim->impl.refresh(); });
+}
+
+ocean_status ocean_sample_many(const ocean_sim* sim, const float* xz, uint64_t count,
+                               ocean_surface_ex* out)
+{
+    if (sim == nullptr || (count > 0 && (xz == nullptr || out == nullptr))) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] {
+        sim->impl.sample_many(xz, count, reinterpret_cast<ocean_b200::SurfaceEx*>(out));
+    });
+}
+
+void ocean_foam_desc_init(ocean_foam_desc* desc)
+{
+    if (desc != nullptr) ocean_b200::foam_desc_defaults(desc);
+}
+
+void ocean_batch_desc_init(ocean_batch_desc* desc)
+{
+    if (desc == nullptr) return;
+    std::memset(desc, 0, sizeof(*desc));
+    desc->struct_size = sizeof(ocean_batch_desc);
+    desc->fft_form = ocean_b200::g_form.load();
+    ocean_b200::foam_desc_defaults(&desc->foam);
+}
+
+ocean_batch* ocean_batch_create(const ocean_batch_desc* desc, ocean_status* out_status)
+{
+    ocean_batch* b = nullptr;
+    ocean_status st = OCEAN_OK;
+    if (desc == nullptr || desc->struct_size != sizeof(ocean_batch_desc) ||
+        (desc->fft_form != OCEAN_FFT_EXACT && desc->fft_form != OCEAN_FFT_FAST)) {
+        st = OCEAN_ERROR_INVALID_ARG;
+    } else {
+        ocean_foam_desc foam;
+        ocean_b200::foam_desc_defaults(&foam);
+        if (desc->persistent_foam) {
+            if (desc->foam.struct_size == 0 || desc->foam.struct_size > sizeof(ocean_foam_desc)) {
+                st = OCEAN_ERROR_INVALID_ARG;
+            } else {
+                std::memcpy(&foam, &desc->foam, desc->foam.struct_size);
+                foam.struct_size = sizeof(ocean_foam_desc);
+            }
+        }
+        if (st == OCEAN_OK) {
+            st = guarded([&] {
+                b = new ocean_batch(desc->oceans, desc->count, desc->fft_form,
+                                    desc->persistent_foam != 0, foam, desc->chunk);
+            });
+        }
+    }
+    if (out_status != nullptr) *out_status = st;
+    return st == OCEAN_OK ? b : nullptr;
+}
+
+void ocean_batch_destroy(ocean_batch* batch) { delete batch; }
+
+uint32_t ocean_batch_count(const ocean_batch* batch) { return batch ? batch->impl.count() : 0u; }
+
+ocean_status ocean_batch_update(ocean_batch* batch, const double* times, int32_t per_ocean_times,
+                                float foam_dt, void* stream)
+{
+    if (batch == nullptr || times == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] {
+        batch->impl.update(times, per_ocean_times != 0, foam_dt, static_cast<cudaStream_t>(stream));
+    });
+}
+
+ocean_status ocean_batch_update_host(ocean_batch* batch, const double* times, int32_t per_ocean_times,
+                                     float foam_dt, float* displacement, float* normal, float* velocity,
+                                     float* foam)
+{
+    if (batch == nullptr || times == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] {
+        batch->impl.update_host(times, per_ocean_times != 0, foam_dt, displacement, normal, velocity, foam);
+    });
+}
+
+ocean_status ocean_batch_get_device_buffers(const ocean_batch* batch, uint32_t index,
+                                            ocean_device_buffers* out)
+{
+    if (batch == nullptr || out == nullptr || index >= batch->impl.count()) return OCEAN_ERROR_INVALID_ARG;
+    fill_device_buffers(batch->impl, index, out);
+    return OCEAN_OK;
+}
+
+uint32_t ocean_batch_last_foam_substeps(const ocean_batch* batch)
+{
+    return batch ? batch->impl.last_foam_substeps() : 0u;
+}
+
+ocean_status ocean_batch_synchronize(ocean_batch* batch)
+{
+    if (batch == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { ocean_b200::check(cudaStreamSynchronize(batch->impl.stream()), "sync"); });
+}
+
+ocean_status ocean_batch_read_spectrum(const ocean_batch* batch, uint32_t index, float* h0,
+                                       float* omega_kinv)
+{
+    if (batch == nullptr || index >= batch->impl.count()) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] {
+        batch->impl.read_spectrum(index, h0, omega_kinv);
+    });
+}
+
+ocean_status ocean_batch_set_profiling(ocean_batch* batch, int32_t enable)
+{
+    if (batch == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { batch->impl.set_profiling(enable != 0); });
+}
+
+ocean_status ocean_batch_read_profile(ocean_batch* batch, ocean_pass_profile* out)
+{
+    if (batch == nullptr || out == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { *out = batch->impl.read_profile(); });
+}
+
+uint64_t ocean_batch_launch_count(const ocean_batch* batch)
+{
+    return batch ? batch->impl.launch_count() : 0u;
+}
+
+const char* ocean_device_arch(void) { return "sm_100a"; }
+
+}  // extern "C"

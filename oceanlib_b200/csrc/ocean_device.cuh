@@ -1,0 +1,176 @@
+// oceanlib-b200: device building blocks shared by the frame kernels.
+//
+// Everything here is compiled with -fmad=false (see build.py): no multiply is
+// ever fused into an add, so each float/double operation rounds exactly where
+// the reference's scalar kernels round. Where the "fast" FFT form wants fused
+// multiply-adds it asks for them explicitly with __fmaf_rn.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ocean_b200 {
+
+// ---------------------------------------------------------------------------
+// Constants shared with the reference's arithmetic. These are the values of
+// src/core/trig.hpp:33-55 and src/core/spectrum.hpp:85-92 (the same IEEE
+// numbers have to be used for the results to match bit for bit).
+// ---------------------------------------------------------------------------
+constexpr double kInvTwoPiD = 0.159154943091895335769;
+constexpr double kTwoPiD = 6.28318530717958647692;
+
+// ---------------------------------------------------------------------------
+// Phase fold and sine/cosine (reference: src/core/trig.hpp:76-129).
+// omega*t is folded into [0, 2pi) in double - the one place FP64 is used per
+// frame - then a Cody-Waite quadrant reduction and two short minimax
+// polynomials give sin and cos together in float.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fold_phase(float omega, double t_over_2pi)
+{
+    const double d = static_cast<double>(omega) * t_over_2pi;
+    return static_cast<float>((d - floor(d)) * kTwoPiD);
+}
+
+__device__ __forceinline__ void sincos_poly(float x, float& s_out, float& c_out)
+{
+    const float qf = floorf(x * 0.636619772367581343076f + 0.5f);
+    const int q = static_cast<int>(qf);
+    float y = x - qf * 1.5707963705062866f;
+    y = y - qf * -4.3711388286737929e-8f;
+    const float z = y * y;
+    const float sy = y + ((-1.9515295891e-4f * z + 8.3321608736e-3f) * z + -1.6666654611e-1f) * z * y;
+    const float cy = 1.0f - 0.5f * z +
+                     ((2.443315711809948e-5f * z + -1.388731625493765e-3f) * z + 4.166664568298827e-2f) * z * z;
+    const int quad = q & 3;
+    const bool swap = (quad & 1) != 0;
+    const float bs = swap ? cy : sy;
+    const float bc = swap ? sy : cy;
+    s_out = (quad & 2) ? -bs : bs;
+    c_out = ((quad + 1) & 2) ? -bc : bc;
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory swizzle for one N-point sequence: XOR the low 4 index bits
+// with the next 4. Every access pattern of the Stockham stage blocks below
+// (lanes walking consecutive indices, or lanes writing 2^r-element runs) then
+// touches 16 distinct 8-byte bank pairs per half-warp.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 4) & 15); }
+
+__host__ __device__ constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
+__host__ __device__ constexpr int cmin(int a, int b) { return a < b ? a : b; }
+
+template <int R>
+__device__ __forceinline__ int bitrev(int s)
+{
+    int o = 0;
+#pragma unroll
+    for (int i = 0; i < R; ++i) o |= ((s >> i) & 1) << (R - 1 - i);
+    return o;
+}
+
+// Butterfly of the radix-2 Stockham stage (reference:
+// src/core/fft_kernel_scalar.cpp:19-33): a' = a + b, b' = (a - b) * w.
+// EXACT keeps the reference's separate multiplies and adds; FAST fuses.
+template <bool FAST>
+__device__ __forceinline__ void butterfly(float2& a, float2& b, float2 w)
+{
+    const float ar = a.x, ai = a.y, br = b.x, bi = b.y;
+    a.x = ar + br;
+    a.y = ai + bi;
+    const float dr = ar - br;
+    const float di = ai - bi;
+    if (FAST) {
+        b.x = __fmaf_rn(dr, w.x, -(di * w.y));
+        b.y = __fmaf_rn(dr, w.y, di * w.x);
+    } else {
+        b.x = dr * w.x - di * w.y;
+        b.y = dr * w.y + di * w.x;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One block of r consecutive radix-2 Stockham stages, L0 .. L0+r-1, on a
+// sequence of N = 2^LOG_N points held (swizzled) in shared memory and worked
+// on by a group of G lanes.
+//
+// Index algebra. At stage L0 an element index is [T : r bits][P : w bits]
+// [q : L0 bits] with w = LOG_N - r - L0. The r stages pair the elements that
+// differ only in T; a lane owns fixed (P, q) and keeps the 2^r values of T in
+// registers. At block-local stage k the twiddle is W^(p << (L0+k)) with
+// p = (R_k << w) | P, R_k being the T bits below the pairing bit; the table
+// `tw` holds, for every stage l, the entries W^(p << l) contiguously from
+// offset N - (N >> l). After the r stages the value in register slot S
+// belongs at [P][bitrev_r(S)][q]. This performs exactly the butterflies of
+// the reference's stage loop (src/core/fft.cpp:70-74) with the same operands
+// and twiddles, so the EXACT form is bit-identical to it.
+// ---------------------------------------------------------------------------
+template <int LOG_N, int G, int L0, bool FAST>
+struct StageBlock {
+    static constexpr int N = 1 << LOG_N;
+    static constexpr int E = N / G;                  // values per lane
+    static constexpr int RMAX = ilog2c(E);
+    static constexpr int r = cmin(RMAX, LOG_N - L0);
+    static constexpr int RR = 1 << r;
+    static constexpr int C = (N >> r) / G;           // (P,q) combos per lane
+    static constexpr int w = LOG_N - r - L0;
+
+    __device__ __forceinline__ static void run(float2* seq, const float2* tw, int lane)
+    {
+        float2 v[C][RR];
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const int c = lane + G * k;
+#pragma unroll
+            for (int t = 0; t < RR; ++t) v[k][t] = seq[swz((t << (LOG_N - r)) | c)];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const int c = lane + G * k;
+            const int P = c >> L0;
+#pragma unroll
+            for (int s = 0; s < r; ++s) {
+                const int half = RR >> (s + 1);
+                const int l = L0 + s;
+                const float2* twl = tw + (N - (N >> l));
+#pragma unroll
+                for (int S = 0; S < RR; ++S) {
+                    if (S & half) continue;
+                    const int Rk = S & (half - 1);
+                    const float2 wv = twl[(Rk << w) | P];
+                    butterfly<FAST>(v[k][S], v[k][S + half], wv);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const int c = lane + G * k;
+            const int P = c >> L0;
+            const int q = c & ((1 << L0) - 1);
+#pragma unroll
+            for (int S = 0; S < RR; ++S) {
+                const int out = (P << (L0 + r)) | (bitrev<r>(S) << L0) | q;
+                seq[swz(out)] = v[k][S];
+            }
+        }
+        __syncwarp();
+        if constexpr (L0 + r < LOG_N) StageBlock<LOG_N, G, L0 + r, FAST>::run(seq, tw, lane);
+    }
+};
+
+// The complete unnormalised inverse transform of one sequence.
+template <int LOG_N, int G, bool FAST>
+__device__ __forceinline__ void fft_sequence(float2* seq, const float2* tw, int lane)
+{
+    StageBlock<LOG_N, G, 0, FAST>::run(seq, tw, lane);
+}
+
+// Lanes per sequence: each lane keeps 16 values (a 4-stage block) where the
+// sequence is long enough, capped at one warp.
+__host__ __device__ constexpr int lanes_for(int log_n)
+{
+    return (log_n - 4) >= 5 ? 32 : (1 << (log_n - 4 < 0 ? 0 : log_n - 4));
+}
+
+}  // namespace ocean_b200

@@ -1,0 +1,80 @@
+// oceanlib-b200: host-side interface of the device kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ocean_b200 {
+
+// Inputs of the init-time spectrum build (the fields of ocean::OceanDesc the
+// reference's build_spectrum reads, src/core/spectrum.cpp:264-339).
+struct SpectrumParams {
+    uint32_t n;
+    float patch_length;
+    float wind_speed, fetch, wind_direction, peak_enhancement, swell;
+    float small_wave_cutoff, gravity, depth;
+    uint64_t seed;
+};
+
+cudaError_t launch_h0(const SpectrumParams& p, float2* h0, cudaStream_t stream);
+cudaError_t launch_geometry(const SpectrumParams& p, float2* omega_kinv, float* kvec,
+                            cudaStream_t stream);
+
+// Per-ocean constants of the finalize stage (src/core/evolve.cpp:238-327).
+struct OceanConsts {
+    float lambda;         // choppiness
+    float foam_threshold;
+    float inv_threshold;  // 1/threshold, or 0 for a degenerate threshold
+    int32_t geom;         // index of the ocean's (omega, 1/|k|) table
+};
+
+// One frame's worth of device pointers for a batch of same-N oceans.
+struct FrameArgs {
+    const float2* h0;          // [count][N*N]
+    const float2* omega_kinv;  // [geoms][N*N]
+    const float* kvec;         // [geoms][N]
+    const float2* twiddles;    // [N-1] per-stage inverse twiddles
+    const OceanConsts* consts; // [count]
+    const double* t_over_2pi;  // [count]
+    float2* inter;             // [chunk][N][N][NF] row-pass output
+    float4* disp;              // [count][N*N]
+    float4* normal;            // [count][N*N]
+    float4* velocity;          // [count][N*N] or null
+    // persistent foam (only read when a foam substep is fused)
+    const float* foam_cur;     // [count][N*N]
+    float* foam_next;          // [count][N*N]
+    float foam_dt, foam_decay, foam_gain, foam_scale, foam_drift_x, foam_drift_z;
+    float foam_inv_cell;       // 1 / (patch_length / N); per batch (same L)
+    int32_t ocean_base;        // first ocean of this chunk
+    int32_t chunk;             // oceans in this chunk
+};
+
+// Row pass (evolve + row FFTs) and column pass (column FFTs + finalize, with
+// an optional fused foam substep) for `args.chunk` oceans starting at
+// args.ocean_base. log_n in [4, 10]; nf is 4 or 6 complex fields.
+cudaError_t launch_row_pass(int log_n, int nf, bool fast, const FrameArgs& args,
+                            cudaStream_t stream);
+cudaError_t launch_col_pass(int log_n, int nf, bool fast, bool fuse_foam,
+                            const FrameArgs& args, cudaStream_t stream);
+
+// Stand-alone foam substep for oceans [0, count) (used for substeps after the
+// first in one update).
+cudaError_t launch_foam_step(int n, int count, const float4* disp, const float4* velocity,
+                             const float* cur, float* next, float dt, float decay, float gain,
+                             float scale, float drift_x, float drift_z, float inv_cell,
+                             cudaStream_t stream);
+
+// Batched world queries (src/ocean.cpp:375-452), one thread per point.
+struct SurfaceEx {
+    float height, offset_x, offset_z, normal_x, normal_y, normal_z, foam;
+    float velocity_x, velocity_y, velocity_z;
+};
+cudaError_t launch_sample(int n, float inv_cell, const float4* disp, const float4* normal,
+                          const float4* velocity, const float2* xz, uint64_t count,
+                          SurfaceEx* out, cudaStream_t stream);
+
+// Shared-memory bytes each pass needs at a given size (for checks).
+size_t row_pass_smem(int log_n, int nf);
+size_t col_pass_smem(int log_n, int nf);
+
+}  // namespace ocean_b200

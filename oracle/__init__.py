@@ -1,0 +1,446 @@
+"""Test infrastructure: the CPU checkers for oceanlib_b200.
+
+Two libraries, both built by oracle/Makefile:
+
+* ``liboracle.so``           - ocean_oracle.c, a plain-C restatement of the
+                               reference's per-frame path (the oracle).
+* ``_ref/libocean_ref.so``   - the reference oceanlib itself, compiled from its
+                               own sources, behind ref_shim.cpp. Used to pin the
+                               oracle and as the timed CPU baseline.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this package. Nothing in oceanlib_b200 may.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+from typing import Optional
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_SO = HERE / "_ref" / "libocean_ref.so"
+REF_SRC = Path(os.environ.get("OCEAN_REF_SRC", "/root/reference"))
+
+
+class OrDesc(C.Structure):
+    _fields_ = [
+        ("n", C.c_uint32),
+        ("patch_length", C.c_float),
+        ("wind_speed", C.c_float),
+        ("fetch", C.c_float),
+        ("wind_direction", C.c_float),
+        ("peak_enhancement", C.c_float),
+        ("swell", C.c_float),
+        ("small_wave_cutoff", C.c_float),
+        ("gravity", C.c_float),
+        ("depth", C.c_float),
+        ("choppiness", C.c_float),
+        ("foam_threshold", C.c_float),
+        ("seed", C.c_uint64),
+        ("velocity", C.c_int32),
+    ]
+
+
+class OrefFoamDesc(C.Structure):
+    _fields_ = [(n, C.c_float) for n in
+                ("decay", "source_gain", "advect_scale", "wind_drift_x", "wind_drift_z", "fixed_dt")] + \
+               [("max_substeps", C.c_uint32), ("thread_count", C.c_uint32)]
+
+
+def build(quiet: bool = True) -> None:
+    """Compile the oracle (and, when the reference sources are present, the
+    reference library) in place."""
+    cmd = ["make", "-s", "-C", str(HERE), f"REF={REF_SRC}"]
+    subprocess.run(cmd, check=True, capture_output=quiet)
+
+
+_oracle: Optional[C.CDLL] = None
+_ref: Optional[C.CDLL] = None
+
+_F = C.POINTER(C.c_float)
+_P = C.c_void_p
+
+
+def oracle() -> C.CDLL:
+    global _oracle
+    if _oracle is None:
+        if not ORACLE_SO.exists():
+            build()
+        l = C.CDLL(str(ORACLE_SO))
+        sig = {
+            "or_pcg32_fill": (None, [C.c_uint64, C.c_uint64, C.c_uint32, _P]),
+            "or_mix64": (C.c_uint64, [C.c_uint64]),
+            "or_row_gaussians": (None, [C.c_uint64, C.c_uint32, C.c_uint32, _P]),
+            "or_build_spectrum": (None, [C.POINTER(OrDesc), _P]),
+            "or_evolve": (None, [C.POINTER(OrDesc), _P, C.c_double, _P]),
+            "or_fft_1d": (None, [C.c_uint32, _P, _P, C.c_int]),
+            "or_fft_2d": (None, [C.c_uint32, _P, _P, C.c_int]),
+            "or_finalize": (None, [C.POINTER(OrDesc), _P, _P, _P, _P]),
+            "or_update": (None, [C.POINTER(OrDesc), _P, C.c_double, _P, _P, _P, _P]),
+            "or_sample_many": (None, [C.c_uint32, C.c_float, _P, _P, _P, _P, C.c_uint64, _P]),
+            "or_foam_step": (None, [C.c_uint32] + [C.c_float] * 7 + [_P, _P, _P, _P]),
+            "or_dft2d_points": (None, [C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P, _P]),
+            "or_dft2d_full": (None, [C.c_uint32, _P, _P, _P, _P]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _oracle = l
+    return _oracle
+
+
+def ref_available() -> bool:
+    if REF_SO.exists():
+        return True
+    if (REF_SRC / "src" / "ocean.cpp").exists():
+        try:
+            build()
+        except Exception:
+            return False
+    return REF_SO.exists()
+
+
+def ref() -> C.CDLL:
+    """The reference library (raises if it was never built)."""
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise FileNotFoundError(f"{REF_SO} not built (reference sources absent)")
+        l = C.CDLL(str(REF_SO))
+        sig = {
+            "oref_c_create": (_P, [_P, C.POINTER(C.c_int)]),
+            "oref_c_destroy": (None, [_P]),
+            "oref_c_update": (None, [_P, C.c_double]),
+            "oref_c_get_buffers": (None, [_P, _P]),
+            "oref_c_get_velocity": (_F, [_P]),
+            "oref_c_height_at": (C.c_float, [_P, C.c_float, C.c_float]),
+            "oref_c_sample_ex": (None, [_P, C.c_float, C.c_float, _P]),
+            "oref_c_sample_many": (None, [_P, _P, C.c_uint64, _P]),
+            "oref_c_desc_init": (None, [_P]),
+            "oref_c_force_simd_level": (C.c_char_p, [C.c_char_p]),
+            "oref_c_simd_level": (C.c_char_p, []),
+            "oref_stage_create": (_P, [_P]),
+            "oref_stage_destroy": (None, [_P]),
+            "oref_stage_tables": (None, [_P, _P]),
+            "oref_stage_evolve": (None, [_P, C.c_double]),
+            "oref_stage_fft": (None, [_P]),
+            "oref_stage_plane_count": (C.c_int, [_P]),
+            "oref_stage_get_fields": (None, [_P, _P]),
+            "oref_stage_set_fields": (None, [_P, _P]),
+            "oref_stage_finalize": (None, [_P, _P, _P, _P]),
+            "oref_fft_1d": (None, [C.c_uint32, _P, _P, C.c_int]),
+            "oref_fft_2d": (None, [C.c_uint32, _P, _P, C.c_int]),
+            "oref_pcg32": (None, [C.c_uint64, C.c_uint64, C.c_uint32, _P]),
+            "oref_row_gaussians": (None, [C.c_uint64, C.c_uint32, C.c_uint32, _P]),
+            "oref_foam_create": (_P, [_P, C.POINTER(OrefFoamDesc), C.POINTER(C.c_int)]),
+            "oref_foam_destroy": (None, [_P]),
+            "oref_foam_update": (None, [_P, C.c_float]),
+            "oref_foam_data": (_F, [_P]),
+            "oref_foam_last_substeps": (C.c_uint32, [_P]),
+            "oref_foam_coverage": (C.c_double, [_P]),
+            "oref_foam_at": (C.c_float, [_P, C.c_float, C.c_float]),
+            "oref_foam_clear": (None, [_P]),
+            "oref_cascade_create": (_P, [_P, C.c_uint32, C.POINTER(C.c_int)]),
+            "oref_cascade_destroy": (None, [_P]),
+            "oref_cascade_update": (None, [_P, C.c_double]),
+            "oref_cascade_sample_many": (None, [_P, _P, C.c_uint64, _P]),
+            "oref_time_updates": (C.c_double, [_P, _P, C.c_uint32, C.c_uint32, C.c_double,
+                                               C.c_double, C.c_float]),
+            "oref_hardware_concurrency": (C.c_uint32, []),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _ref = l
+    return _ref
+
+
+# ---------------------------------------------------------------------------
+# Descriptor plumbing. `desc` is any object with the OceanDesc attribute names
+# used by oceanlib_b200.OceanDesc (size, patch_length, wind_speed, ...).
+# ---------------------------------------------------------------------------
+def or_desc(desc) -> OrDesc:
+    d = OrDesc()
+    d.n = desc.size
+    d.patch_length = desc.patch_length
+    d.wind_speed = desc.wind_speed
+    d.fetch = desc.fetch
+    d.wind_direction = desc.wind_direction
+    d.peak_enhancement = desc.peak_enhancement
+    d.swell = desc.swell
+    d.small_wave_cutoff = desc.small_wave_cutoff
+    d.gravity = desc.gravity
+    d.depth = desc.depth
+    d.choppiness = desc.choppiness
+    d.foam_threshold = desc.foam_threshold
+    d.seed = desc.seed
+    d.velocity = 1 if desc.compute_velocity else 0
+    return d
+
+
+def c_desc_bytes(desc) -> C.Array:
+    """The reference's `ocean_desc` for `desc`, built through the reference's
+    own ocean_desc_init, as raw bytes (96 on LP64)."""
+    from oceanlib_b200.abi import OceanDescC  # layout only
+
+    d = OceanDescC()
+    ref().oref_c_desc_init(C.byref(d))
+    d.size = desc.size
+    d.patch_length = desc.patch_length
+    s = d.spectrum
+    s.wind_speed = desc.wind_speed
+    s.fetch = desc.fetch
+    s.wind_direction = desc.wind_direction
+    s.peak_enhancement = desc.peak_enhancement
+    s.swell = desc.swell
+    s.small_wave_cutoff = desc.small_wave_cutoff
+    s.gravity = desc.gravity
+    d.water_depth = desc.depth
+    d.choppiness = desc.choppiness
+    d.foam_threshold = desc.foam_threshold
+    d.seed = desc.seed
+    d.compute_velocity = 1 if desc.compute_velocity else 0
+    d.thread_count = getattr(desc, "thread_count", 0)
+    return d
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data
+
+
+# ---------------------------------------------------------------------------
+# Oracle (C restatement) helpers
+# ---------------------------------------------------------------------------
+def spectrum(desc) -> np.ndarray:
+    """(8, N*N) float32 tables: h0_re, h0_im, h0c_re, h0c_im, omega, kx, kz, k_inv."""
+    n = desc.size
+    t = np.empty((8, n * n), dtype=np.float32)
+    d = or_desc(desc)
+    oracle().or_build_spectrum(C.byref(d), t.ctypes.data)
+    return t
+
+
+def update(desc, t: float, tables: Optional[np.ndarray] = None):
+    """One frame on the CPU oracle -> (disp (N*N,4), normal (N*N,4), velocity or None)."""
+    n = desc.size
+    if tables is None:
+        tables = spectrum(desc)
+    d = or_desc(desc)
+    planes = 12 if desc.compute_velocity else 8
+    fields = np.empty((planes, n * n), dtype=np.float32)
+    disp = np.empty((n * n, 4), dtype=np.float32)
+    normal = np.empty((n * n, 4), dtype=np.float32)
+    vel = np.empty((n * n, 4), dtype=np.float32) if desc.compute_velocity else None
+    oracle().or_update(C.byref(d), tables.ctypes.data, float(t), fields.ctypes.data,
+                       disp.ctypes.data, normal.ctypes.data, _ptr(vel))
+    return disp, normal, vel
+
+
+def evolve(desc, t: float, tables: Optional[np.ndarray] = None) -> np.ndarray:
+    n = desc.size
+    if tables is None:
+        tables = spectrum(desc)
+    d = or_desc(desc)
+    fields = np.empty((12 if desc.compute_velocity else 8, n * n), dtype=np.float32)
+    oracle().or_evolve(C.byref(d), tables.ctypes.data, float(t), fields.ctypes.data)
+    return fields
+
+
+def fft_2d(re: np.ndarray, im: np.ndarray, sign: int = +1):
+    re = np.ascontiguousarray(re, dtype=np.float32).copy()
+    im = np.ascontiguousarray(im, dtype=np.float32).copy()
+    oracle().or_fft_2d(int(round(np.sqrt(re.size))), re.ctypes.data, im.ctypes.data, sign)
+    return re, im
+
+
+def fft_1d(re: np.ndarray, im: np.ndarray, sign: int = +1):
+    re = np.ascontiguousarray(re, dtype=np.float32).copy()
+    im = np.ascontiguousarray(im, dtype=np.float32).copy()
+    oracle().or_fft_1d(re.size, re.ctypes.data, im.ctypes.data, sign)
+    return re, im
+
+
+def sample_many(n: int, patch_length: float, disp, normal, vel, xz: np.ndarray) -> np.ndarray:
+    xz = np.ascontiguousarray(xz, dtype=np.float32)
+    out = np.empty((xz.shape[0], 10), dtype=np.float32)
+    oracle().or_sample_many(n, patch_length, disp.ctypes.data, normal.ctypes.data, _ptr(vel),
+                            xz.ctypes.data, xz.shape[0], out.ctypes.data)
+    return out
+
+
+def foam_step(n, cell, dt, decay, gain, scale, drift_x, drift_z, disp, vel, cur) -> np.ndarray:
+    nxt = np.empty(n * n, dtype=np.float32)
+    oracle().or_foam_step(n, cell, dt, decay, gain, scale, drift_x, drift_z, disp.ctypes.data,
+                          vel.ctypes.data, np.ascontiguousarray(cur, np.float32).ctypes.data,
+                          nxt.ctypes.data)
+    return nxt
+
+
+def dft_points(re: np.ndarray, im: np.ndarray, xs, ys):
+    """FP64 direct inverse DFT of one complex field at points (xs[i], ys[i])."""
+    n = int(round(np.sqrt(re.size)))
+    xs = np.ascontiguousarray(xs, dtype=np.uint32)
+    ys = np.ascontiguousarray(ys, dtype=np.uint32)
+    o_re = np.empty(xs.size, dtype=np.float64)
+    o_im = np.empty(xs.size, dtype=np.float64)
+    oracle().or_dft2d_points(n, np.ascontiguousarray(re, np.float32).ctypes.data,
+                             np.ascontiguousarray(im, np.float32).ctypes.data, xs.size,
+                             xs.ctypes.data, ys.ctypes.data, o_re.ctypes.data, o_im.ctypes.data)
+    return o_re, o_im
+
+
+def pcg32(seed: int, stream: int, count: int) -> np.ndarray:
+    out = np.empty(count, dtype=np.uint32)
+    oracle().or_pcg32_fill(seed, stream, count, out.ctypes.data)
+    return out
+
+
+def row_gaussians(seed: int, row: int, pairs: int) -> np.ndarray:
+    out = np.empty(2 * pairs, dtype=np.float32)
+    oracle().or_row_gaussians(seed, row, pairs, out.ctypes.data)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Reference helpers
+# ---------------------------------------------------------------------------
+class RefOcean:
+    """The reference ocean::Ocean behind its own C ABI."""
+
+    def __init__(self, desc):
+        self.desc = desc
+        self._cd = c_desc_bytes(desc)
+        st = C.c_int(-1)
+        self.h = ref().oref_c_create(C.byref(self._cd), C.byref(st))
+        if not self.h:
+            raise ValueError(f"reference rejected descriptor (status {st.value})")
+        self.n = desc.size
+
+    def update(self, t: float) -> None:
+        ref().oref_c_update(self.h, float(t))
+
+    def buffers(self):
+        from oceanlib_b200.abi import Buffers
+
+        b = Buffers()
+        ref().oref_c_get_buffers(self.h, C.byref(b))
+        cells = self.n * self.n
+        disp = np.ctypeslib.as_array(b.displacement, shape=(cells * 4,)).reshape(cells, 4).copy()
+        normal = np.ctypeslib.as_array(b.normal, shape=(cells * 4,)).reshape(cells, 4).copy()
+        v = ref().oref_c_get_velocity(self.h)
+        vel = np.ctypeslib.as_array(v, shape=(cells * 4,)).reshape(cells, 4).copy() if v else None
+        return disp, normal, vel
+
+    def sample_many(self, xz: np.ndarray) -> np.ndarray:
+        xz = np.ascontiguousarray(xz, dtype=np.float32)
+        out = np.empty((xz.shape[0], 10), dtype=np.float32)
+        ref().oref_c_sample_many(self.h, xz.ctypes.data, xz.shape[0], out.ctypes.data)
+        return out
+
+    def close(self):
+        if self.h:
+            ref().oref_c_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RefFoam:
+    """The reference ocean::FoamField over a RefOcean."""
+
+    def __init__(self, ocean: RefOcean, foam_desc, thread_count: int = 0):
+        d = OrefFoamDesc()
+        for k in ("decay", "source_gain", "advect_scale", "wind_drift_x", "wind_drift_z", "fixed_dt"):
+            setattr(d, k, getattr(foam_desc, k))
+        d.max_substeps = foam_desc.max_substeps
+        d.thread_count = thread_count
+        st = C.c_int(-1)
+        self.h = ref().oref_foam_create(ocean.h, C.byref(d), C.byref(st))
+        if not self.h:
+            raise ValueError("reference FoamField rejected")
+        self.n = ocean.n
+        self._ocean = ocean
+
+    def update(self, dt: float) -> None:
+        ref().oref_foam_update(self.h, dt)
+
+    def data(self) -> np.ndarray:
+        p = ref().oref_foam_data(self.h)
+        return np.ctypeslib.as_array(p, shape=(self.n * self.n,)).copy()
+
+    @property
+    def last_substeps(self) -> int:
+        return ref().oref_foam_last_substeps(self.h)
+
+    def close(self):
+        if self.h:
+            ref().oref_foam_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_stage(desc):
+    """Reference internal stages: returns (tables (8,N*N), callable evolve, ...)."""
+    cd = c_desc_bytes(desc)
+    h = ref().oref_stage_create(C.byref(cd))
+    return h
+
+
+def ref_tables(desc) -> np.ndarray:
+    h = ref_stage(desc)
+    try:
+        t = np.empty((8, desc.size * desc.size), dtype=np.float32)
+        ref().oref_stage_tables(h, t.ctypes.data)
+        return t
+    finally:
+        ref().oref_stage_destroy(h)
+
+
+def ref_evolve_fields(desc, t: float, transform: bool = False) -> np.ndarray:
+    h = ref_stage(desc)
+    try:
+        ref().oref_stage_evolve(h, float(t))
+        if transform:
+            ref().oref_stage_fft(h)
+        planes = ref().oref_stage_plane_count(h)
+        f = np.empty((planes, desc.size * desc.size), dtype=np.float32)
+        ref().oref_stage_get_fields(h, f.ctypes.data)
+        return f
+    finally:
+        ref().oref_stage_destroy(h)
+
+
+def ref_pcg32(seed: int, stream: int, count: int) -> np.ndarray:
+    out = np.empty(count, dtype=np.uint32)
+    ref().oref_pcg32(seed, stream, count, out.ctypes.data)
+    return out
+
+
+def ref_fft_2d(re: np.ndarray, im: np.ndarray, sign: int = +1):
+    re = np.ascontiguousarray(re, dtype=np.float32).copy()
+    im = np.ascontiguousarray(im, dtype=np.float32).copy()
+    ref().oref_fft_2d(int(round(np.sqrt(re.size))), re.ctypes.data, im.ctypes.data, sign)
+    return re, im
+
+
+def ref_fft_1d(re: np.ndarray, im: np.ndarray, sign: int = +1):
+    re = np.ascontiguousarray(re, dtype=np.float32).copy()
+    im = np.ascontiguousarray(im, dtype=np.float32).copy()
+    ref().oref_fft_1d(re.size, re.ctypes.data, im.ctypes.data, sign)
+    return re, im

@@ -1,0 +1,88 @@
+/* Test infrastructure: a plain-C restatement of oceanlib's per-frame path.
+ *
+ * This is the CHECKER for the CUDA library, never part of it. Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg load it. Each
+ * function names the reference file:line whose arithmetic it restates; every
+ * float operation is written in the same order as the reference and the file
+ * is compiled with -ffp-contract=off, so results are bit-identical to the
+ * reference's scalar kernels (pinned by tests/test_oracle_pins.py against the
+ * reference compiled from its own sources, and against its known answers).
+ */
+#ifndef OCEAN_ORACLE_H
+#define OCEAN_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Flat descriptor (the fields of ocean::OceanDesc that the path reads). */
+typedef struct or_desc {
+    uint32_t n;
+    float patch_length;
+    float wind_speed, fetch, wind_direction, peak_enhancement, swell;
+    float small_wave_cutoff, gravity, depth;
+    float choppiness, foam_threshold;
+    uint64_t seed;
+    int32_t velocity;
+} or_desc;
+
+typedef struct or_pcg32 {
+    uint64_t state, inc;
+} or_pcg32;
+
+or_pcg32 or_pcg32_seed(uint64_t seed, uint64_t stream);
+uint32_t or_pcg32_next(or_pcg32* r);
+void or_pcg32_fill(uint64_t seed, uint64_t stream, uint32_t count, uint32_t* out);
+uint64_t or_mix64(uint64_t x);
+void or_row_gaussians(uint64_t seed, uint32_t row, uint32_t pairs, float* out);
+
+/* Spectrum tables: 8 planes of n*n floats, in the order
+ * h0_re, h0_im, h0c_re, h0c_im, omega, kx, kz, k_inv. */
+void or_build_spectrum(const or_desc* d, float* tables);
+
+/* Per-frame evolve into 8 (or 12 with velocity) planes re0, im0, re1, im1, ... */
+void or_evolve(const or_desc* d, const float* tables, double t, float* fields);
+
+/* Unnormalised radix-2 Stockham FFT; sign +1 = inverse, -1 = forward. */
+void or_fft_1d(uint32_t n, float* re, float* im, int sign);
+void or_fft_2d(uint32_t n, float* re, float* im, int sign);
+
+/* Finalize: displacement and normal RGBA32F (n*n*4 each), velocity if non-NULL. */
+void or_finalize(const or_desc* d, const float* fields, float* disp, float* normal,
+                 float* velocity);
+
+/* Whole update: evolve -> 2-D inverse FFTs -> finalize. `fields` is scratch of
+ * 8 (12) * n*n floats. */
+void or_update(const or_desc* d, const float* tables, double t, float* fields,
+               float* disp, float* normal, float* velocity);
+
+/* World query (Ocean::sample_at). out[10] = height, offset_x, offset_z,
+ * normal xyz, foam, velocity xyz. velocity may be NULL. */
+void or_sample_at(uint32_t n, float patch_length, const float* disp, const float* normal,
+                  const float* velocity, float x, float z, float* out);
+void or_sample_many(uint32_t n, float patch_length, const float* disp, const float* normal,
+                    const float* velocity, const float* xz, uint64_t count, float* out);
+
+/* One persistent-foam substep (FoamField step_rows). `decay` is the already
+ * evaluated expf(-decay_rate * dt), as the reference computes it on the host. */
+void or_foam_step(uint32_t n, float cell, float dt, float decay, float gain, float scale,
+                  float drift_x, float drift_z, const float* disp, const float* velocity,
+                  const float* cur, float* next);
+
+/* FP64 oracle: the direct 2-D inverse DFT of a complex n*n field evaluated in
+ * double at `count` output points (x[i], y[i]); O(n^2) per point, sharing no
+ * structure with the FFT. */
+void or_dft2d_points(uint32_t n, const float* re, const float* im, uint32_t count,
+                     const uint32_t* xs, const uint32_t* ys, double* out_re, double* out_im);
+/* Full O(n^4) direct 2-D inverse DFT (small n only). */
+void or_dft2d_full(uint32_t n, const float* re, const float* im, double* out_re,
+                   double* out_im);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

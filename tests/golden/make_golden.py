@@ -1,0 +1,142 @@
+"""Regenerates the golden fixtures in this folder from the REFERENCE library
+(oracle/_ref/libocean_ref.so, compiled from the reference's own sources by
+oracle/Makefile). Run here, where the reference sources exist:
+
+    python tests/golden/make_golden.py
+
+Outputs
+  ref_small.npz    full tables and frame outputs for small grids (N <= 64)
+  ref_hashes.json  sha256 of the reference's output bytes at full sizes,
+                   so GPU tests can check bit-exactness at N = 256 / 512 / 1024
+                   without storing the arrays
+  ref_queries.npz  reference sample_at results for seeded query points
+  abi_layout.json  offsets/sizes of the reference's C structs (include/ocean/ocean.h)
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+import oracle as O  # noqa: E402
+from tests.workloads import (SMALL_CASES, HASH_CASES, FOAM_CASE, QUERY_CASE, desc_to_json,  # noqa: E402
+                             query_points)
+
+HERE = Path(__file__).resolve().parent
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def small() -> None:
+    arrays = {}
+    meta = []
+    for i, (desc, times) in enumerate(SMALL_CASES):
+        arrays[f"c{i}_tables"] = O.ref_tables(desc)
+        ro = O.RefOcean(desc)
+        for j, t in enumerate(times):
+            ro.update(t)
+            d, n, v = ro.buffers()
+            arrays[f"c{i}_t{j}_disp"] = d
+            arrays[f"c{i}_t{j}_normal"] = n
+            if v is not None:
+                arrays[f"c{i}_t{j}_vel"] = v
+        meta.append({"desc": desc_to_json(desc), "times": list(times)})
+    arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    np.savez_compressed(HERE / "ref_small.npz", **arrays)
+
+
+def hashes() -> None:
+    out = {"cases": []}
+    for desc, times in HASH_CASES:
+        tables = O.ref_tables(desc)
+        h0 = np.stack([tables[0], tables[1]], axis=1)  # interleaved complex
+        entry = {"desc": desc_to_json(desc), "h0": sha(h0), "frames": []}
+        ro = O.RefOcean(desc)
+        for t in times:
+            ro.update(t)
+            d, n, v = ro.buffers()
+            fr = {"t": t, "disp": sha(d), "normal": sha(n)}
+            if v is not None:
+                fr["vel"] = sha(v)
+            entry["frames"].append(fr)
+        out["cases"].append(entry)
+    # Persistent foam: the reference FoamField after each of `frames` frames.
+    desc, foam, frames, dt = FOAM_CASE
+    ro = O.RefOcean(desc)
+    rf = O.RefFoam(ro, foam)
+    foam_hashes = []
+    for k in range(frames):
+        ro.update((k + 1) * dt)
+        rf.update(dt)
+        foam_hashes.append(sha(rf.data()))
+    out["foam"] = {"desc": desc_to_json(desc), "frames": frames, "dt": dt,
+                   "hashes": foam_hashes, "coverage_last": float(rf.data().mean())}
+    (HERE / "ref_hashes.json").write_text(json.dumps(out, indent=1))
+
+
+def queries() -> None:
+    desc, t, count = QUERY_CASE
+    ro = O.RefOcean(desc)
+    ro.update(t)
+    xz = query_points(desc, count)
+    res = ro.sample_many(xz)
+    np.savez_compressed(HERE / "ref_queries.npz", xz=xz, out=res)
+
+
+def abi_layout() -> None:
+    src = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "ocean/ocean.h"
+#define OFF(T, f) printf("\"%s.%s\": %zu,\n", #T, #f, offsetof(T, f))
+int main(void) {
+  printf("{\n");
+  printf("\"sizeof.ocean_desc\": %zu,\n", sizeof(ocean_desc));
+  printf("\"sizeof.ocean_spectrum_desc\": %zu,\n", sizeof(ocean_spectrum_desc));
+  printf("\"sizeof.ocean_buffers\": %zu,\n", sizeof(ocean_buffers));
+  printf("\"sizeof.ocean_surface\": %zu,\n", sizeof(ocean_surface));
+  printf("\"sizeof.ocean_surface_ex\": %zu,\n", sizeof(ocean_surface_ex));
+  OFF(ocean_desc, struct_size); OFF(ocean_desc, size); OFF(ocean_desc, patch_length);
+  OFF(ocean_desc, spectrum); OFF(ocean_desc, choppiness); OFF(ocean_desc, foam_threshold);
+  OFF(ocean_desc, seed); OFF(ocean_desc, parallel_for); OFF(ocean_desc, parallel_for_user);
+  OFF(ocean_desc, thread_count); OFF(ocean_desc, water_depth); OFF(ocean_desc, compute_velocity);
+  OFF(ocean_buffers, displacement); OFF(ocean_buffers, normal); OFF(ocean_buffers, size);
+  OFF(ocean_buffers, patch_length);
+  printf("\"end\": 0\n}\n");
+  return 0;
+}
+"""
+    with tempfile.TemporaryDirectory() as td:
+        c = Path(td) / "layout.c"
+        c.write_text(src)
+        exe = Path(td) / "layout"
+        subprocess.run(["gcc", "-I", str(O.REF_SRC / "include"), str(c), "-o", str(exe)], check=True)
+        res = subprocess.run([str(exe)], check=True, capture_output=True, text=True)
+    layout = json.loads(res.stdout)
+    layout.pop("end")
+    (HERE / "abi_layout.json").write_text(json.dumps(layout, indent=1))
+
+
+def main() -> None:
+    if not O.ref_available():
+        raise SystemExit("the reference library could not be built (reference sources absent)")
+    O.ref().oref_c_force_simd_level(None)
+    small()
+    hashes()
+    queries()
+    abi_layout()
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

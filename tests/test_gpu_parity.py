@@ -1,0 +1,256 @@
+"""GPU parity: libocean_b200.so through its C ABI against the reference.
+
+Bar: bit-exact for the exact FFT form (the reference's scalar op order), for
+the PRNG/h0 tables, the world queries and the persistent foam; the fast (FMA)
+form within max-abs 1e-5 x field RMS per output channel. Full-size cases are
+checked against sha256 digests of the reference's own output bytes
+(tests/golden/ref_hashes.json); smaller ones against the oracle directly.
+"""
+import ctypes as C
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oceanlib_b200 as ob
+import oracle as O
+from oceanlib_b200 import abi, workloads as W
+from tests.workloads import (FOAM_CASE, HASH_CASES, QUERY_CASE, SMALL_CASES, desc_from_json,
+                             query_points)
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+FAST_TOL = 1e-5  # max-abs error / field RMS, per output channel (fast form)
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def frame(ocean):
+    b = ocean.buffers()
+    v = b["velocity"]
+    return b["displacement"].copy(), b["normal"].copy(), None if v is None else v.copy()
+
+
+@pytest.fixture(autouse=True)
+def _exact_level(cuda_device):
+    ob.force_simd_level(None)
+    yield
+    ob.force_simd_level(None)
+
+
+def test_device_h0_tables_are_bit_exact():
+    for desc, _ in HASH_CASES + SMALL_CASES:
+        batch = ob.OceanBatch([desc])
+        h0, wk = batch.read_spectrum(0)
+        tables = O.spectrum(desc)
+        ref_h0 = np.stack([tables[0], tables[1]], axis=1)
+        mism = int(np.count_nonzero(bits(h0) != bits(ref_h0)))
+        assert mism == 0, f"N={desc.size}: {mism} h0 words differ from the reference"
+        assert np.array_equal(bits(wk[:, 0]), bits(tables[4])), "omega table"
+        assert np.array_equal(bits(wk[:, 1]), bits(tables[7])), "1/|k| table"
+        batch.close()
+
+
+def test_small_grids_bit_exact_against_reference_arrays():
+    g = np.load(GOLDEN / "ref_small.npz")
+    meta = json.loads(bytes(g["meta"]).decode())
+    for i, m in enumerate(meta):
+        desc = desc_from_json(m["desc"])
+        oc = ob.Ocean(desc)
+        for j, t in enumerate(m["times"]):
+            oc.update(t)
+            d, n, v = frame(oc)
+            assert np.array_equal(bits(d), bits(g[f"c{i}_t{j}_disp"])), (desc.size, t)
+            assert np.array_equal(bits(n), bits(g[f"c{i}_t{j}_normal"])), (desc.size, t)
+            if v is not None:
+                assert np.array_equal(bits(v), bits(g[f"c{i}_t{j}_vel"])), (desc.size, t)
+        oc.close()
+
+
+def test_full_size_frames_bit_exact_against_reference_digests():
+    golden = json.loads((GOLDEN / "ref_hashes.json").read_text())
+    for case in golden["cases"]:
+        desc = desc_from_json(case["desc"])
+        oc = ob.Ocean(desc)
+        for fr in case["frames"]:
+            oc.update(fr["t"])
+            d, n, v = frame(oc)
+            if sha(d) != fr["disp"] or sha(n) != fr["normal"]:
+                od, on, _ = O.update(desc, fr["t"])
+                bad = int(np.count_nonzero(bits(d) != bits(od)) + np.count_nonzero(bits(n) != bits(on)))
+                pytest.fail(f"N={desc.size} t={fr['t']}: {bad} words differ from the reference")
+            if v is not None:
+                assert sha(v) == fr["vel"], (desc.size, fr["t"])
+        oc.close()
+
+
+def test_every_size_matches_oracle():
+    for n in (16, 32, 64, 128, 256, 512, 1024):
+        for vel in (False, True):
+            desc = ob.OceanDesc(size=n, patch_length=3.0 * n, wind_speed=14.0, wind_direction=1.1,
+                                choppiness=1.3, seed=n + vel, compute_velocity=vel)
+            oc = ob.Ocean(desc)
+            oc.update(123.456)
+            d, nn, v = frame(oc)
+            od, on, ov = O.update(desc, 123.456)
+            assert np.array_equal(bits(d), bits(od)), (n, vel)
+            assert np.array_equal(bits(nn), bits(on)), (n, vel)
+            if vel:
+                assert np.array_equal(bits(v), bits(ov)), n
+            oc.close()
+
+
+def test_batch_equals_single_oceans_and_chunking_is_invisible():
+    descs = [W.foam_patch_512(seed=7 + k) for k in range(5)]
+    times = [0.25 * k + 3.0 for k in range(5)]
+    outs = {}
+    for chunk in (1, 2, 0):
+        batch = ob.OceanBatch(descs, chunk=chunk)
+        batch.update(times)
+        batch.synchronize()
+        cells = 512 * 512
+        disp = np.empty((5, cells, 4), np.float32)
+        nrm = np.empty_like(disp)
+        vel = np.empty_like(disp)
+        batch.update_host(times, 0.0, disp, nrm, vel)
+        outs[chunk] = (disp, nrm, vel)
+        batch.close()
+    for chunk in (1, 2):
+        for a, b in zip(outs[chunk], outs[0]):
+            assert np.array_equal(bits(a), bits(b))
+    for k in (0, 4):
+        od, on, ov = O.update(descs[k], times[k])
+        assert np.array_equal(bits(outs[0][0][k]), bits(od))
+        assert np.array_equal(bits(outs[0][1][k]), bits(on))
+        assert np.array_equal(bits(outs[0][2][k]), bits(ov))
+
+
+def test_fast_form_within_tolerance():
+    desc, t = W.single_patch_256()
+    for d0 in (desc, W.foam_patch_512()):
+        b = ob.OceanBatch([d0], form=abi.OCEAN_FFT_FAST)
+        cells = d0.size ** 2
+        disp = np.empty((cells, 4), np.float32)
+        nrm = np.empty_like(disp)
+        vel = np.empty_like(disp) if d0.compute_velocity else None
+        b.update_host([t], 0.0, disp, nrm, vel)
+        od, on, ov = O.update(d0, t)
+        pairs = [(disp, od), (nrm, on)] + ([(vel, ov)] if vel is not None else [])
+        for got, ref in pairs:
+            for ch in range(4):
+                rms = float(np.sqrt(np.mean(ref[:, ch].astype(np.float64) ** 2)))
+                if rms == 0.0:
+                    assert np.all(got[:, ch] == 0)
+                    continue
+                err = float(np.abs(got[:, ch].astype(np.float64) - ref[:, ch]).max())
+                assert err <= FAST_TOL * rms, (d0.size, ch, err / rms)
+        b.close()
+
+
+def test_queries_bit_exact_against_reference():
+    g = np.load(GOLDEN / "ref_queries.npz")
+    desc, t, count = QUERY_CASE
+    oc = ob.Ocean(desc)
+    oc.update(t)
+    res = oc.sample_many(g["xz"])
+    assert np.array_equal(bits(res), bits(g["out"]))
+    # the single-point reference entry points give the same bits
+    for i in (0, 17, count - 1, count - 3):
+        x, z = map(float, g["xz"][i])
+        s = oc.sample_at(x, z)
+        assert np.float32(s["height"]).view(np.uint32) == g["out"][i, 0].view(np.uint32)
+        assert np.float32(oc.height_at(x, z)) == g["out"][i, 0]
+    oc.close()
+
+
+def test_persistent_foam_bit_exact_against_reference_foamfield():
+    golden = json.loads((GOLDEN / "ref_hashes.json").read_text())["foam"]
+    desc, foam, frames, dt = FOAM_CASE
+    cells = desc.size * desc.size
+    batch = ob.OceanBatch([desc], foam=foam)
+    disp = np.empty((cells, 4), np.float32)
+    nrm = np.empty_like(disp)
+    vel = np.empty_like(disp)
+    fo = np.empty(cells, np.float32)
+    for k in range(frames):
+        batch.update_host([(k + 1) * dt], dt, disp, nrm, vel, fo)
+        assert batch.last_foam_substeps == 1
+        assert sha(fo) == golden["hashes"][k], f"frame {k}"
+    assert abs(float(fo.mean()) - golden["coverage_last"]) < 1e-12
+    batch.close()
+
+
+def test_foam_substep_clamp_and_zero_steps():
+    desc = ob.OceanDesc(size=64, patch_length=60.0, wind_speed=20.0, choppiness=1.8,
+                        compute_velocity=True, seed=4)
+    foam = ob.FoamDesc(max_substeps=2)
+    batch = ob.OceanBatch([desc], foam=foam)
+    batch.update([0.1], foam_dt=0.0)
+    assert batch.last_foam_substeps == 0
+    batch.update([0.2], foam_dt=1.0)  # backlog of 60 steps, clamped to 2
+    assert batch.last_foam_substeps == 2
+    batch.update([0.3], foam_dt=1.0 / 120.0)  # half a step: none run
+    assert batch.last_foam_substeps == 0
+    batch.close()
+
+
+def test_parallel_for_hook_called_four_times_per_frame():
+    # tests/test_c_api.cpp:370-392
+    calls = []
+
+    @abi.PARALLEL_FOR_FN
+    def hook(user, task, ctx, count):
+        calls.append(count)
+        for i in range(count):
+            task(ctx, i)
+
+    desc = ob.OceanDesc(size=64, seed=9)
+    cd = desc.to_c()
+    cd.parallel_for = C.cast(hook, C.c_void_p)
+    oc = ob.Ocean(cd)
+    assert len(calls) == 4
+    oc.update(1.0)
+    assert len(calls) == 8
+    d, n, _ = frame(oc)
+    od, on, _ = O.update(desc, 1.0)
+    assert np.array_equal(bits(d), bits(od)) and np.array_equal(bits(n), bits(on))
+    oc.close()
+
+
+def test_seek_back_and_instances_are_identical():
+    # tests/test_simulation.cpp:42-81
+    desc, _ = W.single_patch_256()
+    a, b = ob.Ocean(desc), ob.Ocean(desc)
+    for t in (0.0, 1.5, 97.25, 3600.0):
+        a.update(t)
+        b.update(t)
+        assert np.array_equal(bits(frame(a)[0]), bits(frame(b)[0]))
+    a.update(97.25)
+    first = frame(a)[0]
+    a.update(5.0)
+    a.update(97.25)
+    assert np.array_equal(bits(first), bits(frame(a)[0]))
+    assert a.time == 97.25
+    a.close()
+    b.close()
+
+
+def test_forced_scalar_level_matches_native():
+    # tests/test_c_api.cpp:435-461
+    desc = ob.OceanDesc(size=32, seed=555)
+    ob.force_simd_level("scalar")
+    s = ob.Ocean(desc)
+    s.update(4.0)
+    ob.force_simd_level(None)
+    nat = ob.Ocean(desc)
+    nat.update(4.0)
+    assert np.array_equal(bits(frame(s)[0]), bits(frame(nat)[0]))
+    assert np.array_equal(bits(frame(s)[1]), bits(frame(nat)[1]))

@@ -1,0 +1,183 @@
+"""Pins the CPU oracle (oracle/ocean_oracle.c) before anything trusts it.
+
+* against the reference's own known answers (the PCG32 KAT of
+  tests/test_rng.cpp:17-20 and the FFT-vs-DFT bound of tests/test_fft.cpp:166);
+* against golden fixtures produced by the reference itself
+  (tests/golden/make_golden.py, compiled from the reference's sources);
+* live against the reference library when it is built here.
+"""
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+from oceanlib_b200 import workloads as W
+from tests.workloads import (FOAM_CASE, HASH_CASES, QUERY_CASE, SMALL_CASES, desc_from_json,
+                             query_points)
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def test_pcg32_known_answers():
+    # seed 42, stream 54: the canonical pcg32 demo outputs (tests/test_rng.cpp:17-20)
+    want = [0xA15C02B7, 0x7B47F409, 0xBA1D3330, 0x83D2F293,
+            0xBFA4784B, 0xCBED606E, 0xBFC6A3AD, 0x812FFF6D]
+    assert O.pcg32(42, 54, 8).tolist() == want
+    r = W.Pcg32(42, 54)
+    assert [r.next_u32() for _ in range(8)] == want
+    # the vectorised generator continues the same stream
+    r1, r2 = W.Pcg32(3, 0), W.Pcg32(3, 0)
+    scalar = [r1.next_u32() for _ in range(10000)]
+    assert r2.many_u32(10000).tolist() == scalar
+    assert r1.next_u32() == r2.next_u32()
+
+
+def test_oracle_matches_reference_small_grids():
+    g = np.load(GOLDEN / "ref_small.npz")
+    meta = json.loads(bytes(g["meta"]).decode())
+    for i, m in enumerate(meta):
+        desc = desc_from_json(m["desc"])
+        tables = O.spectrum(desc)
+        assert np.array_equal(bits(tables), bits(g[f"c{i}_tables"])), f"tables case {i}"
+        for j, t in enumerate(m["times"]):
+            d, n, v = O.update(desc, t, tables)
+            assert np.array_equal(bits(d), bits(g[f"c{i}_t{j}_disp"])), (i, t)
+            assert np.array_equal(bits(n), bits(g[f"c{i}_t{j}_normal"])), (i, t)
+            if v is not None:
+                assert np.array_equal(bits(v), bits(g[f"c{i}_t{j}_vel"])), (i, t)
+
+
+def test_choppiness_zero_gives_unit_jacobian():
+    # tests/test_simulation.cpp:275-296: lambda = 0 => J == 1 exactly.
+    desc, times = SMALL_CASES[2]
+    _, n, _ = O.update(desc, times[0])
+    assert np.all(n[:, 3] == 1.0)
+
+
+def test_oracle_matches_reference_hashes_full_size():
+    golden = json.loads((GOLDEN / "ref_hashes.json").read_text())
+    for case in golden["cases"]:
+        desc = desc_from_json(case["desc"])
+        tables = O.spectrum(desc)
+        assert sha(np.stack([tables[0], tables[1]], axis=1)) == case["h0"], desc
+        for fr in case["frames"]:
+            d, n, v = O.update(desc, fr["t"], tables)
+            assert sha(d) == fr["disp"], (desc.size, fr["t"])
+            assert sha(n) == fr["normal"], (desc.size, fr["t"])
+            if v is not None:
+                assert sha(v) == fr["vel"], (desc.size, fr["t"])
+
+
+class FoamAccumulator:
+    """FoamField::update's fixed-step accumulator (src/foam.cpp:218-252)."""
+
+    def __init__(self, fixed_dt, max_substeps):
+        self.step = float(np.float32(fixed_dt))
+        self.max = max_substeps
+        self.accum = 0.0
+
+    def steps(self, dt):
+        dt = float(np.float32(dt)) if dt > 0 else 0.0
+        self.accum += dt
+        eps = self.step * 1e-6
+        s = int((self.accum + eps) / self.step) if self.accum + eps >= self.step else 0
+        if s > self.max:
+            s, self.accum = self.max, 0.0
+        else:
+            self.accum = max(0.0, self.accum - s * self.step)
+        return s
+
+
+def run_oracle_foam(desc, foam, frames, dt):
+    n = desc.size
+    tables = O.spectrum(desc)
+    cur = np.zeros(n * n, np.float32)
+    acc = FoamAccumulator(foam.fixed_dt, foam.max_substeps)
+    fdt = np.float32(foam.fixed_dt)
+    decay = np.exp(np.float32(-np.float32(foam.decay) * fdt), dtype=np.float32)
+    gain = np.float32(np.float32(foam.source_gain) * fdt)
+    cell = np.float32(np.float32(desc.patch_length) / np.float32(n))
+    out = []
+    for k in range(frames):
+        d, _, v = O.update(desc, (k + 1) * dt, tables)
+        for _ in range(acc.steps(dt)):
+            cur = O.foam_step(n, cell, fdt, decay, gain, foam.advect_scale, foam.wind_drift_x,
+                              foam.wind_drift_z, d, v, cur)
+        out.append(cur)
+    return out
+
+
+def test_oracle_foam_matches_reference():
+    golden = json.loads((GOLDEN / "ref_hashes.json").read_text())["foam"]
+    desc, foam, frames, dt = FOAM_CASE
+    # 24 frames keep the CPU suite fast; the GPU test checks all of them.
+    got = run_oracle_foam(desc, foam, 24, dt)
+    for k in range(24):
+        assert sha(got[k]) == golden["hashes"][k], k
+
+
+def test_oracle_queries_match_reference():
+    g = np.load(GOLDEN / "ref_queries.npz")
+    desc, t, count = QUERY_CASE
+    d, n, v = O.update(desc, t)
+    assert np.array_equal(g["xz"], query_points(desc, count))
+    res = O.sample_many(desc.size, desc.patch_length, d, n, v, g["xz"])
+    assert np.array_equal(bits(res), bits(g["out"]))
+
+
+def test_fft_matches_fp64_direct_dft():
+    # tests/test_fft.cpp:138-169: 2-D transform vs the O(N^4) direct sum < 1e-6
+    # relative to the peak.
+    rng = np.random.default_rng(5)
+    n = 32
+    re = rng.standard_normal(n * n).astype(np.float32)
+    im = rng.standard_normal(n * n).astype(np.float32)
+    fr, fi = O.fft_2d(re, im, +1)
+    xs = np.tile(np.arange(n), n)
+    ys = np.repeat(np.arange(n), n)
+    dr, di = O.dft_points(re, im, xs, ys)
+    err = np.sqrt((fr - dr) ** 2 + (fi - di) ** 2).max()
+    scale = np.sqrt(dr ** 2 + di ** 2).max()
+    assert err / scale < 1e-6
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+def test_oracle_matches_live_reference_random_descriptors():
+    rng = np.random.default_rng(77)
+    from oceanlib_b200 import OceanDesc
+
+    for k in range(6):
+        desc = OceanDesc(size=int(rng.choice([16, 32, 64, 128])),
+                         patch_length=float(rng.uniform(20, 900)),
+                         wind_speed=float(rng.uniform(0, 30)),
+                         fetch=float(rng.uniform(1e3, 5e5)),
+                         wind_direction=float(rng.uniform(-7, 7)),
+                         peak_enhancement=float(rng.uniform(1, 7)),
+                         swell=float(rng.uniform(0, 1)),
+                         depth=float(rng.choice([0.0, 5.0, 40.0])),
+                         choppiness=float(rng.uniform(0, 2)),
+                         seed=int(rng.integers(0, 2 ** 63)),
+                         compute_velocity=bool(k % 2))
+        t = float(rng.uniform(0, 1e4))
+        ro = O.RefOcean(desc)
+        ro.update(t)
+        rd, rn, rv = ro.buffers()
+        d, n, v = O.update(desc, t)
+        assert np.array_equal(bits(d), bits(rd))
+        assert np.array_equal(bits(n), bits(rn))
+        if v is not None:
+            assert np.array_equal(bits(v), bits(rv))
+        xz = rng.uniform(-2 * desc.patch_length, 2 * desc.patch_length, (256, 2)).astype(np.float32)
+        assert np.array_equal(bits(ro.sample_many(xz)),
+                              bits(O.sample_many(desc.size, desc.patch_length, d, n, v, xz)))

@@ -1,0 +1,62 @@
+"""Test cases shared by the golden-fixture generator and the tests."""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from oceanlib_b200 import OceanDesc, FoamDesc
+from oceanlib_b200 import workloads as W
+
+
+def desc_to_json(d: OceanDesc) -> dict:
+    return dataclasses.asdict(d)
+
+
+def desc_from_json(j: dict) -> OceanDesc:
+    return OceanDesc(**j)
+
+
+# Small grids: full arrays are stored. Covers every size class of the kernels'
+# shape table below 128, velocity, finite depth, swell, choppiness 0 (J == 1
+# exactly), a degenerate foam threshold and a large absolute time.
+SMALL_CASES = [
+    (OceanDesc(size=16, patch_length=50.0, wind_speed=8.0, seed=3), (0.0, 1.5, 97.25)),
+    (OceanDesc(size=32, patch_length=100.0, wind_speed=12.0, wind_direction=0.4, seed=555,
+               compute_velocity=True), (0.0, 4.0, 3600.0)),
+    (OceanDesc(size=64, patch_length=200.0, wind_speed=12.0, depth=30.0, swell=0.6,
+               choppiness=0.0, seed=11), (10.0,)),
+    (OceanDesc(size=64, patch_length=80.0, wind_speed=20.0, choppiness=1.8, foam_threshold=0.0,
+               seed=99, compute_velocity=True), (1e5,)),
+]
+
+# Full sizes: only sha256 of the reference's bytes is stored.
+_s256, _t256 = W.single_patch_256()
+HASH_CASES = [
+    (_s256, (_t256, 0.0, 3600.0)),
+    (W.bench_update_patch(512), (100.0, 100.0137, 1e4)),
+    (W.foam_patch_512(), (0.0, 1.0 / 60.0, 1e3, 1e4, 1e5)),
+    (OceanDesc(size=128, patch_length=150.0, wind_speed=15.0, depth=30.0, seed=2,
+               compute_velocity=True), (5.0,)),
+    (OceanDesc(size=1024, patch_length=1000.0, wind_speed=25.0, wind_direction=2.0, choppiness=1.2,
+               seed=5), (42.0,)),
+]
+
+# Persistent foam on the foam patch: 120 frames at 60 Hz.
+FOAM_CASE = (W.foam_patch_512(), W.foam_desc(), 120, 1.0 / 60.0)
+
+# World queries on the single 256 patch at t = 10.
+QUERY_CASE = (_s256, _t256, 4096)
+
+
+def query_points(desc: OceanDesc, count: int) -> np.ndarray:
+    """Seeded points over three tiles (negative coordinates included) plus
+    edge cases: cell corners, the tile seam, far-away points."""
+    rng = np.random.default_rng(1234)
+    L = desc.patch_length
+    pts = rng.uniform(-1.5 * L, 1.5 * L, size=(count - 8, 2)).astype(np.float32)
+    cell = L / desc.size
+    edge = np.array([[0, 0], [L, L], [-L, 0], [cell, 2 * cell], [L - 1e-3, 0.5],
+                     [1e4 * L, -1e4 * L], [-0.0, 0.0], [3 * cell, -5 * cell]], dtype=np.float32)
+    return np.concatenate([pts, edge]).astype(np.float32)
