@@ -143,15 +143,21 @@ def test_fast_form_within_tolerance():
         vel = np.empty_like(disp) if d0.compute_velocity else None
         b.update_host([t], 0.0, disp, nrm, vel)
         od, on, ov = O.update(d0, t)
-        pairs = [(disp, od), (nrm, on)] + ([(vel, ov)] if vel is not None else [])
-        for got, ref in pairs:
+        pairs = [("disp", disp, od), ("normal", nrm, on)] + \
+            ([("vel", vel, ov)] if vel is not None else [])
+        for name, got, ref in pairs:
             for ch in range(4):
+                err = float(np.abs(got[:, ch].astype(np.float64) - ref[:, ch]).max())
+                if name == "disp" and ch == 3:
+                    # foam: a clamped ramp in [0, 1], mostly exactly 0, so its
+                    # RMS says nothing about scale; held to 1e-5 absolute.
+                    assert err <= FAST_TOL, (d0.size, name, ch, err)
+                    continue
                 rms = float(np.sqrt(np.mean(ref[:, ch].astype(np.float64) ** 2)))
                 if rms == 0.0:
                     assert np.all(got[:, ch] == 0)
                     continue
-                err = float(np.abs(got[:, ch].astype(np.float64) - ref[:, ch]).max())
-                assert err <= FAST_TOL * rms, (d0.size, ch, err / rms)
+                assert err <= FAST_TOL * rms, (d0.size, name, ch, err / rms)
         b.close()
 
 
