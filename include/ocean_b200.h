@@ -300,6 +300,28 @@ OCEAN_API ocean_status ocean_batch_read_profile(ocean_batch* batch, ocean_pass_p
 /* Kernels this batch has launched (all kinds) since it was created. */
 OCEAN_API uint64_t ocean_batch_launch_count(const ocean_batch* batch);
 
+/* One frame of one ocean (exact form) that allocates no device memory. No
+ * counterpart in the reference, which never touches a GPU: this is for
+ * callers that are not allowed to call cudaMalloc - an engine or renderer
+ * whose GPU memory is owned by its own allocator and budget, or a real-time
+ * thread that cannot take cudaMalloc's implicit synchronisation. The caller
+ * passes every input and output as its own device buffer (16-byte aligned):
+ *   h0          N*N float2 (re, im)      \  as ocean_batch_read_spectrum
+ *   omega_kinv  N*N float2 (omega, 1/|k|) /  returns them
+ *   displacement, normal (and velocity, or NULL)  N*N float4 each.
+ * The row-pass intermediate lives in a fixed device array inside this
+ * library (about 12 MiB, held on every GPU that loads it until exit), so N
+ * is limited to 16..512; larger N returns OCEAN_ERROR_INVALID_ARG. All calls
+ * on a device share that array: calls whose GPU work overlaps (e.g. on two
+ * streams) race and corrupt each other. The first call on a device looks up
+ * the array's device address, so make it before any stream capture. Work is
+ * queued on `stream` (a cudaStream_t, NULL = legacy default stream). */
+OCEAN_API ocean_status ocean_frame_static_scratch(uint32_t size, float patch_length, double time,
+                                                  float choppiness, float foam_threshold,
+                                                  const float* h0, const float* omega_kinv,
+                                                  float* displacement, float* normal,
+                                                  float* velocity, void* stream);
+
 /* Name of the device the library was built for ("sm_100a"). */
 OCEAN_API const char* ocean_device_arch(void);
 

@@ -153,5 +153,8 @@ SIGNATURES = {
     "ocean_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "ocean_batch_read_profile": (C.c_int, [C.c_void_p, C.POINTER(PassProfile)]),
     "ocean_batch_launch_count": (C.c_uint64, [C.c_void_p]),
+    "ocean_frame_static_scratch": (C.c_int, [C.c_uint32, C.c_float, C.c_double, C.c_float,
+                                             C.c_float, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]),
     "ocean_device_arch": (C.c_char_p, []),
 }
