@@ -67,7 +67,7 @@ typedef struct ocean_spectrum_desc {
     float gravity;
 } ocean_spectrum_desc;
 
-/* include/ocean/ocean.h:85-134. 88 bytes on LP64; struct_size prefix
+/* include/ocean/ocean.h:85-134. 96 bytes on LP64; struct_size prefix
  * versioning: a smaller struct_size takes defaults for the missing tail, zero
  * or a larger one is OCEAN_ERROR_INVALID_ARG. thread_count is accepted and
  * ignored (the GPU does the work). */
@@ -127,9 +127,9 @@ OCEAN_API ocean_buffers ocean_get_buffers(const ocean_sim* sim);
 /* include/ocean/ocean.h:197 */
 OCEAN_API double ocean_get_time(const ocean_sim* sim);
 
-/* include/ocean/ocean.h:205. Runs the reference's 4-step fixed-point
- * inversion on the host mirror (one query is latency-bound; use
- * ocean_sample_many for many). */
+/* include/ocean/ocean.h:205. The reference's 4-step fixed-point inversion,
+ * run by the GPU query kernel on the device outputs (one query is a launch
+ * plus a copy; use ocean_sample_many for many). */
 OCEAN_API float ocean_height_at(const ocean_sim* sim, float world_x, float world_z);
 
 /* include/ocean/ocean.h:215 (frozen: returned by value). */
@@ -156,8 +156,8 @@ OCEAN_API void ocean_sample_ex(const ocean_sim* sim, float world_x, float world_
 /* include/ocean/ocean.h:240 */
 OCEAN_API const float* ocean_get_velocity(const ocean_sim* sim);
 
-/* include/ocean/ocean.h:249. Reports "CUDA sm_100a (exact)" or
- * "CUDA sm_100a (fast)". */
+/* include/ocean/ocean.h:249. Reports "sm_100a" by default, or the level name
+ * last forced with ocean_force_simd_level. */
 OCEAN_API const char* ocean_simd_level(void);
 
 /* include/ocean/ocean.h:262. "scalar" (and "sse2", "avx2", "neon", "exact")
@@ -230,6 +230,13 @@ OCEAN_API void ocean_foam_desc_init(ocean_foam_desc* desc);
 
 typedef struct ocean_batch ocean_batch;
 
+/* How a batch frame is scheduled on the device. */
+typedef enum ocean_schedule {
+    OCEAN_SCHEDULE_PERSISTENT = 0, /* one persistent launch per frame: CTAs pull
+                                      row and column tasks from an ordered queue */
+    OCEAN_SCHEDULE_CHUNKED    = 1  /* a row launch and a column launch per chunk */
+} ocean_schedule;
+
 typedef struct ocean_batch_desc {
     size_t            struct_size;
     const ocean_desc* oceans;          /* `count` descriptors, all the same size N */
@@ -240,6 +247,7 @@ typedef struct ocean_batch_desc {
     ocean_foam_desc   foam;
     uint32_t          chunk;           /* oceans per row/column pass pair; 0 = auto
                                           (sized so the intermediate stays in L2) */
+    int32_t           schedule;        /* ocean_schedule                            */
 } ocean_batch_desc;
 
 OCEAN_API void ocean_batch_desc_init(ocean_batch_desc* desc);
@@ -270,7 +278,9 @@ OCEAN_API ocean_status ocean_batch_get_device_buffers(const ocean_batch* batch, 
 /* Number of foam substeps the last update ran (0..max_substeps). */
 OCEAN_API uint32_t ocean_batch_last_foam_substeps(const ocean_batch* batch);
 
-/* Waits for all work queued on the batch's own stream. */
+/* Waits for all work queued on the batch's own stream. Returns
+ * OCEAN_ERROR_TIMEOUT (once) if a bounded device wait of the persistent
+ * frame kernel gave up since the last check. */
 OCEAN_API ocean_status ocean_batch_synchronize(ocean_batch* batch);
 
 /* Device spectrum tables of ocean `index`, written to HOST memory as
@@ -288,6 +298,8 @@ typedef struct ocean_pass_profile {
     double   row_ms;   /* summed launch durations */
     double   col_ms;
     double   foam_ms;
+    uint64_t frame_launches; /* persistent frame kernel */
+    double   frame_ms;
 } ocean_pass_profile;
 
 /* Turn per-launch event timing on or off (allocates its event pool when
@@ -321,6 +333,12 @@ OCEAN_API ocean_status ocean_frame_static_scratch(uint32_t size, float patch_len
                                                   const float* h0, const float* omega_kinv,
                                                   float* displacement, float* normal,
                                                   float* velocity, void* stream);
+
+/* Runs the persistent kernel's bounded wait on a counter that nothing
+ * increments, with the given limit, and reports OCEAN_ERROR_TIMEOUT when the
+ * wait gave up and returned (the expected outcome) - a self-test of the
+ * timeout path that leaves the device usable. */
+OCEAN_API ocean_status ocean_check_bounded_wait(uint32_t timeout_ms);
 
 /* Name of the device the library was built for ("sm_100a"). */
 OCEAN_API const char* ocean_device_arch(void);

@@ -233,7 +233,8 @@ class OceanBatch:
     per chunk of oceans)."""
 
     def __init__(self, descs: Sequence[OceanDesc], *, form: int = abi.OCEAN_FFT_EXACT,
-                 foam: Optional[FoamDesc] = None, chunk: int = 0):
+                 foam: Optional[FoamDesc] = None, chunk: int = 0,
+                 schedule: int = abi.OCEAN_SCHEDULE_PERSISTENT):
         arr = (OceanDescC * len(descs))(*[d.to_c() for d in descs])
         bd = BatchDescC()
         lib().ocean_batch_desc_init(C.byref(bd))
@@ -244,6 +245,7 @@ class OceanBatch:
         if foam is not None:
             bd.foam = foam.to_c()
         bd.chunk = chunk
+        bd.schedule = schedule
         st = C.c_int(-1)
         h = lib().ocean_batch_create(C.byref(bd), C.byref(st))
         if not h:

@@ -14,6 +14,9 @@ OCEAN_ERROR_TIMEOUT = 5
 OCEAN_FFT_EXACT = 0
 OCEAN_FFT_FAST = 1
 
+OCEAN_SCHEDULE_PERSISTENT = 0
+OCEAN_SCHEDULE_CHUNKED = 1
+
 TASK_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_uint32)
 PARALLEL_FOR_FN = C.CFUNCTYPE(None, C.c_void_p, TASK_FN, C.c_void_p, C.c_uint32)
 
@@ -104,6 +107,7 @@ class BatchDescC(C.Structure):
         ("persistent_foam", C.c_int32),
         ("foam", FoamDescC),
         ("chunk", C.c_uint32),
+        ("schedule", C.c_int32),
     ]
 
 
@@ -115,6 +119,8 @@ class PassProfile(C.Structure):
         ("row_ms", C.c_double),
         ("col_ms", C.c_double),
         ("foam_ms", C.c_double),
+        ("frame_launches", C.c_uint64),
+        ("frame_ms", C.c_double),
     ]
 
 
@@ -156,5 +162,6 @@ SIGNATURES = {
     "ocean_frame_static_scratch": (C.c_int, [C.c_uint32, C.c_float, C.c_double, C.c_float,
                                              C.c_float, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ocean_check_bounded_wait": (C.c_int, [C.c_uint32]),
     "ocean_device_arch": (C.c_char_p, []),
 }

@@ -33,52 +33,52 @@ struct Shape {
     static constexpr int G = lanes_for(LOG_N);                       // lanes / sequence
     static constexpr int SEQ = N + kPad;                             // sequence stride
     static constexpr int RP = cmin(N / 2, 32 / G > 1 ? 32 / G : 1); // row pairs / CTA
-    // columns / CTA: 4 at N = 512 (128-byte rows of the intermediate); 2 at
-    // N = 1024, where 32 values per lane leave room for fewer threads only.
+    // columns / CTA of the per-chunk column kernel: 4 at N = 512 (128-byte
+    // rows of the intermediate); 2 at N = 1024, where 32 values per lane
+    // leave room for fewer threads only.
     static constexpr int W = LOG_N >= 10 ? 2 : cmin(N, (128 / G) > 4 ? 128 / G : 4);
+    // columns / task of the persistent kernel: 2*RP, so a row task and a
+    // column task use the same thread count (2 * NF * G * RP).
+    static constexpr int PW = 2 * RP;
 };
 
 // ---------------------------------------------------------------------------
-// Row pass
+// Row task: RP row pairs of one ocean (evolve + row FFTs), written to the
+// intermediate slot `inter_slot` (N*N*NF float2). `tws` already holds the
+// twiddles in shared memory.
 // ---------------------------------------------------------------------------
 template <int LOG_N, int NF, bool FAST>
-__global__ void __launch_bounds__(Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G)
-row_pass_kernel(FrameArgs a)
+__device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int group,
+                                         float2* __restrict__ inter_slot, float2* smem,
+                                         const float2* tws, int tid)
 {
     using S = Shape<LOG_N>;
     constexpr int N = S::N, G = S::G, SEQ = S::SEQ, RP = S::RP;
     constexpr int NT = RP * 2 * NF * G;
 
-    extern __shared__ float4 smem4[];
-    float2* data = reinterpret_cast<float2*>(smem4);  // [RP*2*NF][SEQ]
-    float2* h0s = data + RP * 2 * NF * SEQ;           // [RP*2][N]
-    float2* tws = h0s + RP * 2 * N;                   // [N-1]
+    float2* data = smem;                      // [RP*2*NF][SEQ]
+    float2* h0s = data + RP * 2 * NF * SEQ;   // [RP*2][N]
 
-    const int tid = threadIdx.x;
-    const int o = blockIdx.y;
-    const int ocean = a.ocean_base + o;
     const OceanConsts cst = a.consts[ocean];
     const double top = a.t_over_2pi[ocean];
     const float2* geom = a.omega_kinv + static_cast<size_t>(cst.geom) * N * N;
     const float* kvec = a.kvec + static_cast<size_t>(cst.geom) * N;
     const float2* h0 = a.h0 + static_cast<size_t>(ocean) * N * N;
 
-    // Rows handled by pair slot j of this CTA: (p, N-p), or (0, N/2) for p = 0.
+    // Rows handled by pair slot j: (p, N-p), or (0, N/2) for p = 0.
     auto row_of = [&](int j, int r) -> int {
-        const int p = blockIdx.x * RP + j;
+        const int p = group * RP + j;
         if (p == 0) return r ? N / 2 : 0;
         return r ? N - p : p;
     };
 
-    // Stage the 2*RP h0 rows and the twiddles.
     for (int i = tid; i < RP * 2 * (N / 2); i += NT) {
         const int jr = i / (N / 2);
         const int c = i % (N / 2);
         const int row = row_of(jr >> 1, jr & 1);
         reinterpret_cast<float4*>(h0s + jr * N)[c] =
-            reinterpret_cast<const float4*>(h0 + static_cast<size_t>(row) * N)[c];
+            __ldcs(reinterpret_cast<const float4*>(h0 + static_cast<size_t>(row) * N) + c);
     }
-    for (int i = tid; i < N - 1; i += NT) tws[i] = a.twiddles[i];
     __syncthreads();
 
     // Evolve (src/core/evolve.cpp:28-121 and :123-184), one cell at a time.
@@ -86,7 +86,7 @@ row_pass_kernel(FrameArgs a)
         const int jr = cell >> LOG_N;  // j*2 + r
         const int x = cell & (N - 1);
         const int j = jr >> 1, r = jr & 1;
-        const int p = blockIdx.x * RP + j;
+        const int p = group * RP + j;
         const int row = row_of(j, r);
         const int mr = (p == 0) ? r : 1 - r;  // row holding h0 at -kz
         const float2 av = h0s[jr * N + x];
@@ -138,9 +138,9 @@ row_pass_kernel(FrameArgs a)
     fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);
     __syncthreads();
 
-    // Write both rows cell-major: inter[o][row][x][f], NF/2 float4 per cell.
+    // Write the rows cell-major: inter[row][x][f], NF/2 float4 per cell.
     constexpr int Q = NF / 2;
-    float4* inter = reinterpret_cast<float4*>(a.inter + static_cast<size_t>(o) * N * N * NF);
+    float4* inter = reinterpret_cast<float4*>(inter_slot);
     for (int i = tid; i < RP * 2 * N * Q; i += NT) {
         const int jr = i / (N * Q);
         const int rem = i % (N * Q);
@@ -154,7 +154,7 @@ row_pass_kernel(FrameArgs a)
 }
 
 // ---------------------------------------------------------------------------
-// Column pass
+// Column task helpers
 // ---------------------------------------------------------------------------
 
 // Periodic bilinear fetch from one channel grid (src/foam.cpp:22-41).
@@ -193,36 +193,34 @@ __device__ __forceinline__ float foam_cell(const float* cur, int n, int x, int z
     return f;
 }
 
-template <int LOG_N, int NF, bool FAST, bool FOAM>
-__global__ void __launch_bounds__(NF * Shape<LOG_N>::W * Shape<LOG_N>::G)
-col_pass_kernel(FrameArgs a)
+// ---------------------------------------------------------------------------
+// Column task: W columns of one ocean from intermediate slot `inter_slot`
+// (column FFTs + finalize + optional foam substep). CG loads read the
+// intermediate from L2: another CTA wrote it during this launch.
+// ---------------------------------------------------------------------------
+template <int LOG_N, int NF, bool FAST, bool FOAM, int W, bool CG>
+__device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int strip,
+                                         const float2* __restrict__ inter_slot, float2* smem,
+                                         const float2* tws, int tid)
 {
     using S = Shape<LOG_N>;
-    constexpr int N = S::N, G = S::G, SEQ = S::SEQ, W = S::W;
+    constexpr int N = S::N, G = S::G, SEQ = S::SEQ;
     constexpr int NT = NF * W * G;
     constexpr int Q = NF / 2;
+    float2* data = smem;  // [NF*W][SEQ], sequence = f*W + w
+    const int x0 = strip * W;
 
-    extern __shared__ float4 smem4[];
-    float2* data = reinterpret_cast<float2*>(smem4);  // [NF*W][SEQ], sequence = f*W + w
-    float2* tws = data + NF * W * SEQ;
-
-    const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * W;
-    const int o = blockIdx.y;
-    const int ocean = a.ocean_base + o;
-
-    const float4* inter =
-        reinterpret_cast<const float4*>(a.inter + static_cast<size_t>(o) * N * N * NF);
+    const float4* inter = reinterpret_cast<const float4*>(inter_slot);
     for (int i = tid; i < N * W * Q; i += NT) {
         const int y = i / (W * Q);
         const int rem = i % (W * Q);
         const int w = rem / Q;
         const int fp = rem % Q;
-        const float4 v = inter[(static_cast<size_t>(y) * N + x0 + w) * Q + fp];
+        const float4* src = inter + (static_cast<size_t>(y) * N + x0 + w) * Q + fp;
+        const float4 v = CG ? __ldcg(src) : *src;
         data[((2 * fp) * W + w) * SEQ + swz(y)] = make_float2(v.x, v.y);
         data[((2 * fp + 1) * W + w) * SEQ + swz(y)] = make_float2(v.z, v.w);
     }
-    for (int i = tid; i < N - 1; i += NT) tws[i] = a.twiddles[i];
     __syncthreads();
 
     fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);
@@ -270,12 +268,185 @@ col_pass_kernel(FrameArgs a)
             __stcs(&a.velocity[idx], make_float4(f4.x, f4.y, f5.x, 0.0f));
             if constexpr (FOAM) {
                 const float* cur = a.foam_cur + base;
-                a.foam_next[idx] = foam_cell(cur, N, x, y, f4.x, f5.x, foam, a.foam_dt,
-                                             a.foam_decay, a.foam_gain, a.foam_scale,
-                                             a.foam_drift_x, a.foam_drift_z, a.foam_inv_cell);
+                __stcs(&a.foam_next[idx],
+                       foam_cell(cur, N, x, y, f4.x, f5.x, foam, a.foam_dt, a.foam_decay,
+                                 a.foam_gain, a.foam_scale, a.foam_drift_x, a.foam_drift_z,
+                                 a.foam_inv_cell));
             }
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Per-chunk kernels: grid (groups, oceans in the chunk); ocean o of the chunk
+// uses intermediate slot o.
+// ---------------------------------------------------------------------------
+template <int LOG_N, int NF, bool FAST>
+__global__ void __launch_bounds__(Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G)
+row_pass_kernel(FrameArgs a)
+{
+    using S = Shape<LOG_N>;
+    constexpr int NT = S::RP * 2 * NF * S::G;
+    extern __shared__ float4 smem4[];
+    float2* smem = reinterpret_cast<float2*>(smem4);
+    float2* tws = smem + S::RP * 2 * NF * S::SEQ + S::RP * 2 * S::N;
+    for (int i = threadIdx.x; i < S::N - 1; i += NT) tws[i] = a.twiddles[i];
+    const int o = blockIdx.y;
+    row_task<LOG_N, NF, FAST>(a, a.ocean_base + o, blockIdx.x,
+                              a.inter + static_cast<size_t>(o) * S::N * S::N * NF, smem, tws,
+                              threadIdx.x);
+}
+
+template <int LOG_N, int NF, bool FAST, bool FOAM>
+__global__ void __launch_bounds__(NF * Shape<LOG_N>::W * Shape<LOG_N>::G)
+col_pass_kernel(FrameArgs a)
+{
+    using S = Shape<LOG_N>;
+    constexpr int NT = NF * S::W * S::G;
+    extern __shared__ float4 smem4[];
+    float2* smem = reinterpret_cast<float2*>(smem4);
+    float2* tws = smem + NF * S::W * S::SEQ;
+    for (int i = threadIdx.x; i < S::N - 1; i += NT) tws[i] = a.twiddles[i];
+    const int o = blockIdx.y;
+    col_task<LOG_N, NF, FAST, FOAM, S::W, false>(
+        a, a.ocean_base + o, blockIdx.x, a.inter + static_cast<size_t>(o) * S::N * S::N * NF,
+        smem, tws, threadIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent frame kernel: one launch per frame for every ocean of the batch.
+//
+// CTAs take tickets from an ordered queue R(0) | R(1) C(0) | R(2) C(1) | ...
+// | C(count-1), where R(b) are ocean b's row tasks and C(b) its column tasks.
+// C(b) waits until all of R(b) finished; R(b) writes intermediate slot
+// b % slots and first waits until C(b - slots) finished reading it. Every
+// awaited task holds an earlier ticket, so it is already running on some CTA
+// and never waits on a later one: the queue cannot deadlock, co-resident or
+// not. Waits are bounded (kWaitNs); a CTA that gives up sets the error word
+// and leaves, and the others give up in turn.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Spin until *counter >= target or the error word is set or kWaitNs passes.
+// Returns false on timeout / abort.
+__device__ bool wait_at_least(const unsigned* counter, unsigned target, unsigned* error,
+                              unsigned long long limit_ns)
+{
+    if (ld_acquire(counter) >= target) return true;
+    const unsigned long long t0 = global_ns();
+    while (true) {
+        __nanosleep(64);
+        if (ld_acquire(counter) >= target) return true;
+        if (ld_acquire(error) != 0u) return false;
+        if (global_ns() - t0 > limit_ns) {
+            atomicCAS(error, 0u, 1u);
+            return false;
+        }
+    }
+}
+
+// Resident CTAs the persistent kernel is compiled for: 768 threads per SM
+// (one CTA at N = 1024, whose 32 values per lane need the registers).
+template <int LOG_N, int NF>
+constexpr int frame_min_blocks()
+{
+    constexpr int nt = Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G;
+    return LOG_N >= 10 ? 1 : (768 / nt < 1 ? 1 : (768 / nt > 16 ? 16 : 768 / nt));
+}
+
+template <int LOG_N, int NF, bool FAST, bool FOAM>
+__global__ void __launch_bounds__(Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G,
+                                  frame_min_blocks<LOG_N, NF>())
+frame_kernel(FrameArgs a, QueueArgs q)
+{
+    using S = Shape<LOG_N>;
+    constexpr int N = S::N;
+    constexpr int NT = S::RP * 2 * NF * S::G;
+    constexpr int RT = (N / 2) / S::RP;  // row tasks per ocean
+    constexpr int CT = N / S::PW;        // column tasks per ocean
+    constexpr size_t kDataFloat2 =
+        (S::RP * 2 * NF * S::SEQ + S::RP * 2 * N) > (NF * S::PW * S::SEQ)
+            ? (S::RP * 2 * NF * S::SEQ + S::RP * 2 * N)
+            : (NF * S::PW * S::SEQ);
+    extern __shared__ float4 smem4[];
+    float2* smem = reinterpret_cast<float2*>(smem4);
+    float2* tws = smem + kDataFloat2;
+    __shared__ unsigned s_ticket;
+    __shared__ int s_ok;
+
+    const int tid = threadIdx.x;
+    for (int i = tid; i < N - 1; i += NT) tws[i] = a.twiddles[i];
+
+    const unsigned count = static_cast<unsigned>(q.count);
+    const unsigned total = count * (RT + CT);
+    const size_t slot_f2 = static_cast<size_t>(N) * N * NF;
+    while (true) {
+        __syncthreads();  // previous task done with smem and s_ticket
+        if (tid == 0) s_ticket = atomicAdd(q.ticket, 1u);
+        __syncthreads();
+        const unsigned t = s_ticket;
+        if (t >= total) break;
+        bool row;
+        unsigned ocean, idx;
+        if (t < RT) {
+            row = true, ocean = 0, idx = t;
+        } else {
+            const unsigned u = t - RT, per = RT + CT, blk = u / per, off = u % per;
+            if (blk + 1 < count) {
+                row = off < RT;
+                ocean = row ? blk + 1 : blk;
+                idx = row ? off : off - RT;
+            } else {
+                row = false, ocean = count - 1, idx = off;
+            }
+        }
+        const unsigned slot = ocean % static_cast<unsigned>(q.slots);
+        if (tid == 0) {
+            bool ok = true;
+            if (row) {
+                if (ocean >= static_cast<unsigned>(q.slots))
+                    ok = wait_at_least(q.cols_done + (ocean - q.slots), CT, q.error, q.wait_ns);
+            } else {
+                ok = wait_at_least(q.rows_done + ocean, RT, q.error, q.wait_ns);
+            }
+            s_ok = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (!s_ok) break;
+        const int abs_ocean = a.ocean_base + static_cast<int>(ocean);
+        if (row) {
+            row_task<LOG_N, NF, FAST>(a, abs_ocean, static_cast<int>(idx),
+                                      a.inter + slot * slot_f2, smem, tws, tid);
+        } else {
+            col_task<LOG_N, NF, FAST, FOAM, S::PW, true>(a, abs_ocean, static_cast<int>(idx),
+                                                         a.inter + slot * slot_f2, smem, tws, tid);
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) atomicAdd(row ? q.rows_done + ocean : q.cols_done + ocean, 1u);
+    }
+}
+
+// A single bounded wait on a counter that nothing increments: exercises the
+// timeout path of wait_at_least on its own.
+__global__ void wait_probe_kernel(const unsigned* counter, unsigned target, unsigned* error,
+                                  unsigned long long limit_ns)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) wait_at_least(counter, target, error, limit_ns);
 }
 
 __global__ void foam_step_kernel(int n, int count, const float4* __restrict__ disp,
@@ -442,6 +613,72 @@ cudaError_t col_launch(const FrameArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
+template <int LOG_N, int NF>
+constexpr size_t frame_smem_bytes()
+{
+    using S = Shape<LOG_N>;
+    constexpr size_t row = S::RP * 2 * NF * S::SEQ + S::RP * 2 * S::N;
+    constexpr size_t col = NF * S::PW * S::SEQ;
+    return sizeof(float2) * ((row > col ? row : col) + (S::N - 1));
+}
+
+template <int LOG_N, int NF, bool FAST, bool FOAM>
+struct FrameLaunch {
+    static constexpr int threads() { return Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G; }
+
+    static cudaError_t prepare()
+    {
+        return cudaFuncSetAttribute(frame_kernel<LOG_N, NF, FAST, FOAM>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(frame_smem_bytes<LOG_N, NF>()));
+    }
+
+    static int blocks_per_sm()
+    {
+        if (prepare() != cudaSuccess) return 0;
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<LOG_N, NF, FAST, FOAM>,
+                                                          threads(),
+                                                          frame_smem_bytes<LOG_N, NF>()) !=
+            cudaSuccess)
+            return 0;
+        return n;
+    }
+
+    static cudaError_t launch(const FrameArgs& a, const QueueArgs& q, int grid, cudaStream_t st)
+    {
+        cudaError_t e = prepare();
+        if (e != cudaSuccess) return e;
+        frame_kernel<LOG_N, NF, FAST, FOAM>
+            <<<grid, threads(), frame_smem_bytes<LOG_N, NF>(), st>>>(a, q);
+        return cudaGetLastError();
+    }
+};
+
+template <int LOG_N, typename Fn>
+auto frame_variant(int nf, bool fast, bool foam, Fn&& fn)
+{
+    if (nf == 4) return fast ? fn(FrameLaunch<LOG_N, 4, true, false>{})
+                             : fn(FrameLaunch<LOG_N, 4, false, false>{});
+    if (foam) return fast ? fn(FrameLaunch<LOG_N, 6, true, true>{})
+                          : fn(FrameLaunch<LOG_N, 6, false, true>{});
+    return fast ? fn(FrameLaunch<LOG_N, 6, true, false>{}) : fn(FrameLaunch<LOG_N, 6, false, false>{});
+}
+
+template <typename Fn>
+auto frame_dispatch(int log_n, int nf, bool fast, bool foam, Fn&& fn)
+{
+    switch (log_n) {
+        case 4: return frame_variant<4>(nf, fast, foam, fn);
+        case 5: return frame_variant<5>(nf, fast, foam, fn);
+        case 6: return frame_variant<6>(nf, fast, foam, fn);
+        case 7: return frame_variant<7>(nf, fast, foam, fn);
+        case 8: return frame_variant<8>(nf, fast, foam, fn);
+        case 9: return frame_variant<9>(nf, fast, foam, fn);
+        default: return frame_variant<10>(nf, fast, foam, fn);
+    }
+}
+
 template <int LOG_N>
 cudaError_t row_dispatch_n(int nf, bool fast, const FrameArgs& a, cudaStream_t st)
 {
@@ -460,6 +697,27 @@ cudaError_t col_dispatch_n(int nf, bool fast, bool foam, const FrameArgs& a, cud
 }
 
 }  // namespace
+
+int frame_blocks_per_sm(int log_n, int nf, bool fast, bool fuse_foam)
+{
+    if (log_n < 4 || log_n > 10) return 0;
+    return frame_dispatch(log_n, nf, fast, fuse_foam, [](auto L) { return decltype(L)::blocks_per_sm(); });
+}
+
+cudaError_t launch_frame(int log_n, int nf, bool fast, bool fuse_foam, const FrameArgs& a,
+                         const QueueArgs& q, int grid, cudaStream_t st)
+{
+    if (log_n < 4 || log_n > 10) return cudaErrorInvalidValue;
+    return frame_dispatch(log_n, nf, fast, fuse_foam,
+                          [&](auto L) { return decltype(L)::launch(a, q, grid, st); });
+}
+
+cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned* error,
+                              unsigned long long limit_ns, cudaStream_t stream)
+{
+    wait_probe_kernel<<<1, 32, 0, stream>>>(counter, target, error, limit_ns);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_row_pass(int log_n, int nf, bool fast, const FrameArgs& a, cudaStream_t st)
 {

@@ -36,6 +36,11 @@ struct DeviceError : std::runtime_error {
     DeviceError(cudaError_t c, const char* what) : std::runtime_error(what), code(c) {}
 };
 
+// A bounded device wait gave up (the persistent kernel's error word was set).
+struct TimeoutError : std::runtime_error {
+    TimeoutError() : std::runtime_error("device wait timed out") {}
+};
+
 void check(cudaError_t e, const char* what)
 {
     if (e != cudaSuccess) throw DeviceError(e, what);
@@ -226,7 +231,8 @@ SpectrumParams spectrum_params(const ocean_desc& d)
 class Batch {
 public:
     Batch(const ocean_desc* descs, uint32_t count, int form, bool foam_on,
-          const ocean_foam_desc& foam, uint32_t chunk_hint)
+          const ocean_foam_desc& foam, uint32_t chunk_hint, bool persistent = true)
+        : persistent_(persistent)
     {
         if (descs == nullptr || count == 0) throw std::invalid_argument("no oceans");
         descs_.resize(count);
@@ -297,7 +303,11 @@ public:
         consts_ = DevBuf<OceanConsts>(count_);
         top_ = DevBuf<double>(count_ * kTimeSlots);
         top_host_ = HostBuf<double>(count_ * kTimeSlots);
-        inter_ = DevBuf<float2>(cells_ * nf_ * chunk_);
+        slots_ = static_cast<int>(std::min<uint32_t>(count_, 3));
+        inter_ = DevBuf<float2>(cells_ * nf_ * std::max<uint32_t>(chunk_, static_cast<uint32_t>(slots_)));
+        queue_ = DevBuf<unsigned>(1 + 2 * size_t(count_));
+        error_ = DevBuf<unsigned>(1);
+        check(cudaMemsetAsync(error_.p, 0, sizeof(unsigned), stream_), "memset");
         disp_ = DevBuf<float4>(cells_ * count_);
         normal_ = DevBuf<float4>(cells_ * count_);
         if (velocity_) velocity_buf_ = DevBuf<float4>(cells_ * count_);
@@ -388,11 +398,15 @@ public:
         const uint32_t steps = foam_on_ ? foam_accumulate(foam_dt) : 0u;
         FrameArgs a = frame_args(dev);
         if (steps > 0) set_foam_args(a);
-        for (uint32_t base = 0, c = 0; base < count_; base += chunk_, ++c) {
-            a.ocean_base = static_cast<int32_t>(base);
-            a.chunk = static_cast<int32_t>(std::min(chunk_, count_ - base));
-            run_row(a, st);
-            run_col(a, st, steps > 0);
+        if (persistent_) {
+            run_frame(a, 0, count_, steps > 0, st);
+        } else {
+            for (uint32_t base = 0; base < count_; base += chunk_) {
+                a.ocean_base = static_cast<int32_t>(base);
+                a.chunk = static_cast<int32_t>(std::min(chunk_, count_ - base));
+                run_row(a, st);
+                run_col(a, st, steps > 0);
+            }
         }
         if (steps > 0) {
             foam_cur_ ^= 1;
@@ -456,8 +470,12 @@ public:
             const uint32_t k = std::min(chunk_, count_ - base);
             a.ocean_base = static_cast<int32_t>(base);
             a.chunk = static_cast<int32_t>(k);
-            run_row(a, stream_);
-            run_col(a, stream_, steps > 0);
+            if (persistent_) {
+                run_frame(a, base, k, steps > 0, stream_);
+            } else {
+                run_row(a, stream_);
+                run_col(a, stream_, steps > 0);
+            }
             if (pipelined) {
                 check(cudaEventRecord(chunk_events_[c], stream_), "event");
                 check(cudaStreamWaitEvent(copy_stream_, chunk_events_[c], 0), "wait");
@@ -482,6 +500,19 @@ public:
         }
         check(cudaStreamSynchronize(copy_stream_), "copy back");
         check(cudaStreamSynchronize(stream_), "frame");
+        if (take_error()) throw TimeoutError();
+    }
+
+    // Reads and clears the sticky error word of the persistent kernel (set
+    // when one of its bounded waits gave up). Synchronises the batch stream.
+    bool take_error()
+    {
+        unsigned e = 0;
+        check(cudaMemcpyAsync(&e, error_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, stream_), "error word");
+        check(cudaStreamSynchronize(stream_), "error word");
+        if (e == 0) return false;
+        check(cudaMemsetAsync(error_.p, 0, sizeof(unsigned), stream_), "error word");
+        return true;
     }
 
     void read_spectrum(uint32_t i, float* h0, float* omega_kinv) const
@@ -518,7 +549,9 @@ public:
         p.row_ms = prof_ms_[0];
         p.col_ms = prof_ms_[1];
         p.foam_ms = prof_ms_[2];
-        for (int k = 0; k < 3; ++k) {
+        p.frame_launches = prof_n_[3];
+        p.frame_ms = prof_ms_[3];
+        for (int k = 0; k < 4; ++k) {
             prof_n_[k] = 0;
             prof_ms_[k] = 0.0;
         }
@@ -562,6 +595,36 @@ private:
     void run_row(const FrameArgs& a, cudaStream_t st)
     {
         timed(0, st, [&] { check(launch_row_pass(log_n_, nf_, form_ == OCEAN_FFT_FAST, a, st), "row pass"); });
+    }
+
+    // One persistent launch for oceans [base, base + k) (csrc/frame.cu
+    // frame_kernel): reset its work queue, then launch one wave of resident CTAs.
+    void run_frame(FrameArgs a, uint32_t base, uint32_t k, bool foam, cudaStream_t st)
+    {
+        a.ocean_base = static_cast<int32_t>(base);
+        a.chunk = static_cast<int32_t>(k);
+        check(cudaMemsetAsync(queue_.p, 0, (1 + 2 * size_t(k)) * sizeof(unsigned), st), "queue reset");
+        QueueArgs q;
+        q.ticket = queue_.p;
+        q.rows_done = queue_.p + 1;
+        q.cols_done = queue_.p + 1 + k;
+        q.error = error_.p;
+        q.count = static_cast<int32_t>(k);
+        q.slots = slots_;
+        q.wait_ns = 1000000000ull;
+        int& grid = frame_grid_[foam ? 1 : 0];
+        if (grid == 0) {
+            int sms = 0;
+            check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "SM count");
+            const int per_sm = frame_blocks_per_sm(log_n_, nf_, form_ == OCEAN_FFT_FAST, foam);
+            if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "frame occupancy");
+            grid = per_sm * sms;
+        }
+        const int launch_grid = static_cast<int>(std::min<uint64_t>(grid, uint64_t(k) * n_));
+        timed(3, st, [&] {
+            check(launch_frame(log_n_, nf_, form_ == OCEAN_FFT_FAST, foam, a, q, launch_grid, st),
+                  "frame kernel");
+        });
     }
 
     void run_col(const FrameArgs& a, cudaStream_t st, bool foam)
@@ -671,8 +734,12 @@ private:
     std::vector<cudaEvent_t> prof_events_;
     std::vector<int> prof_kind_;
     size_t prof_used_ = 0;
-    uint64_t prof_n_[3] = {0, 0, 0};
-    double prof_ms_[3] = {0.0, 0.0, 0.0};
+    uint64_t prof_n_[4] = {0, 0, 0, 0};
+    double prof_ms_[4] = {0.0, 0.0, 0.0, 0.0};
+    bool persistent_ = true;
+    int slots_ = 1;
+    int frame_grid_[2] = {0, 0};
+    DevBuf<unsigned> queue_, error_;
     uint64_t launches_ = 0;
     int slot_next_ = 0;
     double* staged_top_ = nullptr;
@@ -856,8 +923,8 @@ struct ocean_sim {
 struct ocean_batch {
     Batch impl;
     ocean_batch(const ocean_desc* d, uint32_t n, int form, bool foam, const ocean_foam_desc& f,
-                uint32_t chunk)
-        : impl(d, n, form, foam, f, chunk) {}
+                uint32_t chunk, bool persistent)
+        : impl(d, n, form, foam, f, chunk, persistent) {}
 };
 
 namespace {
@@ -870,6 +937,8 @@ ocean_status guarded(Fn&& fn)
         return OCEAN_OK;
     } catch (const std::invalid_argument&) {
         return OCEAN_ERROR_INVALID_ARG;
+    } catch (const ocean_b200::TimeoutError&) {
+        return OCEAN_ERROR_TIMEOUT;
     } catch (const DeviceError& e) {
         return ocean_b200::status_of(e);
     } catch (const std::bad_alloc&) {
@@ -1094,7 +1163,8 @@ ocean_batch* ocean_batch_create(const ocean_batch_desc* desc, ocean_status* out_
     ocean_batch* b = nullptr;
     ocean_status st = OCEAN_OK;
     if (desc == nullptr || desc->struct_size != sizeof(ocean_batch_desc) ||
-        (desc->fft_form != OCEAN_FFT_EXACT && desc->fft_form != OCEAN_FFT_FAST)) {
+        (desc->fft_form != OCEAN_FFT_EXACT && desc->fft_form != OCEAN_FFT_FAST) ||
+        (desc->schedule != OCEAN_SCHEDULE_PERSISTENT && desc->schedule != OCEAN_SCHEDULE_CHUNKED)) {
         st = OCEAN_ERROR_INVALID_ARG;
     } else {
         ocean_foam_desc foam;
@@ -1110,7 +1180,8 @@ ocean_batch* ocean_batch_create(const ocean_batch_desc* desc, ocean_status* out_
         if (st == OCEAN_OK) {
             st = guarded([&] {
                 b = new ocean_batch(desc->oceans, desc->count, desc->fft_form,
-                                    desc->persistent_foam != 0, foam, desc->chunk);
+                                    desc->persistent_foam != 0, foam, desc->chunk,
+                                    desc->schedule == OCEAN_SCHEDULE_PERSISTENT);
             });
         }
     }
@@ -1157,7 +1228,10 @@ uint32_t ocean_batch_last_foam_substeps(const ocean_batch* batch)
 ocean_status ocean_batch_synchronize(ocean_batch* batch)
 {
     if (batch == nullptr) return OCEAN_ERROR_INVALID_ARG;
-    return guarded([&] { ocean_b200::check(cudaStreamSynchronize(batch->impl.stream()), "sync"); });
+    return guarded([&] {
+        ocean_b200::check(cudaStreamSynchronize(batch->impl.stream()), "sync");
+        if (batch->impl.take_error()) throw ocean_b200::TimeoutError();
+    });
 }
 
 ocean_status ocean_batch_read_spectrum(const ocean_batch* batch, uint32_t index, float* h0,
@@ -1184,6 +1258,22 @@ ocean_status ocean_batch_read_profile(ocean_batch* batch, ocean_pass_profile* ou
 uint64_t ocean_batch_launch_count(const ocean_batch* batch)
 {
     return batch ? batch->impl.launch_count() : 0u;
+}
+
+ocean_status ocean_check_bounded_wait(uint32_t timeout_ms)
+{
+    return guarded([&] {
+        unsigned* d = nullptr;
+        ocean_b200::check(cudaMalloc(&d, 2 * sizeof(unsigned)), "cudaMalloc");
+        unsigned h[2] = {0, 0};
+        cudaError_t e = cudaMemset(d, 0, 2 * sizeof(unsigned));
+        if (e == cudaSuccess)
+            e = ocean_b200::launch_wait_probe(d, 1u, d + 1, uint64_t(timeout_ms) * 1000000ull, nullptr);
+        if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
+        cudaFree(d);
+        ocean_b200::check(e, "wait probe");
+        if (h[1] != 0) throw ocean_b200::TimeoutError();
+    });
 }
 
 const char* ocean_device_arch(void) { return "sm_100a"; }

@@ -49,6 +49,28 @@ struct FrameArgs {
     int32_t chunk;             // oceans in this chunk
 };
 
+// Work queue of the persistent frame kernel. `ticket`, `rows_done[count]` and
+// `cols_done[count]` must be zero at launch (one contiguous block).
+struct QueueArgs {
+    unsigned* ticket;
+    unsigned* rows_done;
+    unsigned* cols_done;
+    unsigned* error;      // sticky: set to 1 when a bounded wait gives up
+    int32_t count;        // oceans in the frame (inter holds `slots` of them)
+    int32_t slots;        // intermediate ring slots
+    unsigned long long wait_ns;
+};
+
+// One persistent launch for the whole frame of `q.count` oceans (foam fused
+// when fuse_foam). `grid` = CTAs to launch (0 = one wave of resident CTAs).
+cudaError_t launch_frame(int log_n, int nf, bool fast, bool fuse_foam, const FrameArgs& args,
+                         const QueueArgs& q, int grid, cudaStream_t stream);
+// Resident CTAs per SM of the persistent frame kernel, and its thread count.
+int frame_blocks_per_sm(int log_n, int nf, bool fast, bool fuse_foam);
+// A bounded wait on `counter` that nothing increments (tests the timeout path).
+cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned* error,
+                              unsigned long long limit_ns, cudaStream_t stream);
+
 // Row pass (evolve + row FFTs) and column pass (column FFTs + finalize, with
 // an optional fused foam substep) for `args.chunk` oceans starting at
 // args.ocean_base. log_n in [4, 10]; nf is 4 or 6 complex fields.

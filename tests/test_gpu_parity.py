@@ -260,3 +260,50 @@ def test_forced_scalar_level_matches_native():
     nat.update(4.0)
     assert np.array_equal(bits(frame(s)[0]), bits(frame(nat)[0]))
     assert np.array_equal(bits(frame(s)[1]), bits(frame(nat)[1]))
+
+
+def test_persistent_and_chunked_schedules_are_bit_identical():
+    descs = [W.foam_patch_512(seed=20 + k) for k in range(7)]
+    cells = 512 * 512
+    results = []
+    for schedule in (abi.OCEAN_SCHEDULE_PERSISTENT, abi.OCEAN_SCHEDULE_CHUNKED):
+        batch = ob.OceanBatch(descs, foam=W.foam_desc(), schedule=schedule)
+        outs = []
+        for k in range(3):
+            d = np.empty((7, cells, 4), np.float32)
+            n, v = np.empty_like(d), np.empty_like(d)
+            f = np.empty((7, cells), np.float32)
+            batch.update_host([(k + 1) / 60.0], 1.0 / 60.0, d, n, v, f)
+            outs.append((d, n, v, f))
+        # the device-resident path (one persistent launch for all 7 oceans)
+        batch.update([(4) / 60.0], foam_dt=1.0 / 60.0)
+        batch.synchronize()
+        results.append(outs)
+        batch.close()
+    for fa, fb in zip(results[0], results[1]):
+        for a, b in zip(fa, fb):
+            assert np.array_equal(bits(a), bits(b))
+
+
+def test_single_ocean_update_uses_persistent_frame_and_matches_oracle():
+    desc = W.foam_patch_512(seed=3)
+    oc = ob.Ocean(desc)
+    oc.update(77.0)
+    d, n, v = frame(oc)
+    od, on, ov = O.update(desc, 77.0)
+    assert np.array_equal(bits(d), bits(od)) and np.array_equal(bits(v), bits(ov))
+    oc.close()
+
+
+def test_bounded_wait_gives_up_and_device_stays_usable():
+    # The persistent kernel's waits are bounded: a wait on a counter nothing
+    # increments returns after its limit with a timeout status ...
+    assert ob.lib().ocean_check_bounded_wait(50) == abi.OCEAN_ERROR_TIMEOUT
+    # ... and the context is still healthy afterwards.
+    desc = ob.OceanDesc(size=64, seed=5)
+    oc = ob.Ocean(desc)
+    oc.update(2.0)
+    d, _, _ = frame(oc)
+    od, _, _ = O.update(desc, 2.0)
+    assert np.array_equal(bits(d), bits(od))
+    oc.close()
