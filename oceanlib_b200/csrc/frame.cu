@@ -31,7 +31,7 @@ template <int LOG_N>
 struct Shape {
     static constexpr int N = 1 << LOG_N;
     static constexpr int G = lanes_for(LOG_N);                       // lanes / sequence
-    static constexpr int SEQ = N + kPad;                             // sequence stride
+    static constexpr int SEQ = padded_len(N) + kPad;                 // sequence stride
     static constexpr int RP = cmin(N / 2, 32 / G > 1 ? 32 / G : 1); // row pairs / CTA
     // columns / CTA of the per-chunk column kernel: 4 at N = 512 (128-byte
     // rows of the intermediate); 2 at N = 1024, where 32 values per lane
@@ -116,7 +116,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         const float jzz_re = jzz * hr, jzz_im = jzz * hi;
         const float jxz_re = jxz * hr, jxz_im = jxz * hi;
 
-        float2* base = data + (jr * NF) * SEQ + swz(x);
+        float2* base = data + (jr * NF) * SEQ + pad_idx(x);
         base[0 * SEQ] = make_float2(hr - dx_im, hi + dx_re);
         base[1 * SEQ] = make_float2(dz_re - hx_im, dz_im + hx_re);
         base[2 * SEQ] = make_float2(hz_re - jxx_im, hz_im + jxx_re);
@@ -139,16 +139,19 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     __syncthreads();
 
     // Write the rows cell-major: inter[row][x][f], NF/2 float4 per cell.
+    // NT is a multiple of Q, so each thread keeps one field pair fp and walks
+    // cells with a constant stride (no division in the loop).
     constexpr int Q = NF / 2;
+    constexpr int CSTEP = NT / Q;
     float4* inter = reinterpret_cast<float4*>(inter_slot);
-    for (int i = tid; i < RP * 2 * N * Q; i += NT) {
-        const int jr = i / (N * Q);
-        const int rem = i % (N * Q);
-        const int x = rem / Q;
-        const int fp = rem % Q;
+    const int fp = tid % Q;
+#pragma unroll 4
+    for (int cell = tid / Q; cell < RP * 2 * N; cell += CSTEP) {
+        const int jr = cell >> LOG_N;
+        const int x = cell & (N - 1);
         const int row = row_of(jr >> 1, jr & 1);
-        const float2 v0 = data[(jr * NF + 2 * fp) * SEQ + swz(x)];
-        const float2 v1 = data[(jr * NF + 2 * fp + 1) * SEQ + swz(x)];
+        const float2 v0 = data[(jr * NF + 2 * fp) * SEQ + pad_idx(x)];
+        const float2 v1 = data[(jr * NF + 2 * fp + 1) * SEQ + pad_idx(x)];
         inter[(static_cast<size_t>(row) * N + x) * Q + fp] = make_float4(v0.x, v0.y, v1.x, v1.y);
     }
 }
@@ -211,15 +214,16 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     const int x0 = strip * W;
 
     const float4* inter = reinterpret_cast<const float4*>(inter_slot);
-    for (int i = tid; i < N * W * Q; i += NT) {
-        const int y = i / (W * Q);
-        const int rem = i % (W * Q);
-        const int w = rem / Q;
-        const int fp = rem % Q;
+    constexpr int CSTEP = NT / Q;  // NT is a multiple of Q
+    const int fp = tid % Q;
+#pragma unroll 4
+    for (int cw = tid / Q; cw < N * W; cw += CSTEP) {
+        const int y = cw / W;
+        const int w = cw % W;
         const float4* src = inter + (static_cast<size_t>(y) * N + x0 + w) * Q + fp;
         const float4 v = CG ? __ldcg(src) : *src;
-        data[((2 * fp) * W + w) * SEQ + swz(y)] = make_float2(v.x, v.y);
-        data[((2 * fp + 1) * W + w) * SEQ + swz(y)] = make_float2(v.z, v.w);
+        data[((2 * fp) * W + w) * SEQ + pad_idx(y)] = make_float2(v.x, v.y);
+        data[((2 * fp + 1) * W + w) * SEQ + pad_idx(y)] = make_float2(v.z, v.w);
     }
     __syncthreads();
 
@@ -233,7 +237,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
         const int y = i / W;
         const int w = i % W;
         const int x = x0 + w;
-        const int sy = swz(y);
+        const int sy = pad_idx(y);
         const float2 f0 = data[(0 * W + w) * SEQ + sy];
         const float2 f1 = data[(1 * W + w) * SEQ + sy];
         const float2 f2 = data[(2 * W + w) * SEQ + sy];
@@ -394,39 +398,59 @@ frame_kernel(FrameArgs a, QueueArgs q)
     const unsigned count = static_cast<unsigned>(q.count);
     const unsigned total = count * (RT + CT);
     const size_t slot_f2 = static_cast<size_t>(N) * N * NF;
-    while (true) {
-        __syncthreads();  // previous task done with smem and s_ticket
-        if (tid == 0) s_ticket = atomicAdd(q.ticket, 1u);
-        __syncthreads();
-        const unsigned t = s_ticket;
-        if (t >= total) break;
-        bool row;
-        unsigned ocean, idx;
+    // Ticket -> (row?, ocean, task index) for the queue order above.
+    auto decode = [&](unsigned t, bool& row, unsigned& ocean, unsigned& idx) {
         if (t < RT) {
             row = true, ocean = 0, idx = t;
-        } else {
-            const unsigned u = t - RT, per = RT + CT, blk = u / per, off = u % per;
-            if (blk + 1 < count) {
-                row = off < RT;
-                ocean = row ? blk + 1 : blk;
-                idx = row ? off : off - RT;
-            } else {
-                row = false, ocean = count - 1, idx = off;
-            }
+            return;
         }
-        const unsigned slot = ocean % static_cast<unsigned>(q.slots);
+        const unsigned u = t - RT, per = RT + CT, blk = u / per, off = u % per;
+        if (blk + 1 < count) {
+            row = off < RT;
+            ocean = row ? blk + 1 : blk;
+            idx = row ? off : off - RT;
+        } else {
+            row = false, ocean = count - 1, idx = off;
+        }
+    };
+
+    // Thread 0 publishes the previous task (the barrier above it orders every
+    // thread's writes before its fence + atomic, the pattern grid-wide
+    // barriers use), then takes the next ticket and waits for that task's
+    // inputs; one barrier hands the ticket to the CTA.
+    unsigned* publish = nullptr;
+    while (true) {
+        __syncthreads();  // previous task's writes issued; shared memory free
         if (tid == 0) {
-            bool ok = true;
-            if (row) {
-                if (ocean >= static_cast<unsigned>(q.slots))
-                    ok = wait_at_least(q.cols_done + (ocean - q.slots), CT, q.error, q.wait_ns);
-            } else {
-                ok = wait_at_least(q.rows_done + ocean, RT, q.error, q.wait_ns);
+            if (publish != nullptr) {
+                __threadfence();
+                atomicAdd(publish, 1u);
             }
-            s_ok = ok ? 1 : 0;
+            const unsigned t = atomicAdd(q.ticket, 1u);
+            int ok = 1;
+            publish = nullptr;
+            if (t < total) {
+                bool row;
+                unsigned ocean, idx;
+                decode(t, row, ocean, idx);
+                if (row) {
+                    if (ocean >= static_cast<unsigned>(q.slots))
+                        ok = wait_at_least(q.cols_done + (ocean - q.slots), CT, q.error, q.wait_ns);
+                } else {
+                    ok = wait_at_least(q.rows_done + ocean, RT, q.error, q.wait_ns);
+                }
+                publish = row ? q.rows_done + ocean : q.cols_done + ocean;
+            }
+            s_ticket = t;
+            s_ok = ok;
         }
         __syncthreads();
-        if (!s_ok) break;
+        const unsigned t = s_ticket;
+        if (t >= total || !s_ok) break;
+        bool row;
+        unsigned ocean, idx;
+        decode(t, row, ocean, idx);
+        const unsigned slot = ocean % static_cast<unsigned>(q.slots);
         const int abs_ocean = a.ocean_base + static_cast<int>(ocean);
         if (row) {
             row_task<LOG_N, NF, FAST>(a, abs_ocean, static_cast<int>(idx),
@@ -435,9 +459,6 @@ frame_kernel(FrameArgs a, QueueArgs q)
             col_task<LOG_N, NF, FAST, FOAM, S::PW, true>(a, abs_ocean, static_cast<int>(idx),
                                                          a.inter + slot * slot_f2, smem, tws, tid);
         }
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) atomicAdd(row ? q.rows_done + ocean : q.cols_done + ocean, 1u);
     }
 }
 

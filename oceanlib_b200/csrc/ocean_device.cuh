@@ -50,12 +50,17 @@ __device__ __forceinline__ void sincos_poly(float x, float& s_out, float& c_out)
 }
 
 // ---------------------------------------------------------------------------
-// Shared-memory swizzle for one N-point sequence: XOR the low 4 index bits
-// with the next 4. Every access pattern of the Stockham stage blocks below
+// Shared-memory layout of one N-point sequence: one float2 of padding after
+// every 16 values. Every access pattern of the Stockham stage blocks below
 // (lanes walking consecutive indices, or lanes writing 2^r-element runs) then
-// touches 16 distinct 8-byte bank pairs per half-warp.
+// touches 16 distinct 8-byte bank pairs per half-warp, and because the
+// padding is additive the per-register offsets are compile-time constants
+// (an XOR swizzle would cost integer work on every access).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 4) & 15); }
+__device__ __forceinline__ int pad_idx(int i) { return i + (i >> 4); }
+
+// float2 slots one padded sequence of n values occupies.
+__host__ __device__ constexpr int padded_len(int n) { return n + n / 16; }
 
 __host__ __device__ constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
 __host__ __device__ constexpr int cmin(int a, int b) { return a < b ? a : b; }
@@ -122,7 +127,7 @@ struct StageBlock {
         for (int k = 0; k < C; ++k) {
             const int c = lane + G * k;
 #pragma unroll
-            for (int t = 0; t < RR; ++t) v[k][t] = seq[swz((t << (LOG_N - r)) | c)];
+            for (int t = 0; t < RR; ++t) v[k][t] = seq[pad_idx((t << (LOG_N - r)) | c)];
         }
         __syncwarp();
 #pragma unroll
@@ -151,7 +156,7 @@ struct StageBlock {
 #pragma unroll
             for (int S = 0; S < RR; ++S) {
                 const int out = (P << (L0 + r)) | (bitrev<r>(S) << L0) | q;
-                seq[swz(out)] = v[k][S];
+                seq[pad_idx(out)] = v[k][S];
             }
         }
         __syncwarp();
