@@ -289,6 +289,40 @@ OCEAN_API ocean_status ocean_batch_synchronize(ocean_batch* batch);
 OCEAN_API ocean_status ocean_batch_read_spectrum(const ocean_batch* batch, uint32_t index,
                                                  float* h0, float* omega_kinv);
 
+/* --- Cascades (reference: CascadeStack, include/ocean/cascade.hpp:45-92,
+ *     C++ only there; a C API is the reference's planned v1.1 item) -------- */
+
+typedef struct ocean_cascade ocean_cascade;
+
+/* `count` levels (at most 8), each an ordinary ocean descriptor; levels of
+ * equal size advance together in one launch. Evaluates t = 0. */
+OCEAN_API ocean_cascade* ocean_cascade_create(const ocean_desc* levels, uint32_t count,
+                                              ocean_status* out_status);
+OCEAN_API void ocean_cascade_destroy(ocean_cascade* cascade);
+
+/* Advances every level to absolute time `time` (CascadeStack::update,
+ * src/cascade.cpp:42-55). Asynchronous on the cascade's stream. */
+OCEAN_API ocean_status ocean_cascade_update(ocean_cascade* cascade, double time);
+OCEAN_API uint32_t ocean_cascade_level_count(const ocean_cascade* cascade);
+OCEAN_API double ocean_cascade_get_time(const ocean_cascade* cascade);
+OCEAN_API ocean_status ocean_cascade_level_device_buffers(const ocean_cascade* cascade,
+                                                          uint32_t level,
+                                                          ocean_device_buffers* out);
+OCEAN_API ocean_status ocean_cascade_synchronize(ocean_cascade* cascade);
+
+/* Summed surface of all levels at `count` world points (CascadeStack::sample_at,
+ * src/cascade.cpp:82-153): per level `iterations` fixed-point steps (4 is the
+ * reference's), stopping early once a step moves both parameter coordinates
+ * by <= `tolerance` metres (0 = always run all of them). With
+ * device_pointers == 0, xz/out are host arrays and the call waits; otherwise
+ * they are device arrays and the work is queued on `stream` (a cudaStream_t,
+ * NULL = the cascade's stream). With iterations = 4 and tolerance = 0 each
+ * record is bit-identical to the reference's. */
+OCEAN_API ocean_status ocean_cascade_sample_many(ocean_cascade* cascade, const float* xz,
+                                                 uint64_t count, ocean_surface_ex* out,
+                                                 int32_t iterations, float tolerance,
+                                                 int32_t device_pointers, void* stream);
+
 /* Per-kernel device time of the frame passes, from CUDA events recorded on
  * the launching stream around every launch while profiling is on. */
 typedef struct ocean_pass_profile {
@@ -339,6 +373,11 @@ OCEAN_API ocean_status ocean_frame_static_scratch(uint32_t size, float patch_len
  * wait gave up and returned (the expected outcome) - a self-test of the
  * timeout path that leaves the device usable. */
 OCEAN_API ocean_status ocean_check_bounded_wait(uint32_t timeout_ms);
+
+/* Synchronous copy of `bytes` from a device pointer this library handed out
+ * (e.g. an ocean_device_buffers member) into host memory, for callers that
+ * have no CUDA binding of their own. */
+OCEAN_API ocean_status ocean_copy_to_host(void* host_dst, const void* device_src, uint64_t bytes);
 
 /* Name of the device the library was built for ("sm_100a"). */
 OCEAN_API const char* ocean_device_arch(void);

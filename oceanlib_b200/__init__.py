@@ -325,6 +325,70 @@ class OceanBatch:
         return h0, wk
 
 
+class CascadeStack:
+    """ocean::CascadeStack (include/ocean/cascade.hpp:45-92): several ocean
+    levels summed at query time, updated together on the GPU."""
+
+    def __init__(self, levels: Sequence[OceanDesc]):
+        arr = (OceanDescC * len(levels))(*[d.to_c() for d in levels])
+        st = C.c_int(-1)
+        h = lib().ocean_cascade_create(arr, len(levels), C.byref(st))
+        if not h:
+            if st.value == abi.OCEAN_ERROR_INVALID_ARG:
+                raise ValueError(f"invalid cascade ({status_string(st.value)})")
+            raise OceanError(st.value, "ocean_cascade_create")
+        self._h = h
+        self.levels = list(levels)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().ocean_cascade_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> int:
+        return self._h
+
+    def update(self, time: float) -> None:
+        _check(lib().ocean_cascade_update(self._h, float(time)), "ocean_cascade_update")
+
+    def synchronize(self) -> None:
+        _check(lib().ocean_cascade_synchronize(self._h), "ocean_cascade_synchronize")
+
+    @property
+    def time(self) -> float:
+        return lib().ocean_cascade_get_time(self._h)
+
+    def device_buffers(self, level: int) -> DeviceBuffers:
+        d = DeviceBuffers()
+        _check(lib().ocean_cascade_level_device_buffers(self._h, level, C.byref(d)),
+               "ocean_cascade_level_device_buffers")
+        return d
+
+    def sample_many(self, xz: np.ndarray, iterations: int = 4, tolerance: float = 0.0) -> np.ndarray:
+        """(count, 2) host points -> (count, 10) records (SURFACE_FIELDS order)."""
+        xz = np.ascontiguousarray(xz, dtype=np.float32)
+        out = np.empty((xz.shape[0], 10), dtype=np.float32)
+        _check(lib().ocean_cascade_sample_many(self._h, xz.ctypes.data, xz.shape[0], out.ctypes.data,
+                                               iterations, tolerance, 0, None),
+               "ocean_cascade_sample_many")
+        return out
+
+    def sample_many_device(self, xz_ptr: int, count: int, out_ptr: int, iterations: int = 4,
+                           tolerance: float = 0.0, stream: int = 0) -> None:
+        """Device-resident queries: `xz_ptr` -> count float2, `out_ptr` -> count
+        records of 10 floats; queued on `stream`."""
+        _check(lib().ocean_cascade_sample_many(self._h, C.c_void_p(xz_ptr), count, C.c_void_p(out_ptr),
+                                               iterations, tolerance, 1, C.c_void_p(stream)),
+               "ocean_cascade_sample_many")
+
+
 def force_simd_level(name: Optional[str]) -> str:
     r = lib().ocean_force_simd_level(None if name is None else name.encode())
     return r.decode()

@@ -162,6 +162,16 @@ SIGNATURES = {
     "ocean_frame_static_scratch": (C.c_int, [C.c_uint32, C.c_float, C.c_double, C.c_float,
                                              C.c_float, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ocean_cascade_create": (C.c_void_p, [C.POINTER(OceanDescC), C.c_uint32, C.POINTER(C.c_int)]),
+    "ocean_cascade_destroy": (None, [C.c_void_p]),
+    "ocean_cascade_update": (C.c_int, [C.c_void_p, C.c_double]),
+    "ocean_cascade_level_count": (C.c_uint32, [C.c_void_p]),
+    "ocean_cascade_get_time": (C.c_double, [C.c_void_p]),
+    "ocean_cascade_level_device_buffers": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(DeviceBuffers)]),
+    "ocean_cascade_synchronize": (C.c_int, [C.c_void_p]),
+    "ocean_cascade_sample_many": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                                            C.c_int32, C.c_float, C.c_int32, C.c_void_p]),
     "ocean_check_bounded_wait": (C.c_int, [C.c_uint32]),
+    "ocean_copy_to_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "ocean_device_arch": (C.c_char_p, []),
 }

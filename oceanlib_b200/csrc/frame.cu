@@ -538,21 +538,26 @@ __device__ __forceinline__ Texels load_texels(const float4* __restrict__ buf, co
 // buf[i00+c]*w00 + buf[i10+c]*w10 + buf[i01+c]*w01 + buf[i11+c]*w11, in that order.
 #define OCEAN_FETCH(T, t, C) ((T).a.C * (t).w00 + (T).b.C * (t).w10 + (T).c.C * (t).w01 + (T).d.C * (t).w11)
 
-__global__ void sample_kernel(int n, float inv_cell, const float4* __restrict__ disp,
-                              const float4* __restrict__ normal, const float4* __restrict__ vel,
-                              const float2* __restrict__ xz, uint64_t count,
-                              SurfaceEx* __restrict__ out)
+// One ocean's surface at world (x, z): `iters` fixed-point steps of the
+// displacement inversion (the reference takes 4, src/ocean.cpp:366), stopping
+// early once both parameter coordinates move by <= tol (tol = 0: never), then
+// the final bilinear taps and the renormalised normal.
+__device__ __forceinline__ SurfaceEx sample_one(int n, float inv_cell,
+                                                const float4* __restrict__ disp,
+                                                const float4* __restrict__ normal,
+                                                const float4* __restrict__ vel, float2 p,
+                                                int iters, float tol)
 {
-    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= count) return;
-    const float2 p = xz[i];
     float u = p.x, v = p.y;
-#pragma unroll
-    for (int it = 0; it < 4; ++it) {
+    for (int it = 0; it < iters; ++it) {
         const Tap t = make_tap(u, v, n, inv_cell);
         const Texels d = load_texels(disp, t);
-        u = p.x - OCEAN_FETCH(d, t, x);
-        v = p.y - OCEAN_FETCH(d, t, z);
+        const float un = p.x - OCEAN_FETCH(d, t, x);
+        const float vn = p.y - OCEAN_FETCH(d, t, z);
+        const bool done = tol > 0.0f && fabsf(un - u) <= tol && fabsf(vn - v) <= tol;
+        u = un;
+        v = vn;
+        if (done) break;
     }
     const Tap t = make_tap(u, v, n, inv_cell);
     const Texels d = load_texels(disp, t);
@@ -587,7 +592,68 @@ __global__ void sample_kernel(int n, float inv_cell, const float4* __restrict__ 
     } else {
         s.velocity_x = s.velocity_y = s.velocity_z = 0.0f;
     }
-    out[i] = s;
+    return s;
+}
+
+__global__ void sample_kernel(int n, float inv_cell, const float4* __restrict__ disp,
+                              const float4* __restrict__ normal, const float4* __restrict__ vel,
+                              const float2* __restrict__ xz, uint64_t count,
+                              SurfaceEx* __restrict__ out)
+{
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    out[i] = sample_one(n, inv_cell, disp, normal, vel, xz[i], 4, 0.0f);
+}
+
+// Summed surface of several cascade levels (src/cascade.cpp:82-153): height,
+// offsets and velocity add exactly; normals add then renormalise; foam
+// combines as 1 - prod(1 - foam_i). Levels are visited in order, so the float
+// sums round as the reference's loop does.
+__global__ void cascade_sample_kernel(CascadeLevels lv, const float2* __restrict__ xz,
+                                      uint64_t count, SurfaceEx* __restrict__ out, int iters,
+                                      float tol)
+{
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float2 p = xz[i];
+    float height = 0.0f, offset_x = 0.0f, offset_z = 0.0f;
+    float normal_x = 0.0f, normal_y = 0.0f, normal_z = 0.0f;
+    float transparency = 1.0f;
+    float vx = 0.0f, vy = 0.0f, vz = 0.0f;
+    for (int l = 0; l < lv.count; ++l) {
+        const LevelView& L = lv.level[l];
+        const SurfaceEx s = sample_one(L.n, L.inv_cell, L.disp, L.normal, L.velocity, p, iters, tol);
+        height += s.height;
+        offset_x += s.offset_x;
+        offset_z += s.offset_z;
+        normal_x += s.normal_x;
+        normal_y += s.normal_y;
+        normal_z += s.normal_z;
+        vx += s.velocity_x;
+        vy += s.velocity_y;
+        vz += s.velocity_z;
+        transparency *= (1.0f - s.foam);
+    }
+    SurfaceEx o;
+    o.height = height;
+    o.offset_x = offset_x;
+    o.offset_z = offset_z;
+    o.foam = 1.0f - transparency;
+    o.velocity_x = vx;
+    o.velocity_y = vy;
+    o.velocity_z = vz;
+    const float len2 = normal_x * normal_x + normal_y * normal_y + normal_z * normal_z;
+    if (len2 > 0.0f) {
+        const float inv = 1.0f / sqrtf(len2);
+        o.normal_x = normal_x * inv;
+        o.normal_y = normal_y * inv;
+        o.normal_z = normal_z * inv;
+    } else {
+        o.normal_x = 0.0f;
+        o.normal_y = 1.0f;
+        o.normal_z = 0.0f;
+    }
+    out[i] = o;
 }
 
 // ---------------------------------------------------------------------------
@@ -806,6 +872,15 @@ cudaError_t launch_foam_step(int n, int count, const float4* disp, const float4*
     const unsigned blocks = static_cast<unsigned>((total + 255) / 256);
     foam_step_kernel<<<blocks, 256, 0, stream>>>(n, count, disp, velocity, cur, next, dt, decay,
                                                  gain, scale, drift_x, drift_z, inv_cell);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cascade_sample(const CascadeLevels& levels, const float2* xz, uint64_t count,
+                                  SurfaceEx* out, int iters, float tol, cudaStream_t stream)
+{
+    if (count == 0) return cudaSuccess;
+    const unsigned blocks = static_cast<unsigned>((count + 255) / 256);
+    cascade_sample_kernel<<<blocks, 256, 0, stream>>>(levels, xz, count, out, iters, tol);
     return cudaGetLastError();
 }
 

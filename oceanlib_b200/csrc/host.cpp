@@ -245,8 +245,9 @@ public:
         for (const ocean_desc& d : descs_) {
             if (d.size != n_) throw std::invalid_argument("mixed sizes");
             if ((d.compute_velocity != 0) != velocity_) throw std::invalid_argument("mixed velocity");
-            if (d.patch_length != descs_[0].patch_length)
-                throw std::invalid_argument("mixed patch lengths");
+            // Foam advection uses one cell size for the whole batch.
+            if (foam_on && d.patch_length != descs_[0].patch_length)
+                throw std::invalid_argument("mixed patch lengths with persistent foam");
         }
         foam_on_ = foam_on;
         if (foam_on_) {
@@ -910,6 +911,134 @@ private:
     ocean_status last_error_ = OCEAN_OK;
 };
 
+// ---------------------------------------------------------------------------
+// Cascade: several oceans summed at query time (reference CascadeStack,
+// include/ocean/cascade.hpp:45-92). Levels of equal N share one Batch, so all
+// cascades of a size advance in one persistent launch per frame.
+// ---------------------------------------------------------------------------
+class Cascade {
+public:
+    Cascade(const ocean_desc* levels, uint32_t count)
+    {
+        if (levels == nullptr || count == 0) throw std::invalid_argument("no levels");
+        if (count > static_cast<uint32_t>(kMaxCascadeLevels)) throw std::invalid_argument("too many levels");
+        std::vector<ocean_desc> descs(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            if (!copy_desc(&levels[i], descs[i])) throw std::invalid_argument("desc");
+            validate(descs[i]);
+        }
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        // Group levels by (N, velocity) and remember each level's place.
+        std::vector<std::vector<uint32_t>> groups;
+        for (uint32_t i = 0; i < count; ++i) {
+            size_t g = 0;
+            for (; g < groups.size(); ++g) {
+                const ocean_desc& r = descs[groups[g][0]];
+                if (r.size == descs[i].size && r.compute_velocity == descs[i].compute_velocity) break;
+            }
+            if (g == groups.size()) groups.emplace_back();
+            groups[g].push_back(i);
+        }
+        where_.resize(count);
+        ocean_foam_desc foam;
+        foam_desc_defaults(&foam);
+        for (size_t g = 0; g < groups.size(); ++g) {
+            std::vector<ocean_desc> gd;
+            for (uint32_t i : groups[g]) {
+                where_[i] = {static_cast<uint32_t>(g), static_cast<uint32_t>(gd.size())};
+                gd.push_back(descs[i]);
+            }
+            batches_.push_back(std::make_unique<Batch>(gd.data(), static_cast<uint32_t>(gd.size()),
+                                                       g_form.load(), false, foam, 0));
+        }
+        levels_ = descs;
+        // Evaluate t = 0, as a freshly built reference Ocean has.
+        update(0.0);
+        check(cudaStreamSynchronize(stream_), "cascade init");
+    }
+
+    ~Cascade()
+    {
+        if (stream_) {
+            cudaStreamSynchronize(stream_);
+            cudaStreamDestroy(stream_);
+        }
+    }
+
+    void update(double t)
+    {
+        for (auto& b : batches_) b->update(&t, false, 0.0f, stream_);
+        time_ = t;
+    }
+
+    uint32_t count() const { return static_cast<uint32_t>(levels_.size()); }
+    double time() const { return time_; }
+    cudaStream_t stream() const { return stream_; }
+    const Batch& level_batch(uint32_t i) const { return *batches_[where_[i].first]; }
+    uint32_t level_index(uint32_t i) const { return where_[i].second; }
+
+    CascadeLevels views() const
+    {
+        CascadeLevels lv{};
+        lv.count = static_cast<int32_t>(levels_.size());
+        for (uint32_t i = 0; i < levels_.size(); ++i) {
+            const Batch& b = level_batch(i);
+            const uint32_t k = level_index(i);
+            lv.level[i].disp = b.disp(k);
+            lv.level[i].normal = b.normal(k);
+            lv.level[i].velocity = b.velocity_ptr(k);
+            lv.level[i].n = static_cast<int32_t>(levels_[i].size);
+            lv.level[i].inv_cell = static_cast<float>(levels_[i].size) / levels_[i].patch_length;
+        }
+        return lv;
+    }
+
+    // Queries; `device` selects device-resident xz/out (asynchronous on
+    // `st`), otherwise host arrays that are copied across and waited for.
+    void sample_many(const float* xz, uint64_t count, SurfaceEx* out, int iters, float tol,
+                     bool device, cudaStream_t st)
+    {
+        if (count == 0) return;
+        if (device) {
+            if (st == nullptr) st = stream_;
+            if (st != stream_) {
+                check(cudaEventRecord(ready_event(), stream_), "event");
+                check(cudaStreamWaitEvent(st, ready_event(), 0), "wait");
+            }
+            check(launch_cascade_sample(views(), reinterpret_cast<const float2*>(xz), count, out, iters,
+                                        tol, st), "cascade query");
+            return;
+        }
+        std::lock_guard<std::mutex> lock(mutex_);
+        if (in_.n < count) {
+            in_ = DevBuf<float2>(count);
+            out_ = DevBuf<SurfaceEx>(count);
+        }
+        check(cudaMemcpyAsync(in_.p, xz, count * sizeof(float2), cudaMemcpyHostToDevice, stream_), "query");
+        check(launch_cascade_sample(views(), in_.p, count, out_.p, iters, tol, stream_), "cascade query");
+        check(cudaMemcpyAsync(out, out_.p, count * sizeof(SurfaceEx), cudaMemcpyDeviceToHost, stream_),
+              "query");
+        check(cudaStreamSynchronize(stream_), "query");
+    }
+
+private:
+    cudaEvent_t ready_event()
+    {
+        if (ready_ == nullptr) check(cudaEventCreateWithFlags(&ready_, cudaEventDisableTiming), "event");
+        return ready_;
+    }
+
+    std::vector<ocean_desc> levels_;
+    std::vector<std::unique_ptr<Batch>> batches_;
+    std::vector<std::pair<uint32_t, uint32_t>> where_;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ready_ = nullptr;
+    double time_ = 0.0;
+    std::mutex mutex_;
+    DevBuf<float2> in_;
+    DevBuf<SurfaceEx> out_;
+};
+
 }  // namespace ocean_b200
 
 using ocean_b200::Batch;
@@ -919,6 +1048,10 @@ using ocean_b200::Sim;
 struct ocean_sim {
     Sim impl;
     explicit ocean_sim(const ocean_desc& d) : impl(d) {}
+};
+struct ocean_cascade {
+    ocean_b200::Cascade impl;
+    ocean_cascade(const ocean_desc* levels, uint32_t count) : impl(levels, count) {}
 };
 struct ocean_batch {
     Batch impl;
@@ -1260,6 +1393,60 @@ uint64_t ocean_batch_launch_count(const ocean_batch* batch)
     return batch ? batch->impl.launch_count() : 0u;
 }
 
+ocean_cascade* ocean_cascade_create(const ocean_desc* levels, uint32_t count, ocean_status* out_status)
+{
+    ocean_cascade* c = nullptr;
+    const ocean_status st = guarded([&] { c = new ocean_cascade(levels, count); });
+    if (out_status != nullptr) *out_status = st;
+    return st == OCEAN_OK ? c : nullptr;
+}
+
+void ocean_cascade_destroy(ocean_cascade* cascade) { delete cascade; }
+
+ocean_status ocean_cascade_update(ocean_cascade* cascade, double time)
+{
+    if (cascade == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { cascade->impl.update(time); });
+}
+
+uint32_t ocean_cascade_level_count(const ocean_cascade* cascade)
+{
+    return cascade ? cascade->impl.count() : 0u;
+}
+
+double ocean_cascade_get_time(const ocean_cascade* cascade)
+{
+    return cascade ? cascade->impl.time() : 0.0;
+}
+
+ocean_status ocean_cascade_level_device_buffers(const ocean_cascade* cascade, uint32_t level,
+                                                ocean_device_buffers* out)
+{
+    if (cascade == nullptr || out == nullptr || level >= cascade->impl.count())
+        return OCEAN_ERROR_INVALID_ARG;
+    fill_device_buffers(cascade->impl.level_batch(level), cascade->impl.level_index(level), out);
+    return OCEAN_OK;
+}
+
+ocean_status ocean_cascade_synchronize(ocean_cascade* cascade)
+{
+    if (cascade == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { ocean_b200::check(cudaStreamSynchronize(cascade->impl.stream()), "sync"); });
+}
+
+ocean_status ocean_cascade_sample_many(ocean_cascade* cascade, const float* xz, uint64_t count,
+                                       ocean_surface_ex* out, int32_t iterations, float tolerance,
+                                       int32_t device_pointers, void* stream)
+{
+    if (cascade == nullptr || iterations < 0 || !(tolerance >= 0.0f) ||
+        (count > 0 && (xz == nullptr || out == nullptr)))
+        return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] {
+        cascade->impl.sample_many(xz, count, reinterpret_cast<ocean_b200::SurfaceEx*>(out), iterations,
+                                  tolerance, device_pointers != 0, static_cast<cudaStream_t>(stream));
+    });
+}
+
 ocean_status ocean_check_bounded_wait(uint32_t timeout_ms)
 {
     return guarded([&] {
@@ -1273,6 +1460,14 @@ ocean_status ocean_check_bounded_wait(uint32_t timeout_ms)
         cudaFree(d);
         ocean_b200::check(e, "wait probe");
         if (h[1] != 0) throw ocean_b200::TimeoutError();
+    });
+}
+
+ocean_status ocean_copy_to_host(void* host_dst, const void* device_src, uint64_t bytes)
+{
+    if (bytes > 0 && (host_dst == nullptr || device_src == nullptr)) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] {
+        ocean_b200::check(cudaMemcpy(host_dst, device_src, bytes, cudaMemcpyDeviceToHost), "copy");
     });
 }
 

@@ -95,6 +95,22 @@ cudaError_t launch_sample(int n, float inv_cell, const float4* disp, const float
                           const float4* velocity, const float2* xz, uint64_t count,
                           SurfaceEx* out, cudaStream_t stream);
 
+// Cascade levels for the summed query (at most kMaxCascadeLevels).
+constexpr int kMaxCascadeLevels = 8;
+struct LevelView {
+    const float4* disp;
+    const float4* normal;
+    const float4* velocity;  // may be null
+    int32_t n;
+    float inv_cell;          // N / patch_length
+};
+struct CascadeLevels {
+    LevelView level[kMaxCascadeLevels];
+    int32_t count;
+};
+cudaError_t launch_cascade_sample(const CascadeLevels& levels, const float2* xz, uint64_t count,
+                                  SurfaceEx* out, int iters, float tol, cudaStream_t stream);
+
 // Shared-memory bytes each pass needs at a given size (for checks).
 size_t row_pass_smem(int log_n, int nf);
 size_t col_pass_smem(int log_n, int nf);

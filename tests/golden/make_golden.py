@@ -10,6 +10,7 @@ Outputs
                    so GPU tests can check bit-exactness at N = 256 / 512 / 1024
                    without storing the arrays
   ref_queries.npz  reference sample_at results for seeded query points
+  ref_cascade.npz  reference CascadeStack::sample_at results (3 levels)
   abi_layout.json  offsets/sizes of the reference's C structs (include/ocean/ocean.h)
 """
 from __future__ import annotations
@@ -27,8 +28,9 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 import oracle as O  # noqa: E402
-from tests.workloads import (SMALL_CASES, HASH_CASES, FOAM_CASE, QUERY_CASE, desc_to_json,  # noqa: E402
-                             query_points)
+from oceanlib_b200.abi import OceanDescC  # noqa: E402
+from tests.workloads import (SMALL_CASES, HASH_CASES, FOAM_CASE, QUERY_CASE, CASCADE_CASE,  # noqa: E402
+                             desc_to_json, query_points, cascade_points)
 
 HERE = Path(__file__).resolve().parent
 
@@ -93,6 +95,22 @@ def queries() -> None:
     np.savez_compressed(HERE / "ref_queries.npz", xz=xz, out=res)
 
 
+def cascades() -> None:
+    import ctypes as C
+
+    levels, t, count = CASCADE_CASE
+    arr = (OceanDescC * len(levels))(*[O.c_desc_bytes(d) for d in levels])
+    st = C.c_int(-1)
+    h = O.ref().oref_cascade_create(arr, len(levels), C.byref(st))
+    assert h, st.value
+    O.ref().oref_cascade_update(h, t)
+    xz = cascade_points(count)
+    out = np.empty((count, 10), np.float32)
+    O.ref().oref_cascade_sample_many(h, xz.ctypes.data, count, out.ctypes.data)
+    O.ref().oref_cascade_destroy(h)
+    np.savez_compressed(HERE / "ref_cascade.npz", xz=xz, out=out)
+
+
 def abi_layout() -> None:
     src = r"""
 #include <stddef.h>
@@ -134,6 +152,7 @@ def main() -> None:
     small()
     hashes()
     queries()
+    cascades()
     abi_layout()
     print("golden fixtures written to", HERE)
 

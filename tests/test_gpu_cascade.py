@@ -1,0 +1,103 @@
+"""GPU cascades (reference CascadeStack, src/cascade.cpp) and batched
+multi-level queries, through the C ABI.
+
+Bar: with the reference's 4 fixed-point steps the summed records are
+bit-identical to the reference's CascadeStack::sample_at; the converged mode
+(steps until both parameter coordinates move by <= 1e-6 m) is checked for
+convergence itself.
+"""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oceanlib_b200 as ob
+import oracle as O
+from oceanlib_b200 import workloads as W
+from tests.workloads import CASCADE_CASE
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+@pytest.fixture(autouse=True)
+def _device(cuda_device):
+    ob.force_simd_level(None)
+    yield
+
+
+def test_cascade_queries_bit_exact_against_reference():
+    g = np.load(GOLDEN / "ref_cascade.npz")
+    levels, t, count = CASCADE_CASE
+    cs = ob.CascadeStack(levels)
+    cs.update(t)
+    got = cs.sample_many(g["xz"])
+    assert np.array_equal(bits(got), bits(g["out"]))
+    assert cs.time == t
+    cs.close()
+
+
+def test_cascade_levels_are_the_single_ocean_frames():
+    levels, t, _ = CASCADE_CASE
+    cs = ob.CascadeStack(levels)
+    cs.update(t)
+    cs.synchronize()
+    for i, d in enumerate(levels):
+        db = cs.device_buffers(i)
+        n = d.size * d.size
+        host = np.empty((n, 4), np.float32)
+        assert ob.lib().ocean_copy_to_host(host.ctypes.data, db.displacement, host.nbytes) == 0
+        od, _, _ = O.update(d, t)
+        assert np.array_equal(bits(host), bits(od)), i
+    cs.close()
+
+
+def test_cascade_device_queries_match_host_queries():
+    import torch
+
+    levels, t, _ = CASCADE_CASE
+    cs = ob.CascadeStack(levels)
+    cs.update(t)
+    xz = W.cascade_query_points(100_000)
+    host = cs.sample_many(xz)
+    xz_d = torch.from_numpy(xz).cuda()
+    out_d = torch.empty((xz.shape[0], 10), dtype=torch.float32, device="cuda")
+    cs.sample_many_device(xz_d.data_ptr(), xz.shape[0], out_d.data_ptr(),
+                          stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(bits(out_d.cpu().numpy()), bits(host))
+    cs.close()
+
+
+def test_converged_inversion_reaches_one_micrometre():
+    levels, t, _ = CASCADE_CASE
+    cs = ob.CascadeStack(levels)
+    cs.update(t)
+    xz = W.cascade_query_points(65_536)
+    conv = cs.sample_many(xz, iterations=64, tolerance=1e-6)
+    more = cs.sample_many(xz, iterations=200, tolerance=0.0)
+    four = cs.sample_many(xz, iterations=4, tolerance=0.0)
+    dh = np.abs(conv[:, 0].astype(np.float64) - more[:, 0])
+    # where the surface has not folded the fixed point is a contraction and
+    # the converged height no longer moves (float32 rounding aside)
+    assert np.quantile(dh, 0.999) < 1e-5
+    # and convergence does change the answer relative to the 4-step default
+    assert np.abs(four[:, 0] - conv[:, 0]).max() > 0.0
+    cs.close()
+
+
+def test_cascade_rejects_bad_input():
+    with pytest.raises(ValueError):
+        ob.CascadeStack([])
+    with pytest.raises(ValueError):
+        ob.CascadeStack([ob.OceanDesc(size=64, seed=i) for i in range(9)])
+    levels, t, _ = CASCADE_CASE
+    cs = ob.CascadeStack(levels[:1])
+    st = ob.lib().ocean_cascade_sample_many(cs.handle, None, 4, None, 4, 0.0, 0, None)
+    assert st == ob.abi.OCEAN_ERROR_INVALID_ARG
+    cs.close()

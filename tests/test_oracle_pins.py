@@ -181,3 +181,39 @@ def test_oracle_matches_live_reference_random_descriptors():
         xz = rng.uniform(-2 * desc.patch_length, 2 * desc.patch_length, (256, 2)).astype(np.float32)
         assert np.array_equal(bits(ro.sample_many(xz)),
                               bits(O.sample_many(desc.size, desc.patch_length, d, n, v, xz)))
+
+
+def oracle_cascade(levels, t, xz):
+    """CascadeStack::sample_at (src/cascade.cpp:82-153) composed from the
+    oracle's per-level queries, in float32, in the reference's order."""
+    f32 = np.float32
+    acc = {k: np.zeros(len(xz), f32) for k in ("h", "ox", "oz", "nx", "ny", "nz", "vx", "vy", "vz")}
+    transparency = np.ones(len(xz), f32)
+    for d in levels:
+        disp, nrm, vel = O.update(d, t)
+        s = O.sample_many(d.size, d.patch_length, disp, nrm, vel, xz)
+        for k, col in (("h", 0), ("ox", 1), ("oz", 2), ("nx", 3), ("ny", 4), ("nz", 5),
+                       ("vx", 7), ("vy", 8), ("vz", 9)):
+            acc[k] = (acc[k] + s[:, col]).astype(f32)
+        transparency = (transparency * (f32(1.0) - s[:, 6])).astype(f32)
+    len2 = (acc["nx"] * acc["nx"] + acc["ny"] * acc["ny"] + acc["nz"] * acc["nz"]).astype(f32)
+    out = np.zeros((len(xz), 10), f32)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = (f32(1.0) / np.sqrt(len2)).astype(f32)
+    pos = len2 > 0
+    out[:, 3] = np.where(pos, acc["nx"] * inv, f32(0.0))
+    out[:, 4] = np.where(pos, acc["ny"] * inv, f32(1.0))
+    out[:, 5] = np.where(pos, acc["nz"] * inv, f32(0.0))
+    out[:, 0], out[:, 1], out[:, 2] = acc["h"], acc["ox"], acc["oz"]
+    out[:, 6] = (f32(1.0) - transparency).astype(f32)
+    out[:, 7], out[:, 8], out[:, 9] = acc["vx"], acc["vy"], acc["vz"]
+    return out
+
+
+def test_oracle_cascade_matches_reference():
+    from tests.workloads import CASCADE_CASE
+
+    g = np.load(GOLDEN / "ref_cascade.npz")
+    levels, t, count = CASCADE_CASE
+    got = oracle_cascade(levels, t, g["xz"])
+    assert np.array_equal(bits(got), bits(g["out"]))

@@ -49,6 +49,17 @@ FOAM_CASE = (W.foam_patch_512(), W.foam_desc(), 120, 1.0 / 60.0)
 # World queries on the single 256 patch at t = 10.
 QUERY_CASE = (_s256, _t256, 4096)
 
+# Three 256^2 cascades (800 / 150 / 25 m, 30 m depth, velocity on) at t = 10,
+# queried at the first 4096 points of the seeded uniform stream over the
+# 800 m tile plus a few far / negative points.
+CASCADE_CASE = (W.cascade_3x256(), 10.0, 4096)
+
+
+def cascade_points(count: int) -> np.ndarray:
+    pts = W.cascade_query_points(count - 4)
+    edge = np.array([[-5.0, -7.5], [1600.0, 2400.0], [0.0, 0.0], [799.999, 0.001]], np.float32)
+    return np.concatenate([pts, edge]).astype(np.float32)
+
 
 def query_points(desc: OceanDesc, count: int) -> np.ndarray:
     """Seeded points over three tiles (negative coordinates included) plus
