@@ -171,6 +171,113 @@ OCEAN_API const char* ocean_force_simd_level(const char* name);
  * library implements. */
 OCEAN_API void ocean_version(uint32_t* major, uint32_t* minor, uint32_t* patch);
 
+/* -------------------------------------------------------------------------
+ * Local interaction (iWave), include/ocean/ocean.h:267-415. The field lives
+ * on the GPU; ocean_interaction_get_buffers returns a pinned host mirror that
+ * ocean_interaction_update / _recenter refresh before returning.
+ * ------------------------------------------------------------------------- */
+
+/* include/ocean/ocean.h:285 */
+typedef struct ocean_interaction ocean_interaction;
+
+/* include/ocean/ocean.h:290-293 */
+typedef enum ocean_obstruction {
+    OCEAN_OBSTRUCTION_NEUMANN   = 0,
+    OCEAN_OBSTRUCTION_DIRICHLET = 1
+} ocean_obstruction;
+
+/* include/ocean/ocean.h:295-298 */
+typedef enum ocean_source_kind {
+    OCEAN_SOURCE_IMPULSE    = 0,
+    OCEAN_SOURCE_CONTINUOUS = 1
+} ocean_source_kind;
+
+/* include/ocean/ocean.h:300-318; same struct_size rules as ocean_desc.
+ * thread_count and the parallel_for hook are accepted and ignored. */
+typedef struct ocean_interaction_desc {
+    size_t struct_size;
+    uint32_t size;
+    float    extent;
+    uint32_t kernel_radius;
+    float    damping;
+    uint32_t absorb_cells;
+    float    fixed_dt;
+    uint32_t max_substeps;
+    uint32_t max_sources;
+    float    gravity;
+    float    water_depth;
+    int32_t  obstruction;
+    ocean_parallel_for_fn parallel_for;
+    void*                 parallel_for_user;
+    uint32_t              thread_count;
+} ocean_interaction_desc;
+
+/* include/ocean/ocean.h:320 */
+OCEAN_API void ocean_interaction_desc_init(ocean_interaction_desc* desc);
+/* include/ocean/ocean.h:322 */
+OCEAN_API ocean_interaction* ocean_interaction_create(const ocean_interaction_desc* desc,
+                                                      ocean_status* out_status);
+/* include/ocean/ocean.h:324 */
+OCEAN_API void ocean_interaction_destroy(ocean_interaction* field);
+
+/* include/ocean/ocean.h:335-345 */
+typedef struct ocean_disturbance {
+    float world_x;
+    float world_z;
+    float radius;
+    float strength;
+    float velocity_y;
+    float velocity_x;
+    float velocity_z;
+    int32_t kind;
+} ocean_disturbance;
+
+/* include/ocean/ocean.h:349 */
+OCEAN_API void ocean_interaction_add(ocean_interaction* field, const ocean_disturbance* d);
+/* include/ocean/ocean.h:351 */
+OCEAN_API uint64_t ocean_interaction_dropped(const ocean_interaction* field);
+/* include/ocean/ocean.h:356. Substeps, sources and the stencil all run on the
+ * device; the host mirror is refreshed before returning. */
+OCEAN_API void ocean_interaction_update(ocean_interaction* field, float dt);
+/* include/ocean/ocean.h:362 */
+OCEAN_API int32_t ocean_interaction_recenter(ocean_interaction* field, float world_x,
+                                             float world_z);
+/* include/ocean/ocean.h:367 */
+OCEAN_API void ocean_interaction_set_obstruction(ocean_interaction* field, const uint8_t* mask);
+
+/* include/ocean/ocean.h:369-381 */
+typedef struct ocean_interaction_buffers {
+    const float* field;
+    uint32_t     size;
+    float        extent;
+    float        origin_x;
+    float        origin_z;
+} ocean_interaction_buffers;
+
+/* include/ocean/ocean.h:383 */
+OCEAN_API ocean_interaction_buffers ocean_interaction_get_buffers(const ocean_interaction* field);
+
+/* include/ocean/ocean.h:386-391 */
+typedef struct ocean_interaction_sample {
+    float height;
+    float slope_x;
+    float slope_z;
+    float velocity_y;
+} ocean_interaction_sample;
+
+/* include/ocean/ocean.h:393, :396 (GPU query kernel) */
+OCEAN_API void ocean_interaction_sample_at(const ocean_interaction* field, float world_x,
+                                           float world_z, ocean_interaction_sample* out);
+OCEAN_API float ocean_interaction_height_at(const ocean_interaction* field, float world_x,
+                                            float world_z);
+/* include/ocean/ocean.h:403, :404, :408 */
+OCEAN_API float ocean_interaction_fixed_dt(const ocean_interaction* field);
+OCEAN_API float ocean_interaction_dt_limit(const ocean_interaction* field);
+OCEAN_API float ocean_interaction_dispersion_error(const ocean_interaction* field);
+/* include/ocean/ocean.h:413 */
+OCEAN_API void ocean_sample_combined(const ocean_sim* sim, const ocean_interaction* field,
+                                     float world_x, float world_z, ocean_surface_ex* out);
+
 /* =========================================================================
  * Part 2: GPU entry points (no reference counterpart; new symbols only)
  * ========================================================================= */
@@ -322,6 +429,41 @@ OCEAN_API ocean_status ocean_cascade_sample_many(ocean_cascade* cascade, const f
                                                  uint64_t count, ocean_surface_ex* out,
                                                  int32_t iterations, float tolerance,
                                                  int32_t device_pointers, void* stream);
+
+/* --- Interaction field extensions ---------------------------------------- */
+
+/* Device pointer of the N*N float4 (eta, dEta/dx, dEta/dz, dEta/dt) output. */
+OCEAN_API const float* ocean_interaction_device_field(const ocean_interaction* field);
+
+/* Substeps the last update ran, and whether it hit max_substeps
+ * (InteractionField::last_substeps / last_update_clamped). */
+OCEAN_API uint32_t ocean_interaction_last_substeps(const ocean_interaction* field);
+OCEAN_API int32_t ocean_interaction_last_clamped(const ocean_interaction* field);
+
+/* Discrete energy the undamped leapfrog conserves (InteractionField::energy,
+ * src/interaction.cpp:803-846), evaluated on the device. */
+OCEAN_API double ocean_interaction_energy(const ocean_interaction* field);
+
+/* Snapshot / restore of the two time levels (host arrays of N*N floats each,
+ * row-major): a session checkpoint, and a way to replay a known state. */
+OCEAN_API ocean_status ocean_interaction_get_state(const ocean_interaction* field, float* cur,
+                                                   float* old);
+OCEAN_API ocean_status ocean_interaction_set_state(ocean_interaction* field, const float* cur,
+                                                   const float* old);
+
+/* The (2P+1)^2 stencil taps in use (host array, row-major over (j, i)). */
+OCEAN_API ocean_status ocean_interaction_kernel_taps(const ocean_interaction* field, float* taps);
+
+/* Batched queries of the interaction field alone (`out` = count records of
+ * ocean_interaction_sample) and of the combined surface (FFT ocean plus
+ * field, as ocean_sample_combined). Host arrays; the calls wait. */
+OCEAN_API ocean_status ocean_interaction_sample_many(const ocean_interaction* field,
+                                                     const float* xz, uint64_t count,
+                                                     ocean_interaction_sample* out);
+OCEAN_API ocean_status ocean_sample_combined_many(const ocean_sim* sim,
+                                                  const ocean_interaction* field,
+                                                  const float* xz, uint64_t count,
+                                                  ocean_surface_ex* out);
 
 /* Per-kernel device time of the frame passes, from CUDA events recorded on
  * the launching stream around every launch while profiling is on. */

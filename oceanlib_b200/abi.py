@@ -111,6 +111,54 @@ class BatchDescC(C.Structure):
     ]
 
 
+class InteractionDescC(C.Structure):
+    """`ocean_interaction_desc` (include/ocean/ocean.h:300-318 in the reference)."""
+
+    _fields_ = [
+        ("struct_size", C.c_size_t),
+        ("size", C.c_uint32),
+        ("extent", C.c_float),
+        ("kernel_radius", C.c_uint32),
+        ("damping", C.c_float),
+        ("absorb_cells", C.c_uint32),
+        ("fixed_dt", C.c_float),
+        ("max_substeps", C.c_uint32),
+        ("max_sources", C.c_uint32),
+        ("gravity", C.c_float),
+        ("water_depth", C.c_float),
+        ("obstruction", C.c_int32),
+        ("parallel_for", C.c_void_p),
+        ("parallel_for_user", C.c_void_p),
+        ("thread_count", C.c_uint32),
+    ]
+
+
+class DisturbanceC(C.Structure):
+    _fields_ = [(n, C.c_float) for n in
+                ("world_x", "world_z", "radius", "strength", "velocity_y", "velocity_x",
+                 "velocity_z")] + [("kind", C.c_int32)]
+
+
+class InteractionBuffers(C.Structure):
+    _fields_ = [
+        ("field", C.POINTER(C.c_float)),
+        ("size", C.c_uint32),
+        ("extent", C.c_float),
+        ("origin_x", C.c_float),
+        ("origin_z", C.c_float),
+    ]
+
+
+class InteractionSample(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("height", "slope_x", "slope_z", "velocity_y")]
+
+
+OCEAN_OBSTRUCTION_NEUMANN = 0
+OCEAN_OBSTRUCTION_DIRICHLET = 1
+OCEAN_SOURCE_IMPULSE = 0
+OCEAN_SOURCE_CONTINUOUS = 1
+
+
 class PassProfile(C.Structure):
     _fields_ = [
         ("row_launches", C.c_uint64),
@@ -171,6 +219,30 @@ SIGNATURES = {
     "ocean_cascade_synchronize": (C.c_int, [C.c_void_p]),
     "ocean_cascade_sample_many": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
                                             C.c_int32, C.c_float, C.c_int32, C.c_void_p]),
+    "ocean_interaction_desc_init": (None, [C.POINTER(InteractionDescC)]),
+    "ocean_interaction_create": (C.c_void_p, [C.POINTER(InteractionDescC), C.POINTER(C.c_int)]),
+    "ocean_interaction_destroy": (None, [C.c_void_p]),
+    "ocean_interaction_add": (None, [C.c_void_p, C.POINTER(DisturbanceC)]),
+    "ocean_interaction_dropped": (C.c_uint64, [C.c_void_p]),
+    "ocean_interaction_update": (None, [C.c_void_p, C.c_float]),
+    "ocean_interaction_recenter": (C.c_int32, [C.c_void_p, C.c_float, C.c_float]),
+    "ocean_interaction_set_obstruction": (None, [C.c_void_p, C.c_void_p]),
+    "ocean_interaction_get_buffers": (InteractionBuffers, [C.c_void_p]),
+    "ocean_interaction_sample_at": (None, [C.c_void_p, C.c_float, C.c_float, C.POINTER(InteractionSample)]),
+    "ocean_interaction_height_at": (C.c_float, [C.c_void_p, C.c_float, C.c_float]),
+    "ocean_interaction_fixed_dt": (C.c_float, [C.c_void_p]),
+    "ocean_interaction_dt_limit": (C.c_float, [C.c_void_p]),
+    "ocean_interaction_dispersion_error": (C.c_float, [C.c_void_p]),
+    "ocean_sample_combined": (None, [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.POINTER(SurfaceEx)]),
+    "ocean_interaction_device_field": (C.c_void_p, [C.c_void_p]),
+    "ocean_interaction_last_substeps": (C.c_uint32, [C.c_void_p]),
+    "ocean_interaction_last_clamped": (C.c_int32, [C.c_void_p]),
+    "ocean_interaction_energy": (C.c_double, [C.c_void_p]),
+    "ocean_interaction_get_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ocean_interaction_set_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ocean_interaction_kernel_taps": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ocean_interaction_sample_many": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
+    "ocean_sample_combined_many": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]),
     "ocean_check_bounded_wait": (C.c_int, [C.c_uint32]),
     "ocean_copy_to_host": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64]),
     "ocean_device_arch": (C.c_char_p, []),

@@ -9,6 +9,7 @@
 // Every compute step is a CUDA launch; there is no host compute path.
 
 #include "../../include/ocean_b200.h"
+#include "host_util.h"
 #include "spectrum.h"
 
 #include <cuda_runtime.h>
@@ -27,72 +28,6 @@
 
 namespace ocean_b200 {
 namespace {
-
-// ---------------------------------------------------------------------------
-// Errors
-// ---------------------------------------------------------------------------
-struct DeviceError : std::runtime_error {
-    cudaError_t code;
-    DeviceError(cudaError_t c, const char* what) : std::runtime_error(what), code(c) {}
-};
-
-// A bounded device wait gave up (the persistent kernel's error word was set).
-struct TimeoutError : std::runtime_error {
-    TimeoutError() : std::runtime_error("device wait timed out") {}
-};
-
-void check(cudaError_t e, const char* what)
-{
-    if (e != cudaSuccess) throw DeviceError(e, what);
-}
-
-ocean_status status_of(const DeviceError& e)
-{
-    return e.code == cudaErrorMemoryAllocation ? OCEAN_ERROR_OUT_OF_MEMORY : OCEAN_ERROR_DEVICE;
-}
-
-template <typename T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    DevBuf() = default;
-    explicit DevBuf(size_t count) : n(count)
-    {
-        if (count) check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
-    }
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
-    DevBuf& operator=(DevBuf&& o) noexcept
-    {
-        std::swap(p, o.p);
-        std::swap(n, o.n);
-        return *this;
-    }
-    ~DevBuf() { if (p) cudaFree(p); }
-};
-
-template <typename T>
-struct HostBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    HostBuf() = default;
-    explicit HostBuf(size_t count) : n(count)
-    {
-        if (count) check(cudaMallocHost(&p, count * sizeof(T)), "cudaMallocHost");
-        if (p) std::memset(p, 0, count * sizeof(T));
-    }
-    HostBuf(const HostBuf&) = delete;
-    HostBuf& operator=(const HostBuf&) = delete;
-    HostBuf(HostBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
-    HostBuf& operator=(HostBuf&& o) noexcept
-    {
-        std::swap(p, o.p);
-        std::swap(n, o.n);
-        return *this;
-    }
-    ~HostBuf() { if (p) cudaFreeHost(p); }
-};
 
 // ---------------------------------------------------------------------------
 // Global kernel-form selection (ocean_force_simd_level)
@@ -1044,6 +979,7 @@ private:
 using ocean_b200::Batch;
 using ocean_b200::DeviceError;
 using ocean_b200::Sim;
+using ocean_b200::guarded;
 
 struct ocean_sim {
     Sim impl;
@@ -1061,25 +997,6 @@ struct ocean_batch {
 };
 
 namespace {
-
-template <typename Fn>
-ocean_status guarded(Fn&& fn)
-{
-    try {
-        fn();
-        return OCEAN_OK;
-    } catch (const std::invalid_argument&) {
-        return OCEAN_ERROR_INVALID_ARG;
-    } catch (const ocean_b200::TimeoutError&) {
-        return OCEAN_ERROR_TIMEOUT;
-    } catch (const DeviceError& e) {
-        return ocean_b200::status_of(e);
-    } catch (const std::bad_alloc&) {
-        return OCEAN_ERROR_OUT_OF_MEMORY;
-    } catch (...) {
-        return OCEAN_ERROR_UNKNOWN;
-    }
-}
 
 void fill_device_buffers(const Batch& b, uint32_t index, ocean_device_buffers* out)
 {

@@ -1,0 +1,397 @@
+// oceanlib-b200: iWave interaction field kernels.
+//
+// Per substep (reference: src/interaction.cpp:531-587):
+//   sources  - Ricker stamps, 4-sigma clipped, mean-removed, added to both
+//              time levels (src/interaction.cpp:322-391); one kernel computes
+//              each source's stamp mean, a second adds every source to every
+//              cell in submission order (so overlapping sources add in the
+//              reference's order);
+//   obstruction - Dirichlet zero or Neumann copy-from-nearest-fluid
+//              (src/interaction.cpp:295-318);
+//   step     - h_new = c1 * (2h - c2 h_old - g dt^2 (G * h)), the (2P+1)^2
+//              convolution accumulated j-outer / i-inner in one float, no FMA,
+//              flushed below 1e-30 (src/core/iwave_step.cpp:7-54). Shared-memory
+//              tile with a P-cell halo; each thread keeps four vertically
+//              adjacent outputs, so every loaded value feeds up to four
+//              accumulators while each accumulator still sees its taps in the
+//              reference order. The taps travel as kernel parameters (constant
+//              bank), so each multiply takes its tap as an operand, no load.
+// After the substeps, finalize writes (eta, d/dx, d/dz, d/dt)
+// (src/core/iwave_step.cpp:93-124). Compiled with -fmad=false.
+#include "iwave.h"
+
+namespace ocean_b200 {
+namespace {
+
+constexpr float kFlush = 1.0e-30f;
+constexpr int kTileX = 32;
+constexpr int kTileY = 32;
+constexpr int kRowsPerThread = 4;
+
+template <int P>
+__global__ void __launch_bounds__(kTileX * (kTileY / kRowsPerThread))
+iwave_step_kernel(const IWaveField* __restrict__ fields, IWaveTaps taps)
+{
+    constexpr int W = 2 * P + 1;
+    constexpr int SX = kTileX + 2 * P;
+    constexpr int SY = kTileY + 2 * P;
+    __shared__ float tile[SY][SX + 1];
+
+    const IWaveField f = fields[blockIdx.z];
+    const int x0 = blockIdx.x * kTileX;
+    const int y0 = blockIdx.y * kTileY;
+    if (x0 >= f.n || y0 >= f.n) return;  // fields of a smaller size in the batch
+    const int tx = threadIdx.x;
+    const int ty = threadIdx.y;
+    const int tid = ty * kTileX + tx;
+    constexpr int NT = kTileX * (kTileY / kRowsPerThread);
+
+    // The halo reads land in the plane's P-cell zero border.
+    for (int i = tid; i < SY * SX; i += NT) {
+        const int r = i / SX, c = i % SX;
+        tile[r][c] = f.cur[static_cast<ptrdiff_t>(y0 + r - P) * f.stride + (x0 + c - P)];
+    }
+    __syncthreads();
+
+    float acc[kRowsPerThread];
+#pragma unroll
+    for (int q = 0; q < kRowsPerThread; ++q) acc[q] = 0.0f;
+    const int ry = ty * kRowsPerThread;  // first output row of this thread in the tile
+#pragma unroll
+    for (int r = 0; r < kRowsPerThread + 2 * P; ++r) {
+#pragma unroll
+        for (int i = 0; i < W; ++i) {
+            const float v = tile[ry + r][tx + i];
+#pragma unroll
+            for (int q = 0; q < kRowsPerThread; ++q) {
+                const int j = r - q;  // tap row (0 .. 2P) for output q
+                if (j >= 0 && j < W) acc[q] += taps.t[j * W + i] * v;
+            }
+        }
+    }
+
+#pragma unroll
+    for (int q = 0; q < kRowsPerThread; ++q) {
+        const int y = y0 + ry + q;
+        const int x = x0 + tx;
+        const ptrdiff_t pi = static_cast<ptrdiff_t>(y) * f.stride + x;
+        const size_t ci = static_cast<size_t>(y) * f.n + x;
+        const float hc = tile[ry + q + P][tx + P];
+        const float hp = f.old[pi];
+        const float v = f.c1[ci] * (2.0f * hc - f.c2[ci] * hp - f.gdt2 * acc[q]);
+        f.old[pi] = (v > -kFlush && v < kFlush) ? 0.0f : v;
+    }
+}
+
+__global__ void iwave_finalize_kernel(const IWaveField* __restrict__ fields)
+{
+    const IWaveField f = fields[blockIdx.z];
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= f.n || y >= f.n) return;
+    const float* c = f.cur + static_cast<ptrdiff_t>(y) * f.stride + x;
+    const float gx = (c[1] - c[-1]) * f.inv_two_cell;
+    const float gz = (c[f.stride] - c[-static_cast<ptrdiff_t>(f.stride)]) * f.inv_two_cell;
+    const float vy = (*c - f.old[static_cast<ptrdiff_t>(y) * f.stride + x]) * f.inv_dt;
+    f.out[static_cast<size_t>(y) * f.n + x] = make_float4(*c, gx, gz, vy);
+}
+
+// The 2-D Ricker profile (1 - u) e^-u, u = r^2 / (2 sigma^2).
+__device__ __forceinline__ float ricker(float r2, float inv_two_sigma2)
+{
+    const float u = r2 * inv_two_sigma2;
+    return (1.0f - u) * expf(-u);
+}
+
+__device__ __forceinline__ float stamp_r2(const IWaveSource& s, int x, int z)
+{
+    const float px = (static_cast<float>(x) + 0.5f) - s.gx;
+    const float pz = (static_cast<float>(z) + 0.5f) - s.gz;
+    return (px * px + pz * pz) * s.cell * s.cell;
+}
+
+// Mean of each source's clipped stamp, summed in double (deterministic tree
+// order). One CTA per source.
+__global__ void source_mean_kernel(IWaveSource* __restrict__ src, int count)
+{
+    const int k = blockIdx.x;
+    if (k >= count) return;
+    IWaveSource& s = src[k];
+    const int wx = s.x1 - s.x0 + 1;
+    const int wz = s.z1 - s.z0 + 1;
+    const long long cells = static_cast<long long>(wx) * wz;
+    double sum = 0.0;
+    for (long long i = threadIdx.x; i < cells; i += blockDim.x) {
+        const int x = s.x0 + static_cast<int>(i % wx);
+        const int z = s.z0 + static_cast<int>(i / wx);
+        sum += static_cast<double>(ricker(stamp_r2(s, x, z), s.inv_two_sigma2));
+    }
+    __shared__ double part[256];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        s.mean = static_cast<float>(part[0] / (static_cast<double>(wx) * static_cast<double>(wz)));
+}
+
+// Adds every source, in submission order, to each cell it covers.
+__global__ void source_apply_kernel(IWaveField f, const IWaveSource* __restrict__ src, int count)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= f.n || z >= f.n) return;
+    const ptrdiff_t ci = static_cast<ptrdiff_t>(z) * f.stride + x;
+    float cur = f.cur[ci];
+    float old = f.old[ci];
+    bool touched = false;
+    for (int k = 0; k < count; ++k) {
+        const IWaveSource& s = src[k];
+        if (x < s.x0 || x > s.x1 || z < s.z0 || z > s.z1) continue;
+        const float sh = ricker(stamp_r2(s, x, z), s.inv_two_sigma2) - s.mean;
+        const float dd = s.disp * sh;
+        const float dv = s.vel * sh;
+        cur += dd;
+        old += dd - dv * s.dt;
+        touched = true;
+    }
+    if (touched) {
+        f.cur[ci] = cur;
+        f.old[ci] = old;
+    }
+}
+
+// Boundary condition on h^n before the step (src/interaction.cpp:295-318).
+__global__ void obstruction_kernel(IWaveField f, const uint32_t* __restrict__ solid,
+                                   const uint32_t* __restrict__ nearest, uint32_t count,
+                                   int dirichlet)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= count) return;
+    const uint32_t i = solid[s];
+    float* dst = f.cur + static_cast<ptrdiff_t>(i / f.n) * f.stride + (i % f.n);
+    if (dirichlet) {
+        *dst = 0.0f;
+    } else {
+        const uint32_t fl = nearest[i];
+        if (fl == 0xFFFFFFFFu) return;
+        *dst = f.cur[static_cast<ptrdiff_t>(fl / f.n) * f.stride + (fl % f.n)];
+    }
+}
+
+// Integer recentre: dst(x, z) = src(x + dx, z + dz), zero where that falls
+// outside the grid (src/interaction.cpp:601-705). Out of place.
+__global__ void shift_kernel(const float* __restrict__ src, float* __restrict__ dst, int n,
+                             int stride, int dx, int dz)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int z = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= n || z >= n) return;
+    const int sx = x + dx, sz = z + dz;
+    float v = 0.0f;
+    if (sx >= 0 && sx < n && sz >= 0 && sz < n) v = src[static_cast<ptrdiff_t>(sz) * stride + sx];
+    dst[static_cast<ptrdiff_t>(z) * stride + x] = v;
+}
+
+// Bilinear, zero outside the grid (src/interaction.cpp:729-770).
+__device__ __forceinline__ float4 interaction_tap(const float4* __restrict__ out, int n, float cell,
+                                                  float origin_x, float origin_z, float wx, float wz,
+                                                  bool& inside)
+{
+    const float gx = (wx - origin_x) / cell - 0.5f;
+    const float gz = (wz - origin_z) / cell - 0.5f;
+    inside = !(gx < 0.0f || gz < 0.0f || gx >= static_cast<float>(n - 1) ||
+               gz >= static_cast<float>(n - 1));
+    if (!inside) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const int x0 = static_cast<int>(gx);
+    const int z0 = static_cast<int>(gz);
+    const float tx = gx - static_cast<float>(x0);
+    const float tz = gz - static_cast<float>(z0);
+    const size_t i00 = static_cast<size_t>(z0) * n + x0;
+    const float4 a = out[i00], b = out[i00 + 1], c = out[i00 + n], d = out[i00 + n + 1];
+    const float w00 = (1.0f - tx) * (1.0f - tz);
+    const float w10 = tx * (1.0f - tz);
+    const float w01 = (1.0f - tx) * tz;
+    const float w11 = tx * tz;
+    return make_float4(a.x * w00 + b.x * w10 + c.x * w01 + d.x * w11,
+                       a.y * w00 + b.y * w10 + c.y * w01 + d.y * w11,
+                       a.z * w00 + b.z * w10 + c.z * w01 + d.z * w11,
+                       a.w * w00 + b.w * w10 + c.w * w01 + d.w * w11);
+}
+
+__global__ void interaction_sample_kernel(const float4* __restrict__ out, int n, float cell,
+                                          float origin_x, float origin_z,
+                                          const float2* __restrict__ xz, uint64_t count,
+                                          float4* __restrict__ res)
+{
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    bool inside;
+    res[i] = interaction_tap(out, n, cell, origin_x, origin_z, xz[i].x, xz[i].y, inside);
+}
+
+// Energy terms (src/interaction.cpp:803-846) per row, in double; the host
+// adds the rows in order.
+__global__ void energy_rows_kernel(IWaveField f, const float* __restrict__ taps, int p,
+                                   double* __restrict__ row_kin, double* __restrict__ row_pot)
+{
+    const int z = blockIdx.x;
+    const int w = 2 * p + 1;
+    double kin = 0.0, pot = 0.0;
+    for (int x = threadIdx.x; x < f.n; x += blockDim.x) {
+        const ptrdiff_t pi = static_cast<ptrdiff_t>(z) * f.stride + x;
+        const double hc = f.cur[pi];
+        const double hp = f.old[pi];
+        const double v = (hc - hp) * f.inv_dt_d;
+        kin += v * v;
+        const float* centre = f.old + pi;
+        double acc = 0.0;
+        for (int j = -p; j <= p; ++j)
+            for (int i = 0; i < w; ++i)
+                acc += taps[(j + p) * w + i] * centre[static_cast<ptrdiff_t>(j) * f.stride - p + i];
+        pot += hc * acc;
+    }
+    __shared__ double sk[256], sp[256];
+    sk[threadIdx.x] = kin;
+    sp[threadIdx.x] = pot;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            sk[threadIdx.x] += sk[threadIdx.x + s];
+            sp[threadIdx.x] += sp[threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        row_kin[z] = sk[0];
+        row_pot[z] = sp[0];
+    }
+}
+
+// FFT surface + interaction field (WaterSurface::sample_at,
+// src/interaction.cpp:868-906): heights and vertical velocity add; normals
+// compose through slopes when the FFT normal points up.
+__global__ void combine_kernel(const SurfaceEx* __restrict__ ocean_s, const float4* __restrict__ e,
+                               uint64_t count, SurfaceEx* __restrict__ out)
+{
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    SurfaceEx s = ocean_s[i];
+    const float4 f = e[i];
+    s.height += f.x;
+    s.velocity_y += f.w;
+    if (s.normal_y > 1.0e-6f) {
+        const float inv = 1.0f / s.normal_y;
+        const float sx = -s.normal_x * inv + f.y;
+        const float sz = -s.normal_z * inv + f.z;
+        const float len = sqrtf(sx * sx + sz * sz + 1.0f);
+        const float il = 1.0f / len;
+        s.normal_x = -sx * il;
+        s.normal_y = il;
+        s.normal_z = -sz * il;
+    }
+    out[i] = s;
+}
+
+template <int P>
+cudaError_t step_launch(const IWaveField* fields, int count, int max_n, const IWaveTaps& taps,
+                        cudaStream_t st)
+{
+    dim3 grid((max_n + kTileX - 1) / kTileX, (max_n + kTileY - 1) / kTileY, count);
+    dim3 block(kTileX, kTileY / kRowsPerThread);
+    iwave_step_kernel<P><<<grid, block, 0, st>>>(fields, taps);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_iwave_step(int p, const IWaveField* fields, int count, int max_n,
+                              const IWaveTaps& taps, cudaStream_t st)
+{
+    switch (p) {
+        case 1: return step_launch<1>(fields, count, max_n, taps, st);
+        case 2: return step_launch<2>(fields, count, max_n, taps, st);
+        case 3: return step_launch<3>(fields, count, max_n, taps, st);
+        case 4: return step_launch<4>(fields, count, max_n, taps, st);
+        case 5: return step_launch<5>(fields, count, max_n, taps, st);
+        case 6: return step_launch<6>(fields, count, max_n, taps, st);
+        case 7: return step_launch<7>(fields, count, max_n, taps, st);
+        case 8: return step_launch<8>(fields, count, max_n, taps, st);
+        case 9: return step_launch<9>(fields, count, max_n, taps, st);
+        case 10: return step_launch<10>(fields, count, max_n, taps, st);
+        case 11: return step_launch<11>(fields, count, max_n, taps, st);
+        case 12: return step_launch<12>(fields, count, max_n, taps, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_iwave_finalize(const IWaveField* fields, int count, int max_n, cudaStream_t st)
+{
+    dim3 block(32, 8);
+    dim3 grid((max_n + 31) / 32, (max_n + 7) / 8, count);
+    iwave_finalize_kernel<<<grid, block, 0, st>>>(fields);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_source_mean(IWaveSource* sources, int count, cudaStream_t st)
+{
+    if (count == 0) return cudaSuccess;
+    source_mean_kernel<<<count, 256, 0, st>>>(sources, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_source_apply(const IWaveField& f, const IWaveSource* sources, int count,
+                                cudaStream_t st)
+{
+    if (count == 0) return cudaSuccess;
+    dim3 block(32, 8);
+    dim3 grid((f.n + 31) / 32, (f.n + 7) / 8);
+    source_apply_kernel<<<grid, block, 0, st>>>(f, sources, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_obstruction(const IWaveField& f, const uint32_t* solid, const uint32_t* nearest,
+                               uint32_t count, bool dirichlet, cudaStream_t st)
+{
+    if (count == 0) return cudaSuccess;
+    obstruction_kernel<<<(count + 255) / 256, 256, 0, st>>>(f, solid, nearest, count, dirichlet ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shift(const float* src, float* dst, int n, int stride, int dx, int dz,
+                         cudaStream_t st)
+{
+    dim3 block(32, 8);
+    dim3 grid((n + 31) / 32, (n + 7) / 8);
+    shift_kernel<<<grid, block, 0, st>>>(src, dst, n, stride, dx, dz);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_interaction_sample(const float4* out, int n, float cell, float origin_x,
+                                      float origin_z, const float2* xz, uint64_t count,
+                                      float4* res, cudaStream_t st)
+{
+    if (count == 0) return cudaSuccess;
+    interaction_sample_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, st>>>(
+        out, n, cell, origin_x, origin_z, xz, count, res);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_combine(const SurfaceEx* ocean_s, const float4* e, uint64_t count, SurfaceEx* out,
+                           cudaStream_t st)
+{
+    if (count == 0) return cudaSuccess;
+    combine_kernel<<<static_cast<unsigned>((count + 255) / 256), 256, 0, st>>>(ocean_s, e, count, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_energy_rows(const IWaveField& f, const float* taps, int p, double* row_kin,
+                               double* row_pot, cudaStream_t st)
+{
+    energy_rows_kernel<<<f.n, 256, 0, st>>>(f, taps, p, row_kin, row_pot);
+    return cudaGetLastError();
+}
+
+}  // namespace ocean_b200

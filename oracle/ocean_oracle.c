@@ -699,3 +699,177 @@ void or_dft2d_full(uint32_t n, const float* re, const float* im, double* out_re,
     free(xs);
     free(ys);
 }
+
+/* ------------------------------------------------------------------------ */
+/* iWave interaction field: src/core/iwave_step.cpp:7-124 and               */
+/* src/interaction.cpp:212-391                                               */
+/* ------------------------------------------------------------------------ */
+
+void or_iwave_damping(uint32_t n, float damping, uint32_t absorb, float dt, float* c1, float* c2)
+{
+    /* src/interaction.cpp:212-241 */
+    const float a0 = damping;
+    const int w = (int)absorb;
+    const float span = dt * (float)(w > 1 ? w : 1);
+    const float a_edge = 4.0f / (span > 1e-6f ? span : 1e-6f);
+    for (uint32_t z = 0; z < n; ++z) {
+        for (uint32_t x = 0; x < n; ++x) {
+            int dx = (int)x < (int)(n - 1 - x) ? (int)x : (int)(n - 1 - x);
+            int dz = (int)z < (int)(n - 1 - z) ? (int)z : (int)(n - 1 - z);
+            int d = dx < dz ? dx : dz;
+            float alpha = a0;
+            if (w > 0 && d < w) {
+                float t = (float)(w - d) / (float)w;
+                alpha += a_edge * t * t;
+            }
+            float ad = alpha * dt;
+            size_t i = (size_t)z * n + x;
+            c1[i] = 1.0f / (1.0f + ad);
+            c2[i] = 1.0f - ad;
+        }
+    }
+}
+
+void or_iwave_step(uint32_t n, uint32_t p, size_t stride, const float* taps, const float* c1,
+                   const float* c2, float gdt2, const float* cur, float* old)
+{
+    /* src/core/iwave_step.cpp:7-54: j outer, i inner, one float accumulator */
+    const int pp = (int)p, w = 2 * pp + 1;
+    for (uint32_t z = 0; z < n; ++z) {
+        for (uint32_t x = 0; x < n; ++x) {
+            const float* centre = cur + (size_t)z * stride + x;
+            float acc = 0.0f;
+            const float* tap = taps;
+            for (int j = -pp; j <= pp; ++j) {
+                const float* srow = centre + (ptrdiff_t)j * (ptrdiff_t)stride - pp;
+                for (int i = 0; i < w; ++i) acc += tap[i] * srow[i];
+                tap += w;
+            }
+            const size_t oi = (size_t)z * n + x;
+            const float hc = *centre;
+            const float hp = old[(size_t)z * stride + x];
+            const float v = c1[oi] * (2.0f * hc - c2[oi] * hp - gdt2 * acc);
+            old[(size_t)z * stride + x] = (v > -1.0e-30f && v < 1.0e-30f) ? 0.0f : v;
+        }
+    }
+}
+
+void or_iwave_finalize(uint32_t n, size_t stride, const float* cur, const float* old,
+                       float inv_two_cell, float inv_dt, float* out)
+{
+    /* src/core/iwave_step.cpp:93-124 */
+    for (uint32_t z = 0; z < n; ++z) {
+        for (uint32_t x = 0; x < n; ++x) {
+            const float* c = cur + (size_t)z * stride + x;
+            float gx = (c[1] - c[-1]) * inv_two_cell;
+            float gz = (c[stride] - c[-(ptrdiff_t)stride]) * inv_two_cell;
+            float vy = (*c - old[(size_t)z * stride + x]) * inv_dt;
+            float* d = out + ((size_t)z * n + x) * 4;
+            d[0] = *c;
+            d[1] = gx;
+            d[2] = gz;
+            d[3] = vy;
+        }
+    }
+}
+
+static float ricker(float r2, float inv2s2)
+{
+    float u = r2 * inv2s2;
+    return (1.0f - u) * expf(-u);
+}
+
+/* One disturbance (world_x, world_z, radius, strength, velocity_y,
+ * velocity_x, velocity_z) stamped into both levels (src/interaction.cpp:322-391). */
+void or_iwave_inject(uint32_t n, size_t stride, float cell, int32_t origin_x, int32_t origin_z,
+                     float dt, const float* d, float sub_time, float scale, float* cur, float* old)
+{
+    float sigma = d[2] > 0.25f * cell ? d[2] : 0.25f * cell;
+    float inv2s2 = 1.0f / (2.0f * sigma * sigma);
+    float wx = d[0] + d[5] * sub_time;
+    float wz = d[1] + d[6] * sub_time;
+    float gx = (wx - (float)origin_x * cell) / cell;
+    float gz = (wz - (float)origin_z * cell) / cell;
+    int rad = (int)ceilf(4.0f * sigma / cell);
+    int fx = (int)floorf(gx), fz = (int)floorf(gz);
+    int x0 = fx - rad < 0 ? 0 : fx - rad;
+    int x1 = fx + rad > (int)n - 1 ? (int)n - 1 : fx + rad;
+    int z0 = fz - rad < 0 ? 0 : fz - rad;
+    int z1 = fz + rad > (int)n - 1 ? (int)n - 1 : fz + rad;
+    if (x1 < x0 || z1 < z0) return;
+    double sum = 0.0;
+    for (int z = z0; z <= z1; ++z) {
+        for (int x = x0; x <= x1; ++x) {
+            float px = ((float)x + 0.5f) - gx;
+            float pz = ((float)z + 0.5f) - gz;
+            sum += ricker((px * px + pz * pz) * cell * cell, inv2s2);
+        }
+    }
+    float mean = (float)(sum / ((double)(x1 - x0 + 1) * (double)(z1 - z0 + 1)));
+    float disp = -d[3] * scale;
+    float vel = d[4] * scale;
+    for (int z = z0; z <= z1; ++z) {
+        for (int x = x0; x <= x1; ++x) {
+            float px = ((float)x + 0.5f) - gx;
+            float pz = ((float)z + 0.5f) - gz;
+            float r2 = (px * px + pz * pz) * cell * cell;
+            float s = ricker(r2, inv2s2) - mean;
+            float dd = disp * s;
+            float dv = vel * s;
+            size_t ci = (size_t)z * stride + (size_t)x;
+            cur[ci] += dd;
+            old[ci] += dd - dv * dt;
+        }
+    }
+}
+
+/* Nearest-fluid table by multi-source BFS (src/interaction.cpp:255-292);
+ * returns the number of solid cells written to `solid`. */
+uint32_t or_iwave_nearest(uint32_t n, const uint8_t* mask, uint32_t* nearest, uint32_t* solid)
+{
+    size_t cells = (size_t)n * n;
+    uint32_t* q = (uint32_t*)malloc(sizeof(uint32_t) * cells);
+    size_t head = 0, tail = 0;
+    uint32_t ns = 0;
+    for (size_t i = 0; i < cells; ++i) {
+        if (mask[i] == 0) {
+            nearest[i] = (uint32_t)i;
+            q[tail++] = (uint32_t)i;
+        } else {
+            nearest[i] = 0xFFFFFFFFu;
+            solid[ns++] = (uint32_t)i;
+        }
+    }
+    const int dx[4] = {1, -1, 0, 0}, dz[4] = {0, 0, 1, -1};
+    while (head < tail) {
+        uint32_t i = q[head++];
+        int x = (int)(i % n), z = (int)(i / n);
+        for (int e = 0; e < 4; ++e) {
+            int nx = x + dx[e], nz = z + dz[e];
+            if (nx < 0 || nz < 0 || nx >= (int)n || nz >= (int)n) continue;
+            uint32_t j = (uint32_t)nz * n + (uint32_t)nx;
+            if (nearest[j] == 0xFFFFFFFFu) {
+                nearest[j] = nearest[i];
+                q[tail++] = j;
+            }
+        }
+    }
+    free(q);
+    return ns;
+}
+
+void or_iwave_obstruction(uint32_t n, size_t stride, const uint32_t* solid, uint32_t count,
+                          const uint32_t* nearest, int dirichlet, float* cur)
+{
+    /* src/interaction.cpp:295-318 */
+    for (uint32_t s = 0; s < count; ++s) {
+        uint32_t i = solid[s];
+        if (dirichlet) {
+            cur[(i / n) * stride + (i % n)] = 0.0f;
+        } else {
+            uint32_t f = nearest[i];
+            if (f == 0xFFFFFFFFu) continue;
+            cur[(i / n) * stride + (i % n)] = cur[(f / n) * stride + (f % n)];
+        }
+    }
+}

@@ -81,6 +81,21 @@ void or_dft2d_points(uint32_t n, const float* re, const float* im, uint32_t coun
 void or_dft2d_full(uint32_t n, const float* re, const float* im, double* out_re,
                    double* out_im);
 
+/* iWave interaction field (src/core/iwave_step.cpp, src/interaction.cpp).
+ * Planes are interior pointers into arrays with a p-cell halo and row stride
+ * `stride`; `d` is (world_x, world_z, radius, strength, velocity_y,
+ * velocity_x, velocity_z). */
+void or_iwave_damping(uint32_t n, float damping, uint32_t absorb, float dt, float* c1, float* c2);
+void or_iwave_step(uint32_t n, uint32_t p, size_t stride, const float* taps, const float* c1,
+                   const float* c2, float gdt2, const float* cur, float* old);
+void or_iwave_finalize(uint32_t n, size_t stride, const float* cur, const float* old,
+                       float inv_two_cell, float inv_dt, float* out);
+void or_iwave_inject(uint32_t n, size_t stride, float cell, int32_t origin_x, int32_t origin_z,
+                     float dt, const float* d, float sub_time, float scale, float* cur, float* old);
+uint32_t or_iwave_nearest(uint32_t n, const uint8_t* mask, uint32_t* nearest, uint32_t* solid);
+void or_iwave_obstruction(uint32_t n, size_t stride, const uint32_t* solid, uint32_t count,
+                          const uint32_t* nearest, int dirichlet, float* cur);
+
 #ifdef __cplusplus
 }
 #endif

@@ -14,8 +14,11 @@
 #include "ocean/foam.hpp"
 #include "ocean/cascade.hpp"
 
+#include "ocean/interaction.hpp"
+
 #include "core/cpu_features.hpp"
 #include "core/evolve.hpp"
+#include "core/iwave_kernel.hpp"
 #include "core/fft.hpp"
 #include "core/rng.hpp"
 #include "core/spectrum.hpp"
@@ -323,4 +326,85 @@ OREF_API double oref_time_updates(void* const* sims, void* const* foams, uint32_
 OREF_API uint32_t oref_hardware_concurrency(void)
 {
     return std::thread::hardware_concurrency();
+}
+
+// ---------------------------------------------------------------------------
+// iWave: the reference's stencil builder and its interaction C ABI.
+// ---------------------------------------------------------------------------
+
+// taps: (2P+1)^2 floats; stats: max_symbol, min_symbol, peak_relative_error.
+OREF_API int oref_iwave_taps(uint32_t radius, double cell, double depth, float* taps, double* stats)
+{
+    try {
+        ocean::detail::IWaveKernel k;
+        ocean::detail::build_iwave_kernel(radius, cell, depth,
+                                          ocean::detail::KernelMethod::LeastSquares, k);
+        std::memcpy(taps, k.taps.data(), sizeof(float) * k.width * k.width);
+        stats[0] = k.max_symbol;
+        stats[1] = k.min_symbol;
+        stats[2] = k.peak_relative_error;
+        return 0;
+    } catch (...) {
+        return 1;
+    }
+}
+
+OREF_API void* oref_i_create(const ocean_interaction_desc* d, int* status)
+{
+    ocean_status st = OCEAN_OK;
+    ocean_interaction* f = ocean_interaction_create(d, &st);
+    if (status) *status = static_cast<int>(st);
+    return f;
+}
+OREF_API void oref_i_destroy(void* f) { ocean_interaction_destroy(static_cast<ocean_interaction*>(f)); }
+OREF_API void oref_i_desc_init(ocean_interaction_desc* d) { ocean_interaction_desc_init(d); }
+OREF_API void oref_i_add(void* f, const ocean_disturbance* d)
+{
+    ocean_interaction_add(static_cast<ocean_interaction*>(f), d);
+}
+OREF_API void oref_i_update(void* f, float dt) { ocean_interaction_update(static_cast<ocean_interaction*>(f), dt); }
+OREF_API int oref_i_recenter(void* f, float x, float z)
+{
+    return ocean_interaction_recenter(static_cast<ocean_interaction*>(f), x, z);
+}
+OREF_API void oref_i_set_obstruction(void* f, const uint8_t* m)
+{
+    ocean_interaction_set_obstruction(static_cast<ocean_interaction*>(f), m);
+}
+OREF_API void oref_i_buffers(void* f, ocean_interaction_buffers* out)
+{
+    *out = ocean_interaction_get_buffers(static_cast<ocean_interaction*>(f));
+}
+OREF_API void oref_i_sample_many(void* f, const float* xz, uint64_t count, ocean_interaction_sample* out)
+{
+    for (uint64_t i = 0; i < count; ++i)
+        ocean_interaction_sample_at(static_cast<ocean_interaction*>(f), xz[2 * i], xz[2 * i + 1], &out[i]);
+}
+OREF_API float oref_i_fixed_dt(void* f) { return ocean_interaction_fixed_dt(static_cast<ocean_interaction*>(f)); }
+OREF_API float oref_i_dt_limit(void* f) { return ocean_interaction_dt_limit(static_cast<ocean_interaction*>(f)); }
+OREF_API float oref_i_dispersion_error(void* f)
+{
+    return ocean_interaction_dispersion_error(static_cast<ocean_interaction*>(f));
+}
+OREF_API double oref_i_energy(void* f) { return reinterpret_cast<ocean::InteractionField*>(f)->energy(); }
+OREF_API uint64_t oref_i_dropped(void* f) { return ocean_interaction_dropped(static_cast<ocean_interaction*>(f)); }
+OREF_API void oref_sample_combined_many(void* sim, void* f, const float* xz, uint64_t count, ocean_surface_ex* out)
+{
+    for (uint64_t i = 0; i < count; ++i)
+        ocean_sample_combined(static_cast<ocean_sim*>(sim), static_cast<ocean_interaction*>(f), xz[2 * i],
+                              xz[2 * i + 1], &out[i]);
+}
+
+// Wall time of `updates` interaction updates of dt each (one disturbance set
+// re-queued before every update), for the CPU baseline.
+OREF_API double oref_i_time_updates(void* f, const ocean_disturbance* d, uint32_t nd, uint32_t updates, float dt)
+{
+    auto* h = static_cast<ocean_interaction*>(f);
+    const auto start = std::chrono::steady_clock::now();
+    for (uint32_t u = 0; u < updates; ++u) {
+        for (uint32_t i = 0; i < nd; ++i) ocean_interaction_add(h, &d[i]);
+        ocean_interaction_update(h, dt);
+    }
+    const auto end = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(end - start).count();
 }

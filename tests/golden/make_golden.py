@@ -111,6 +111,25 @@ def cascades() -> None:
     np.savez_compressed(HERE / "ref_cascade.npz", xz=xz, out=out)
 
 
+def interaction() -> None:
+    from oracle import iwave as OI
+    from tests.workloads import interaction_script, run_interaction
+
+    desc, script, frames, dt = interaction_script()
+    r = OI.RefInteraction(desc)
+    fields = []
+    run_interaction(r, script, frames, dt, lambda f, fld: fields.append(fld.field()))
+    rng = np.random.default_rng(9)
+    xz = rng.uniform(-4.0, 40.0, size=(2048, 2)).astype(np.float32)
+    samples = r.sample_many(xz)
+    taps, stats = OI.ref_taps(desc.kernel_radius, float(np.float32(desc.extent) / np.float32(desc.size)),
+                              desc.depth)
+    np.savez_compressed(HERE / "ref_interaction.npz", fields=np.stack(fields), xz=xz, samples=samples,
+                        taps=taps, stats=stats, fixed_dt=np.float32(r.fixed_dt),
+                        dt_limit=np.float32(r.dt_limit), dispersion_error=np.float32(r.dispersion_error),
+                        energy=np.float64(r.energy()))
+
+
 def abi_layout() -> None:
     src = r"""
 #include <stddef.h>
@@ -153,6 +172,7 @@ def main() -> None:
     hashes()
     queries()
     cascades()
+    interaction()
     abi_layout()
     print("golden fixtures written to", HERE)
 

@@ -55,6 +55,50 @@ QUERY_CASE = (_s256, _t256, 4096)
 CASCADE_CASE = (W.cascade_3x256(), 10.0, 4096)
 
 
+def interaction_script():
+    """A 128^2, 32 m interaction field driven for 12 frames at 60 Hz: an
+    impulse, a moving continuous source, a second impulse, a Neumann
+    obstruction block from frame 3 and a recentre at frame 8. Returns
+    (desc, [(frame, action, args)]) with actions applied before each frame's
+    update in list order."""
+    from oceanlib_b200.interaction import Disturbance, InteractionDesc
+
+    desc = InteractionDesc(size=128, extent=32.0, kernel_radius=6, absorb_cells=12)
+    n = desc.size
+    mask = np.zeros((n, n), np.uint8)
+    mask[70:84, 40:52] = 1
+    moving = Disturbance(world_x=16.0, world_z=16.0, radius=1.0, strength=0.2, velocity_y=-0.5,
+                         velocity_x=2.0, velocity_z=-0.5, kind=1)
+    script = [
+        (0, "add", Disturbance(world_x=10.0, world_z=12.0, radius=0.6, strength=0.3)),
+        (3, "obstruct", mask.ravel()),
+        (5, "add", Disturbance(world_x=22.0, world_z=9.0, radius=0.8, strength=-0.2, velocity_y=0.4)),
+        (8, "recenter", (18.0, 17.0)),
+    ]
+    for f in range(12):
+        script.append((f, "add_moving", moving))
+    script.sort(key=lambda a: (a[0], a[1] != "obstruct", a[1] != "recenter"))
+    return desc, script, 12, 1.0 / 60.0
+
+
+def run_interaction(field, script, frames, dt, on_frame=None):
+    """Drive any object with add / update / set_obstruction / recenter."""
+    by_frame = {}
+    for f, action, arg in script:
+        by_frame.setdefault(f, []).append((action, arg))
+    for f in range(frames):
+        for action, arg in by_frame.get(f, []):
+            if action in ("add", "add_moving"):
+                field.add(arg)
+            elif action == "obstruct":
+                field.set_obstruction(arg)
+            elif action == "recenter":
+                field.recenter(*arg)
+        field.update(dt)
+        if on_frame is not None:
+            on_frame(f, field)
+
+
 def cascade_points(count: int) -> np.ndarray:
     pts = W.cascade_query_points(count - 4)
     edge = np.array([[-5.0, -7.5], [1600.0, 2400.0], [0.0, 0.0], [799.999, 0.001]], np.float32)
