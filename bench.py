@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--schedule", default="persistent", choices=["persistent", "chunked"])
     ap.add_argument("--form", default="exact", choices=["exact", "fast"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
 
@@ -230,6 +231,138 @@ def run_reference_arm(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
+# Secondary workloads (reported under "extra"; not the headline metric)
+# ---------------------------------------------------------------------------
+def bench_cascade(torch, queries: int = 1_000_000, frames: int = 20):
+    """3 x 256^2 cascades (800/150/25 m, 30 m depth, velocity on): frames of
+    all levels plus `queries` device-resident summed queries per frame."""
+    import oceanlib_b200 as ob
+    from oceanlib_b200 import workloads as W
+
+    cs = ob.CascadeStack(W.cascade_3x256())
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        xz = torch.from_numpy(W.cascade_query_points(queries)).cuda()
+        out = torch.empty((queries, 10), dtype=torch.float32, device="cuda")
+    for k in range(3):
+        cs.update(k / 60.0, stream=sh)
+        cs.sample_many_device(xz.data_ptr(), queries, out.data_ptr(), stream=sh)
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    upd_ms = q_ms = 0.0
+    for k in range(frames):
+        e0.record(stream)
+        cs.update(1.0 + k / 60.0, stream=sh)
+        e1.record(stream)
+        cs.sample_many_device(xz.data_ptr(), queries, out.data_ptr(), stream=sh)
+        e2.record(stream)
+        torch.cuda.synchronize()
+        upd_ms += e0.elapsed_time(e1)
+        q_ms += e1.elapsed_time(e2)
+    res = {"workload": "cascade_3x256 + 1M summed queries (4 fixed-point steps)",
+           "cascade_frames_per_s": frames / (upd_ms / 1000.0),
+           "queries_per_s": queries * frames / (q_ms / 1000.0),
+           "query_ms_per_1M": q_ms / frames * (1_000_000 / queries)}
+    # converged inversion (to 1e-6 m, at most 64 steps)
+    e1.record(stream)
+    cs.sample_many_device(xz.data_ptr(), queries, out.data_ptr(), iterations=64, tolerance=1e-6, stream=sh)
+    e2.record(stream)
+    torch.cuda.synchronize()
+    res["converged_queries_per_s"] = queries / (e1.elapsed_time(e2) / 1000.0)
+    cs.close()
+    return res
+
+
+def bench_cascade_reference(seconds: float = 4.0):
+    import ctypes as C
+
+    import oracle as O
+    from oceanlib_b200 import workloads as W
+    from oceanlib_b200.abi import OceanDescC
+
+    levels = W.cascade_3x256()
+    arr = (OceanDescC * 3)(*[O.c_desc_bytes(d) for d in levels])
+    st = C.c_int(-1)
+    h = O.ref().oref_cascade_create(arr, 3, C.byref(st))
+    t0 = time.perf_counter()
+    frames = 0
+    while time.perf_counter() - t0 < seconds / 2 or frames < 2:
+        O.ref().oref_cascade_update(h, 1.0 + frames / 60.0)
+        frames += 1
+    upd = frames / (time.perf_counter() - t0)
+    xz = W.cascade_query_points(20_000)
+    out = np.empty((xz.shape[0], 10), np.float32)
+    t0 = time.perf_counter()
+    reps = 0
+    while time.perf_counter() - t0 < seconds / 2 or reps < 1:
+        O.ref().oref_cascade_sample_many(h, xz.ctypes.data, xz.shape[0], out.ctypes.data)
+        reps += 1
+    q = reps * xz.shape[0] / (time.perf_counter() - t0)
+    O.ref().oref_cascade_destroy(h)
+    return {"cascade_frames_per_s": upd, "queries_per_s": q, "query_threads": 1,
+            "update_threads": int(O.ref().oref_hardware_concurrency())}
+
+
+def iwave_sources(extent: float, count: int = 32, seed: int = 11):
+    """`count` continuous disc sources, radius 0.5-4 m, speed 0-8 m/s."""
+    from oceanlib_b200.interaction import Disturbance
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        sp, hd = rng.uniform(0, 8), rng.uniform(0, 2 * np.pi)
+        out.append(Disturbance(world_x=float(rng.uniform(0.2, 0.8) * extent),
+                               world_z=float(rng.uniform(0.2, 0.8) * extent),
+                               radius=float(rng.uniform(0.5, 4.0)), strength=0.05, velocity_y=-0.1,
+                               velocity_x=float(sp * np.cos(hd)), velocity_z=float(sp * np.sin(hd)),
+                               kind=1))
+    return out
+
+
+def bench_iwave(updates: int = 60):
+    """A 512^2, 64 m iWave field (P = 6) with 32 moving disc sources, one
+    1/60 s substep per update, through the reference-shaped update call (which
+    also refreshes the host mirror)."""
+    from oceanlib_b200.interaction import InteractionDesc, InteractionField
+
+    desc = InteractionDesc(size=512, extent=64.0, kernel_radius=6, max_sources=64)
+    f = InteractionField(desc)
+    src = iwave_sources(desc.extent)
+    for _ in range(5):
+        for d in src:
+            f.add(d)
+        f.update(1.0 / 60.0)
+    t0 = time.perf_counter()
+    for _ in range(updates):
+        for d in src:
+            f.add(d)
+        f.update(1.0 / 60.0)
+    el = time.perf_counter() - t0
+    f.close()
+    return {"workload": "iwave 512^2 x 64 m, P=6, 32 moving disc sources, dt=1/60 s",
+            "updates_per_s": updates / el, "ms_per_update": 1000.0 * el / updates,
+            "includes": "source stamps, 169-tap step, finalize, 4 MiB host mirror copy"}
+
+
+def bench_iwave_reference(updates: int = 20):
+    import ctypes as C
+
+    import oracle as O
+    from oracle import iwave as OI
+    from oceanlib_b200.interaction import InteractionDesc
+
+    desc = InteractionDesc(size=512, extent=64.0, kernel_radius=6, max_sources=64)
+    r = OI.RefInteraction(desc)
+    src = iwave_sources(desc.extent)
+    arr = (type(src[0].to_c()) * len(src))(*[d.to_c() for d in src])
+    O.ref().oref_i_time_updates(r.h, arr, len(src), 3, 1.0 / 60.0)
+    el = O.ref().oref_i_time_updates(r.h, arr, len(src), updates, 1.0 / 60.0)
+    return {"updates_per_s": updates / el, "ms_per_update": 1000.0 * el / updates,
+            "threads": int(O.ref().oref_hardware_concurrency())}
+
+
+# ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
 def main():
@@ -260,8 +393,12 @@ def main():
                           form=abi.OCEAN_FFT_FAST if args.form == "fast" else abi.OCEAN_FFT_EXACT,
                           schedule=abi.OCEAN_SCHEDULE_CHUNKED if args.schedule == "chunked"
                           else abi.OCEAN_SCHEDULE_PERSISTENT)
-    stream = torch.cuda.current_stream()
+    # An explicit stream: the library launches on it and the CUDA events
+    # below are recorded on it, so they bracket exactly the frame kernels.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
+    assert sh != 0
     dt = W.FOAM_DT
     frame = 0
 
@@ -385,6 +522,20 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "api": "ocean_batch_update_host (pinned host buffers)"},
         }
+        if not args.no_extra and world == 1:
+            extra = {}
+            for name, fn in (("cascade", lambda: bench_cascade(torch)), ("iwave", bench_iwave)):
+                try:
+                    extra[name] = fn()
+                except Exception as e:  # report, do not lose the headline line
+                    extra[name] = {"error": str(e)}
+            if not args.no_cpu_baseline:
+                for name, fn in (("cascade", bench_cascade_reference), ("iwave", bench_iwave_reference)):
+                    try:
+                        extra[name]["reference_cpu"] = fn()
+                    except Exception as e:
+                        extra[name]["reference_cpu"] = {"error": str(e)}
+            line["extra"] = extra
         if not args.no_cpu_baseline and world == 1:
             try:
                 rate, cores, frames = reference_rate(args.cpu_seconds)

@@ -408,8 +408,9 @@ OCEAN_API ocean_cascade* ocean_cascade_create(const ocean_desc* levels, uint32_t
 OCEAN_API void ocean_cascade_destroy(ocean_cascade* cascade);
 
 /* Advances every level to absolute time `time` (CascadeStack::update,
- * src/cascade.cpp:42-55). Asynchronous on the cascade's stream. */
-OCEAN_API ocean_status ocean_cascade_update(ocean_cascade* cascade, double time);
+ * src/cascade.cpp:42-55). Asynchronous on `stream` (a cudaStream_t; NULL =
+ * the cascade's own stream); later work on the cascade's stream waits for it. */
+OCEAN_API ocean_status ocean_cascade_update(ocean_cascade* cascade, double time, void* stream);
 OCEAN_API uint32_t ocean_cascade_level_count(const ocean_cascade* cascade);
 OCEAN_API double ocean_cascade_get_time(const ocean_cascade* cascade);
 OCEAN_API ocean_status ocean_cascade_level_device_buffers(const ocean_cascade* cascade,

@@ -355,8 +355,9 @@ class CascadeStack:
     def handle(self) -> int:
         return self._h
 
-    def update(self, time: float) -> None:
-        _check(lib().ocean_cascade_update(self._h, float(time)), "ocean_cascade_update")
+    def update(self, time: float, stream: int = 0) -> None:
+        _check(lib().ocean_cascade_update(self._h, float(time), C.c_void_p(stream)),
+               "ocean_cascade_update")
 
     def synchronize(self) -> None:
         _check(lib().ocean_cascade_synchronize(self._h), "ocean_cascade_synchronize")

@@ -212,7 +212,7 @@ SIGNATURES = {
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
     "ocean_cascade_create": (C.c_void_p, [C.POINTER(OceanDescC), C.c_uint32, C.POINTER(C.c_int)]),
     "ocean_cascade_destroy": (None, [C.c_void_p]),
-    "ocean_cascade_update": (C.c_int, [C.c_void_p, C.c_double]),
+    "ocean_cascade_update": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
     "ocean_cascade_level_count": (C.c_uint32, [C.c_void_p]),
     "ocean_cascade_get_time": (C.c_double, [C.c_void_p]),
     "ocean_cascade_level_device_buffers": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(DeviceBuffers)]),

@@ -900,9 +900,16 @@ public:
         }
     }
 
-    void update(double t)
+    // Queued on `st` (null = the cascade's stream); later work on the
+    // cascade's stream is ordered after it.
+    void update(double t, cudaStream_t st = nullptr)
     {
-        for (auto& b : batches_) b->update(&t, false, 0.0f, stream_);
+        if (st == nullptr) st = stream_;
+        for (auto& b : batches_) b->update(&t, false, 0.0f, st);
+        if (st != stream_) {
+            check(cudaEventRecord(ready_event(), st), "event");
+            check(cudaStreamWaitEvent(stream_, ready_event(), 0), "wait");
+        }
         time_ = t;
     }
 
@@ -1320,10 +1327,10 @@ ocean_cascade* ocean_cascade_create(const ocean_desc* levels, uint32_t count, oc
 
 void ocean_cascade_destroy(ocean_cascade* cascade) { delete cascade; }
 
-ocean_status ocean_cascade_update(ocean_cascade* cascade, double time)
+ocean_status ocean_cascade_update(ocean_cascade* cascade, double time, void* stream)
 {
     if (cascade == nullptr) return OCEAN_ERROR_INVALID_ARG;
-    return guarded([&] { cascade->impl.update(time); });
+    return guarded([&] { cascade->impl.update(time, static_cast<cudaStream_t>(stream)); });
 }
 
 uint32_t ocean_cascade_level_count(const ocean_cascade* cascade)
