@@ -68,6 +68,21 @@ def dist_env():
     return rank, world, local
 
 
+def rank_seeds(rank: int, batch: int, base: int = 7):
+    """Seeds of the oceans rank `rank` owns: replicas never share a sea state,
+    so the ranks' work is disjoint and needs no exchange."""
+    return [base + rank * batch + b for b in range(batch)]
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """The slowest rank's time (every rank takes this same collective)."""
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -386,7 +401,7 @@ def main():
     from oceanlib_b200 import workloads as W
 
     B = args.batch
-    descs = [W.foam_patch_512(seed=7 + rank * B + b) for b in range(B)]
+    descs = [W.foam_patch_512(seed=s) for s in rank_seeds(rank, B)]
     from oceanlib_b200 import abi
 
     batch = ob.OceanBatch(descs, foam=W.foam_desc(), chunk=args.chunk,
@@ -437,9 +452,7 @@ def main():
     launches = batch.launch_count - launches0
 
     if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = max_over_ranks(total_ms, torch.distributed, "cuda")
     updates = B * args.steps * world
     value = updates / (total_ms / 1000.0)
 
@@ -460,9 +473,7 @@ def main():
         batch.update_host([frame * dt], dt, disp, nrm, vel, foam)
     e2e_s = time.perf_counter() - t0
     if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s, torch.distributed, "cuda")
     e2e_value = B * e2e_steps * world / e2e_s
     d2h = B * CELLS * (3 * 16 + 4)
     h2d = 8  # one absolute time per frame (double)
