@@ -289,6 +289,37 @@ def bench_cascade(torch, queries: int = 1_000_000, frames: int = 20):
     return res
 
 
+def bench_ensemble(torch, frames: int = 30):
+    """64 seeded sea states of uneven N (64..1024), schedule picked by the
+    autotuner; one frame = every ocean advanced once."""
+    import oceanlib_b200 as ob
+    from oceanlib_b200 import workloads as W
+
+    descs = W.ensemble_64()
+    ens = ob.OceanEnsemble(descs, autotune=True)
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    for k in range(3):
+        ens.update(k / 60.0, stream=sh)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for k in range(frames):
+        ens.update(1.0 + k / 60.0, stream=sh)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / frames
+    cells = sum(d.size * d.size for d in descs)
+    res = {"workload": "ensemble_64 (N in 64..1024, seeded, velocity off)",
+           "frames_per_s": 1000.0 / ms, "ms_per_frame": ms,
+           "ocean_updates_per_s": len(descs) * 1000.0 / ms,
+           "cells_per_s": cells * 1000.0 / ms,
+           "equiv_512sq_updates_per_s": cells / (512 * 512) * 1000.0 / ms,
+           "schedule": ens.schedule}
+    ens.close()
+    return res
+
+
 def bench_cascade_reference(seconds: float = 4.0):
     import ctypes as C
 
@@ -535,7 +566,8 @@ def main():
         }
         if not args.no_extra and world == 1:
             extra = {}
-            for name, fn in (("cascade", lambda: bench_cascade(torch)), ("iwave", bench_iwave)):
+            for name, fn in (("cascade", lambda: bench_cascade(torch)), ("iwave", bench_iwave),
+                             ("ensemble", lambda: bench_ensemble(torch))):
                 try:
                     extra[name] = fn()
                 except Exception as e:  # report, do not lose the headline line

@@ -396,6 +396,30 @@ OCEAN_API ocean_status ocean_batch_synchronize(ocean_batch* batch);
 OCEAN_API ocean_status ocean_batch_read_spectrum(const ocean_batch* batch, uint32_t index,
                                                  float* h0, float* omega_kinv);
 
+/* --- Ensembles: independent sea states of uneven size (no reference
+ *     counterpart; the reference updates oceans one at a time) ------------ */
+
+typedef struct ocean_ensemble ocean_ensemble;
+
+/* Groups the oceans by size; each frame forks one stream per size and runs
+ * that size's persistent kernel on it. With autotune != 0 the schedule
+ * (sizes in sequence, or concurrently with SM shares by estimated or by
+ * measured cost) is chosen by timing each candidate on this GPU at creation. */
+OCEAN_API ocean_ensemble* ocean_ensemble_create(const ocean_desc* oceans, uint32_t count,
+                                                int32_t autotune, ocean_status* out_status);
+OCEAN_API void ocean_ensemble_destroy(ocean_ensemble* ensemble);
+OCEAN_API uint32_t ocean_ensemble_count(const ocean_ensemble* ensemble);
+/* All oceans to absolute time `time`, asynchronously on `stream` (NULL = the
+ * ensemble's stream). */
+OCEAN_API ocean_status ocean_ensemble_update(ocean_ensemble* ensemble, double time, void* stream);
+OCEAN_API ocean_status ocean_ensemble_synchronize(ocean_ensemble* ensemble);
+OCEAN_API ocean_status ocean_ensemble_device_buffers(const ocean_ensemble* ensemble, uint32_t index,
+                                                     ocean_device_buffers* out);
+/* The chosen schedule in words (with the timings that chose it); returns the
+ * full length, writes at most capacity - 1 characters and a terminator. */
+OCEAN_API uint64_t ocean_ensemble_describe(const ocean_ensemble* ensemble, char* buf,
+                                           uint64_t capacity);
+
 /* --- Cascades (reference: CascadeStack, include/ocean/cascade.hpp:45-92,
  *     C++ only there; a C API is the reference's planned v1.1 item) -------- */
 

@@ -325,6 +325,60 @@ class OceanBatch:
         return h0, wk
 
 
+class OceanEnsemble:
+    """Independent sea states of uneven size, advanced together: one stream
+    and one persistent kernel per size, schedule chosen by the autotuner."""
+
+    def __init__(self, descs: Sequence[OceanDesc], autotune: bool = True):
+        arr = (OceanDescC * len(descs))(*[d.to_c() for d in descs])
+        st = C.c_int(-1)
+        h = lib().ocean_ensemble_create(arr, len(descs), 1 if autotune else 0, C.byref(st))
+        if not h:
+            if st.value == abi.OCEAN_ERROR_INVALID_ARG:
+                raise ValueError(f"invalid ensemble ({status_string(st.value)})")
+            raise OceanError(st.value, "ocean_ensemble_create")
+        self._h = h
+        self.descs = list(descs)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().ocean_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def update(self, time: float, stream: int = 0) -> None:
+        _check(lib().ocean_ensemble_update(self._h, float(time), C.c_void_p(stream)), "ocean_ensemble_update")
+
+    def synchronize(self) -> None:
+        _check(lib().ocean_ensemble_synchronize(self._h), "ocean_ensemble_synchronize")
+
+    def device_buffers(self, index: int) -> DeviceBuffers:
+        d = DeviceBuffers()
+        _check(lib().ocean_ensemble_device_buffers(self._h, index, C.byref(d)), "ocean_ensemble_device_buffers")
+        return d
+
+    def read(self, index: int):
+        """(displacement, normal) of ocean `index` copied to host arrays."""
+        d = self.device_buffers(index)
+        n = d.size * d.size
+        disp = np.empty((n, 4), np.float32)
+        nrm = np.empty((n, 4), np.float32)
+        _check(lib().ocean_copy_to_host(disp.ctypes.data, d.displacement, disp.nbytes), "copy")
+        _check(lib().ocean_copy_to_host(nrm.ctypes.data, d.normal, nrm.nbytes), "copy")
+        return disp, nrm
+
+    @property
+    def schedule(self) -> str:
+        buf = C.create_string_buffer(512)
+        lib().ocean_ensemble_describe(self._h, buf, 512)
+        return buf.value.decode()
+
+
 class CascadeStack:
     """ocean::CascadeStack (include/ocean/cascade.hpp:45-92): several ocean
     levels summed at query time, updated together on the GPU."""

@@ -17,6 +17,8 @@
 #include <algorithm>
 #include <atomic>
 #include <cctype>
+#include <cstdio>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -496,6 +498,13 @@ public:
 
     uint64_t launch_count() const { return launches_; }
 
+    // Fraction of one wave of resident CTAs the persistent frame kernel
+    // launches with (1 = the whole GPU).
+    void set_grid_share(double s) { grid_share_ = std::min(1.0, std::max(1e-3, s)); }
+    double grid_share() const { return grid_share_; }
+    void set_persistent(bool p) { persistent_ = p; }
+    bool persistent() const { return persistent_; }
+
 private:
     static constexpr int kTimeSlots = 4;
     static constexpr size_t kProfilePairs = 8192;
@@ -556,7 +565,10 @@ private:
             if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "frame occupancy");
             grid = per_sm * sms;
         }
-        const int launch_grid = static_cast<int>(std::min<uint64_t>(grid, uint64_t(k) * n_));
+        // A share below 1 leaves SMs to batches of other sizes running
+        // concurrently (the ensemble's schedule).
+        const int shared = std::max(1, static_cast<int>(std::lround(grid * grid_share_)));
+        const int launch_grid = static_cast<int>(std::min<uint64_t>(shared, uint64_t(k) * n_));
         timed(3, st, [&] {
             check(launch_frame(log_n_, nf_, form_ == OCEAN_FFT_FAST, foam, a, q, launch_grid, st),
                   "frame kernel");
@@ -675,6 +687,7 @@ private:
     bool persistent_ = true;
     int slots_ = 1;
     int frame_grid_[2] = {0, 0};
+    double grid_share_ = 1.0;
     DevBuf<unsigned> queue_, error_;
     uint64_t launches_ = 0;
     int slot_next_ = 0;
@@ -981,6 +994,179 @@ private:
     DevBuf<SurfaceEx> out_;
 };
 
+// ---------------------------------------------------------------------------
+// Ensemble: independent sea states of uneven N. Oceans are grouped by size
+// into Batches; a frame forks one stream per size, runs each size's
+// persistent kernel on it, and joins. The schedule - sequential, or
+// concurrent with each size given a share of the SMs - is picked by
+// autotune(), which times the candidates on this GPU.
+// ---------------------------------------------------------------------------
+class Ensemble {
+public:
+    Ensemble(const ocean_desc* descs, uint32_t count, bool tune)
+    {
+        if (descs == nullptr || count == 0) throw std::invalid_argument("no oceans");
+        std::vector<ocean_desc> all(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            if (!copy_desc(&descs[i], all[i])) throw std::invalid_argument("desc");
+            validate(all[i]);
+        }
+        std::vector<std::vector<uint32_t>> groups;
+        for (uint32_t i = 0; i < count; ++i) {
+            size_t g = 0;
+            for (; g < groups.size(); ++g) {
+                const ocean_desc& r = all[groups[g][0]];
+                if (r.size == all[i].size && r.compute_velocity == all[i].compute_velocity) break;
+            }
+            if (g == groups.size()) groups.emplace_back();
+            groups[g].push_back(i);
+        }
+        where_.resize(count);
+        ocean_foam_desc foam;
+        foam_desc_defaults(&foam);
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "event");
+        for (size_t g = 0; g < groups.size(); ++g) {
+            std::vector<ocean_desc> gd;
+            for (uint32_t i : groups[g]) {
+                where_[i] = {static_cast<uint32_t>(g), static_cast<uint32_t>(gd.size())};
+                gd.push_back(all[i]);
+            }
+            batches_.push_back(std::make_unique<Batch>(gd.data(), static_cast<uint32_t>(gd.size()),
+                                                       g_form.load(), false, foam, 0));
+            work_.push_back(static_cast<double>(gd.size()) * gd[0].size * gd[0].size *
+                            (gd[0].compute_velocity ? 6.0 : 4.0));
+            cudaStream_t s;
+            check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+            streams_.push_back(s);
+            cudaEvent_t e;
+            check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+            done_.push_back(e);
+        }
+        apply_shares(work_);
+        concurrent_ = true;
+        describe_ = "concurrent, SM shares by work estimate";
+        if (tune) autotune();
+    }
+
+    ~Ensemble()
+    {
+        if (stream_) cudaStreamSynchronize(stream_);
+        for (auto s : streams_) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+        for (auto e : done_) cudaEventDestroy(e);
+        if (fork_) cudaEventDestroy(fork_);
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+
+    void update(double t, cudaStream_t st)
+    {
+        if (st == nullptr) st = stream_;
+        if (!concurrent_) {
+            for (auto& b : batches_) b->update(&t, false, 0.0f, st);
+            return;
+        }
+        check(cudaEventRecord(fork_, st), "event");
+        for (size_t g = 0; g < batches_.size(); ++g) {
+            check(cudaStreamWaitEvent(streams_[g], fork_, 0), "wait");
+            batches_[g]->update(&t, false, 0.0f, streams_[g]);
+            check(cudaEventRecord(done_[g], streams_[g]), "event");
+            check(cudaStreamWaitEvent(st, done_[g], 0), "wait");
+        }
+    }
+
+    uint32_t count() const { return static_cast<uint32_t>(where_.size()); }
+    cudaStream_t stream() const { return stream_; }
+    const Batch& batch_of(uint32_t i) const { return *batches_[where_[i].first]; }
+    uint32_t index_of(uint32_t i) const { return where_[i].second; }
+    const std::string& description() const { return describe_; }
+
+private:
+    void apply_shares(const std::vector<double>& weights)
+    {
+        double total = 0.0;
+        for (double w : weights) total += w;
+        for (size_t g = 0; g < batches_.size(); ++g)
+            batches_[g]->set_grid_share(total > 0.0 ? weights[g] / total : 1.0);
+    }
+
+    void full_grids()
+    {
+        for (auto& b : batches_) b->set_grid_share(1.0);
+    }
+
+    // Median time of `frames` frames (after two untimed ones), on stream_.
+    double time_frames(int frames, const std::function<void(double)>& frame)
+    {
+        cudaEvent_t a, b;
+        check(cudaEventCreate(&a), "event");
+        check(cudaEventCreate(&b), "event");
+        frame(0.5);
+        frame(0.6);
+        std::vector<float> ms;
+        for (int k = 0; k < frames; ++k) {
+            check(cudaEventRecord(a, stream_), "event");
+            frame(1.0 + k / 60.0);
+            check(cudaEventRecord(b, stream_), "event");
+            check(cudaEventSynchronize(b), "event");
+            float m = 0.0f;
+            check(cudaEventElapsedTime(&m, a, b), "elapsed");
+            ms.push_back(m);
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        std::sort(ms.begin(), ms.end());
+        return ms[ms.size() / 2];
+    }
+
+    // Candidates: (1) sizes one after another, each with the whole GPU;
+    // (2) concurrent, SM shares by the work estimate; (3) concurrent, shares
+    // by each size's measured stand-alone time. The fastest is kept.
+    void autotune()
+    {
+        const int frames = 5;
+        std::vector<double> alone(batches_.size());
+        full_grids();
+        for (size_t g = 0; g < batches_.size(); ++g)
+            alone[g] = time_frames(frames, [&](double t) { batches_[g]->update(&t, false, 0.0f, stream_); });
+        concurrent_ = false;
+        const double t_seq = time_frames(frames, [&](double t) { update(t, stream_); });
+        concurrent_ = true;
+        apply_shares(work_);
+        const double t_work = time_frames(frames, [&](double t) { update(t, stream_); });
+        apply_shares(alone);
+        const double t_meas = time_frames(frames, [&](double t) { update(t, stream_); });
+        char buf[256];
+        if (t_seq <= t_work && t_seq <= t_meas) {
+            concurrent_ = false;
+            full_grids();
+            std::snprintf(buf, sizeof(buf), "sequential (%.3f ms; concurrent %.3f / %.3f ms)", t_seq, t_work,
+                          t_meas);
+        } else if (t_work <= t_meas) {
+            apply_shares(work_);
+            std::snprintf(buf, sizeof(buf), "concurrent, shares by work estimate (%.3f ms; sequential %.3f, "
+                          "measured-share %.3f)", t_work, t_seq, t_meas);
+        } else {
+            std::snprintf(buf, sizeof(buf), "concurrent, shares by measured time (%.3f ms; sequential %.3f, "
+                          "work-share %.3f)", t_meas, t_seq, t_work);
+        }
+        describe_ = buf;
+        check(cudaStreamSynchronize(stream_), "autotune");
+    }
+
+    std::vector<std::unique_ptr<Batch>> batches_;
+    std::vector<std::pair<uint32_t, uint32_t>> where_;
+    std::vector<double> work_;
+    std::vector<cudaStream_t> streams_;
+    std::vector<cudaEvent_t> done_;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t fork_ = nullptr;
+    bool concurrent_ = true;
+    std::string describe_;
+};
+
 }  // namespace ocean_b200
 
 using ocean_b200::Batch;
@@ -991,6 +1177,10 @@ using ocean_b200::guarded;
 struct ocean_sim {
     Sim impl;
     explicit ocean_sim(const ocean_desc& d) : impl(d) {}
+};
+struct ocean_ensemble {
+    ocean_b200::Ensemble impl;
+    ocean_ensemble(const ocean_desc* d, uint32_t n, bool tune) : impl(d, n, tune) {}
 };
 struct ocean_cascade {
     ocean_b200::Cascade impl;
@@ -1315,6 +1505,51 @@ ocean_status ocean_batch_read_profile(ocean_batch* batch, ocean_pass_profile* ou
 uint64_t ocean_batch_launch_count(const ocean_batch* batch)
 {
     return batch ? batch->impl.launch_count() : 0u;
+}
+
+ocean_ensemble* ocean_ensemble_create(const ocean_desc* oceans, uint32_t count, int32_t autotune,
+                                      ocean_status* out_status)
+{
+    ocean_ensemble* e = nullptr;
+    const ocean_status st = guarded([&] { e = new ocean_ensemble(oceans, count, autotune != 0); });
+    if (out_status != nullptr) *out_status = st;
+    return st == OCEAN_OK ? e : nullptr;
+}
+
+void ocean_ensemble_destroy(ocean_ensemble* ensemble) { delete ensemble; }
+
+uint32_t ocean_ensemble_count(const ocean_ensemble* ensemble) { return ensemble ? ensemble->impl.count() : 0u; }
+
+ocean_status ocean_ensemble_update(ocean_ensemble* ensemble, double time, void* stream)
+{
+    if (ensemble == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { ensemble->impl.update(time, static_cast<cudaStream_t>(stream)); });
+}
+
+ocean_status ocean_ensemble_synchronize(ocean_ensemble* ensemble)
+{
+    if (ensemble == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { ocean_b200::check(cudaStreamSynchronize(ensemble->impl.stream()), "sync"); });
+}
+
+ocean_status ocean_ensemble_device_buffers(const ocean_ensemble* ensemble, uint32_t index,
+                                           ocean_device_buffers* out)
+{
+    if (ensemble == nullptr || out == nullptr || index >= ensemble->impl.count()) return OCEAN_ERROR_INVALID_ARG;
+    fill_device_buffers(ensemble->impl.batch_of(index), ensemble->impl.index_of(index), out);
+    return OCEAN_OK;
+}
+
+uint64_t ocean_ensemble_describe(const ocean_ensemble* ensemble, char* buf, uint64_t capacity)
+{
+    if (ensemble == nullptr) return 0;
+    const std::string& s = ensemble->impl.description();
+    if (buf != nullptr && capacity > 0) {
+        const size_t n = std::min<size_t>(s.size(), capacity - 1);
+        std::memcpy(buf, s.data(), n);
+        buf[n] = '\0';
+    }
+    return s.size();
 }
 
 ocean_cascade* ocean_cascade_create(const ocean_desc* levels, uint32_t count, ocean_status* out_status)
