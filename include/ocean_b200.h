@@ -490,6 +490,118 @@ OCEAN_API ocean_status ocean_sample_combined_many(const ocean_sim* sim,
                                                   const float* xz, uint64_t count,
                                                   ocean_surface_ex* out);
 
+/* --- Serving loop (no reference counterpart; the reference serves one
+ *     caller per object, on the calling thread) -------------------------- */
+
+typedef struct ocean_server ocean_server;
+
+typedef struct ocean_server_desc {
+    size_t   struct_size;        /* sizeof(ocean_server_desc) */
+    uint64_t hbm_budget;         /* device bytes sessions may hold (default 120e9) */
+    uint32_t max_inflight;       /* batches queued on the GPU at once (default 2) */
+    uint32_t max_batch_requests; /* requests one batch takes at most (default 4096) */
+    uint32_t max_batch_points;   /* query points one batch takes at most (default 1 << 20) */
+    uint32_t max_query_points;   /* points one query request may carry (default 65536) */
+    int32_t  fft_form;           /* ocean_fft_form of every session's ocean (default exact) */
+    uint32_t reserved;
+} ocean_server_desc;
+
+typedef enum ocean_session_state {
+    OCEAN_SESSION_WAITING = 0, /* queued for admission: the budget is full */
+    OCEAN_SESSION_ACTIVE  = 1, /* admitted: its state lives on the device */
+    OCEAN_SESSION_CLOSED  = 2  /* closed, or an unknown id */
+} ocean_session_state;
+
+typedef struct ocean_server_stats {
+    uint64_t sessions_active;
+    uint64_t sessions_waiting;
+    uint64_t sessions_closed;
+    uint64_t bytes_in_use;        /* admitted sessions plus shared tables and staging */
+    uint64_t hbm_budget;
+    uint64_t requests_submitted;
+    uint64_t requests_completed;
+    uint64_t requests_failed;
+    uint64_t updates_completed;
+    uint64_t queries_completed;
+    uint64_t query_points_completed;
+    uint64_t batches;             /* batches launched */
+    uint64_t kernel_launches;     /* kernels those batches launched */
+    uint64_t bytes_staging;       /* per-batch device staging (outside the budget) */
+    double   mean_batch_requests;
+    double   latency_p50_ms;      /* submit -> result ready (host clock), all requests */
+    double   latency_p99_ms;
+    double   latency_max_ms;
+    double   update_p50_ms;
+    double   update_p99_ms;
+    double   query_p50_ms;
+    double   query_p99_ms;
+    double   gpu_busy_ms;         /* summed device time of the batches (CUDA events) */
+    double   wall_ms;             /* since creation or the last reset */
+} ocean_server_stats;
+
+OCEAN_API void ocean_server_desc_init(ocean_server_desc* desc);
+/* Starts the server's dispatcher thread, stream and memory pool on the
+ * current device. */
+OCEAN_API ocean_server* ocean_server_create(const ocean_server_desc* desc, ocean_status* out_status);
+/* Finishes every request of admitted sessions, fails those of sessions still
+ * waiting for admission, then frees everything. */
+OCEAN_API void ocean_server_destroy(ocean_server* server);
+
+/* Device bytes one session with these descriptors holds (field may be NULL). */
+OCEAN_API uint64_t ocean_server_session_bytes(const ocean_desc* ocean,
+                                              const ocean_interaction_desc* field);
+
+/* Opens a session: an ocean (ocean_create) and, when `field` is not NULL, an
+ * interaction field over it (ocean_interaction_create; origin fixed at 0, no
+ * obstruction). Ids start at 1. The session is admitted as soon as its
+ * device state fits in the budget, in the order sessions were opened;
+ * until then it waits, and requests submitted to it queue behind its
+ * admission. A session larger than the whole budget is refused with
+ * OCEAN_ERROR_OUT_OF_MEMORY. Invalid descriptors: OCEAN_ERROR_INVALID_ARG. */
+OCEAN_API ocean_status ocean_server_open_session(ocean_server* server, const ocean_desc* ocean,
+                                                 const ocean_interaction_desc* field,
+                                                 uint64_t* out_session);
+/* Closes a session after every request submitted to it before; its memory
+ * returns to the budget and waiting sessions are admitted. */
+OCEAN_API ocean_status ocean_server_close_session(ocean_server* server, uint64_t session);
+OCEAN_API ocean_session_state ocean_server_session_state(ocean_server* server, uint64_t session);
+
+/* Queues one frame of a session: the ocean to absolute `time` (ocean_update)
+ * and, with a field, the `count` disturbances added in order
+ * (ocean_interaction_add) and the field advanced by `dt`
+ * (ocean_interaction_update). `sources` is copied before the call returns. */
+OCEAN_API ocean_status ocean_server_submit_update(ocean_server* server, uint64_t session,
+                                                  double time, float dt,
+                                                  const ocean_disturbance* sources,
+                                                  uint32_t count, uint64_t* out_ticket);
+/* Queues `count` surface heights at world points xz[2*count] (copied before
+ * the call returns): ocean_height_at plus, with a field,
+ * ocean_interaction_height_at, as WaterSurface::height_at. A query sees every
+ * update submitted to its session before it and none after. `heights` (count
+ * floats of host memory) is written when the ticket completes and must stay
+ * valid until then. */
+OCEAN_API ocean_status ocean_server_submit_query(ocean_server* server, uint64_t session,
+                                                 const float* xz, uint32_t count,
+                                                 float* heights, uint64_t* out_ticket);
+
+/* Waits up to timeout_ms for a ticket: OCEAN_OK once its result is written,
+ * OCEAN_ERROR_TIMEOUT while it is still pending, OCEAN_ERROR_DEVICE if its
+ * batch failed, OCEAN_ERROR_INVALID_ARG for a ticket never issued. */
+OCEAN_API ocean_status ocean_server_wait(ocean_server* server, uint64_t ticket, uint32_t timeout_ms);
+/* Waits up to timeout_ms for every request submitted so far. */
+OCEAN_API ocean_status ocean_server_drain(ocean_server* server, uint32_t timeout_ms);
+
+/* Copies a session's current state to host memory after waiting for every
+ * request submitted to it: ocean displacement and normal (N*N*4 floats
+ * each) and the field output (M*M*4 floats); any pointer may be NULL. */
+OCEAN_API ocean_status ocean_server_read_session(ocean_server* server, uint64_t session,
+                                                 float* displacement, float* normal,
+                                                 float* field);
+
+OCEAN_API ocean_status ocean_server_get_stats(ocean_server* server, ocean_server_stats* out);
+/* Clears latencies and counters (not the session counts or bytes). */
+OCEAN_API ocean_status ocean_server_reset_stats(ocean_server* server);
+
 /* Per-kernel device time of the frame passes, from CUDA events recorded on
  * the launching stream around every launch while profiling is on. */
 typedef struct ocean_pass_profile {

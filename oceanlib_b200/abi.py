@@ -172,8 +172,55 @@ class PassProfile(C.Structure):
     ]
 
 
+class ServerDescC(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_size_t),
+        ("hbm_budget", C.c_uint64),
+        ("max_inflight", C.c_uint32),
+        ("max_batch_requests", C.c_uint32),
+        ("max_batch_points", C.c_uint32),
+        ("max_query_points", C.c_uint32),
+        ("fft_form", C.c_int32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+OCEAN_SESSION_WAITING = 0
+OCEAN_SESSION_ACTIVE = 1
+OCEAN_SESSION_CLOSED = 2
+
+
+class ServerStatsC(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in (
+        "sessions_active", "sessions_waiting", "sessions_closed", "bytes_in_use", "hbm_budget",
+        "requests_submitted", "requests_completed", "requests_failed", "updates_completed",
+        "queries_completed", "query_points_completed", "batches", "kernel_launches",
+        "bytes_staging")] + \
+        [(n, C.c_double) for n in (
+            "mean_batch_requests", "latency_p50_ms", "latency_p99_ms", "latency_max_ms",
+            "update_p50_ms", "update_p99_ms", "query_p50_ms", "query_p99_ms", "gpu_busy_ms",
+            "wall_ms")]
+
+
 # Every function include/ocean_b200.h declares, with its ctypes signature.
 SIGNATURES = {
+    "ocean_server_desc_init": (None, [C.POINTER(ServerDescC)]),
+    "ocean_server_create": (C.c_void_p, [C.POINTER(ServerDescC), C.POINTER(C.c_int)]),
+    "ocean_server_destroy": (None, [C.c_void_p]),
+    "ocean_server_session_bytes": (C.c_uint64, [C.POINTER(OceanDescC), C.POINTER(InteractionDescC)]),
+    "ocean_server_open_session": (C.c_int, [C.c_void_p, C.POINTER(OceanDescC), C.POINTER(InteractionDescC),
+                                            C.POINTER(C.c_uint64)]),
+    "ocean_server_close_session": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "ocean_server_session_state": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "ocean_server_submit_update": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double, C.c_float, C.c_void_p,
+                                             C.c_uint32, C.POINTER(C.c_uint64)]),
+    "ocean_server_submit_query": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint32, C.c_void_p,
+                                            C.POINTER(C.c_uint64)]),
+    "ocean_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint32]),
+    "ocean_server_drain": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "ocean_server_read_session": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ocean_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStatsC)]),
+    "ocean_server_reset_stats": (C.c_int, [C.c_void_p]),
     "ocean_status_string": (C.c_char_p, [C.c_int]),
     "ocean_desc_init": (None, [C.POINTER(OceanDescC)]),
     "ocean_create": (C.c_void_p, [C.POINTER(OceanDescC), C.POINTER(C.c_int)]),

@@ -20,6 +20,7 @@
 // reference stores separately (src/core/spectrum.cpp:329-338) - is read from
 // the other row already in shared memory, so h0 is read from HBM once.
 #include "ocean_device.cuh"
+#include "query_device.cuh"
 #include "spectrum.h"
 
 namespace ocean_b200 {
@@ -59,11 +60,23 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     float2* data = smem;                      // [RP*2*NF][SEQ]
     float2* h0s = data + RP * 2 * NF * SEQ;   // [RP*2][N]
 
-    const OceanConsts cst = a.consts[ocean];
+    OceanConsts cst;
+    const float2* geom;
+    const float* kvec;
+    const float2* h0;
+    if (a.table != nullptr) {
+        const OceanSlot& s = a.table[ocean];
+        cst = s.cst;
+        geom = s.omega_kinv;
+        kvec = s.kvec;
+        h0 = s.h0;
+    } else {
+        cst = a.consts[ocean];
+        geom = a.omega_kinv + static_cast<size_t>(cst.geom) * N * N;
+        kvec = a.kvec + static_cast<size_t>(cst.geom) * N;
+        h0 = a.h0 + static_cast<size_t>(ocean) * N * N;
+    }
     const double top = a.t_over_2pi[ocean];
-    const float2* geom = a.omega_kinv + static_cast<size_t>(cst.geom) * N * N;
-    const float* kvec = a.kvec + static_cast<size_t>(cst.geom) * N;
-    const float2* h0 = a.h0 + static_cast<size_t>(ocean) * N * N;
 
     // Rows handled by pair slot j: (p, N-p), or (0, N/2) for p = 0.
     auto row_of = [&](int j, int r) -> int {
@@ -230,9 +243,24 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);
     __syncthreads();
 
-    const OceanConsts cst = a.consts[ocean];
-    const float lambda = cst.lambda;
     const size_t base = static_cast<size_t>(ocean) * N * N;
+    OceanConsts cst;
+    float4* out_disp;
+    float4* out_normal;
+    float4* out_vel;
+    if (a.table != nullptr) {
+        const OceanSlot& s = a.table[ocean];
+        cst = s.cst;
+        out_disp = s.disp;
+        out_normal = s.normal;
+        out_vel = s.velocity;
+    } else {
+        cst = a.consts[ocean];
+        out_disp = a.disp + base;
+        out_normal = a.normal + base;
+        out_vel = a.velocity + base;
+    }
+    const float lambda = cst.lambda;
     for (int i = tid; i < N * W; i += NT) {
         const int y = i / W;
         const int w = i % W;
@@ -263,16 +291,16 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
         if (foam < 0.0f) foam = 0.0f;
         if (foam > 1.0f) foam = 1.0f;
 
-        const size_t idx = base + static_cast<size_t>(y) * N + x;
-        __stcs(&a.disp[idx], make_float4(disp_x, h, disp_z, foam));
-        __stcs(&a.normal[idx], make_float4(nx, ny, nz, jac));
+        const size_t idx = static_cast<size_t>(y) * N + x;
+        __stcs(&out_disp[idx], make_float4(disp_x, h, disp_z, foam));
+        __stcs(&out_normal[idx], make_float4(nx, ny, nz, jac));
         if constexpr (NF == 6) {
             const float2 f4 = data[(4 * W + w) * SEQ + sy];
             const float2 f5 = data[(5 * W + w) * SEQ + sy];
-            __stcs(&a.velocity[idx], make_float4(f4.x, f4.y, f5.x, 0.0f));
+            __stcs(&out_vel[idx], make_float4(f4.x, f4.y, f5.x, 0.0f));
             if constexpr (FOAM) {
                 const float* cur = a.foam_cur + base;
-                __stcs(&a.foam_next[idx],
+                __stcs(&a.foam_next[base + idx],
                        foam_cell(cur, N, x, y, f4.x, f5.x, foam, a.foam_dt, a.foam_decay,
                                  a.foam_gain, a.foam_scale, a.foam_drift_x, a.foam_drift_z,
                                  a.foam_inv_cell));
@@ -488,112 +516,9 @@ __global__ void foam_step_kernel(int n, int count, const float4* __restrict__ di
 }
 
 // ---------------------------------------------------------------------------
-// World queries (src/ocean.cpp:322-452)
+// World queries (src/ocean.cpp:322-452; sample_one in query_device.cuh)
 // ---------------------------------------------------------------------------
-struct Tap {
-    uint32_t i00, i10, i01, i11;
-    float w00, w10, w01, w11;
-};
-
-__device__ __forceinline__ uint32_t wrap_index(int i, int n)
-{
-    i %= n;
-    if (i < 0) i += n;
-    return static_cast<uint32_t>(i);
-}
-
-__device__ __forceinline__ Tap make_tap(float u, float v, int n, float inv_cell)
-{
-    const float gu = u * inv_cell;
-    const float gv = v * inv_cell;
-    const float fu = floorf(gu);
-    const float fv = floorf(gv);
-    const uint32_t x0 = wrap_index(__float2int_rz(fu), n);
-    const uint32_t z0 = wrap_index(__float2int_rz(fv), n);
-    const uint32_t x1 = (x0 + 1u) % static_cast<uint32_t>(n);
-    const uint32_t z1 = (z0 + 1u) % static_cast<uint32_t>(n);
-    const float tu = gu - fu;
-    const float tv = gv - fv;
-    Tap t;
-    t.i00 = z0 * n + x0;
-    t.i10 = z0 * n + x1;
-    t.i01 = z1 * n + x0;
-    t.i11 = z1 * n + x1;
-    t.w00 = (1.0f - tu) * (1.0f - tv);
-    t.w10 = tu * (1.0f - tv);
-    t.w01 = (1.0f - tu) * tv;
-    t.w11 = tu * tv;
-    return t;
-}
-
-struct Texels {
-    float4 a, b, c, d;
-};
-
-__device__ __forceinline__ Texels load_texels(const float4* __restrict__ buf, const Tap& t)
-{
-    return Texels{__ldg(&buf[t.i00]), __ldg(&buf[t.i10]), __ldg(&buf[t.i01]), __ldg(&buf[t.i11])};
-}
-
-// buf[i00+c]*w00 + buf[i10+c]*w10 + buf[i01+c]*w01 + buf[i11+c]*w11, in that order.
-#define OCEAN_FETCH(T, t, C) ((T).a.C * (t).w00 + (T).b.C * (t).w10 + (T).c.C * (t).w01 + (T).d.C * (t).w11)
-
-// One ocean's surface at world (x, z): `iters` fixed-point steps of the
-// displacement inversion (the reference takes 4, src/ocean.cpp:366), stopping
-// early once both parameter coordinates move by <= tol (tol = 0: never), then
-// the final bilinear taps and the renormalised normal.
-__device__ __forceinline__ SurfaceEx sample_one(int n, float inv_cell,
-                                                const float4* __restrict__ disp,
-                                                const float4* __restrict__ normal,
-                                                const float4* __restrict__ vel, float2 p,
-                                                int iters, float tol)
-{
-    float u = p.x, v = p.y;
-    for (int it = 0; it < iters; ++it) {
-        const Tap t = make_tap(u, v, n, inv_cell);
-        const Texels d = load_texels(disp, t);
-        const float un = p.x - OCEAN_FETCH(d, t, x);
-        const float vn = p.y - OCEAN_FETCH(d, t, z);
-        const bool done = tol > 0.0f && fabsf(un - u) <= tol && fabsf(vn - v) <= tol;
-        u = un;
-        v = vn;
-        if (done) break;
-    }
-    const Tap t = make_tap(u, v, n, inv_cell);
-    const Texels d = load_texels(disp, t);
-    SurfaceEx s;
-    s.offset_x = OCEAN_FETCH(d, t, x);
-    s.height = OCEAN_FETCH(d, t, y);
-    s.offset_z = OCEAN_FETCH(d, t, z);
-    s.foam = OCEAN_FETCH(d, t, w);
-    const Texels nm = load_texels(normal, t);
-    float nx = OCEAN_FETCH(nm, t, x);
-    float ny = OCEAN_FETCH(nm, t, y);
-    float nz = OCEAN_FETCH(nm, t, z);
-    const float len2 = nx * nx + ny * ny + nz * nz;
-    if (len2 > 0.0f) {
-        const float inv = 1.0f / sqrtf(len2);
-        nx *= inv;
-        ny *= inv;
-        nz *= inv;
-    } else {
-        nx = 0.0f;
-        ny = 1.0f;
-        nz = 0.0f;
-    }
-    s.normal_x = nx;
-    s.normal_y = ny;
-    s.normal_z = nz;
-    if (vel != nullptr) {
-        const Texels vv = load_texels(vel, t);
-        s.velocity_x = OCEAN_FETCH(vv, t, x);
-        s.velocity_y = OCEAN_FETCH(vv, t, y);
-        s.velocity_z = OCEAN_FETCH(vv, t, z);
-    } else {
-        s.velocity_x = s.velocity_y = s.velocity_z = 0.0f;
-    }
-    return s;
-}
+using qdev::sample_one;
 
 __global__ void sample_kernel(int n, float inv_cell, const float4* __restrict__ disp,
                               const float4* __restrict__ normal, const float4* __restrict__ vel,

@@ -10,6 +10,7 @@
 
 #include "../../include/ocean_b200.h"
 #include "host_util.h"
+#include "ocean_host.h"
 #include "spectrum.h"
 
 #include <cuda_runtime.h>
@@ -38,8 +39,11 @@ std::mutex g_level_mutex;
 std::string g_level_name = "sm_100a";
 std::atomic<int> g_form{OCEAN_FFT_EXACT};
 
+}  // namespace
+
 // ---------------------------------------------------------------------------
-// Descriptor handling (src/c_api.cpp:46-60, src/ocean.cpp:28-59)
+// Descriptor handling (src/c_api.cpp:46-60, src/ocean.cpp:28-59); shared with
+// the serving loop through ocean_host.h
 // ---------------------------------------------------------------------------
 void desc_defaults(ocean_desc* d)
 {
@@ -160,7 +164,7 @@ SpectrumParams spectrum_params(const ocean_desc& d)
     return p;
 }
 
-}  // namespace
+int current_form() { return g_form.load(); }
 
 // ---------------------------------------------------------------------------
 // Batch: `count` oceans of one size on one device.

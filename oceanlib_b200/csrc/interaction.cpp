@@ -10,6 +10,7 @@
 #include "../../include/ocean_b200.h"
 #include "host_util.h"
 #include "iwave.h"
+#include "iwave_host.h"
 #include "iwave_stencil.h"
 #include "spectrum.h"
 
@@ -21,74 +22,19 @@
 #include <vector>
 
 namespace ocean_b200 {
-namespace {
-
-bool pow2(uint32_t v) { return v != 0 && (v & (v - 1)) == 0; }
-
-void desc_defaults(ocean_interaction_desc* d)
-{
-    // include/ocean/interaction.hpp:64-139 (InteractionDesc defaults)
-    std::memset(d, 0, sizeof(*d));
-    d->struct_size = sizeof(ocean_interaction_desc);
-    d->size = 256;
-    d->extent = 64.0f;
-    d->kernel_radius = 6;
-    d->damping = 0.20f;
-    d->absorb_cells = 16;
-    d->fixed_dt = 0.0f;
-    d->max_substeps = 8;
-    d->max_sources = 64;
-    d->gravity = 9.81f;
-    d->water_depth = 0.0f;
-    d->obstruction = OCEAN_OBSTRUCTION_NEUMANN;
-}
-
-bool copy_desc(const ocean_interaction_desc* src, ocean_interaction_desc& dst)
-{
-    if (src == nullptr) return false;
-    if (src->struct_size == 0 || src->struct_size > sizeof(ocean_interaction_desc)) return false;
-    desc_defaults(&dst);
-    std::memcpy(&dst, src, src->struct_size);
-    dst.struct_size = sizeof(ocean_interaction_desc);
-    return true;
-}
-
-void validate(const ocean_interaction_desc& d)
-{
-    // src/interaction.cpp:439-476
-    if (!pow2(d.size) || d.size < 32 || d.size > 1024) throw std::invalid_argument("size");
-    if (!(d.extent > 0.0f)) throw std::invalid_argument("extent");
-    if (d.kernel_radius < 1 || d.kernel_radius > 12) throw std::invalid_argument("kernel_radius");
-    if (2 * d.kernel_radius >= d.size) throw std::invalid_argument("kernel_radius vs size");
-    if (!(d.damping >= 0.0f)) throw std::invalid_argument("damping");
-    if (d.absorb_cells * 2 >= d.size) throw std::invalid_argument("absorb_cells");
-    if (d.max_substeps < 1) throw std::invalid_argument("max_substeps");
-    if (d.max_sources < 1) throw std::invalid_argument("max_sources");
-    if (!(d.gravity > 0.0f)) throw std::invalid_argument("gravity");
-    if (d.fixed_dt < 0.0f) throw std::invalid_argument("fixed_dt");
-}
-
-}  // namespace
 
 class Interaction {
 public:
-    explicit Interaction(const ocean_interaction_desc& d) : desc_(d)
+    explicit Interaction(const ocean_interaction_desc& d) : desc_(d), setup_(iwave_setup(d))
     {
-        validate(d);
-        n_ = d.size;
-        p_ = d.kernel_radius;
-        cell_ = d.extent / static_cast<float>(d.size);
-        cells_ = static_cast<size_t>(n_) * n_;
-        stride_ = static_cast<int>((n_ + 2 * p_ + 15u) & ~15u);  // src/interaction.cpp:43-46
-        rows_ = n_ + 2 * p_;
-
-        stencil_ = build_iwave_stencil(p_, static_cast<double>(cell_), static_cast<double>(d.water_depth));
-        if (!stencil_.stable())
-            throw std::invalid_argument("interaction stencil has a negative symbol (unstable)");
-        dt_limit_ = static_cast<float>(2.0 / std::sqrt(static_cast<double>(d.gravity) * stencil_.max_symbol));
-        dt_ = (d.fixed_dt > 0.0f) ? d.fixed_dt : std::min(1.0f / 60.0f, 0.35f * dt_limit_);
-        if (d.fixed_dt > 0.0f && d.fixed_dt > dt_limit_)
-            throw std::invalid_argument("interaction fixed_dt exceeds the stability limit");
+        n_ = setup_.n;
+        p_ = setup_.p;
+        cell_ = setup_.cell;
+        cells_ = setup_.cells;
+        stride_ = setup_.stride;
+        rows_ = setup_.rows;
+        dt_limit_ = setup_.dt_limit;
+        dt_ = setup_.dt;
 
         check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
         const size_t plane = static_cast<size_t>(rows_) * stride_;
@@ -105,15 +51,13 @@ public:
         fields_ = DevBuf<IWaveField>(4);
         sources_dev_ = DevBuf<IWaveSource>(static_cast<size_t>(d.max_sources) * d.max_substeps);
         sources_host_ = HostBuf<IWaveSource>(static_cast<size_t>(d.max_sources) * d.max_substeps);
-        queue_.resize(d.max_sources);
-        first_.assign(static_cast<size_t>(d.max_substeps) + 1, 0);
+        queue_.reset(d.max_sources);
         solid_dev_ = DevBuf<uint32_t>(cells_);
         nearest_dev_ = DevBuf<uint32_t>(cells_);
         mask_.assign(cells_, 0);
-        taps_dev_ = DevBuf<float>(stencil_.taps.size());
-        std::memset(&taps_, 0, sizeof(taps_));
-        std::copy(stencil_.taps.begin(), stencil_.taps.end(), taps_.t);
-        check(cudaMemcpyAsync(taps_dev_.p, stencil_.taps.data(), stencil_.taps.size() * sizeof(float),
+        const std::vector<float>& taps = setup_.stencil.taps;
+        taps_dev_ = DevBuf<float>(taps.size());
+        check(cudaMemcpyAsync(taps_dev_.p, taps.data(), taps.size() * sizeof(float),
                               cudaMemcpyHostToDevice, stream_), "taps");
         build_damping();
         upload_fields();
@@ -133,54 +77,23 @@ public:
         }
     }
 
-    void add(const ocean_disturbance& d)
-    {
-        if (queue_count_ >= desc_.max_sources) {
-            ++dropped_;
-            return;
-        }
-        queue_[queue_count_++] = d;
-    }
+    void add(const ocean_disturbance& d) { queue_.add(d); }
 
     // InteractionField::update (src/interaction.cpp:531-587).
     void update(float dt)
     {
         moved_ = false;
-        if (!(dt > 0.0f)) dt = 0.0f;
-        accum_ += static_cast<double>(dt);
-        uint32_t steps = 0;
-        if (accum_ >= dt_) steps = static_cast<uint32_t>(accum_ / static_cast<double>(dt_));
-        clamped_ = steps > desc_.max_substeps;
-        if (clamped_) {
-            steps = desc_.max_substeps;
-            accum_ = 0.0;
-        } else {
-            accum_ -= static_cast<double>(steps) * static_cast<double>(dt_);
-        }
-        last_steps_ = steps;
+        const uint32_t steps = clock_.advance(dt, dt_, desc_.max_substeps);
         if (steps == 0) {
-            uint32_t keep = 0;
-            for (uint32_t i = 0; i < queue_count_; ++i)
-                if (queue_[i].kind == OCEAN_SOURCE_IMPULSE) queue_[keep++] = queue_[i];
-            queue_count_ = keep;
+            queue_.keep_impulses();
             return;
         }
         // Resolve every substep's sources first (one upload), then run.
         std::vector<uint32_t>& first = first_;
-        uint32_t total = 0;
-        for (uint32_t s = 0; s < steps; ++s) {
-            first[s] = total;
-            const float sub_time = static_cast<float>(s) * dt_;
-            for (uint32_t i = 0; i < queue_count_; ++i) {
-                const ocean_disturbance& d = queue_[i];
-                const bool impulse = d.kind != OCEAN_SOURCE_CONTINUOUS;
-                if (impulse && s != 0) continue;
-                IWaveSource src;
-                if (resolve(d, impulse ? 0.0f : sub_time, impulse ? 1.0f : dt_, src))
-                    sources_host_.p[total++] = src;
-            }
-        }
-        first[steps] = total;
+        resolved_.clear();
+        queue_.resolve_all(steps, setup_, origin_x_, origin_z_, resolved_, first);
+        const uint32_t total = first[steps];
+        std::copy(resolved_.begin(), resolved_.end(), sources_host_.p);
         if (total > 0)
             check(cudaMemcpyAsync(sources_dev_.p, sources_host_.p, total * sizeof(IWaveSource),
                                   cudaMemcpyHostToDevice, stream_), "sources");
@@ -192,7 +105,6 @@ public:
             }
             substep();
         }
-        queue_count_ = 0;
         finalize();
         refresh_host();
     }
@@ -320,12 +232,12 @@ public:
     float origin_wz() const { return static_cast<float>(origin_z_) * cell_; }
     float fixed_dt() const { return dt_; }
     float dt_limit() const { return dt_limit_; }
-    float dispersion_error() const { return static_cast<float>(stencil_.peak_relative_error); }
-    uint64_t dropped() const { return dropped_; }
-    uint32_t last_substeps() const { return last_steps_; }
-    bool last_clamped() const { return clamped_; }
+    float dispersion_error() const { return static_cast<float>(setup_.stencil.peak_relative_error); }
+    uint64_t dropped() const { return queue_.dropped; }
+    uint32_t last_substeps() const { return clock_.last_steps; }
+    bool last_clamped() const { return clock_.clamped; }
     bool moved() const { return moved_; }
-    const std::vector<float>& taps() const { return stencil_.taps; }
+    const std::vector<float>& taps() const { return setup_.stencil.taps; }
 
 private:
     float* interior(int b) const { return planes_[b].p + static_cast<size_t>(p_) * stride_ + p_; }
@@ -365,7 +277,7 @@ private:
         if (has_mask_ && solid_count_ > 0)
             check(launch_obstruction(field(), solid_dev_.p, nearest_dev_.p, solid_count_,
                                      desc_.obstruction == OCEAN_OBSTRUCTION_DIRICHLET, stream_), "obstruction");
-        check(launch_iwave_step(static_cast<int>(p_), fields_.p + which_, 1, static_cast<int>(n_), taps_, stream_),
+        check(launch_iwave_step(static_cast<int>(p_), fields_.p + which_, 1, static_cast<int>(n_), setup_.taps, stream_),
               "iwave step");
         std::swap(cur_, old_);
         which_ ^= 1;
@@ -390,53 +302,11 @@ private:
     // as the reference.
     void build_damping()
     {
-        const float a0 = desc_.damping;
-        const int w = static_cast<int>(desc_.absorb_cells);
-        const float a_edge = 4.0f / std::max(dt_ * static_cast<float>(std::max(w, 1)), 1e-6f);
-        std::vector<float> c1(cells_), c2(cells_);
-        for (uint32_t z = 0; z < n_; ++z)
-            for (uint32_t x = 0; x < n_; ++x) {
-                const int dx = std::min<int>(static_cast<int>(x), static_cast<int>(n_ - 1 - x));
-                const int dz = std::min<int>(static_cast<int>(z), static_cast<int>(n_ - 1 - z));
-                const int d = std::min(dx, dz);
-                float alpha = a0;
-                if (w > 0 && d < w) {
-                    const float t = static_cast<float>(w - d) / static_cast<float>(w);
-                    alpha += a_edge * t * t;
-                }
-                const float ad = alpha * dt_;
-                const size_t i = static_cast<size_t>(z) * n_ + x;
-                c1[i] = 1.0f / (1.0f + ad);
-                c2[i] = 1.0f - ad;
-            }
+        std::vector<float> c1, c2;
+        iwave_damping(desc_, setup_, c1, c2);
         check(cudaMemcpyAsync(c1_.p, c1.data(), cells_ * sizeof(float), cudaMemcpyHostToDevice, stream_), "damping");
         check(cudaMemcpyAsync(c2_.p, c2.data(), cells_ * sizeof(float), cudaMemcpyHostToDevice, stream_), "damping");
         check(cudaStreamSynchronize(stream_), "damping");
-    }
-
-    // Resolve a disturbance to grid units (src/interaction.cpp:322-356);
-    // returns false when its clipped box is empty.
-    bool resolve(const ocean_disturbance& d, float sub_time, float scale, IWaveSource& s) const
-    {
-        const float sigma = std::max(d.radius, 0.25f * cell_);
-        s.inv_two_sigma2 = 1.0f / (2.0f * sigma * sigma);
-        const float wx = d.world_x + d.velocity_x * sub_time;
-        const float wz = d.world_z + d.velocity_z * sub_time;
-        s.gx = (wx - static_cast<float>(origin_x_) * cell_) / cell_;
-        s.gz = (wz - static_cast<float>(origin_z_) * cell_) / cell_;
-        const int rad = static_cast<int>(std::ceil(4.0f * sigma / cell_));
-        const int n = static_cast<int>(n_);
-        s.x0 = std::max(0, static_cast<int>(std::floor(s.gx)) - rad);
-        s.x1 = std::min(n - 1, static_cast<int>(std::floor(s.gx)) + rad);
-        s.z0 = std::max(0, static_cast<int>(std::floor(s.gz)) - rad);
-        s.z1 = std::min(n - 1, static_cast<int>(std::floor(s.gz)) + rad);
-        if (s.x1 < s.x0 || s.z1 < s.z0) return false;
-        s.cell = cell_;
-        s.disp = -d.strength * scale;
-        s.vel = d.velocity_y * scale;
-        s.dt = dt_;
-        s.mean = 0.0f;
-        return true;
     }
 
     // Multi-source BFS from every fluid cell (src/interaction.cpp:255-292).
@@ -493,12 +363,11 @@ private:
     }
 
     ocean_interaction_desc desc_;
+    IWaveSetup setup_;
     uint32_t n_ = 0, p_ = 0, rows_ = 0;
     int stride_ = 0;
     size_t cells_ = 0;
     float cell_ = 0.0f, dt_ = 0.0f, dt_limit_ = 0.0f;
-    IWaveStencil stencil_;
-    IWaveTaps taps_;
     cudaStream_t stream_ = nullptr;
     DevBuf<float> planes_[4];
     int cur_ = 0, old_ = 1, which_ = 0;
@@ -508,13 +377,10 @@ private:
     DevBuf<IWaveField> fields_;
     DevBuf<IWaveSource> sources_dev_;
     HostBuf<IWaveSource> sources_host_;
-    std::vector<ocean_disturbance> queue_;
+    IWaveQueue queue_;
+    IWaveClock clock_;
+    std::vector<IWaveSource> resolved_;
     std::vector<uint32_t> first_;
-    uint32_t queue_count_ = 0;
-    uint64_t dropped_ = 0;
-    double accum_ = 0.0;
-    uint32_t last_steps_ = 0;
-    bool clamped_ = false;
     int32_t origin_x_ = 0, origin_z_ = 0, shift_x_ = 0, shift_z_ = 0;
     bool moved_ = false;
     std::vector<uint8_t> mask_;
@@ -541,7 +407,7 @@ extern "C" {
 
 void ocean_interaction_desc_init(ocean_interaction_desc* desc)
 {
-    if (desc != nullptr) ocean_b200::desc_defaults(desc);
+    if (desc != nullptr) ocean_b200::interaction_desc_defaults(desc);
 }
 
 ocean_interaction* ocean_interaction_create(const ocean_interaction_desc* desc, ocean_status* out_status)
@@ -549,7 +415,7 @@ ocean_interaction* ocean_interaction_create(const ocean_interaction_desc* desc, 
     ocean_interaction* f = nullptr;
     ocean_interaction_desc resolved;
     ocean_status st = OCEAN_OK;
-    if (!ocean_b200::copy_desc(desc, resolved)) {
+    if (!ocean_b200::copy_interaction_desc(desc, resolved)) {
         st = OCEAN_ERROR_INVALID_ARG;
     } else {
         st = guarded([&] { f = new ocean_interaction(resolved); });

@@ -19,6 +19,7 @@
 // After the substeps, finalize writes (eta, d/dx, d/dz, d/dt)
 // (src/core/iwave_step.cpp:93-124). Compiled with -fmad=false.
 #include "iwave.h"
+#include "query_device.cuh"
 
 namespace ocean_b200 {
 namespace {
@@ -137,25 +138,85 @@ __global__ void source_mean_kernel(IWaveSource* __restrict__ src, int count)
         s.mean = static_cast<float>(part[0] / (static_cast<double>(wx) * static_cast<double>(wz)));
 }
 
-// Adds every source, in submission order, to each cell it covers.
+// Adds every source, in submission order, to cell (x, z) of one field.
+// One source's contribution to both time levels of a cell it covers.
+__device__ __forceinline__ void apply_source(const IWaveSource& s, int x, int z, float& cur, float& old,
+                                             bool& touched)
+{
+    if (x < s.x0 || x > s.x1 || z < s.z0 || z > s.z1) return;
+    const float sh = ricker(stamp_r2(s, x, z), s.inv_two_sigma2) - s.mean;
+    const float dd = s.disp * sh;
+    const float dv = s.vel * sh;
+    cur += dd;
+    old += dd - dv * s.dt;
+    touched = true;
+}
+
+__device__ __forceinline__ void apply_sources_cell(const IWaveField& f, const IWaveSource* __restrict__ src,
+                                                   int count, int x, int z)
+{
+    const ptrdiff_t ci = static_cast<ptrdiff_t>(z) * f.stride + x;
+    float cur = f.cur[ci];
+    float old = f.old[ci];
+    bool touched = false;
+    for (int k = 0; k < count; ++k) apply_source(src[k], x, z, cur, old, touched);
+    if (touched) {
+        f.cur[ci] = cur;
+        f.old[ci] = old;
+    }
+}
+
 __global__ void source_apply_kernel(IWaveField f, const IWaveSource* __restrict__ src, int count)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int z = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= f.n || z >= f.n) return;
+    apply_sources_cell(f, src, count, x, z);
+}
+
+// Many fields at once (blockIdx.z = field; block 32 x 8 cells): field k
+// takes sources [ranges[k].x, ranges[k].x + ranges[k].y). Warp 0 culls the
+// sources against the block's tile 32 at a time, compacting the hits in
+// submission order (ballot + prefix popcount), so each cell still adds its
+// sources in the reference's order but visits only those near its tile.
+__global__ void __launch_bounds__(256)
+source_apply_batch_kernel(const IWaveField* __restrict__ fields, const int2* __restrict__ ranges,
+                          const IWaveSource* __restrict__ src)
+{
+    const IWaveField f = fields[blockIdx.z];
+    const int2 r = ranges[blockIdx.z];
+    const int bx0 = blockIdx.x * 32, bz0 = blockIdx.y * 8;
+    if (bx0 >= f.n || bz0 >= f.n || r.y == 0) return;  // uniform per block
+    const int bx1 = min(bx0 + 32, f.n) - 1, bz1 = min(bz0 + 8, f.n) - 1;
+    const IWaveSource* s0 = src + r.x;
+    __shared__ int hit[32];
+    __shared__ int nhit;
+    const int x = bx0 + threadIdx.x, z = bz0 + threadIdx.y;
+    const bool in = x < f.n && z < f.n;
     const ptrdiff_t ci = static_cast<ptrdiff_t>(z) * f.stride + x;
-    float cur = f.cur[ci];
-    float old = f.old[ci];
+    float cur = 0.0f, old = 0.0f;
+    if (in) {
+        cur = f.cur[ci];
+        old = f.old[ci];
+    }
     bool touched = false;
-    for (int k = 0; k < count; ++k) {
-        const IWaveSource& s = src[k];
-        if (x < s.x0 || x > s.x1 || z < s.z0 || z > s.z1) continue;
-        const float sh = ricker(stamp_r2(s, x, z), s.inv_two_sigma2) - s.mean;
-        const float dd = s.disp * sh;
-        const float dv = s.vel * sh;
-        cur += dd;
-        old += dd - dv * s.dt;
-        touched = true;
+    for (int c0 = 0; c0 < r.y; c0 += 32) {
+        if (threadIdx.y == 0) {
+            const int k = c0 + threadIdx.x;
+            bool overlap = false;
+            if (k < r.y) {
+                const IWaveSource& s = s0[k];
+                overlap = !(s.x1 < bx0 || s.x0 > bx1 || s.z1 < bz0 || s.z0 > bz1);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, overlap);
+            if (overlap) hit[__popc(m & ((1u << threadIdx.x) - 1u))] = k;
+            if (threadIdx.x == 0) nhit = __popc(m);
+        }
+        __syncthreads();
+        const int nh = nhit;
+        if (in)
+            for (int j = 0; j < nh; ++j) apply_source(s0[hit[j]], x, z, cur, old, touched);
+        __syncthreads();
     }
     if (touched) {
         f.cur[ci] = cur;
@@ -195,31 +256,7 @@ __global__ void shift_kernel(const float* __restrict__ src, float* __restrict__ 
     dst[static_cast<ptrdiff_t>(z) * stride + x] = v;
 }
 
-// Bilinear, zero outside the grid (src/interaction.cpp:729-770).
-__device__ __forceinline__ float4 interaction_tap(const float4* __restrict__ out, int n, float cell,
-                                                  float origin_x, float origin_z, float wx, float wz,
-                                                  bool& inside)
-{
-    const float gx = (wx - origin_x) / cell - 0.5f;
-    const float gz = (wz - origin_z) / cell - 0.5f;
-    inside = !(gx < 0.0f || gz < 0.0f || gx >= static_cast<float>(n - 1) ||
-               gz >= static_cast<float>(n - 1));
-    if (!inside) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const int x0 = static_cast<int>(gx);
-    const int z0 = static_cast<int>(gz);
-    const float tx = gx - static_cast<float>(x0);
-    const float tz = gz - static_cast<float>(z0);
-    const size_t i00 = static_cast<size_t>(z0) * n + x0;
-    const float4 a = out[i00], b = out[i00 + 1], c = out[i00 + n], d = out[i00 + n + 1];
-    const float w00 = (1.0f - tx) * (1.0f - tz);
-    const float w10 = tx * (1.0f - tz);
-    const float w01 = (1.0f - tx) * tz;
-    const float w11 = tx * tz;
-    return make_float4(a.x * w00 + b.x * w10 + c.x * w01 + d.x * w11,
-                       a.y * w00 + b.y * w10 + c.y * w01 + d.y * w11,
-                       a.z * w00 + b.z * w10 + c.z * w01 + d.z * w11,
-                       a.w * w00 + b.w * w10 + c.w * w01 + d.w * w11);
-}
+using qdev::interaction_tap;  // bilinear, zero outside the grid (query_device.cuh)
 
 __global__ void interaction_sample_kernel(const float4* __restrict__ out, int n, float cell,
                                           float origin_x, float origin_z,
@@ -349,6 +386,16 @@ cudaError_t launch_source_apply(const IWaveField& f, const IWaveSource* sources,
     dim3 block(32, 8);
     dim3 grid((f.n + 31) / 32, (f.n + 7) / 8);
     source_apply_kernel<<<grid, block, 0, st>>>(f, sources, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_source_apply_batch(const IWaveField* fields, const int2* ranges,
+                                      const IWaveSource* sources, int count, int max_n, cudaStream_t st)
+{
+    if (count == 0) return cudaSuccess;
+    dim3 block(32, 8);
+    dim3 grid((max_n + 31) / 32, (max_n + 7) / 8, count);
+    source_apply_batch_kernel<<<grid, block, 0, st>>>(fields, ranges, sources);
     return cudaGetLastError();
 }
 

@@ -47,6 +47,10 @@ cudaError_t launch_iwave_finalize(const IWaveField* fields, int count, int max_n
 cudaError_t launch_source_mean(IWaveSource* sources, int count, cudaStream_t st);
 cudaError_t launch_source_apply(const IWaveField& f, const IWaveSource* sources, int count,
                                 cudaStream_t st);
+// `count` fields at once; field k adds sources [ranges[k].x, +ranges[k].y)
+// (ranges on the device, means already filled).
+cudaError_t launch_source_apply_batch(const IWaveField* fields, const int2* ranges,
+                                      const IWaveSource* sources, int count, int max_n, cudaStream_t st);
 cudaError_t launch_obstruction(const IWaveField& f, const uint32_t* solid, const uint32_t* nearest,
                                uint32_t count, bool dirichlet, cudaStream_t st);
 cudaError_t launch_shift(const float* src, float* dst, int n, int stride, int dx, int dz,

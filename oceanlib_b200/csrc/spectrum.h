@@ -28,6 +28,18 @@ struct OceanConsts {
     int32_t geom;         // index of the ocean's (omega, 1/|k|) table
 };
 
+// One ocean's own buffers, for frames over oceans that do not live in one
+// batch array (the serving loop's sessions, each allocated on admission).
+struct OceanSlot {
+    const float2* h0;          // [N*N]
+    const float2* omega_kinv;  // [N*N]
+    const float* kvec;         // [N]
+    float4* disp;              // [N*N]
+    float4* normal;            // [N*N]
+    float4* velocity;          // [N*N] or null
+    OceanConsts cst;           // geom unused
+};
+
 // One frame's worth of device pointers for a batch of same-N oceans.
 struct FrameArgs {
     const float2* h0;          // [count][N*N]
@@ -47,6 +59,10 @@ struct FrameArgs {
     float foam_inv_cell;       // 1 / (patch_length / N); per batch (same L)
     int32_t ocean_base;        // first ocean of this chunk
     int32_t chunk;             // oceans in this chunk
+    // When set, ocean i of the frame is table[i] (h0, geometry, outputs and
+    // constants) and the batch arrays above are unused, except t_over_2pi
+    // (indexed by i) and the intermediate. No persistent foam in this form.
+    const OceanSlot* table;
 };
 
 // Work queue of the persistent frame kernel. `ticket`, `rows_done[count]` and

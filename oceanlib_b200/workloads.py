@@ -129,3 +129,93 @@ def ensemble_64(count: int = 64) -> List[OceanDesc]:
                              wind_direction=2.0 * math.pi * u_d, choppiness=0.5 + 1.3 * u_c,
                              seed=1000 + i))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Serving loop: sessions, moving sources, Poisson arrivals
+# ---------------------------------------------------------------------------
+SERVE_DT = 1.0 / 60.0
+SERVE_FIELD_EXTENT = 64.0
+
+
+def serving_sessions(count: int = 256):
+    """`count` sessions from PCG32(5, 0): ocean N from {128, 256, 512} (the
+    other ocean fields at their defaults, seed 5000 + i), each with a 512^2
+    interaction field over 64 m with a radius-6 stencil. Returns
+    (ocean descriptors, interaction descriptor)."""
+    from .interaction import InteractionDesc
+
+    r = Pcg32(5, 0)
+    sizes = (128, 256, 512)
+    oceans = [OceanDesc(size=sizes[r.next_u32() % 3], seed=5000 + i) for i in range(count)]
+    field = InteractionDesc(size=512, extent=SERVE_FIELD_EXTENT, kernel_radius=6)
+    return oceans, field
+
+
+class DiscPaths:
+    """`per_session` continuous disc sources per session on seeded random-walk
+    paths: radius U(0.5, 4) m, speed U(0, 8) m/s, heading turning by
+    U(-0.4, 0.4) rad per frame, reflected off an 8 m margin inside the field.
+    `frame(s)` returns session s's sources for its next update (positions at
+    the frame start, velocities for the substep motion) and advances them."""
+
+    def __init__(self, sessions: int, per_session: int = 32, seed: int = 17,
+                 extent: float = SERVE_FIELD_EXTENT, dt: float = SERVE_DT):
+        from .serve import DISTURBANCE_DTYPE
+
+        rng = np.random.default_rng(seed)
+        shape = (sessions, per_session)
+        self.dt = dt
+        self.lo, self.hi = 8.0, extent - 8.0
+        self.x = rng.uniform(self.lo, self.hi, shape)
+        self.z = rng.uniform(self.lo, self.hi, shape)
+        self.radius = rng.uniform(0.5, 4.0, shape)
+        self.speed = rng.uniform(0.0, 8.0, shape)
+        self.heading = rng.uniform(0.0, 2.0 * math.pi, shape)
+        self.strength = rng.uniform(0.05, 0.4, shape)
+        self.turn = np.random.default_rng(seed + 1)
+        self.dtype = DISTURBANCE_DTYPE
+
+    def frame(self, s: int) -> np.ndarray:
+        vx = self.speed[s] * np.cos(self.heading[s])
+        vz = self.speed[s] * np.sin(self.heading[s])
+        out = np.zeros(self.x.shape[1], self.dtype)
+        out["world_x"] = self.x[s]
+        out["world_z"] = self.z[s]
+        out["radius"] = self.radius[s]
+        out["strength"] = self.strength[s]
+        out["velocity_x"] = vx
+        out["velocity_z"] = vz
+        out["kind"] = 1  # continuous
+        # advance: move, reflect at the margin, turn
+        x = self.x[s] + vx * self.dt
+        z = self.z[s] + vz * self.dt
+        hx = (x < self.lo) | (x > self.hi)
+        hz = (z < self.lo) | (z > self.hi)
+        h = self.heading[s]
+        h = np.where(hx, math.pi - h, h)
+        h = np.where(hz, -h, h)
+        self.x[s] = np.clip(x, self.lo, self.hi)
+        self.z[s] = np.clip(z, self.lo, self.hi)
+        self.heading[s] = h + self.turn.uniform(-0.4, 0.4, h.shape)
+        return out
+
+
+def serving_points(sets: int = 16, count: int = 4096, seed: int = 23,
+                   extent: float = SERVE_FIELD_EXTENT) -> np.ndarray:
+    """`sets` seeded (count, 2) float32 point sets uniform over the field."""
+    rng = np.random.default_rng(seed)
+    return rng.uniform(0.0, extent, (sets, count, 2)).astype(np.float32)
+
+
+def poisson_arrivals(sessions: int, rate: float, duration: float, p_update: float = 0.5,
+                     seed: int = 29):
+    """A Poisson process of mean `rate` requests/s over `duration` s: sorted
+    arrival times, the session of each, and whether it is an update (else a
+    height query)."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.poisson(rate * duration))
+    times = np.sort(rng.uniform(0.0, duration, n))
+    sess = rng.integers(0, sessions, n)
+    upd = rng.random(n) < p_update
+    return times, sess, upd
