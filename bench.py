@@ -408,6 +408,102 @@ def bench_iwave_reference(updates: int = 20):
             "threads": int(O.ref().oref_hardware_concurrency())}
 
 
+def _serve_script(paths, sess, upd, pts, frames):
+    """Pre-built requests (session, frame number or 0, sources or None,
+    points or None); `frames` holds each session's last frame and advances."""
+    out = []
+    for i, (s, u) in enumerate(zip(sess.tolist(), upd.tolist())):
+        if u:
+            frames[s] += 1
+            out.append((s, frames[s], paths.frame(s), None))
+        else:
+            out.append((s, 0, None, pts[i % len(pts)]))
+    return out
+
+
+def _serve_run(srv, sids, script, times):
+    """Submits `script` at the arrival `times` (open loop; None = as fast as
+    possible), drains, returns the wall seconds from the first submission to
+    the last result."""
+    import numpy as np
+
+    from oceanlib_b200 import workloads as W
+
+    outs = [np.empty(4096, np.float32) for _ in range(256)]
+    t0 = time.perf_counter()
+    for i, (s, f, src, xz) in enumerate(script):
+        if times is not None:
+            while time.perf_counter() - t0 < times[i]:
+                pass
+        if src is not None:
+            srv.submit_update(sids[s], f * W.SERVE_DT, W.SERVE_DT, src)
+        else:
+            srv.submit_query(sids[s], xz, outs[i % 256])
+    srv.drain()
+    return time.perf_counter() - t0
+
+
+def bench_serving(rate: float = 20000.0, seconds: float = 3.0):
+    """The serving loop: 256 sessions (ocean N in {128, 256, 512}, a 512^2
+    interaction field with 32 moving disc sources each), update and
+    4096-point height requests arriving as a Poisson process of mean `rate`
+    per second, admitted under a 120 GB budget. Latency is submit -> result
+    in the caller's buffer (host clock), so it includes the uploads of the
+    sources and points and the download of the heights."""
+    from oceanlib_b200 import workloads as W
+    from oceanlib_b200.serve import OceanServer
+
+    oceans, field = W.serving_sessions(256)
+    srv = OceanServer(hbm_budget=120e9)
+    sids = [srv.open_session(o, field) for o in oceans]
+    pts = W.serving_points(sets=16)
+    frames = [0] * 256
+
+    paths = W.DiscPaths(256)
+
+    def run(duration, seed, paced=True):
+        times, sess, upd = W.poisson_arrivals(256, rate, duration, seed=seed)
+        script = _serve_script(paths, sess, upd, pts, frames)
+        srv.reset_stats()
+        wall = _serve_run(srv, sids, script, times if paced else None)
+        return wall, len(script), srv.stats()
+
+    run(1.0, 1)  # warm-up: admission, t = 0 frames, staging growth
+    wall, n, st = run(seconds, 2)
+    import numpy as np
+
+    _, lat, _ = srv.latency_samples()
+    p999 = float(np.quantile(lat, 0.999)) if len(lat) else 0.0
+    slow = int((lat > 10.0).sum())
+    cap_wall, cap_n, cap = run(seconds / 2, 3, paced=False)
+    out = {
+        "workload": "256 sessions (ocean N from {128,256,512} by PCG32(5,0); 512^2 iWave field, 64 m, "
+                    "P=6, 32 continuous disc sources on random-walk paths), Poisson arrivals, "
+                    "50% updates / 50% 4096-point height queries",
+        "offered_rps": n / seconds,
+        "achieved_rps": st["requests_completed"] / wall,
+        "latency_p50_ms": st["latency_p50_ms"],
+        "latency_p99_ms": st["latency_p99_ms"],
+        "latency_p999_ms": p999,
+        "latency_max_ms": st["latency_max_ms"],
+        "requests_over_10ms": slow,
+        "update_p50_ms": st["update_p50_ms"], "update_p99_ms": st["update_p99_ms"],
+        "query_p50_ms": st["query_p50_ms"], "query_p99_ms": st["query_p99_ms"],
+        "updates_per_s": st["updates_completed"] / wall,
+        "query_points_per_s": st["query_points_completed"] / wall,
+        "batches": st["batches"], "mean_batch_requests": st["mean_batch_requests"],
+        "gpu_busy_fraction": st["gpu_busy_ms"] / (1000.0 * wall),
+        "kernel_launches": st["kernel_launches"],
+        "sessions_active": st["sessions_active"], "bytes_in_use": st["bytes_in_use"],
+        "hbm_budget": st["hbm_budget"], "failed": st["requests_failed"],
+        "capacity_closed_loop_rps": cap["requests_completed"] / cap_wall,
+        "capacity_p99_ms": cap["latency_p99_ms"],
+        "capacity_mean_batch_requests": cap["mean_batch_requests"],
+    }
+    srv.close()
+    return out
+
+
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
@@ -567,7 +663,7 @@ def main():
         if not args.no_extra and world == 1:
             extra = {}
             for name, fn in (("cascade", lambda: bench_cascade(torch)), ("iwave", bench_iwave),
-                             ("ensemble", lambda: bench_ensemble(torch))):
+                             ("ensemble", lambda: bench_ensemble(torch)), ("serving", bench_serving)):
                 try:
                     extra[name] = fn()
                 except Exception as e:  # report, do not lose the headline line

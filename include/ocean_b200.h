@@ -599,6 +599,12 @@ OCEAN_API ocean_status ocean_server_read_session(ocean_server* server, uint64_t 
                                                  float* field);
 
 OCEAN_API ocean_status ocean_server_get_stats(ocean_server* server, ocean_server_stats* out);
+/* Per-request samples since the last reset, in completion order: for each,
+ * submit time (ms since the reset), latency (ms) and kind (0 update, 1
+ * query). Writes at most `capacity` of each; returns how many exist. */
+OCEAN_API uint64_t ocean_server_latency_samples(ocean_server* server, double* submit_ms,
+                                                double* latency_ms, int32_t* kind,
+                                                uint64_t capacity);
 /* Clears latencies and counters (not the session counts or bytes). */
 OCEAN_API ocean_status ocean_server_reset_stats(ocean_server* server);
 

@@ -221,6 +221,7 @@ SIGNATURES = {
     "ocean_server_read_session": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ocean_server_get_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerStatsC)]),
     "ocean_server_reset_stats": (C.c_int, [C.c_void_p]),
+    "ocean_server_latency_samples": (C.c_uint64, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64]),
     "ocean_status_string": (C.c_char_p, [C.c_int]),
     "ocean_desc_init": (None, [C.POINTER(OceanDescC)]),
     "ocean_create": (C.c_void_p, [C.POINTER(OceanDescC), C.POINTER(C.c_int)]),

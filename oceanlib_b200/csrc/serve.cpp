@@ -469,7 +469,20 @@ public:
         gpu_ms_ = 0.0;
         lat_update_.clear();
         lat_query_.clear();
+        samples_.clear();
         stats_t0_ = Clock::now();
+    }
+
+    uint64_t samples(double* submit_ms, double* latency_ms, int32_t* kind, uint64_t capacity)
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        const uint64_t n = std::min<uint64_t>(capacity, samples_.size());
+        for (uint64_t i = 0; i < n; ++i) {
+            if (submit_ms) submit_ms[i] = samples_[i].submit_ms;
+            if (latency_ms) latency_ms[i] = samples_[i].latency_ms;
+            if (kind) kind[i] = samples_[i].kind;
+        }
+        return samples_.size();
     }
 
     const ocean_server_desc& desc() const { return desc_; }
@@ -987,9 +1000,11 @@ private:
                 ++failed_count_;
             } else if (r->kind == Kind::Update) {
                 lat_update_.push_back(lat);
+                samples_.push_back({ms_between(stats_t0_, r->submitted), lat, 0});
                 ++updates_done_;
             } else if (r->kind == Kind::Query) {
                 lat_query_.push_back(lat);
+                samples_.push_back({ms_between(stats_t0_, r->submitted), lat, 1});
                 ++queries_done_;
                 points_done_ += r->xz.size();
             }
@@ -1150,6 +1165,11 @@ private:
     uint64_t batches_ = 0, kernels_ = 0, batched_requests_ = 0;
     double gpu_ms_ = 0.0;
     std::vector<double> lat_update_, lat_query_;
+    struct Sample {
+        double submit_ms, latency_ms;
+        int32_t kind;
+    };
+    std::vector<Sample> samples_;
     Clock::time_point stats_t0_;
 };
 
@@ -1286,6 +1306,13 @@ ocean_status ocean_server_get_stats(ocean_server* server, ocean_server_stats* ou
 {
     if (server == nullptr || out == nullptr) return OCEAN_ERROR_INVALID_ARG;
     return guarded([&] { server->impl.stats(out); });
+}
+
+uint64_t ocean_server_latency_samples(ocean_server* server, double* submit_ms, double* latency_ms, int32_t* kind,
+                                      uint64_t capacity)
+{
+    if (server == nullptr) return 0;
+    return server->impl.samples(submit_ms, latency_ms, kind, capacity);
 }
 
 ocean_status ocean_server_reset_stats(ocean_server* server)

@@ -149,5 +149,17 @@ class OceanServer:
         _check(lib().ocean_server_get_stats(self._h, C.byref(s)), "ocean_server_get_stats")
         return {k: getattr(s, k) for k, _ in ServerStatsC._fields_}
 
+    def latency_samples(self):
+        """(submit_ms, latency_ms, kind) arrays of every request completed since
+        the last reset (kind 0 = update, 1 = query)."""
+        n = int(lib().ocean_server_latency_samples(self._h, None, None, None, 0))
+        sub = np.empty(n, np.float64)
+        lat = np.empty(n, np.float64)
+        kind = np.empty(n, np.int32)
+        m = int(lib().ocean_server_latency_samples(self._h, sub.ctypes.data, lat.ctypes.data,
+                                                   kind.ctypes.data, n))
+        m = min(m, n)
+        return sub[:m], lat[:m], kind[:m]
+
     def reset_stats(self) -> None:
         _check(lib().ocean_server_reset_stats(self._h), "ocean_server_reset_stats")
