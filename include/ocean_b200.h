@@ -297,8 +297,17 @@ typedef struct ocean_device_buffers {
 typedef enum ocean_fft_form {
     OCEAN_FFT_EXACT = 0, /* radix-2 Stockham in the reference's operation order,
                             no FMA: bit-identical to the reference           */
-    OCEAN_FFT_FAST  = 1  /* same dataflow with fused multiply-adds           */
+    OCEAN_FFT_FAST  = 1, /* same dataflow with fused multiply-adds           */
+    OCEAN_FFT_TENSOR = 2 /* four-step DFT on the tensor cores (tcgen05), FP16
+                            hi + lo operands with FP32 accumulation; N = 512 */
 } ocean_fft_form;
+
+/* `count` unnormalised inverse DFTs (sign +, as src/core/fft.cpp) of
+ * complex sequences of length `size`, in the given form. `input` and
+ * `output` are DEVICE arrays of count * size interleaved (re, im) floats;
+ * the call waits for the result. For accuracy checks of the forms. */
+OCEAN_API ocean_status ocean_dft_batch(uint32_t size, uint32_t count, int32_t form, const float* input,
+                                       float* output, void* stream);
 
 /* Device pointers of a single ocean. */
 OCEAN_API ocean_status ocean_get_device_buffers(const ocean_sim* sim, ocean_device_buffers* out);

@@ -13,6 +13,7 @@ OCEAN_ERROR_TIMEOUT = 5
 
 OCEAN_FFT_EXACT = 0
 OCEAN_FFT_FAST = 1
+OCEAN_FFT_TENSOR = 2
 
 OCEAN_SCHEDULE_PERSISTENT = 0
 OCEAN_SCHEDULE_CHUNKED = 1
@@ -204,6 +205,7 @@ class ServerStatsC(C.Structure):
 
 # Every function include/ocean_b200.h declares, with its ctypes signature.
 SIGNATURES = {
+    "ocean_dft_batch": (C.c_int, [C.c_uint32, C.c_uint32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ocean_server_desc_init": (None, [C.POINTER(ServerDescC)]),
     "ocean_server_create": (C.c_void_p, [C.POINTER(ServerDescC), C.POINTER(C.c_int)]),
     "ocean_server_destroy": (None, [C.c_void_p]),

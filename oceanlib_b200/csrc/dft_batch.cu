@@ -1,0 +1,124 @@
+// oceanlib-b200: batched 1-D inverse DFTs of device sequences in each form
+// (ocean_dft_batch): the radix-2 Stockham FFT (exact, bit-identical to
+// src/core/fft.cpp), its fast variant, and the tensor-core DFT (tc_dft.cuh).
+// The frame kernel runs the same code on its rows and columns; this entry
+// point isolates the transform for accuracy checks against FP64.
+#include "ocean_device.cuh"
+#include "spectrum.h"
+#include "tc_dft.cuh"
+
+namespace ocean_b200 {
+namespace {
+
+constexpr int kSeqPad = 4;  // float2 between sequences in shared memory
+
+// CTAs take chunks of 8 sequences in turn (several engine calls per CTA).
+template <int LOG_N, bool FAST>
+__global__ void __launch_bounds__(8 * lanes_for(LOG_N))
+dft_fp32_kernel(const float2* __restrict__ in, float2* __restrict__ out, int count,
+                const float2* __restrict__ tw)
+{
+    constexpr int N = 1 << LOG_N, G = lanes_for(LOG_N), NT = 8 * G;
+    constexpr int SEQ = padded_len(N) + kSeqPad;
+    extern __shared__ float4 smem4[];
+    float2* data = reinterpret_cast<float2*>(smem4);
+    float2* tws = data + 8 * SEQ;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < N - 1; i += NT) tws[i] = tw[i];
+    for (int base = blockIdx.x * 8; base < count; base += gridDim.x * 8) {
+        const int k = min(8, count - base);
+        __syncthreads();
+        for (int i = tid; i < 8 * N; i += NT) {
+            const int s = i >> LOG_N, n = i & (N - 1);
+            data[s * SEQ + pad_idx(n)] = s < k ? in[static_cast<size_t>(base + s) * N + n] : make_float2(0.0f, 0.0f);
+        }
+        __syncthreads();
+        fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);
+        __syncthreads();
+        for (int i = tid; i < k * N; i += NT) {
+            const int s = i >> LOG_N, n = i & (N - 1);
+            out[static_cast<size_t>(base + s) * N + n] = data[s * SEQ + pad_idx(n)];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(tc::kThreads)
+dft_tc512_kernel(const float2* __restrict__ in, float2* __restrict__ out, int count,
+                 const float2* __restrict__ tw, unsigned* error)
+{
+    constexpr int N = 512, NT = tc::kThreads;
+    constexpr int SEQ = padded_len(N) + kSeqPad;
+    extern __shared__ float4 smem4[];
+    float2* data = reinterpret_cast<float2*>(smem4);
+    float2* tws = data + 8 * SEQ;
+    unsigned char* eng_smem = reinterpret_cast<unsigned char*>(smem4) +
+                              ((8 * SEQ + N) * sizeof(float2) + 127) / 128 * 128;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < N - 1; i += NT) tws[i] = tw[i];
+    tc::Engine eng{eng_smem, 0};
+    eng.init(tid, NT);
+    for (int base = blockIdx.x * 8; base < count; base += gridDim.x * 8) {
+        const int k = min(8, count - base);
+        __syncthreads();
+        for (int i = tid; i < k * N; i += NT) {
+            const int s = i >> 9, n = i & (N - 1);
+            data[s * SEQ + pad_idx(n)] = in[static_cast<size_t>(base + s) * N + n];
+        }
+        __syncthreads();
+        eng.dft512(data, SEQ, k, tws, tid, error);
+        for (int i = tid; i < k * N; i += NT) {
+            const int s = i >> 9, n = i & (N - 1);
+            out[static_cast<size_t>(base + s) * N + n] = data[s * SEQ + pad_idx(n)];
+        }
+    }
+    eng.release(tid);
+}
+
+template <int LOG_N>
+cudaError_t fp32_launch(bool fast, const float2* in, float2* out, int count, const float2* tw, int grid,
+                        cudaStream_t st)
+{
+    constexpr int N = 1 << LOG_N, G = lanes_for(LOG_N);
+    const size_t smem = (8 * (padded_len(N) + kSeqPad) + N) * sizeof(float2);
+    auto k = fast ? dft_fp32_kernel<LOG_N, true> : dft_fp32_kernel<LOG_N, false>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    k<<<grid, 8 * G, smem, st>>>(in, out, count, tw);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t tc_dft_smem_bytes()
+{
+    constexpr int N = 512;
+    return ((8 * (padded_len(N) + kSeqPad) + N) * sizeof(float2) + 127) / 128 * 128 + tc::kSmemBytes;
+}
+
+cudaError_t launch_dft_batch(int log_n, int form, const float2* in, float2* out, int count, const float2* tw,
+                             unsigned* error, int grid, cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    if (form == 2) {
+        if (log_n != 9) return cudaErrorInvalidValue;
+        const size_t smem = tc_dft_smem_bytes();
+        cudaError_t e = cudaFuncSetAttribute(dft_tc512_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+        dft_tc512_kernel<<<grid, tc::kThreads, smem, st>>>(in, out, count, tw, error);
+        return cudaGetLastError();
+    }
+    const bool fast = form == 1;
+    switch (log_n) {
+        case 4: return fp32_launch<4>(fast, in, out, count, tw, grid, st);
+        case 5: return fp32_launch<5>(fast, in, out, count, tw, grid, st);
+        case 6: return fp32_launch<6>(fast, in, out, count, tw, grid, st);
+        case 7: return fp32_launch<7>(fast, in, out, count, tw, grid, st);
+        case 8: return fp32_launch<8>(fast, in, out, count, tw, grid, st);
+        case 9: return fp32_launch<9>(fast, in, out, count, tw, grid, st);
+        case 10: return fp32_launch<10>(fast, in, out, count, tw, grid, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace ocean_b200

@@ -22,11 +22,29 @@
 #include "ocean_device.cuh"
 #include "query_device.cuh"
 #include "spectrum.h"
+#include "tc_dft.cuh"
 
 namespace ocean_b200 {
 namespace {
 
 constexpr int kPad = 4;  // float2 padding between sequences in shared memory
+
+// The inverse DFT of the COUNT sequences at data + s * SEQ: the radix-2
+// Stockham FFT (one lane group per sequence), or with TC the tensor-core
+// four-step DFT, 8 sequences per engine call (N = 512).
+template <int LOG_N, int G, bool FAST, bool TC, int COUNT, int SEQ>
+__device__ __forceinline__ void transform_all(float2* data, const float2* tws, int tid, tc::Engine* eng,
+                                              unsigned* error)
+{
+    if constexpr (TC) {
+        static_assert(LOG_N == 9, "the tensor-core form is built for N = 512");
+#pragma unroll 1
+        for (int s0 = 0; s0 < COUNT; s0 += tc::kSeq)
+            eng->dft512(data + s0 * SEQ, SEQ, COUNT - s0 < tc::kSeq ? COUNT - s0 : tc::kSeq, tws, tid, error);
+    } else {
+        fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);
+    }
+}
 
 template <int LOG_N>
 struct Shape {
@@ -48,10 +66,11 @@ struct Shape {
 // intermediate slot `inter_slot` (N*N*NF float2). `tws` already holds the
 // twiddles in shared memory.
 // ---------------------------------------------------------------------------
-template <int LOG_N, int NF, bool FAST>
+template <int LOG_N, int NF, bool FAST, bool TC = false>
 __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int group,
                                          float2* __restrict__ inter_slot, float2* smem,
-                                         const float2* tws, int tid)
+                                         const float2* tws, int tid, tc::Engine* eng = nullptr,
+                                         unsigned* error = nullptr)
 {
     using S = Shape<LOG_N>;
     constexpr int N = S::N, G = S::G, SEQ = S::SEQ, RP = S::RP;
@@ -148,7 +167,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     }
     __syncthreads();
 
-    fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);
+    transform_all<LOG_N, G, FAST, TC, RP * 2 * NF, SEQ>(data, tws, tid, eng, error);
     __syncthreads();
 
     // Write the rows cell-major: inter[row][x][f], NF/2 float4 per cell.
@@ -214,10 +233,11 @@ __device__ __forceinline__ float foam_cell(const float* cur, int n, int x, int z
 // (column FFTs + finalize + optional foam substep). CG loads read the
 // intermediate from L2: another CTA wrote it during this launch.
 // ---------------------------------------------------------------------------
-template <int LOG_N, int NF, bool FAST, bool FOAM, int W, bool CG>
+template <int LOG_N, int NF, bool FAST, bool FOAM, int W, bool CG, bool TC = false>
 __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int strip,
                                          const float2* __restrict__ inter_slot, float2* smem,
-                                         const float2* tws, int tid)
+                                         const float2* tws, int tid, tc::Engine* eng = nullptr,
+                                         unsigned* error = nullptr)
 {
     using S = Shape<LOG_N>;
     constexpr int N = S::N, G = S::G, SEQ = S::SEQ;
@@ -240,7 +260,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     }
     __syncthreads();
 
-    fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);
+    transform_all<LOG_N, G, FAST, TC, NF * W, SEQ>(data, tws, tid, eng, error);
     __syncthreads();
 
     const size_t base = static_cast<size_t>(ocean) * N * N;
@@ -393,16 +413,36 @@ __device__ bool wait_at_least(const unsigned* counter, unsigned target, unsigned
 
 // Resident CTAs the persistent kernel is compiled for: 768 threads per SM
 // (one CTA at N = 1024, whose 32 values per lane need the registers).
-template <int LOG_N, int NF>
+// (The tensor-core form needs about 150-170 KB of shared memory per CTA:
+// one CTA per SM, which also bounds its tensor memory to 256 columns.)
+template <int LOG_N, int NF, bool TC = false>
 constexpr int frame_min_blocks()
 {
     constexpr int nt = Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G;
+    if (TC) return 1;
     return LOG_N >= 10 ? 1 : (768 / nt < 1 ? 1 : (768 / nt > 16 ? 16 : 768 / nt));
 }
 
-template <int LOG_N, int NF, bool FAST, bool FOAM>
+// Shared floats (float2 units) of the persistent kernel's data area, and the
+// byte offset of the tensor-core engine's area behind the twiddles.
+template <int LOG_N, int NF>
+__host__ __device__ constexpr size_t frame_data_float2()
+{
+    using S = Shape<LOG_N>;
+    constexpr size_t row = S::RP * 2 * NF * S::SEQ + S::RP * 2 * S::N;
+    constexpr size_t col = NF * S::PW * S::SEQ;
+    return row > col ? row : col;
+}
+
+template <int LOG_N, int NF>
+__host__ __device__ constexpr size_t frame_engine_offset()
+{
+    return ((frame_data_float2<LOG_N, NF>() + (size_t(1) << LOG_N)) * sizeof(float2) + 127) / 128 * 128;
+}
+
+template <int LOG_N, int NF, bool FAST, bool FOAM, bool TC = false>
 __global__ void __launch_bounds__(Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G,
-                                  frame_min_blocks<LOG_N, NF>())
+                                  frame_min_blocks<LOG_N, NF, TC>())
 frame_kernel(FrameArgs a, QueueArgs q)
 {
     using S = Shape<LOG_N>;
@@ -410,10 +450,7 @@ frame_kernel(FrameArgs a, QueueArgs q)
     constexpr int NT = S::RP * 2 * NF * S::G;
     constexpr int RT = (N / 2) / S::RP;  // row tasks per ocean
     constexpr int CT = N / S::PW;        // column tasks per ocean
-    constexpr size_t kDataFloat2 =
-        (S::RP * 2 * NF * S::SEQ + S::RP * 2 * N) > (NF * S::PW * S::SEQ)
-            ? (S::RP * 2 * NF * S::SEQ + S::RP * 2 * N)
-            : (NF * S::PW * S::SEQ);
+    constexpr size_t kDataFloat2 = frame_data_float2<LOG_N, NF>();
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
     float2* tws = smem + kDataFloat2;
@@ -422,6 +459,11 @@ frame_kernel(FrameArgs a, QueueArgs q)
 
     const int tid = threadIdx.x;
     for (int i = tid; i < N - 1; i += NT) tws[i] = a.twiddles[i];
+    tc::Engine eng{reinterpret_cast<unsigned char*>(smem4) + frame_engine_offset<LOG_N, NF>(), 0};
+    if constexpr (TC) {
+        static_assert(NT >= tc::kThreads, "the tensor-core engine needs 8 warps");
+        eng.init(tid, NT);
+    }
 
     const unsigned count = static_cast<unsigned>(q.count);
     const unsigned total = count * (RT + CT);
@@ -481,13 +523,15 @@ frame_kernel(FrameArgs a, QueueArgs q)
         const unsigned slot = ocean % static_cast<unsigned>(q.slots);
         const int abs_ocean = a.ocean_base + static_cast<int>(ocean);
         if (row) {
-            row_task<LOG_N, NF, FAST>(a, abs_ocean, static_cast<int>(idx),
-                                      a.inter + slot * slot_f2, smem, tws, tid);
+            row_task<LOG_N, NF, FAST, TC>(a, abs_ocean, static_cast<int>(idx), a.inter + slot * slot_f2,
+                                          smem, tws, tid, &eng, q.error);
         } else {
-            col_task<LOG_N, NF, FAST, FOAM, S::PW, true>(a, abs_ocean, static_cast<int>(idx),
-                                                         a.inter + slot * slot_f2, smem, tws, tid);
+            col_task<LOG_N, NF, FAST, FOAM, S::PW, true, TC>(a, abs_ocean, static_cast<int>(idx),
+                                                             a.inter + slot * slot_f2, smem, tws, tid,
+                                                             &eng, q.error);
         }
     }
+    if constexpr (TC) eng.release(tid);
 }
 
 // A single bounded wait on a counter that nothing increments: exercises the
@@ -625,35 +669,34 @@ cudaError_t col_launch(const FrameArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-template <int LOG_N, int NF>
+template <int LOG_N, int NF, bool TC = false>
 constexpr size_t frame_smem_bytes()
 {
     using S = Shape<LOG_N>;
-    constexpr size_t row = S::RP * 2 * NF * S::SEQ + S::RP * 2 * S::N;
-    constexpr size_t col = NF * S::PW * S::SEQ;
-    return sizeof(float2) * ((row > col ? row : col) + (S::N - 1));
+    if (TC) return frame_engine_offset<LOG_N, NF>() + tc::kSmemBytes;
+    return sizeof(float2) * (frame_data_float2<LOG_N, NF>() + (S::N - 1));
 }
 
-template <int LOG_N, int NF, bool FAST, bool FOAM>
+template <int LOG_N, int NF, bool FAST, bool FOAM, bool TC = false>
 struct FrameLaunch {
     static constexpr int threads() { return Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G; }
 
     static cudaError_t prepare()
     {
-        return cudaFuncSetAttribute(frame_kernel<LOG_N, NF, FAST, FOAM>,
+        return cudaFuncSetAttribute(frame_kernel<LOG_N, NF, FAST, FOAM, TC>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(frame_smem_bytes<LOG_N, NF>()));
+                                    static_cast<int>(frame_smem_bytes<LOG_N, NF, TC>()));
     }
 
     static int blocks_per_sm()
     {
         if (prepare() != cudaSuccess) return 0;
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<LOG_N, NF, FAST, FOAM>,
-                                                          threads(),
-                                                          frame_smem_bytes<LOG_N, NF>()) !=
-            cudaSuccess)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<LOG_N, NF, FAST, FOAM, TC>, threads(),
+                                                          frame_smem_bytes<LOG_N, NF, TC>()) != cudaSuccess)
             return 0;
+        // The tensor-core engine's tensor memory bounds its residency.
+        if (TC && n * tc::kTmemCols > 512) n = 512 / tc::kTmemCols;
         return n;
     }
 
@@ -661,15 +704,31 @@ struct FrameLaunch {
     {
         cudaError_t e = prepare();
         if (e != cudaSuccess) return e;
-        frame_kernel<LOG_N, NF, FAST, FOAM>
-            <<<grid, threads(), frame_smem_bytes<LOG_N, NF>(), st>>>(a, q);
+        if (TC) {
+            // Every resident CTA must obtain its tensor memory without waiting.
+            int n = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<LOG_N, NF, FAST, FOAM, TC>,
+                                                              threads(), frame_smem_bytes<LOG_N, NF, TC>());
+            if (e != cudaSuccess) return e;
+            if (n * tc::kTmemCols > 512) return cudaErrorInvalidConfiguration;
+        }
+        frame_kernel<LOG_N, NF, FAST, FOAM, TC><<<grid, threads(), frame_smem_bytes<LOG_N, NF, TC>(), st>>>(a, q);
         return cudaGetLastError();
     }
 };
 
+// form: 0 exact, 1 fast (FMA), 2 tensor cores (N = 512 only).
 template <int LOG_N, typename Fn>
-auto frame_variant(int nf, bool fast, bool foam, Fn&& fn)
+auto frame_variant(int nf, int form, bool foam, Fn&& fn)
 {
+    if constexpr (LOG_N == 9) {
+        if (form == 2) {
+            if (nf == 4) return fn(FrameLaunch<LOG_N, 4, false, false, true>{});
+            if (foam) return fn(FrameLaunch<LOG_N, 6, false, true, true>{});
+            return fn(FrameLaunch<LOG_N, 6, false, false, true>{});
+        }
+    }
+    const bool fast = form == 1;
     if (nf == 4) return fast ? fn(FrameLaunch<LOG_N, 4, true, false>{})
                              : fn(FrameLaunch<LOG_N, 4, false, false>{});
     if (foam) return fast ? fn(FrameLaunch<LOG_N, 6, true, true>{})
@@ -678,16 +737,16 @@ auto frame_variant(int nf, bool fast, bool foam, Fn&& fn)
 }
 
 template <typename Fn>
-auto frame_dispatch(int log_n, int nf, bool fast, bool foam, Fn&& fn)
+auto frame_dispatch(int log_n, int nf, int form, bool foam, Fn&& fn)
 {
     switch (log_n) {
-        case 4: return frame_variant<4>(nf, fast, foam, fn);
-        case 5: return frame_variant<5>(nf, fast, foam, fn);
-        case 6: return frame_variant<6>(nf, fast, foam, fn);
-        case 7: return frame_variant<7>(nf, fast, foam, fn);
-        case 8: return frame_variant<8>(nf, fast, foam, fn);
-        case 9: return frame_variant<9>(nf, fast, foam, fn);
-        default: return frame_variant<10>(nf, fast, foam, fn);
+        case 4: return frame_variant<4>(nf, form, foam, fn);
+        case 5: return frame_variant<5>(nf, form, foam, fn);
+        case 6: return frame_variant<6>(nf, form, foam, fn);
+        case 7: return frame_variant<7>(nf, form, foam, fn);
+        case 8: return frame_variant<8>(nf, form, foam, fn);
+        case 9: return frame_variant<9>(nf, form, foam, fn);
+        default: return frame_variant<10>(nf, form, foam, fn);
     }
 }
 
@@ -710,17 +769,19 @@ cudaError_t col_dispatch_n(int nf, bool fast, bool foam, const FrameArgs& a, cud
 
 }  // namespace
 
-int frame_blocks_per_sm(int log_n, int nf, bool fast, bool fuse_foam)
+int frame_blocks_per_sm(int log_n, int nf, int form, bool fuse_foam)
 {
     if (log_n < 4 || log_n > 10) return 0;
-    return frame_dispatch(log_n, nf, fast, fuse_foam, [](auto L) { return decltype(L)::blocks_per_sm(); });
+    if (form == 2 && log_n != 9) return 0;
+    return frame_dispatch(log_n, nf, form, fuse_foam, [](auto L) { return decltype(L)::blocks_per_sm(); });
 }
 
-cudaError_t launch_frame(int log_n, int nf, bool fast, bool fuse_foam, const FrameArgs& a,
+cudaError_t launch_frame(int log_n, int nf, int form, bool fuse_foam, const FrameArgs& a,
                          const QueueArgs& q, int grid, cudaStream_t st)
 {
     if (log_n < 4 || log_n > 10) return cudaErrorInvalidValue;
-    return frame_dispatch(log_n, nf, fast, fuse_foam,
+    if (form == 2 && log_n != 9) return cudaErrorInvalidValue;
+    return frame_dispatch(log_n, nf, form, fuse_foam,
                           [&](auto L) { return decltype(L)::launch(a, q, grid, st); });
 }
 

@@ -198,6 +198,9 @@ public:
             if (!velocity_) throw std::invalid_argument("foam needs compute_velocity");
         }
         form_ = form;
+        // The tensor-core DFT is built for N = 512 and runs in the persistent kernel.
+        if (form_ == OCEAN_FFT_TENSOR && (n_ != 512 || !persistent_))
+            throw std::invalid_argument("the tensor-core form needs N = 512 and the persistent schedule");
         count_ = count;
         log_n_ = ilog2u(n_);
         nf_ = velocity_ ? 6 : 4;
@@ -565,7 +568,7 @@ private:
         if (grid == 0) {
             int sms = 0;
             check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "SM count");
-            const int per_sm = frame_blocks_per_sm(log_n_, nf_, form_ == OCEAN_FFT_FAST, foam);
+            const int per_sm = frame_blocks_per_sm(log_n_, nf_, form_, foam);
             if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "frame occupancy");
             grid = per_sm * sms;
         }
@@ -574,7 +577,7 @@ private:
         const int shared = std::max(1, static_cast<int>(std::lround(grid * grid_share_)));
         const int launch_grid = static_cast<int>(std::min<uint64_t>(shared, uint64_t(k) * n_));
         timed(3, st, [&] {
-            check(launch_frame(log_n_, nf_, form_ == OCEAN_FFT_FAST, foam, a, q, launch_grid, st),
+            check(launch_frame(log_n_, nf_, form_, foam, a, q, launch_grid, st),
                   "frame kernel");
         });
     }
@@ -1414,8 +1417,10 @@ ocean_batch* ocean_batch_create(const ocean_batch_desc* desc, ocean_status* out_
     ocean_batch* b = nullptr;
     ocean_status st = OCEAN_OK;
     if (desc == nullptr || desc->struct_size != sizeof(ocean_batch_desc) ||
-        (desc->fft_form != OCEAN_FFT_EXACT && desc->fft_form != OCEAN_FFT_FAST) ||
-        (desc->schedule != OCEAN_SCHEDULE_PERSISTENT && desc->schedule != OCEAN_SCHEDULE_CHUNKED)) {
+        (desc->fft_form != OCEAN_FFT_EXACT && desc->fft_form != OCEAN_FFT_FAST &&
+         desc->fft_form != OCEAN_FFT_TENSOR) ||
+        (desc->schedule != OCEAN_SCHEDULE_PERSISTENT && desc->schedule != OCEAN_SCHEDULE_CHUNKED) ||
+        (desc->fft_form == OCEAN_FFT_TENSOR && desc->schedule != OCEAN_SCHEDULE_PERSISTENT)) {
         st = OCEAN_ERROR_INVALID_ARG;
     } else {
         ocean_foam_desc foam;

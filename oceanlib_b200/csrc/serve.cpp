@@ -535,7 +535,7 @@ private:
         const std::vector<float2> tw = stage_twiddles(k->n);
         check(cudaMemcpyAsync(k->tw.p, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, stream_),
               "twiddles");
-        const int per_sm = frame_blocks_per_sm(k->log_n, k->nf, desc_.fft_form == OCEAN_FFT_FAST, false);
+        const int per_sm = frame_blocks_per_sm(k->log_n, k->nf, desc_.fft_form, false);
         if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "frame occupancy");
         k->grid = per_sm * sms_;
         k->bytes = ocean_kind_bytes(od);
@@ -888,7 +888,6 @@ private:
 
         // Launch.
         uint32_t kernels = 0;
-        const bool fast = desc_.fft_form == OCEAN_FFT_FAST;
         check(cudaEventRecord(c->start, stream_), "event");
         if (in_bytes > 0) check(cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, stream_), "batch upload");
         for (const OceanPart& p : oparts) {
@@ -911,7 +910,7 @@ private:
             q.slots = std::min(count, 3);
             q.wait_ns = 1000000000ull;
             const int grid = static_cast<int>(std::min<uint64_t>(k->grid, uint64_t(count) * k->n));
-            check(launch_frame(k->log_n, k->nf, fast, false, a, q, grid, stream_), "frame kernel");
+            check(launch_frame(k->log_n, k->nf, desc_.fft_form, false, a, q, grid, stream_), "frame kernel");
             ++kernels;
         }
         const IWaveSource* dev_src = reinterpret_cast<const IWaveSource*>(d + src_off);

@@ -78,11 +78,12 @@ struct QueueArgs {
 };
 
 // One persistent launch for the whole frame of `q.count` oceans (foam fused
-// when fuse_foam). `grid` = CTAs to launch (0 = one wave of resident CTAs).
-cudaError_t launch_frame(int log_n, int nf, bool fast, bool fuse_foam, const FrameArgs& args,
+// when fuse_foam). `form` is an ocean_fft_form (the tensor form: N = 512).
+// `grid` = CTAs to launch (0 = one wave of resident CTAs).
+cudaError_t launch_frame(int log_n, int nf, int form, bool fuse_foam, const FrameArgs& args,
                          const QueueArgs& q, int grid, cudaStream_t stream);
-// Resident CTAs per SM of the persistent frame kernel, and its thread count.
-int frame_blocks_per_sm(int log_n, int nf, bool fast, bool fuse_foam);
+// Resident CTAs per SM of the persistent frame kernel (0: no such variant).
+int frame_blocks_per_sm(int log_n, int nf, int form, bool fuse_foam);
 // A bounded wait on `counter` that nothing increments (tests the timeout path).
 cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned* error,
                               unsigned long long limit_ns, cudaStream_t stream);

@@ -1,0 +1,478 @@
+// oceanlib-b200: the tensor-core DFT form (sm_100a, tcgen05).
+//
+// A 512-point inverse DFT (sign +, unnormalised, as src/core/fft.cpp) of 8
+// sequences at a time, as the four-step factorisation 512 = 16 x 32:
+//
+//   n = 32 n1 + n2,  k = k1 + 16 k2
+//   Y[n2, k1] = sum_n1 W16^(n1 k1) x[32 n1 + n2]          stage 1 (GEMM)
+//   Z[n2, k1] = W512^(n2 k1) Y[n2, k1]                    twiddle (FP32)
+//   X[k1 + 16 k2] = sum_n2 W32^(n2 k2) Z[n2, k1]           stage 3 (GEMM)
+//
+// Each stage is one real GEMM D = A B^T on the tensor cores
+// (tcgen05.mma kind::f16: FP16 operands in shared memory, FP32 accumulators
+// in tensor memory): the complex DFT matrix becomes the real block matrix
+// [[C, -S], [S, C]] and a row of A holds one short sequence as (re..., im...).
+// Stage 1 has 8 x 32 = 256 rows (two M = 128 tiles), K = 32, N = 32; stage 3
+// has 8 x 16 = 128 rows, K = 64, N = 64.
+//
+// Precision: a plain FP16 split (hi + lo) still rounds every accumulation in
+// FP32 against the dominant spectral terms of a row, which costs 2-3x the
+// FP32 FFT's error. Here the GEMMs are made exact instead. Each row of A is
+// scaled by a power of two so its largest magnitude lies in [2^29, 2^30),
+// rounded to an integer (30 significant bits relative to the row maximum),
+// and cut into four signed 8-bit digits a_i (weights 2^24, 2^16, 2^8, 1);
+// the DFT matrices likewise at 2^30. FP16 holds the digits exactly, every
+// product a_i b_j is an exact integer below 2^14, and a level
+// D_L = sum over i + j = L of A_i B_j^T (at most 4 pairs x 64 terms) stays
+// below 2^22 - so the FP32 accumulators hold every level EXACTLY, whatever
+// order the tensor cores add in. Levels 0..3 (10 products per K step) are
+// kept; the dropped ones weigh 2^-32 of the leading term. The four exact
+// levels are then combined in FP32 (three roundings). The GEMMs are thus
+// as good as FP64 ones; the remaining error is the FP32 twiddle step and the
+// FP32 values between the stages - below the radix-2 FP32 FFT's own.
+//
+// One elected thread issues the MMAs and commits them to an mbarrier; every
+// wait on it is bounded (the error word is set and the engine gives up
+// rather than spin). Tensor memory: 256 columns per CTA, allocated once per
+// kernel by warp 0 and released before exit.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cstdint>
+
+#include "ocean_device.cuh"
+
+namespace ocean_b200 {
+namespace tc {
+
+constexpr int kSeq = 8;          // sequences per engine call
+constexpr int kRows1 = 256;      // stage 1 rows: 8 x 32
+constexpr int kK1 = 32;          // stage 1 K (16 complex)
+constexpr int kN1 = 32;          // stage 1 N (16 complex)
+constexpr int kRows3 = 128;      // stage 3 rows: 8 x 16
+constexpr int kK3 = 64;          // stage 3 K (32 complex)
+constexpr int kN3 = 64;          // stage 3 N (32 complex)
+constexpr int kDigits = 4;       // signed 8-bit digits per value
+constexpr int kLevels = 4;       // digit-pair levels kept (i + j < 4)
+// Accumulators (FP32 columns), one per level: stage 1 tile t, level L at
+// 128 t + 32 L; stage 3 level L at 64 L. All 256 columns.
+constexpr int kTmemCols = 256;
+constexpr int kThreads = 256;    // the engine's working threads (8 warps)
+constexpr int kFixExp = 29;      // row max scaled into [2^29, 2^30)
+constexpr int kBExp = 30;        // DFT matrices scaled by 2^30
+constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
+
+// Shared-memory layout of the engine (bytes, all 128-byte aligned).
+constexpr int kAHalves = kRows1 * kK1;  // == kRows3 * kK3 = 8192 halves per digit
+static_assert(kRows1 * kK1 == kRows3 * kK3, "stage operands share one buffer");
+constexpr int kOffA = 0;                                       // [digit][8192]
+constexpr int kOffB1 = kOffA + kDigits * kAHalves * 2;          // [digit][32*32]
+constexpr int kOffB3 = kOffB1 + kDigits * kN1 * kK1 * 2;        // [digit][64*64]
+constexpr int kOffE3 = kOffB3 + kDigits * kN3 * kK3 * 2;        // int[kRows3]
+constexpr int kOffBar = kOffE3 + kRows3 * 4;                    // uint64 mbarrier
+constexpr int kOffTmem = kOffBar + 8;                           // uint32 tmem base
+constexpr int kSmemBytes = kOffTmem + 8;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Canonical K-major, no-swizzle layout of an R x K FP16 operand: 8-row x
+// 16-byte core matrices; the K chunks of a row group lie 128 B apart (LBO),
+// row groups K * 16 B apart (SBO). Offset in halves.
+__device__ __forceinline__ int kmajor(int row, int k, int K)
+{
+    return (row >> 3) * (K * 8) + (k >> 3) * 64 + (row & 7) * 8 + (k & 7);
+}
+
+// Shared-memory matrix descriptor: start, LBO, SBO (all >> 4), version 1,
+// base offset 0, no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) |
+           (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+           (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor: FP16 A and B (K-major), FP32 accumulator, M x N.
+__host__ __device__ constexpr uint32_t instr_desc(int m, int n)
+{
+    return (1u << 4) | (static_cast<uint32_t>(n >> 3) << 17) | (static_cast<uint32_t>(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ unsigned long long now_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for mbarrier phase `parity`; false (and the error word set)
+// when it does not complete within kWaitNs.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, unsigned* error)
+{
+    uint32_t done = 0;
+    unsigned long long t0 = 0;
+    for (int spin = 0;; ++spin) {
+        asm volatile(
+            "{\n\t.reg .pred P;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (spin == 0) t0 = now_ns();
+        if ((spin & 63) == 63 && now_ns() - t0 > kWaitNs) {
+            if (error) atomicCAS(error, 0u, 2u);
+            return false;
+        }
+    }
+}
+
+#define OCEAN_TMEM_LD32(taddr, r)                                                                       \
+    asm volatile(                                                                                       \
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "                                                       \
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"                                       \
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                      \
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),          \
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),      \
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),   \
+          "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),   \
+          "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])                                           \
+        : "r"(taddr)                                                                                    \
+        : "memory")
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 2^e as a float, e clamped to the normal range.
+__device__ __forceinline__ float pow2f(int e)
+{
+    e = e < -126 ? -126 : (e > 127 ? 127 : e);
+    return __uint_as_float(static_cast<uint32_t>(e + 127) << 23);
+}
+
+// Exponent that scales `maxabs` into [2^29, 2^30) (0 for a zero row).
+__device__ __forceinline__ int row_exp(float maxabs)
+{
+    if (!(maxabs > 0.0f)) return 0;
+    int ex = static_cast<int>((__float_as_uint(maxabs) >> 23) & 0xFFu) - 127;
+    if (ex < -126) ex = -126;  // subnormal maximum
+    const int e = kFixExp - ex;
+    return e > 120 ? 120 : (e < -120 ? -120 : e);
+}
+
+// A signed fixed-point value |v| < 2^30 as four signed 8-bit digits
+// d0 2^24 + d1 2^16 + d2 2^8 + d3, as FP16 bit patterns (exact).
+__device__ __forceinline__ void digits4(int v, uint16_t (&d)[4])
+{
+    const int d0 = (v + (1 << 23)) >> 24;
+    int r = v - (d0 << 24);
+    const int d1 = (r + (1 << 15)) >> 16;
+    r -= d1 << 16;
+    const int d2 = (r + (1 << 7)) >> 8;
+    const int d3 = r - (d2 << 8);
+    d[0] = __half_as_ushort(__int2half_rn(d0));
+    d[1] = __half_as_ushort(__int2half_rn(d1));
+    d[2] = __half_as_ushort(__int2half_rn(d2));
+    d[3] = __half_as_ushort(__int2half_rn(d3));
+}
+
+__device__ __forceinline__ uint32_t pack2(uint16_t a, uint16_t b)
+{
+    return static_cast<uint32_t>(a) | (static_cast<uint32_t>(b) << 16);
+}
+
+// Read back, level D_L of a row with fixed-point exponent e weighs
+// 2^(48 - 8 L - 30 - e) = 2^(18 - 8 L - e); the levels are added largest
+// first.
+struct Engine {
+    unsigned char* smem;  // kSmemBytes, 128-byte aligned
+    uint32_t tmem;        // tensor-memory base (lane 0, column 0)
+
+    __device__ uint16_t* a(int digit) const
+    {
+        return reinterpret_cast<uint16_t*>(smem + kOffA) + digit * kAHalves;
+    }
+    __device__ int* e3() const { return reinterpret_cast<int*>(smem + kOffE3); }
+    __device__ uint32_t bar() const { return smem_u32(smem + kOffBar); }
+
+    // Once per kernel, all threads: the DFT matrices' digits, the mbarrier,
+    // and (warp 0) the tensor-memory allocation.
+    __device__ void init(int tid, int nthreads)
+    {
+        uint16_t* b1 = reinterpret_cast<uint16_t*>(smem + kOffB1);
+        uint16_t* b3 = reinterpret_cast<uint16_t*>(smem + kOffB3);
+        const double scale = static_cast<double>(1ll << kBExp);
+        // B1[j][k]: j = (q, k1) output, k = (p, n1) input, angle 2 pi n1 k1 / 16
+        for (int i = tid; i < kN1 * kK1; i += nthreads) {
+            const int j = i / kK1, k = i % kK1;
+            const int q = j >> 4, k1 = j & 15, p = k >> 4, n1 = k & 15;
+            double s, c;
+            sincospi(static_cast<double>((n1 * k1) & 15) / 8.0, &s, &c);
+            const double v = (q == p) ? c : (q == 0 ? -s : s);
+            uint16_t d[4];
+            digits4(static_cast<int>(rint(v * scale)), d);
+            for (int g = 0; g < kDigits; ++g) b1[g * kN1 * kK1 + kmajor(j, k, kK1)] = d[g];
+        }
+        // B3[j][k]: j = (q, k2), k = (p, n2), angle 2 pi n2 k2 / 32
+        for (int i = tid; i < kN3 * kK3; i += nthreads) {
+            const int j = i / kK3, k = i % kK3;
+            const int q = j >> 5, k2 = j & 31, p = k >> 5, n2 = k & 31;
+            double s, c;
+            sincospi(static_cast<double>((n2 * k2) & 31) / 16.0, &s, &c);
+            const double v = (q == p) ? c : (q == 0 ? -s : s);
+            uint16_t d[4];
+            digits4(static_cast<int>(rint(v * scale)), d);
+            for (int g = 0; g < kDigits; ++g) b3[g * kN3 * kK3 + kmajor(j, k, kK3)] = d[g];
+        }
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar()) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        if (tid < 32) {
+            const uint32_t slot = smem_u32(smem + kOffTmem);
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+                         "r"(kTmemCols)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
+        fence_proxy_async();
+        fence_before_sync();
+        __syncthreads();
+        fence_after_sync();
+        tmem = *reinterpret_cast<volatile uint32_t*>(smem + kOffTmem);
+    }
+
+    // Once per kernel, all threads, after the last engine call.
+    __device__ void release(int tid)
+    {
+        fence_before_sync();
+        __syncthreads();
+        fence_after_sync();
+        if (tid < 32)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+                         : "memory");
+    }
+
+    // The 10 digit-pair MMAs of one K step into the level accumulators at
+    // `d` + 32 L (stage 1) or + 64 L (stage 3). `first` starts each level.
+    __device__ static void issue_levels(uint32_t d, int level_stride, uint32_t a0, uint32_t b0, uint32_t a_digit,
+                                        uint32_t b_digit, uint32_t kofs, uint32_t tile, uint32_t sbo_a,
+                                        uint32_t sbo_b, uint32_t idesc, bool first)
+    {
+#pragma unroll
+        for (int L = 0; L < kLevels; ++L) {
+            bool started = !first;
+#pragma unroll
+            for (int i = 0; i <= L; ++i) {
+                const int j = L - i;
+                if (i >= kDigits || j >= kDigits) continue;
+                const uint64_t da = smem_desc(a0 + i * a_digit + tile + kofs, 128, sbo_a);
+                const uint64_t db = smem_desc(b0 + j * b_digit + kofs, 128, sbo_b);
+                mma_f16(d + L * level_stride, da, db, idesc, started ? 1u : 0u);
+                started = true;
+            }
+        }
+    }
+
+    // In-place inverse DFT of sequences s < count (<= 8) of length 512 at
+    // data + s * seq_stride, element n at pad_idx(n). `tws` holds the FP32
+    // twiddles W^p, p < 256 (W = e^(2 pi i / 512)). All threads of the CTA
+    // call it (the first 256 do the work); data must be complete on entry,
+    // and is complete on return.
+    __device__ void dft512(float2* data, int seq_stride, int count, const float2* tws, int tid, unsigned* error)
+    {
+        const int warp = tid >> 5, lane = tid & 31;
+        const bool worker = tid < kThreads;
+        uint16_t* a0p = a(0);
+
+        // ---- stage 1 operand: row r = (s, n2), 16 complex x[32 n1 + n2] ----
+        int e1 = 0;
+        const int s_row = tid >> 5, n2 = tid & 31;
+        if (worker) {
+            float v[32];
+            float m = 0.0f;
+            if (s_row < count) {
+                const float2* seq = data + s_row * seq_stride;
+#pragma unroll
+                for (int n1 = 0; n1 < 16; ++n1) {
+                    const float2 x = seq[pad_idx(32 * n1 + n2)];
+                    v[n1] = x.x;
+                    v[16 + n1] = x.y;
+                    m = fmaxf(m, fmaxf(fabsf(x.x), fabsf(x.y)));
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < 32; ++k) v[k] = 0.0f;
+            }
+            e1 = row_exp(m);
+            const float sc = pow2f(e1);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                uint16_t d[8][4];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) digits4(__float2int_rn(v[8 * c + q] * sc), d[q]);
+                const int off = kmajor(tid, 8 * c, kK1);
+#pragma unroll
+                for (int g = 0; g < kDigits; ++g)
+                    *reinterpret_cast<uint4*>(a0p + g * kAHalves + off) =
+                        make_uint4(pack2(d[0][g], d[1][g]), pack2(d[2][g], d[3][g]), pack2(d[4][g], d[5][g]),
+                                   pack2(d[6][g], d[7][g]));
+            }
+        }
+        fence_proxy_async();
+        fence_before_sync();
+        __syncthreads();
+        fence_after_sync();
+
+        // ---- stage 1 MMAs: 2 tiles x 2 K steps x 10 digit pairs ----
+        if (tid == 0) {
+            const uint32_t abase = smem_u32(a0p), bbase = smem_u32(smem + kOffB1);
+            constexpr uint32_t sbo = kK1 * 16;
+            constexpr uint32_t idesc = instr_desc(128, kN1);
+#pragma unroll 1
+            for (int t = 0; t < 2; ++t)
+#pragma unroll 1
+                for (int ks = 0; ks < kK1 / 16; ++ks)
+                    issue_levels(tmem + t * 128, kN1, abase, bbase, kAHalves * 2, kN1 * kK1 * 2, ks * 256,
+                                 t * 16 * sbo, sbo, sbo, idesc, ks == 0);
+            mma_commit(bar());
+        }
+        bar_wait(bar(), 0u, error);
+        fence_after_sync();
+
+        // ---- read Y, twiddle, stage 3 operand: row (s, k1), K = (p, n2) ----
+        if (worker) {
+            const int t = warp >> 2;
+            const uint32_t col = tmem + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + t * 128;
+            float y[32];
+            {
+                uint32_t r0[32], r1[32];
+                OCEAN_TMEM_LD32(col, r0);
+                OCEAN_TMEM_LD32(col + 32, r1);
+                tmem_wait_ld();
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    y[j] = __uint_as_float(r0[j]) * pow2f(18 - e1) + __uint_as_float(r1[j]) * pow2f(10 - e1);
+            }
+            {
+                uint32_t r2[32], r3[32];
+                OCEAN_TMEM_LD32(col + 64, r2);
+                OCEAN_TMEM_LD32(col + 96, r3);
+                tmem_wait_ld();
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    y[j] = (y[j] + __uint_as_float(r2[j]) * pow2f(2 - e1)) + __uint_as_float(r3[j]) * pow2f(-6 - e1);
+            }
+            float zr[16], zi[16];
+#pragma unroll
+            for (int k1 = 0; k1 < 16; ++k1) {
+                const int e = n2 * k1;  // < 512
+                float2 w = tws[e & 255];
+                if (e & 256) w = make_float2(-w.x, -w.y);
+                zr[k1] = y[k1] * w.x - y[16 + k1] * w.y;
+                zi[k1] = y[k1] * w.y + y[16 + k1] * w.x;
+            }
+            // per stage-3 row (s, k1): the maximum over the warp's 32 n2
+#pragma unroll
+            for (int k1 = 0; k1 < 16; ++k1) {
+                float m = fmaxf(fabsf(zr[k1]), fabsf(zi[k1]));
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+                const int ex3 = row_exp(m);
+                const float sc = pow2f(ex3);
+                const int row = s_row * 16 + k1;
+                uint16_t dr[4], di[4];
+                digits4(__float2int_rn(zr[k1] * sc), dr);
+                digits4(__float2int_rn(zi[k1] * sc), di);
+                const int o_r = kmajor(row, n2, kK3), o_i = kmajor(row, 32 + n2, kK3);
+#pragma unroll
+                for (int g = 0; g < kDigits; ++g) {
+                    a0p[g * kAHalves + o_r] = dr[g];
+                    a0p[g * kAHalves + o_i] = di[g];
+                }
+                if (lane == 0) e3()[row] = ex3;
+            }
+        }
+        fence_proxy_async();
+        fence_before_sync();
+        __syncthreads();
+        fence_after_sync();
+
+        // ---- stage 3 MMAs: 1 tile x 4 K steps x 10 digit pairs ----
+        if (tid == 0) {
+            const uint32_t abase = smem_u32(a0p), bbase = smem_u32(smem + kOffB3);
+            constexpr uint32_t sbo = kK3 * 16;
+            constexpr uint32_t idesc = instr_desc(128, kN3);
+#pragma unroll 1
+            for (int ks = 0; ks < kK3 / 16; ++ks)
+                issue_levels(tmem, kN3, abase, bbase, kAHalves * 2, kN3 * kK3 * 2, ks * 256, 0u, sbo, sbo, idesc,
+                             ks == 0);
+            mma_commit(bar());
+        }
+        bar_wait(bar(), 1u, error);
+        fence_after_sync();
+
+        // ---- read X: warps 0-3 the real parts, warps 4-7 the imaginary ----
+        if (worker) {
+            const int part = warp >> 2;
+            const uint32_t col = tmem + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + part * 32;
+            const int row = 32 * (warp & 3) + lane;  // (s, k1)
+            const int e = e3()[row];
+            float x[32];
+            {
+                uint32_t r0[32], r1[32];
+                OCEAN_TMEM_LD32(col, r0);
+                OCEAN_TMEM_LD32(col + 64, r1);
+                tmem_wait_ld();
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    x[j] = __uint_as_float(r0[j]) * pow2f(18 - e) + __uint_as_float(r1[j]) * pow2f(10 - e);
+            }
+            {
+                uint32_t r2[32], r3[32];
+                OCEAN_TMEM_LD32(col + 128, r2);
+                OCEAN_TMEM_LD32(col + 192, r3);
+                tmem_wait_ld();
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    x[j] = (x[j] + __uint_as_float(r2[j]) * pow2f(2 - e)) + __uint_as_float(r3[j]) * pow2f(-6 - e);
+            }
+            const int s = row >> 4, k1 = row & 15;
+            if (s < count) {
+                float* seq = reinterpret_cast<float*>(data + s * seq_stride);
+#pragma unroll
+                for (int k2 = 0; k2 < 32; ++k2) seq[2 * pad_idx(k1 + 16 * k2) + part] = x[k2];
+            }
+        }
+        fence_before_sync();
+        __syncthreads();
+        fence_after_sync();
+    }
+};
+
+}  // namespace tc
+}  // namespace ocean_b200

@@ -296,6 +296,47 @@ def dft_points(re: np.ndarray, im: np.ndarray, xs, ys):
     return o_re, o_im
 
 
+def fp64_fields(desc, t: float) -> np.ndarray:
+    """The evolved spectra (or_evolve, FP32 as the reference builds them)
+    inverse-transformed in FP64: (planes, N, N) complex128, unnormalised,
+    sign + (src/core/fft.cpp). numpy's complex128 FFT stands in for the
+    direct sum; dft_points gives the direct sum at chosen points to check it."""
+    n = desc.size
+    f = evolve(desc, t).astype(np.float64)
+    planes = f.shape[0] // 2
+    z = (f[0::2] + 1j * f[1::2]).reshape(planes, n, n)
+    return np.fft.ifft2(z, axes=(1, 2)) * (n * n)
+
+
+def fp64_frame(desc, t: float) -> dict:
+    """One update's outputs in FP64 from fp64_fields, through the finalize
+    arithmetic of src/core/evolve.cpp:238-327 (and :186-203 for velocity):
+    displacement (lambda Dx, h, lambda Dz, foam), normal (n / |n|, J),
+    velocity (ux, uy, uz, 0). Arrays (N, N, 4) float64."""
+    g = fp64_fields(desc, t)
+    h, dx = g[0].real, g[0].imag
+    dz, hx = g[1].real, g[1].imag
+    hz, jxx = g[2].real, g[2].imag
+    jzz, jxz = g[3].real, g[3].imag
+    lam = float(desc.choppiness)
+    axx = 1.0 + lam * jxx
+    azz = 1.0 + lam * jzz
+    axz = lam * jxz
+    jac = axx * azz - axz * axz
+    nx = -(hx * azz - axz * hz)
+    ny = jac
+    nz = -(axx * hz - hx * axz)
+    ln = np.sqrt(nx * nx + ny * ny + nz * nz)
+    inv = np.where(ln > 0, 1.0 / np.where(ln > 0, ln, 1.0), 0.0)
+    thr = float(desc.foam_threshold)
+    foam = np.clip((thr - jac) * (1.0 / thr if thr > 1e-6 else 0.0), 0.0, 1.0)
+    out = {"displacement": np.stack([lam * dx, h, lam * dz, foam], axis=-1),
+           "normal": np.stack([nx * inv, ny * inv, nz * inv, jac], axis=-1)}
+    if g.shape[0] > 4:
+        out["velocity"] = np.stack([g[4].real, g[4].imag, g[5].real, np.zeros_like(h)], axis=-1)
+    return out
+
+
 def pcg32(seed: int, stream: int, count: int) -> np.ndarray:
     out = np.empty(count, dtype=np.uint32)
     oracle().or_pcg32_fill(seed, stream, count, out.ctypes.data)

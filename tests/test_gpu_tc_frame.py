@@ -1,0 +1,95 @@
+"""Whole frames in the tensor-core form against FP64, beside the FP32 form.
+
+Per output channel: max |e| / RMS of the FP64 frame (oracle.fp64_frame: the
+reference's FP32 spectra, an FP64 2-D inverse transform and an FP64
+finalize). The foam channel (a clamp of the Jacobian, mostly zero) is held
+to an absolute bound instead. The FP32 form is the reference's own
+arithmetic, so its errors are the accuracy the reference delivers; the
+tensor-core form must stay within TC_TOL of FP64 on every channel the FP32
+form itself meets 2e-6 on, and within 2x the FP32 form's error elsewhere."""
+import numpy as np
+import pytest
+
+import oceanlib_b200 as ob
+import oracle as O
+from oceanlib_b200 import abi
+from oceanlib_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+TC_TOL = 2e-6
+FOAM_ABS_TOL = 1e-5
+
+
+@pytest.fixture(autouse=True)
+def _device(cuda_device):
+    ob.force_simd_level(None)
+    yield
+
+
+def frame(desc, t, form):
+    b = ob.OceanBatch([desc], form=form)
+    n = desc.size
+    disp = np.empty((n, n, 4), np.float32)
+    normal = np.empty_like(disp)
+    vel = np.empty_like(disp) if desc.compute_velocity else None
+    b.update_host([t], 0.0, disp, normal, vel)
+    b.close()
+    out = {"displacement": disp, "normal": normal}
+    if vel is not None:
+        out["velocity"] = vel
+    return out
+
+
+def channel_errors(got, ref):
+    errs = {}
+    for k in got:
+        for c in range(3 if k == "velocity" else 4):
+            r = ref[k][..., c]
+            e = np.abs(got[k][..., c].astype(np.float64) - r)
+            if k == "displacement" and c == 3:
+                errs[f"{k}.foam(abs)"] = float(e.max())
+            else:
+                errs[f"{k}.{'xyzw'[c]}"] = float(e.max() / np.sqrt(np.mean(r * r)))
+    return errs
+
+
+@pytest.mark.parametrize("case", ["bench_update_512", "foam_patch_512_velocity", "late_time"])
+def test_tensor_form_frame_against_fp64(case):
+    if case == "bench_update_512":
+        desc, t = W.bench_update_patch(512), 100.0
+    elif case == "foam_patch_512_velocity":
+        desc, t = W.foam_patch_512(), 100.0
+    else:
+        desc, t = W.foam_patch_512(), 1.0e5  # FP64 phase reduction at large t
+    ref = O.fp64_frame(desc, t)
+    e32 = channel_errors(frame(desc, t, abi.OCEAN_FFT_EXACT), ref)
+    etc = channel_errors(frame(desc, t, abi.OCEAN_FFT_TENSOR), ref)
+    print(f"\n{case}: channel  FP32-form  tensor-form  (max|e|/RMS vs FP64)")
+    for k in e32:
+        print(f"  {k:22s} {e32[k]:.3e}  {etc[k]:.3e}")
+    for k in e32:
+        if k.endswith("(abs)"):
+            assert etc[k] <= FOAM_ABS_TOL, (k, etc[k])
+        elif e32[k] <= TC_TOL:
+            assert etc[k] <= TC_TOL, (k, etc[k], e32[k])
+        else:
+            assert etc[k] <= 2.0 * e32[k], (k, etc[k], e32[k])
+
+
+def test_tensor_form_batch_is_per_ocean_independent():
+    descs = [W.bench_update_patch(512, seed=s) for s in (11, 12, 13)]
+    b = ob.OceanBatch(descs, form=abi.OCEAN_FFT_TENSOR)
+    n = 512
+    disp = np.empty((3, n, n, 4), np.float32)
+    normal = np.empty_like(disp)
+    b.update_host([7.5], 0.0, disp, normal)
+    b.close()
+    one = frame(descs[1], 7.5, abi.OCEAN_FFT_TENSOR)
+    assert np.array_equal(disp[1].view(np.uint32), one["displacement"].view(np.uint32))
+    assert np.array_equal(normal[1].view(np.uint32), one["normal"].view(np.uint32))
+
+
+def test_tensor_form_needs_n512():
+    with pytest.raises((ValueError, ob.OceanError)):
+        ob.OceanBatch([W.bench_update_patch(256)], form=abi.OCEAN_FFT_TENSOR)
