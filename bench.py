@@ -30,7 +30,10 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "512^2 ocean updates/s (batched, exact FP32 FFT)"
+# `value` is the plain FP32 form (bit-identical to the reference); the
+# tensor-core form's throughput sits beside it in "tensor_core_form", and the
+# serving loop's request latency in "p99_ms".
+METRIC = "512^2 ocean updates/s: batched TC-FFT vs plain FP32 @<=2e-6 rel err; p99 ms"
 UNIT = "updates/s"
 N = 512
 CELLS = N * N
@@ -54,7 +57,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--schedule", default="persistent", choices=["persistent", "chunked"])
-    ap.add_argument("--form", default="exact", choices=["exact", "fast"])
+    ap.add_argument("--form", default="exact", choices=["exact", "fast", "tensor"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -496,6 +499,7 @@ def bench_serving(rate: float = 20000.0, seconds: float = 3.0):
         "kernel_launches": st["kernel_launches"],
         "sessions_active": st["sessions_active"], "bytes_in_use": st["bytes_in_use"],
         "hbm_budget": st["hbm_budget"], "failed": st["requests_failed"],
+        "dispatch_max_ms": st["dispatch_max_ms"], "staging_growths": st["staging_growths"],
         "capacity_closed_loop_rps": cap["requests_completed"] / cap_wall,
         "capacity_p99_ms": cap["latency_p99_ms"],
         "capacity_mean_batch_requests": cap["mean_batch_requests"],
@@ -532,7 +536,8 @@ def main():
     from oceanlib_b200 import abi
 
     batch = ob.OceanBatch(descs, foam=W.foam_desc(), chunk=args.chunk,
-                          form=abi.OCEAN_FFT_FAST if args.form == "fast" else abi.OCEAN_FFT_EXACT,
+                          form={"exact": abi.OCEAN_FFT_EXACT, "fast": abi.OCEAN_FFT_FAST,
+                                "tensor": abi.OCEAN_FFT_TENSOR}[args.form],
                           schedule=abi.OCEAN_SCHEDULE_CHUNKED if args.schedule == "chunked"
                           else abi.OCEAN_SCHEDULE_PERSISTENT)
     # An explicit stream: the library launches on it and the CUDA events
@@ -605,6 +610,39 @@ def main():
     d2h = B * CELLS * (3 * 16 + 4)
     h2d = 8  # one absolute time per frame (double)
 
+    # ---- the tensor-core DFT form on the same workload, beside the FP32 form ----
+    tc = None
+    if args.form != "tensor":
+        tcb = ob.OceanBatch(descs, foam=W.foam_desc(), form=abi.OCEAN_FFT_TENSOR)
+        tframe = 0
+
+        def tc_step():
+            nonlocal tframe
+            tframe += 1
+            tcb.update([tframe * dt], foam_dt=dt, stream=sh)
+
+        for _ in range(max(3, args.warmup)):
+            tc_step()
+        torch.cuda.synchronize()
+        tc_steps = max(5, args.steps // 3)
+        t_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        if world > 1:
+            torch.distributed.barrier()
+        tc_launches0 = tcb.launch_count
+        t_ev[0].record(stream)
+        for _ in range(tc_steps):
+            tc_step()
+        t_ev[1].record(stream)
+        torch.cuda.synchronize()
+        tc_ms = t_ev[0].elapsed_time(t_ev[1])
+        if world > 1:
+            tc_ms = max_over_ranks(tc_ms, torch.distributed, "cuda")
+        tc = {"value": B * tc_steps * world / (tc_ms / 1000.0), "unit": UNIT,
+              "ms_per_step": tc_ms / tc_steps, "steps": tc_steps,
+              "gpu_launches": int(tcb.launch_count - tc_launches0),
+              "kernel": "frame_kernel, tensor form (tcgen05 four-step DFT, exact FP16 digit-slice GEMMs)"}
+        tcb.close()
+
     if rank == 0:
         peak, peak_kind = measured_peaks()
         frame_achieved = ALG_BYTES_PER_CELL * CELLS * (value / world) / 1e9
@@ -660,6 +698,9 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "api": "ocean_batch_update_host (pinned host buffers)"},
         }
+        if tc is not None:
+            tc["vs_plain_fp32"] = tc["value"] / value
+            line["tensor_core_form"] = tc
         if not args.no_extra and world == 1:
             extra = {}
             for name, fn in (("cascade", lambda: bench_cascade(torch)), ("iwave", bench_iwave),
@@ -675,6 +716,11 @@ def main():
                     except Exception as e:
                         extra[name]["reference_cpu"] = {"error": str(e)}
             line["extra"] = extra
+            srv = extra.get("serving", {})
+            if "latency_p99_ms" in srv:
+                line["p99_ms"] = {"value": srv["latency_p99_ms"], "p50": srv["latency_p50_ms"],
+                                  "what": "serving loop request -> result in host memory, "
+                                          f"{srv['offered_rps']:.0f} requests/s offered over 256 sessions"}
         if not args.no_cpu_baseline and world == 1:
             try:
                 rate, cores, frames = reference_rate(args.cpu_seconds)

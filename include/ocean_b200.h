@@ -546,6 +546,8 @@ typedef struct ocean_server_stats {
     double   query_p99_ms;
     double   gpu_busy_ms;         /* summed device time of the batches (CUDA events) */
     double   wall_ms;             /* since creation or the last reset */
+    double   dispatch_max_ms;     /* longest single host step of the dispatcher */
+    uint64_t staging_growths;     /* staging buffers grown past their reserve */
 } ocean_server_stats;
 
 OCEAN_API void ocean_server_desc_init(ocean_server_desc* desc);

@@ -200,7 +200,7 @@ class ServerStatsC(C.Structure):
         [(n, C.c_double) for n in (
             "mean_batch_requests", "latency_p50_ms", "latency_p99_ms", "latency_max_ms",
             "update_p50_ms", "update_p99_ms", "query_p50_ms", "query_p99_ms", "gpu_busy_ms",
-            "wall_ms")]
+            "wall_ms", "dispatch_max_ms")] + [("staging_growths", C.c_uint64)]
 
 
 # Every function include/ocean_b200.h declares, with its ctypes signature.

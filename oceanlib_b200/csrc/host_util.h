@@ -79,10 +79,10 @@ struct HostBuf {
     T* p = nullptr;
     size_t n = 0;
     HostBuf() = default;
-    explicit HostBuf(size_t count) : n(count)
+    explicit HostBuf(size_t count, bool zero = true) : n(count)
     {
         if (count) check(cudaMallocHost(&p, count * sizeof(T)), "cudaMallocHost");
-        if (p) std::memset(p, 0, count * sizeof(T));
+        if (p && zero) std::memset(p, 0, count * sizeof(T));
     }
     HostBuf(const HostBuf&) = delete;
     HostBuf& operator=(const HostBuf&) = delete;

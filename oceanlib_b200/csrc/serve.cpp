@@ -251,13 +251,20 @@ public:
         error_ = DevBuf<unsigned>(1);
         check(cudaMemsetAsync(error_.p, 0, sizeof(unsigned), stream_), "memset");
         ctxs_.resize(desc_.max_inflight);
+        // Staging for a full batch of query points plus the tables and sources
+        // of a few thousand updates, reserved now so that a backlog never
+        // waits on pinned-memory allocation.
+        const size_t in_reserve = static_cast<size_t>(desc_.max_batch_points) * sizeof(float2) + (4u << 20);
+        const size_t out_reserve = static_cast<size_t>(desc_.max_batch_points) + 4;
         for (auto& c : ctxs_) {
             c = std::make_unique<BatchCtx>();
             check(cudaEventCreate(&c->start), "event");
             check(cudaEventCreate(&c->done), "event");
             c->server = this;
+            ensure_host(c.get(), in_reserve, out_reserve);
             free_ctx_.push_back(c.get());
         }
+        staging_growths_ = 0;
         stats_t0_ = Clock::now();
         thread_ = std::thread([this] { run(); });
     }
@@ -447,6 +454,8 @@ public:
             o->mean_batch_requests = batches_ ? static_cast<double>(batched_requests_) / batches_ : 0.0;
             o->gpu_busy_ms = gpu_ms_;
             o->wall_ms = ms_between(stats_t0_, Clock::now());
+            o->dispatch_max_ms = dispatch_max_ms_;
+            o->staging_growths = staging_growths_;
             up = lat_update_;
             qu = lat_query_;
         }
@@ -467,6 +476,8 @@ public:
         submitted_ = completed_ = failed_count_ = updates_done_ = queries_done_ = points_done_ = 0;
         batches_ = kernels_ = batched_requests_ = 0;
         gpu_ms_ = 0.0;
+        dispatch_max_ms_ = 0.0;
+        staging_growths_ = 0;
         lat_update_.clear();
         lat_query_.clear();
         samples_.clear();
@@ -747,15 +758,19 @@ private:
     // ---- staging and launch (dispatcher thread, outside the lock) ----------------
     void ensure_host(BatchCtx* c, size_t in_bytes, size_t out_floats)
     {
+        // Growth past the size reserved at creation pins new host memory (slow,
+        // and freeing the old block synchronises the device): rare by design.
         if (in_bytes > c->host_in_cap) {
             const size_t cap = std::max(in_bytes, c->host_in_cap * 2);
-            c->host_in = HostBuf<unsigned char>(cap);
+            c->host_in = HostBuf<unsigned char>(cap, false);
             c->host_in_cap = cap;
+            ++staging_growths_;
         }
         if (out_floats > c->host_out_cap) {
             const size_t cap = std::max(out_floats, c->host_out_cap * 2);
-            c->host_out = HostBuf<float>(cap);
+            c->host_out = HostBuf<float>(cap, false);
             c->host_out_cap = cap;
+            ++staging_growths_;
         }
         const size_t dev_bytes = in_bytes + round_up(out_floats * sizeof(float), 16);
         if (dev_bytes > c->dev_cap) {
@@ -1038,8 +1053,11 @@ private:
                 BatchCtx* c = inflight_.front();
                 inflight_.pop_front();
                 lk.unlock();
+                const auto t_finish = Clock::now();
                 finish(c);
+                const double host_ms = ms_between(t_finish, Clock::now());
                 lk.lock();
+                dispatch_max_ms_ = std::max(dispatch_max_ms_, host_ms);
                 complete_locked(c);
                 free_ctx_.push_back(c);
                 done_cv_.notify_all();
@@ -1081,12 +1099,15 @@ private:
                     free_ctx_.pop_front();
                     lk.unlock();
                     bool launched = true;
+                    const auto t_launch = Clock::now();
                     try {
                         launch(c, plan);
                     } catch (const std::exception&) {
                         launched = false;
                     }
+                    const double host_ms = ms_between(t_launch, Clock::now());
                     lk.lock();
+                    dispatch_max_ms_ = std::max(dispatch_max_ms_, host_ms);
                     if (launched) {
                         ++batches_;
                         kernels_ += c->kernels;
@@ -1158,6 +1179,8 @@ private:
     uint64_t next_session_ = 1, next_ticket_ = 1;
     size_t in_use_ = 0;        // sessions and their shared tables (the budgeted bytes)
     size_t staging_bytes_ = 0; // per-batch device staging
+    uint64_t staging_growths_ = 0;
+    double dispatch_max_ms_ = 0.0;  // longest host step of the dispatcher (launch or finish)
     // statistics
     uint64_t submitted_ = 0, completed_ = 0, failed_count_ = 0;
     uint64_t updates_done_ = 0, queries_done_ = 0, points_done_ = 0;
