@@ -610,6 +610,25 @@ def main():
     d2h = B * CELLS * (3 * 16 + 4)
     h2d = 8  # one absolute time per frame (double)
 
+    # ---- the same, narrowed to RGBA16F on the device (the viewer's upload format) ----
+    half = [torch.empty((B, CELLS, 4), dtype=torch.int16, pin_memory=True) for _ in range(3)]
+    hd, hn, hv = (t.numpy().view(np.uint16) for t in half)
+    for _ in range(2):
+        frame += 1
+        batch.update_host_rgba16([frame * dt], dt, hd, hn, hv)
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        frame += 1
+        batch.update_host_rgba16([frame * dt], dt, hd, hn, hv)
+    h_s = time.perf_counter() - t0
+    if world > 1:
+        h_s = max_over_ranks(h_s, torch.distributed, "cuda")
+    e2e_half = {"value": B * e2e_steps * world / h_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": B * CELLS * 3 * 8,
+                "api": "ocean_batch_update_host_rgba16 (RGBA16F packed on the device, foam in the alpha)"}
+
     # ---- the tensor-core DFT form on the same workload, beside the FP32 form ----
     tc = None
     if args.form != "tensor":
@@ -696,7 +715,8 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "api": "ocean_batch_update_host (pinned host buffers)"},
+                    "d2h_bytes_per_step": d2h, "api": "ocean_batch_update_host (pinned host buffers)",
+                    "rgba16": e2e_half},
         }
         if tc is not None:
             tc["vs_plain_fp32"] = tc["value"] / value

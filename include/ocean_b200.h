@@ -388,6 +388,25 @@ OCEAN_API ocean_status ocean_batch_update_host(ocean_batch* batch, const double*
                                                float* displacement, float* normal,
                                                float* velocity, float* foam);
 
+/* As ocean_batch_update_host, with every output narrowed to RGBA16F on the
+ * device (IEEE round-to-nearest-even, overflow to infinity) before the copy -
+ * half the bytes. With persistent foam the displacement's alpha is the
+ * persistent foam rather than the frame's Jacobian foam, as the reference
+ * viewer's upload substitutes it (examples/viewer/ocean_view.cpp:830-862).
+ * Arrays of count * N * N * 4 uint16 (binary16 bit patterns); any may be NULL. */
+OCEAN_API ocean_status ocean_batch_update_host_rgba16(ocean_batch* batch, const double* times,
+                                                      int32_t per_ocean_times, float foam_dt,
+                                                      uint16_t* displacement, uint16_t* normal,
+                                                      uint16_t* velocity);
+
+/* The reference viewer's pack_rgba16 (examples/viewer/half.hpp:99-112) on the
+ * device: `texels` RGBA32F texels of `src` to RGBA16F in `dst`, the alpha taken
+ * from `alpha` (one float per texel) when it is not NULL. Device pointers;
+ * queued on `stream` (a cudaStream_t). Bit-identical to the reference's
+ * float_to_half, NaNs included. */
+OCEAN_API ocean_status ocean_pack_rgba16(const float* src, const float* alpha, uint64_t texels,
+                                         uint16_t* dst, void* stream);
+
 OCEAN_API ocean_status ocean_batch_get_device_buffers(const ocean_batch* batch, uint32_t index,
                                                       ocean_device_buffers* out);
 

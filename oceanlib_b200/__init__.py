@@ -291,6 +291,22 @@ class OceanBatch:
                                              ptr(disp), ptr(normal), ptr(velocity), ptr(foam)),
                "ocean_batch_update_host")
 
+    def update_host_rgba16(self, times, foam_dt: float, disp: Optional[np.ndarray],
+                           normal: Optional[np.ndarray] = None,
+                           velocity: Optional[np.ndarray] = None) -> None:
+        """The frame with its outputs narrowed to RGBA16F on the device (uint16
+        arrays of binary16 bits, count * N * N * 4); with persistent foam the
+        displacement alpha carries the foam, as the reference viewer packs it."""
+        t = np.ascontiguousarray(np.atleast_1d(np.asarray(times, dtype=np.float64)))
+        per = 1 if t.size > 1 else 0
+        for a in (disp, normal, velocity):
+            if a is not None and (a.dtype != np.uint16 or not a.flags.c_contiguous):
+                raise ValueError("RGBA16F outputs are contiguous uint16 arrays")
+        ptr = lambda a: None if a is None else a.ctypes.data
+        _check(lib().ocean_batch_update_host_rgba16(self._h, t.ctypes.data, per, float(foam_dt),
+                                                    ptr(disp), ptr(normal), ptr(velocity)),
+               "ocean_batch_update_host_rgba16")
+
     def synchronize(self) -> None:
         _check(lib().ocean_batch_synchronize(self._h), "ocean_batch_synchronize")
 

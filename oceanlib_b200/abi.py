@@ -206,6 +206,9 @@ class ServerStatsC(C.Structure):
 # Every function include/ocean_b200.h declares, with its ctypes signature.
 SIGNATURES = {
     "ocean_dft_batch": (C.c_int, [C.c_uint32, C.c_uint32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ocean_batch_update_host_rgba16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_float, C.c_void_p,
+                                                 C.c_void_p, C.c_void_p]),
+    "ocean_pack_rgba16": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
     "ocean_server_desc_init": (None, [C.POINTER(ServerDescC)]),
     "ocean_server_create": (C.c_void_p, [C.POINTER(ServerDescC), C.POINTER(C.c_int)]),
     "ocean_server_destroy": (None, [C.c_void_p]),

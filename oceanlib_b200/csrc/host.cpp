@@ -448,6 +448,37 @@ public:
         if (take_error()) throw TimeoutError();
     }
 
+    // The frame, then every output narrowed to RGBA16F on the device - the
+    // displacement's alpha replaced by the persistent foam when the batch has
+    // it, as the reference viewer's upload does (examples/viewer/
+    // ocean_view.cpp:830-862) - and copied to the host: half the bytes of
+    // update_host. Any output pointer may be null.
+    void update_host_rgba16(const double* times, bool per_ocean, float foam_dt, uint16_t* h_disp,
+                            uint16_t* h_normal, uint16_t* h_vel)
+    {
+        update(times, per_ocean, foam_dt, stream_);
+        const size_t texels = cells_ * count_;
+        if (half_.n < texels * 3) half_ = DevBuf<ushort4>(texels * 3);
+        ushort4* hd = half_.p;
+        ushort4* hn = hd + texels;
+        ushort4* hv = hn + texels;
+        const size_t bytes = texels * sizeof(ushort4);
+        if (h_disp) {
+            check(launch_pack_rgba16(disp_.p, foam_on_ ? foam_ptr(0) : nullptr, texels, hd, stream_), "pack");
+            check(cudaMemcpyAsync(h_disp, hd, bytes, cudaMemcpyDeviceToHost, stream_), "copy displacement");
+        }
+        if (h_normal) {
+            check(launch_pack_rgba16(normal_.p, nullptr, texels, hn, stream_), "pack");
+            check(cudaMemcpyAsync(h_normal, hn, bytes, cudaMemcpyDeviceToHost, stream_), "copy normal");
+        }
+        if (h_vel && velocity_) {
+            check(launch_pack_rgba16(velocity_buf_.p, nullptr, texels, hv, stream_), "pack");
+            check(cudaMemcpyAsync(h_vel, hv, bytes, cudaMemcpyDeviceToHost, stream_), "copy velocity");
+        }
+        check(cudaStreamSynchronize(stream_), "frame");
+        if (take_error()) throw TimeoutError();
+    }
+
     // Reads and clears the sticky error word of the persistent kernel (set
     // when one of its bounded waits gave up). Synchronises the batch stream.
     bool take_error()
@@ -706,6 +737,7 @@ private:
     DevBuf<double> top_;
     HostBuf<double> top_host_;
     DevBuf<float4> disp_, normal_, velocity_buf_;
+    DevBuf<ushort4> half_;  // RGBA16F staging of update_host_rgba16 (allocated on first use)
     DevBuf<float> foam_a_, foam_b_;
     int foam_cur_ = 0;
     ocean_foam_desc foam_{};
@@ -1465,6 +1497,27 @@ ocean_status ocean_batch_update_host(ocean_batch* batch, const double* times, in
     if (batch == nullptr || times == nullptr) return OCEAN_ERROR_INVALID_ARG;
     return guarded([&] {
         batch->impl.update_host(times, per_ocean_times != 0, foam_dt, displacement, normal, velocity, foam);
+    });
+}
+
+ocean_status ocean_batch_update_host_rgba16(ocean_batch* batch, const double* times, int32_t per_ocean_times,
+                                            float foam_dt, uint16_t* displacement, uint16_t* normal,
+                                            uint16_t* velocity)
+{
+    if (batch == nullptr || times == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] {
+        batch->impl.update_host_rgba16(times, per_ocean_times != 0, foam_dt, displacement, normal, velocity);
+    });
+}
+
+ocean_status ocean_pack_rgba16(const float* src, const float* alpha, uint64_t texels, uint16_t* dst, void* stream)
+{
+    if (texels > 0 && (src == nullptr || dst == nullptr)) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] {
+        ocean_b200::check(ocean_b200::launch_pack_rgba16(reinterpret_cast<const float4*>(src), alpha, texels,
+                                                         reinterpret_cast<ushort4*>(dst),
+                                                         static_cast<cudaStream_t>(stream)),
+                          "pack");
     });
 }
 

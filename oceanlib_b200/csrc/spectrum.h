@@ -128,6 +128,10 @@ struct CascadeLevels {
 cudaError_t launch_cascade_sample(const CascadeLevels& levels, const float2* xz, uint64_t count,
                                   SurfaceEx* out, int iters, float tol, cudaStream_t stream);
 
+// RGBA32F -> RGBA16F, alpha optionally from a separate plane (pack.cu).
+cudaError_t launch_pack_rgba16(const float4* src, const float* alpha, uint64_t cells, ushort4* dst,
+                               cudaStream_t st);
+
 // Shared-memory bytes each pass needs at a given size (for checks).
 size_t row_pass_smem(int log_n, int nf);
 size_t col_pass_smem(int log_n, int nf);

@@ -153,6 +153,7 @@ def ref() -> C.CDLL:
             "oref_time_updates": (C.c_double, [_P, _P, C.c_uint32, C.c_uint32, C.c_double,
                                                C.c_double, C.c_float]),
             "oref_hardware_concurrency": (C.c_uint32, []),
+            "oref_pack_rgba16": (None, [_P, _P, _P, C.c_uint64]),
         }
         for name, (res, args) in sig.items():
             f = getattr(l, name)
@@ -334,6 +335,30 @@ def fp64_frame(desc, t: float) -> dict:
            "normal": np.stack([nx * inv, ny * inv, nz * inv, jac], axis=-1)}
     if g.shape[0] > 4:
         out["velocity"] = np.stack([g[4].real, g[4].imag, g[5].real, np.zeros_like(h)], axis=-1)
+    return out
+
+
+def pack_rgba16(src: np.ndarray, alpha: Optional[np.ndarray] = None) -> np.ndarray:
+    """The viewer's RGBA16F upload pack restated (examples/viewer/half.hpp:58-112):
+    binary32 -> binary16 round-to-nearest-even, overflow to infinity, a NaN
+    becomes sign | 0x7E00; alpha from `alpha` when given. (cells, 4) uint16."""
+    src = np.ascontiguousarray(src, dtype=np.float32).reshape(-1, 4).copy()
+    if alpha is not None:
+        src[:, 3] = np.ascontiguousarray(alpha, dtype=np.float32).reshape(-1)
+    with np.errstate(over="ignore"):
+        h = src.astype(np.float16).view(np.uint16)
+    nan = np.isnan(src)
+    h[nan] = ((src.view(np.uint32)[nan] >> 16) & 0x8000).astype(np.uint16) | np.uint16(0x7E00)
+    return h
+
+
+def ref_pack_rgba16(src: np.ndarray, alpha: Optional[np.ndarray] = None) -> np.ndarray:
+    """The reference's own scalar pack (examples/viewer/half.hpp:99-112)."""
+    src = np.ascontiguousarray(src, dtype=np.float32).reshape(-1, 4)
+    cells = src.shape[0]
+    out = np.empty((cells, 4), np.uint16)
+    a = None if alpha is None else np.ascontiguousarray(alpha, dtype=np.float32).reshape(-1)
+    ref().oref_pack_rgba16(out.ctypes.data, src.ctypes.data, None if a is None else a.ctypes.data, cells)
     return out
 
 

@@ -22,6 +22,7 @@
 #include "core/fft.hpp"
 #include "core/rng.hpp"
 #include "core/spectrum.hpp"
+#include "half.hpp"  // examples/viewer (via -I)
 
 #include <chrono>
 #include <cstring>
@@ -407,4 +408,11 @@ OREF_API double oref_i_time_updates(void* f, const ocean_disturbance* d, uint32_
     }
     const auto end = std::chrono::steady_clock::now();
     return std::chrono::duration<double>(end - start).count();
+}
+
+// The viewer's RGBA16F upload pack (examples/viewer/half.hpp:58-112), the
+// scalar path, header-only: compiled from the reference's header.
+OREF_API void oref_pack_rgba16(uint16_t* dst, const float* src, const float* alpha, uint64_t cells)
+{
+    viewer::pack_rgba16_scalar(dst, src, alpha, static_cast<std::size_t>(cells));
 }

@@ -11,6 +11,7 @@ Outputs
                    without storing the arrays
   ref_queries.npz  reference sample_at results for seeded query points
   ref_cascade.npz  reference CascadeStack::sample_at results (3 levels)
+  ref_pack.json    sha256 of the viewer's RGBA16F pack over seeded bit patterns
   abi_layout.json  offsets/sizes of the reference's C structs (include/ocean/ocean.h)
 """
 from __future__ import annotations
@@ -30,7 +31,7 @@ sys.path.insert(0, str(ROOT))
 import oracle as O  # noqa: E402
 from oceanlib_b200.abi import OceanDescC  # noqa: E402
 from tests.workloads import (SMALL_CASES, HASH_CASES, FOAM_CASE, QUERY_CASE, CASCADE_CASE,  # noqa: E402
-                             desc_to_json, query_points, cascade_points)
+                             desc_to_json, query_points, cascade_points, pack_patterns)
 
 HERE = Path(__file__).resolve().parent
 
@@ -164,6 +165,16 @@ int main(void) {
     (HERE / "abi_layout.json").write_text(json.dumps(layout, indent=1))
 
 
+def pack() -> None:
+    """sha256 of the reference viewer's RGBA16F pack (examples/viewer/half.hpp)
+    over the bit patterns of workloads.pack_patterns, without and with the
+    separate alpha plane."""
+    src, alpha = pack_patterns()
+    out = {"texels": int(src.shape[0]), "plain": sha(O.ref_pack_rgba16(src)),
+           "alpha": sha(O.ref_pack_rgba16(src, alpha))}
+    (HERE / "ref_pack.json").write_text(json.dumps(out, indent=1))
+
+
 def main() -> None:
     if not O.ref_available():
         raise SystemExit("the reference library could not be built (reference sources absent)")
@@ -173,6 +184,7 @@ def main() -> None:
     queries()
     cascades()
     interaction()
+    pack()
     abi_layout()
     print("golden fixtures written to", HERE)
 

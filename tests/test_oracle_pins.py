@@ -217,3 +217,16 @@ def test_oracle_cascade_matches_reference():
     levels, t, count = CASCADE_CASE
     got = oracle_cascade(levels, t, g["xz"])
     assert np.array_equal(bits(got), bits(g["out"]))
+
+
+def test_pack_rgba16_matches_reference_viewer_pack():
+    # examples/viewer/half.hpp: the oracle's RGBA16F pack against the sha256 of
+    # the reference's own pack over every exponent, subnormals, infinities and
+    # NaNs, with and without the separate alpha plane.
+    from tests.workloads import pack_patterns
+
+    golden = json.loads((GOLDEN / "ref_pack.json").read_text())
+    src, alpha = pack_patterns()
+    assert src.shape[0] == golden["texels"]
+    assert sha(O.pack_rgba16(src)) == golden["plain"]
+    assert sha(O.pack_rgba16(src, alpha)) == golden["alpha"]

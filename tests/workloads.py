@@ -115,3 +115,19 @@ def query_points(desc: OceanDesc, count: int) -> np.ndarray:
     edge = np.array([[0, 0], [L, L], [-L, 0], [cell, 2 * cell], [L - 1e-3, 0.5],
                      [1e4 * L, -1e4 * L], [-0.0, 0.0], [3 * cell, -5 * cell]], dtype=np.float32)
     return np.concatenate([pts, edge]).astype(np.float32)
+
+
+def pack_patterns():
+    """Float bit patterns for the RGBA16F pack: every upper half-word with a
+    few low half-words (all exponents, subnormals, infinities, NaNs) plus
+    seeded random words, as (texels, 4) float32, and a seeded alpha plane."""
+    hi = np.arange(1 << 16, dtype=np.uint32) << 16
+    lows = np.array([0, 1, 0x0FFF, 0x1000, 0x1001, 0x2000, 0x3000, 0xFFFF, 0x8000, 0x7FFF, 0xE000, 0xF000],
+                    np.uint32)
+    bits = (hi[:, None] | lows[None, :]).reshape(-1)
+    rng = np.random.default_rng(2024)
+    bits = np.concatenate([bits, rng.integers(0, 2 ** 32, 1 << 20, dtype=np.uint64).astype(np.uint32)])
+    bits = bits[: len(bits) // 4 * 4]
+    src = bits.view(np.float32).reshape(-1, 4)
+    alpha = rng.standard_normal(src.shape[0]).astype(np.float32)
+    return src, alpha
