@@ -48,6 +48,7 @@ dft_tc512_kernel(const float2* __restrict__ in, float2* __restrict__ out, int co
 {
     constexpr int N = 512, NT = tc::kThreads;
     constexpr int SEQ = padded_len(N) + kSeqPad;
+    static_assert(SEQ * 2 >= 16 * tc::kZStride, "a sequence's space must hold its staged stage-3 rows");
     extern __shared__ float4 smem4[];
     float2* data = reinterpret_cast<float2*>(smem4);
     float2* tws = data + 8 * SEQ;

@@ -38,6 +38,7 @@ __device__ __forceinline__ void transform_all(float2* data, const float2* tws, i
 {
     if constexpr (TC) {
         static_assert(LOG_N == 9, "the tensor-core form is built for N = 512");
+        static_assert(SEQ * 2 >= 16 * tc::kZStride, "a sequence's space must hold its staged stage-3 rows");
 #pragma unroll 1
         for (int s0 = 0; s0 < COUNT; s0 += tc::kSeq)
             eng->dft512(data + s0 * SEQ, SEQ, COUNT - s0 < tc::kSeq ? COUNT - s0 : tc::kSeq, tws, tid, error);

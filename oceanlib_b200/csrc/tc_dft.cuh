@@ -58,6 +58,7 @@ constexpr int kLevels = 4;       // digit-pair levels kept (i + j < 4)
 // 128 t + 32 L; stage 3 level L at 64 L. All 256 columns.
 constexpr int kTmemCols = 256;
 constexpr int kThreads = 256;    // the engine's working threads (8 warps)
+constexpr int kZStride = 68;     // floats per staged stage-3 row (64 + 4 against bank conflicts)
 constexpr int kFixExp = 29;      // row max scaled into [2^29, 2^30)
 constexpr int kBExp = 30;        // DFT matrices scaled by 2^30
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
@@ -365,6 +366,7 @@ struct Engine {
         fence_after_sync();
 
         // ---- read Y, twiddle, stage 3 operand: row (s, k1), K = (p, n2) ----
+        float* zbuf = reinterpret_cast<float*>(data);
         if (worker) {
             const int t = warp >> 2;
             const uint32_t col = tmem + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + t * 128;
@@ -387,35 +389,60 @@ struct Engine {
                 for (int j = 0; j < 32; ++j)
                     y[j] = (y[j] + __uint_as_float(r2[j]) * pow2f(2 - e1)) + __uint_as_float(r3[j]) * pow2f(-6 - e1);
             }
-            float zr[16], zi[16];
+            // Z staged as FP32, stage-3 row (s, k1) at zbuf + (s * 16 + k1) *
+            // kZStride, K = (p, n2), in the sequences' own buffer: every
+            // thread's inputs are in registers since stage 1, and the staging
+            // (count * 4352 B) fits inside the count sequences' space.
+            if (s_row < count) {
 #pragma unroll
-            for (int k1 = 0; k1 < 16; ++k1) {
-                const int e = n2 * k1;  // < 512
-                float2 w = tws[e & 255];
-                if (e & 256) w = make_float2(-w.x, -w.y);
-                zr[k1] = y[k1] * w.x - y[16 + k1] * w.y;
-                zi[k1] = y[k1] * w.y + y[16 + k1] * w.x;
-            }
-            // per stage-3 row (s, k1): the maximum over the warp's 32 n2
-#pragma unroll
-            for (int k1 = 0; k1 < 16; ++k1) {
-                float m = fmaxf(fabsf(zr[k1]), fabsf(zi[k1]));
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-                const int ex3 = row_exp(m);
-                const float sc = pow2f(ex3);
-                const int row = s_row * 16 + k1;
-                uint16_t dr[4], di[4];
-                digits4(__float2int_rn(zr[k1] * sc), dr);
-                digits4(__float2int_rn(zi[k1] * sc), di);
-                const int o_r = kmajor(row, n2, kK3), o_i = kmajor(row, 32 + n2, kK3);
-#pragma unroll
-                for (int g = 0; g < kDigits; ++g) {
-                    a0p[g * kAHalves + o_r] = dr[g];
-                    a0p[g * kAHalves + o_i] = di[g];
+                for (int k1 = 0; k1 < 16; ++k1) {
+                    const int e = n2 * k1;  // < 512
+                    float2 w = tws[e & 255];
+                    if (e & 256) w = make_float2(-w.x, -w.y);
+                    float* zrow = zbuf + (s_row * 16 + k1) * kZStride;
+                    zrow[n2] = y[k1] * w.x - y[16 + k1] * w.y;
+                    zrow[32 + n2] = y[k1] * w.y + y[16 + k1] * w.x;
                 }
-                if (lane == 0) e3()[row] = ex3;
             }
+        }
+        __syncthreads();
+        // ---- stage 3 operand: two threads per row (s, k1), each 32 of its K ----
+        if (worker) {
+            const int row = tid >> 1, half_k = tid & 1;
+            const int s = row >> 4;
+            float v[32];
+            float m = 0.0f;
+            if (s < count) {
+                const float4* src = reinterpret_cast<const float4*>(zbuf + row * kZStride + half_k * 32);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const float4 f = src[q];
+                    v[4 * q] = f.x;
+                    v[4 * q + 1] = f.y;
+                    v[4 * q + 2] = f.z;
+                    v[4 * q + 3] = f.w;
+                    m = fmaxf(m, fmaxf(fmaxf(fabsf(f.x), fabsf(f.y)), fmaxf(fabsf(f.z), fabsf(f.w))));
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < 32; ++k) v[k] = 0.0f;
+            }
+            m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
+            const int ex3 = row_exp(m);
+            const float sc = pow2f(ex3);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                uint16_t d[8][4];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) digits4(__float2int_rn(v[8 * c + q] * sc), d[q]);
+                const int off = kmajor(row, half_k * 32 + 8 * c, kK3);
+#pragma unroll
+                for (int g = 0; g < kDigits; ++g)
+                    *reinterpret_cast<uint4*>(a0p + g * kAHalves + off) =
+                        make_uint4(pack2(d[0][g], d[1][g]), pack2(d[2][g], d[3][g]), pack2(d[4][g], d[5][g]),
+                                   pack2(d[6][g], d[7][g]));
+            }
+            if (half_k == 0) e3()[row] = ex3;
         }
         fence_proxy_async();
         fence_before_sync();
