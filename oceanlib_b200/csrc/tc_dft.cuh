@@ -309,11 +309,13 @@ struct Engine {
         const int warp = tid >> 5, lane = tid & 31;
         const bool worker = tid < kThreads;
         uint16_t* a0p = a(0);
+        // Stage-1 tile 1 holds sequences 4..7: skipped when there are none.
+        const int tiles1 = count > 4 ? 2 : 1;
 
         // ---- stage 1 operand: row r = (s, n2), 16 complex x[32 n1 + n2] ----
         int e1 = 0;
         const int s_row = tid >> 5, n2 = tid & 31;
-        if (worker) {
+        if (worker && tid < tiles1 * 128) {
             float v[32];
             float m = 0.0f;
             if (s_row < count) {
@@ -349,13 +351,13 @@ struct Engine {
         __syncthreads();
         fence_after_sync();
 
-        // ---- stage 1 MMAs: 2 tiles x 2 K steps x 10 digit pairs ----
+        // ---- stage 1 MMAs: tiles1 tiles x 2 K steps x 10 digit pairs ----
         if (tid == 0) {
             const uint32_t abase = smem_u32(a0p), bbase = smem_u32(smem + kOffB1);
             constexpr uint32_t sbo = kK1 * 16;
             constexpr uint32_t idesc = instr_desc(128, kN1);
 #pragma unroll 1
-            for (int t = 0; t < 2; ++t)
+            for (int t = 0; t < tiles1; ++t)
 #pragma unroll 1
                 for (int ks = 0; ks < kK1 / 16; ++ks)
                     issue_levels(tmem + t * 128, kN1, abase, bbase, kAHalves * 2, kN1 * kK1 * 2, ks * 256,
@@ -367,7 +369,7 @@ struct Engine {
 
         // ---- read Y, twiddle, stage 3 operand: row (s, k1), K = (p, n2) ----
         float* zbuf = reinterpret_cast<float*>(data);
-        if (worker) {
+        if (worker && (warp >> 2) < tiles1) {
             const int t = warp >> 2;
             const uint32_t col = tmem + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + t * 128;
             float y[32];
