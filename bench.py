@@ -302,23 +302,39 @@ def bench_ensemble(torch, frames: int = 30):
     ens = ob.OceanEnsemble(descs, autotune=True)
     stream = torch.cuda.Stream()
     sh = stream.cuda_stream
-    for k in range(3):
-        ens.update(k / 60.0, stream=sh)
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
-    for k in range(frames):
-        ens.update(1.0 + k / 60.0, stream=sh)
-    b.record(stream)
-    torch.cuda.synchronize()
-    ms = a.elapsed_time(b) / frames
+
+    def timed(graph: bool):
+        ens.set_graph(graph)
+        for k in range(3):
+            ens.update(k / 60.0, stream=sh)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for k in range(frames):
+            ens.update(1.0 + k / 60.0, stream=sh)
+        b.record(stream)
+        torch.cuda.synchronize()
+        # host cost of issuing one frame, with the GPU idle
+        host = []
+        for k in range(10):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ens.update(2.0 + k / 60.0, stream=sh)
+            host.append((time.perf_counter() - t0) * 1e6)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / frames, float(np.median(host))
+
+    ms_calls, host_calls = timed(False)
+    ms, host_graph = timed(True)  # the default: one graph replay per frame
     cells = sum(d.size * d.size for d in descs)
     res = {"workload": "ensemble_64 (N in 64..1024, seeded, velocity off)",
            "frames_per_s": 1000.0 / ms, "ms_per_frame": ms,
            "ocean_updates_per_s": len(descs) * 1000.0 / ms,
            "cells_per_s": cells * 1000.0 / ms,
            "equiv_512sq_updates_per_s": cells / (512 * 512) * 1000.0 / ms,
-           "schedule": ens.schedule}
+           "schedule": ens.schedule,
+           "cuda_graph": {"ms_per_frame": ms, "host_us_per_update": host_graph},
+           "per_call_launches": {"ms_per_frame": ms_calls, "host_us_per_update": host_calls}}
     ens.close()
     return res
 

@@ -441,6 +441,11 @@ OCEAN_API uint32_t ocean_ensemble_count(const ocean_ensemble* ensemble);
  * ensemble's stream). */
 OCEAN_API ocean_status ocean_ensemble_update(ocean_ensemble* ensemble, double time, void* stream);
 OCEAN_API ocean_status ocean_ensemble_synchronize(ocean_ensemble* ensemble);
+/* With enable != 0 (the default) each update replays one CUDA graph of the
+ * whole frame - the time upload, the fork onto one stream per size, every
+ * size's persistent launch and the join - captured at the first update under
+ * the schedule the autotuner chose; with 0, each update issues the calls. */
+OCEAN_API ocean_status ocean_ensemble_set_graph(ocean_ensemble* ensemble, int32_t enable);
 OCEAN_API ocean_status ocean_ensemble_device_buffers(const ocean_ensemble* ensemble, uint32_t index,
                                                      ocean_device_buffers* out);
 /* The chosen schedule in words (with the timings that chose it); returns the

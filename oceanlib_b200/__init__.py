@@ -370,6 +370,10 @@ class OceanEnsemble:
     def update(self, time: float, stream: int = 0) -> None:
         _check(lib().ocean_ensemble_update(self._h, float(time), C.c_void_p(stream)), "ocean_ensemble_update")
 
+    def set_graph(self, enable: bool) -> None:
+        """Replay the frame as one CUDA graph (default) or issue each call."""
+        _check(lib().ocean_ensemble_set_graph(self._h, 1 if enable else 0), "ocean_ensemble_set_graph")
+
     def synchronize(self) -> None:
         _check(lib().ocean_ensemble_synchronize(self._h), "ocean_ensemble_synchronize")
 

@@ -362,6 +362,26 @@ public:
         }
     }
 
+    // One frame of every ocean (no persistent foam) with the per-ocean
+    // t / 2 pi already on the device at `top` (count doubles): device work
+    // only, on `st` - the form a CUDA graph captures. The launch shapes must
+    // be known already (one ordinary update first).
+    void enqueue_frame(const double* top, cudaStream_t st)
+    {
+        if (foam_on_) throw std::invalid_argument("enqueue_frame: no persistent foam in this form");
+        FrameArgs a = frame_args(top);
+        if (persistent_) {
+            run_frame(a, 0, count_, false, st);
+        } else {
+            for (uint32_t base = 0; base < count_; base += chunk_) {
+                a.ocean_base = static_cast<int32_t>(base);
+                a.chunk = static_cast<int32_t>(std::min(chunk_, count_ - base));
+                run_row(a, st);
+                run_col(a, st, false);
+            }
+        }
+    }
+
     // Stage-by-stage form for the parallel_for compatibility path: stage 0 is
     // the row pass of every chunk, stage 1 the column pass (plus foam).
     void update_stage(int stage, const double* times, cudaStream_t st)
@@ -595,14 +615,7 @@ private:
         q.count = static_cast<int32_t>(k);
         q.slots = slots_;
         q.wait_ns = 1000000000ull;
-        int& grid = frame_grid_[foam ? 1 : 0];
-        if (grid == 0) {
-            int sms = 0;
-            check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "SM count");
-            const int per_sm = frame_blocks_per_sm(log_n_, nf_, form_, foam);
-            if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "frame occupancy");
-            grid = per_sm * sms;
-        }
+        const int grid = frame_grid(foam);
         // A share below 1 leaves SMs to batches of other sizes running
         // concurrently (the ensemble's schedule).
         const int shared = std::max(1, static_cast<int>(std::lround(grid * grid_share_)));
@@ -620,6 +633,28 @@ private:
         });
     }
     static constexpr double kInvTwoPi = 0.159154943091895335769;
+
+    // One wave of resident CTAs of the persistent kernel (computed once).
+    int frame_grid(bool foam)
+    {
+        int& grid = frame_grid_[foam ? 1 : 0];
+        if (grid == 0) {
+            int sms = 0;
+            check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "SM count");
+            const int per_sm = frame_blocks_per_sm(log_n_, nf_, form_, foam);
+            if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "frame occupancy");
+            grid = per_sm * sms;
+        }
+        return grid;
+    }
+
+public:
+    // t / 2 pi as every frame hoists it (src/core/evolve.cpp:33).
+    static double time_over_2pi(double t) { return t * kInvTwoPi; }
+    // Settles the launch shapes, so a capture issues launches only.
+    void prime_shapes() { (void)frame_grid(false); }
+
+private:
 
     FrameArgs frame_args(const double* top) const
     {
@@ -1086,11 +1121,24 @@ public:
         concurrent_ = true;
         describe_ = "concurrent, SM shares by work estimate";
         if (tune) autotune();
+        // The frame's times: one pinned block, one device block, batch g's
+        // oceans from toff_[g].
+        size_t off = 0;
+        for (auto& b : batches_) {
+            toff_.push_back(off);
+            off += b->count();
+        }
+        gtimes_ = HostBuf<double>(off);
+        dtimes_ = DevBuf<double>(off);
+        check(cudaEventCreateWithFlags(&copied_, cudaEventDisableTiming), "event");
+        use_graph_ = true;  // after the autotuner, which times per-call launches
     }
 
     ~Ensemble()
     {
         if (stream_) cudaStreamSynchronize(stream_);
+        drop_graph();
+        if (copied_) cudaEventDestroy(copied_);
         for (auto s : streams_) {
             cudaStreamSynchronize(s);
             cudaStreamDestroy(s);
@@ -1103,6 +1151,16 @@ public:
     void update(double t, cudaStream_t st)
     {
         if (st == nullptr) st = stream_;
+        if (use_graph_) {
+            // The whole frame - time upload, fork, every size's persistent
+            // launch, join - is one CUDA graph, captured once and replayed.
+            if (exec_ == nullptr) build_graph();
+            check(cudaEventSynchronize(copied_), "time staging");  // the last replay read it
+            const double top = Batch::time_over_2pi(t);
+            for (size_t i = 0; i < gtimes_.n; ++i) gtimes_.p[i] = top;
+            check(cudaGraphLaunch(exec_, st), "graph launch");
+            return;
+        }
         if (!concurrent_) {
             for (auto& b : batches_) b->update(&t, false, 0.0f, st);
             return;
@@ -1116,6 +1174,17 @@ public:
         }
     }
 
+    // Graph replay on (the default) or per-call launches.
+    void set_graph(bool on)
+    {
+        if (!on) {
+            check(cudaStreamSynchronize(stream_), "sync");
+            drop_graph();
+        }
+        use_graph_ = on;
+    }
+    bool graph() const { return use_graph_; }
+
     uint32_t count() const { return static_cast<uint32_t>(where_.size()); }
     cudaStream_t stream() const { return stream_; }
     const Batch& batch_of(uint32_t i) const { return *batches_[where_[i].first]; }
@@ -1123,6 +1192,50 @@ public:
     const std::string& description() const { return describe_; }
 
 private:
+    // Captures one frame under the chosen schedule: the upload of the pinned
+    // times, an event marking them read, then (concurrent) a fork onto one
+    // stream per size, each size's frame, and the join.
+    void build_graph()
+    {
+        for (auto& b : batches_) b->prime_shapes();
+        check(cudaStreamSynchronize(stream_), "sync");
+        check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed), "begin capture");
+        try {
+            check(cudaMemcpyAsync(dtimes_.p, gtimes_.p, gtimes_.n * sizeof(double), cudaMemcpyHostToDevice,
+                                  stream_), "times");
+            // An event-record node (external), so the host can wait on it
+            // between replays; a plain record inside a capture only orders
+            // the capture's own streams.
+            check(cudaEventRecordWithFlags(copied_, stream_, cudaEventRecordExternal), "event");
+            if (concurrent_) {
+                check(cudaEventRecord(fork_, stream_), "event");
+                for (size_t g = 0; g < batches_.size(); ++g) {
+                    check(cudaStreamWaitEvent(streams_[g], fork_, 0), "wait");
+                    batches_[g]->enqueue_frame(dtimes_.p + toff_[g], streams_[g]);
+                    check(cudaEventRecord(done_[g], streams_[g]), "event");
+                    check(cudaStreamWaitEvent(stream_, done_[g], 0), "wait");
+                }
+            } else {
+                for (size_t g = 0; g < batches_.size(); ++g) batches_[g]->enqueue_frame(dtimes_.p + toff_[g], stream_);
+            }
+        } catch (...) {
+            cudaGraph_t broken = nullptr;
+            cudaStreamEndCapture(stream_, &broken);
+            if (broken) cudaGraphDestroy(broken);
+            throw;
+        }
+        check(cudaStreamEndCapture(stream_, &graph_), "end capture");
+        check(cudaGraphInstantiate(&exec_, graph_, 0), "graph instantiate");
+    }
+
+    void drop_graph()
+    {
+        if (exec_) cudaGraphExecDestroy(exec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        exec_ = nullptr;
+        graph_ = nullptr;
+    }
+
     void apply_shares(const std::vector<double>& weights)
     {
         double total = 0.0;
@@ -1204,6 +1317,14 @@ private:
     cudaEvent_t fork_ = nullptr;
     bool concurrent_ = true;
     std::string describe_;
+    // graph replay of the frame
+    bool use_graph_ = false;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+    HostBuf<double> gtimes_;
+    DevBuf<double> dtimes_;
+    std::vector<size_t> toff_;
+    cudaEvent_t copied_ = nullptr;
 };
 
 }  // namespace ocean_b200
@@ -1586,6 +1707,12 @@ ocean_status ocean_ensemble_update(ocean_ensemble* ensemble, double time, void* 
 {
     if (ensemble == nullptr) return OCEAN_ERROR_INVALID_ARG;
     return guarded([&] { ensemble->impl.update(time, static_cast<cudaStream_t>(stream)); });
+}
+
+ocean_status ocean_ensemble_set_graph(ocean_ensemble* ensemble, int32_t enable)
+{
+    if (ensemble == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { ensemble->impl.set_graph(enable != 0); });
 }
 
 ocean_status ocean_ensemble_synchronize(ocean_ensemble* ensemble)

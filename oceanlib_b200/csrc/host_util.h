@@ -24,7 +24,13 @@ struct TimeoutError : std::runtime_error {
 
 inline void check(cudaError_t e, const char* what)
 {
-    if (e != cudaSuccess) throw DeviceError(e, what);
+    if (e != cudaSuccess) {
+        // Reset the runtime's last-error slot, so a later launch's
+        // cudaGetLastError reports that launch and not this failure (sticky
+        // errors that poison the context stay set regardless).
+        cudaGetLastError();
+        throw DeviceError(e, what);
+    }
 }
 
 inline ocean_status status_of(const DeviceError& e)
