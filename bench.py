@@ -45,6 +45,9 @@ ALG_BYTES_PER_CELL = 64
 # writes the three RGBA32F outputs and reads/writes foam (56 B/cell).
 COL_ALG_BYTES_PER_CELL = 56
 ROW_ALG_BYTES_PER_CELL = 8
+# The reference bench_update unit (velocity and foam off): h0 read 8 B +
+# displacement and normal RGBA32F written 32 B.
+PLAIN_ALG_BYTES_PER_CELL = 40
 L2_BYTES = 126 * 2 ** 20
 
 
@@ -337,6 +340,104 @@ def bench_ensemble(torch, frames: int = 30):
            "per_call_launches": {"ms_per_frame": ms_calls, "host_us_per_update": host_calls}}
     ens.close()
     return res
+
+
+def bench_plain_update(torch, batch: int = 64, steps: int = 60, cpu_seconds: float = 0.0):
+    """The reference bench_update unit of work (bench/bench_update.cpp:91-102,
+    :72): 512^2, 200 m, 12 m/s, wind direction 0.4, choppiness 1, velocity
+    and foam off (4 packed complex FFT fields); `batch` oceans with seeds
+    1337 + b, step i at t = 100 + 0.0137 i. Algorithmic bytes: h0 read 8 B +
+    displacement and normal RGBA32F written 32 B = 40 B/cell."""
+    import oceanlib_b200 as ob
+    from oceanlib_b200 import abi
+    from oceanlib_b200 import workloads as W
+
+    descs = [W.bench_update_patch(512, seed=1337 + b) for b in range(batch)]
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    alg_update = PLAIN_ALG_BYTES_PER_CELL * CELLS
+    peak, peak_kind = measured_peaks()
+    out = {"workload": "bench_update_512 (N=512, L=200 m, U=12 m/s, dir 0.4, choppiness 1, "
+                       "velocity and foam off; seeds 1337+b, t = 100 + 0.0137 i)",
+           "oceans_per_launch": batch, "alg_bytes_per_update": alg_update}
+
+    def run(form):
+        b = ob.OceanBatch(descs, form=form)
+        step = [0]
+
+        def one():
+            b.update([100.0 + step[0] * 0.0137], stream=sh)
+            step[0] += 1
+
+        for _ in range(5):
+            one()
+        torch.cuda.synchronize()
+        b.set_profiling(True)
+        b.read_profile()
+        l0 = b.launch_count
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        ev[0].record(stream)
+        for i in range(steps):
+            one()
+            ev[i + 1].record(stream)
+        torch.cuda.synchronize()
+        prof = b.read_profile()
+        b.set_profiling(False)
+        launches = b.launch_count - l0
+        total_ms = ev[0].elapsed_time(ev[-1])
+        step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
+        res = {"value": batch * steps / (total_ms / 1000.0), "unit": UNIT,
+               "ms_per_step": total_ms / steps, "gpu_launches": int(launches),
+               "latency_ms": {"p50": float(np.percentile(step_ms, 50)),
+                              "p99": float(np.percentile(step_ms, 99))}}
+        if prof["frame_launches"] > 0:
+            launch_ms = prof["frame_ms"] / prof["frame_launches"]
+            alg = alg_update * batch * steps / prof["frame_launches"]
+            ach = alg / (launch_ms / 1000.0) / 1e9
+            res["roofline"] = {"bound": "hbm", "kernel": "frame_kernel", "achieved": ach,
+                               "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                               "peak_kind": peak_kind, "alg_bytes_per_launch": alg,
+                               "avg_launch_ms": launch_ms}
+        return b, res
+
+    b, out["fp32"] = run(abi.OCEAN_FFT_EXACT)
+    # end to end: displacement + normal copied to pinned host memory every step
+    pinned = [torch.empty((batch, CELLS, 4), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    disp, nrm = (t.numpy() for t in pinned)
+    for i in range(2):
+        b.update_host([100.0 + i * 0.0137], 0.0, disp, nrm)
+    e2e_steps = max(3, steps // 3)
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        b.update_host([100.0 + i * 0.0137], 0.0, disp, nrm)
+    e2e_s = time.perf_counter() - t0
+    out["e2e"] = {"value": batch * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8,
+                  "d2h_bytes_per_step": batch * CELLS * 32,
+                  "api": "ocean_batch_update_host (pinned host buffers)"}
+    b.close()
+    del pinned
+    tb, out["tensor_core_form"] = run(abi.OCEAN_FFT_TENSOR)
+    tb.close()
+    out["tensor_core_form"]["vs_plain_fp32"] = out["tensor_core_form"]["value"] / out["fp32"]["value"]
+    if cpu_seconds > 0:
+        import oracle as O
+
+        ro = O.RefOcean(W.bench_update_patch(512))
+        cores = int(O.ref().oref_hardware_concurrency())
+        for i in range(2):
+            ro.update(i * 0.013)
+        done, t0 = 0, time.perf_counter()
+        while True:
+            ro.update(100.0 + done * 0.0137)
+            done += 1
+            el = time.perf_counter() - t0
+            if el >= cpu_seconds and done >= 3:
+                break
+        out["reference_cpu"] = {"value": done / el, "unit": UNIT, "cores": cores,
+                                "kind": "reference",
+                                "sample": f"{done} sequential updates of one 512^2 ocean, "
+                                          f"reference thread pool over {cores} hardware threads"}
+    return out
 
 
 def bench_cascade_reference(seconds: float = 4.0):
@@ -739,7 +840,9 @@ def main():
             line["tensor_core_form"] = tc
         if not args.no_extra and world == 1:
             extra = {}
-            for name, fn in (("cascade", lambda: bench_cascade(torch)), ("iwave", bench_iwave),
+            plain_cpu = 0.0 if args.no_cpu_baseline else 4.0
+            for name, fn in (("bench_update_512", lambda: bench_plain_update(torch, cpu_seconds=plain_cpu)),
+                             ("cascade", lambda: bench_cascade(torch)), ("iwave", bench_iwave),
                              ("ensemble", lambda: bench_ensemble(torch)), ("serving", bench_serving)):
                 try:
                     extra[name] = fn()
