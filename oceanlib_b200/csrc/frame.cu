@@ -27,31 +27,16 @@
 namespace ocean_b200 {
 namespace {
 
-constexpr int kPad = 4;  // float2 padding between sequences in shared memory
-
-// The inverse DFT of the COUNT sequences at data + s * SEQ: the radix-2
-// Stockham FFT (one lane group per sequence), or with TC the tensor-core
-// four-step DFT, 8 sequences per engine call (N = 512).
-template <int LOG_N, int G, bool FAST, bool TC, int COUNT, int SEQ>
-__device__ __forceinline__ void transform_all(float2* data, const float2* tws, int tid, tc::Engine* eng,
-                                              unsigned* error)
-{
-    if constexpr (TC) {
-        static_assert(LOG_N == 9, "the tensor-core form is built for N = 512");
-        static_assert(SEQ * 2 >= 16 * tc::kZStride, "a sequence's space must hold its staged stage-3 rows");
-#pragma unroll 1
-        for (int s0 = 0; s0 < COUNT; s0 += tc::kSeq)
-            eng->dft512(data + s0 * SEQ, SEQ, COUNT - s0 < tc::kSeq ? COUNT - s0 : tc::kSeq, tws, tid, error);
-    } else {
-        fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);
-    }
-}
+constexpr int kPad = 4;   // float2 padding between sequences in shared memory
+constexpr int kPad4 = 3;  // float4 padding between sequence pairs (stride = 3 mod 8 float4)
 
 template <int LOG_N>
 struct Shape {
     static constexpr int N = 1 << LOG_N;
     static constexpr int G = lanes_for(LOG_N);                       // lanes / sequence
-    static constexpr int SEQ = padded_len(N) + kPad;                 // sequence stride
+    static constexpr int G2 = pair_lanes(LOG_N);                     // lanes / sequence pair
+    static constexpr int SEQ = padded_len(N) + kPad;                 // sequence stride (float2)
+    static constexpr int SEQ4 = padded_len4(N) + kPad4;              // pair stride (float4)
     static constexpr int RP = cmin(N / 2, 32 / G > 1 ? 32 / G : 1); // row pairs / CTA
     // columns / CTA of the per-chunk column kernel: 4 at N = 512 (128-byte
     // rows of the intermediate); 2 at N = 1024, where 32 values per lane
@@ -61,6 +46,61 @@ struct Shape {
     // column task use the same thread count (2 * NF * G * RP).
     static constexpr int PW = 2 * RP;
 };
+
+// Shared-memory layouts of the sequences a task transforms. The FP32 forms
+// keep fields 2p and 2p+1 of a row or column as one pair (float4 per index,
+// stride SEQ4 float4 = 2 SEQ4 float2 per pair, so SEQ4 float2 per sequence);
+// the tensor-core form keeps every sequence on its own (float2 per index,
+// stride SEQ). Twiddles follow the data: float4 (wx, wx, wy, wy) entries for
+// the pairs, float2 for the tensor-core form.
+template <int LOG_N, bool TC>
+__host__ __device__ constexpr int seq_f2()
+{
+    return TC ? Shape<LOG_N>::SEQ : Shape<LOG_N>::SEQ4;
+}
+template <int LOG_N, bool TC>
+__host__ __device__ constexpr int twiddle_f2()
+{
+    return TC ? (1 << LOG_N) - 1 : 2 * ((1 << LOG_N) - 1);
+}
+
+// Fill the twiddle table at `tws` (layout of the form) from the FP32 table.
+template <int LOG_N, bool TC>
+__device__ __forceinline__ void load_twiddles(float2* tws, const float2* __restrict__ src, int tid, int nt)
+{
+    constexpr int N = 1 << LOG_N;
+    if constexpr (TC) {
+        for (int i = tid; i < N - 1; i += nt) tws[i] = src[i];
+    } else {
+        float4* t4 = reinterpret_cast<float4*>(tws);
+        for (int i = tid; i < N - 1; i += nt) t4[i] = pair_twiddle(src[i]);
+    }
+}
+
+// The inverse DFT of the COUNT sequences of a task: the radix-2 Stockham FFT
+// on sequence pairs (one lane group of G2 per pair, named barrier 1 + pair
+// where a pair spans two warps), or with TC the tensor-core four-step DFT,
+// 8 sequences per engine call (N = 512).
+template <int LOG_N, bool FAST, bool TC, int COUNT>
+__device__ __forceinline__ void transform_all(float2* data, const float2* tws, int tid, tc::Engine* eng,
+                                              unsigned* error)
+{
+    using S = Shape<LOG_N>;
+    if constexpr (TC) {
+        static_assert(LOG_N == 9, "the tensor-core form is built for N = 512");
+        static_assert(S::SEQ * 2 >= 16 * tc::kZStride, "a sequence's space must hold its staged stage-3 rows");
+#pragma unroll 1
+        for (int s0 = 0; s0 < COUNT; s0 += tc::kSeq)
+            eng->dft512(data + s0 * S::SEQ, S::SEQ, COUNT - s0 < tc::kSeq ? COUNT - s0 : tc::kSeq, tws, tid,
+                        error);
+    } else {
+        static_assert(COUNT % 2 == 0, "sequences come in pairs");
+        static_assert(S::G2 <= 32 || (COUNT / 2) < 16, "one named barrier per pair");
+        const int pair = tid / S::G2;
+        fft_pair<LOG_N, S::G2, FAST>(reinterpret_cast<ulonglong2*>(data) + pair * S::SEQ4,
+                                     reinterpret_cast<const ulonglong2*>(tws), tid % S::G2, 1 + pair);
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Row task: RP row pairs of one ocean (evolve + row FFTs), written to the
@@ -74,11 +114,13 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
                                          unsigned* error = nullptr)
 {
     using S = Shape<LOG_N>;
-    constexpr int N = S::N, G = S::G, SEQ = S::SEQ, RP = S::RP;
+    constexpr int N = S::N, G = S::G, SEQ = S::SEQ, SEQ4 = S::SEQ4, RP = S::RP;
     constexpr int NT = RP * 2 * NF * G;
+    constexpr int Q = NF / 2;
 
-    float2* data = smem;                      // [RP*2*NF][SEQ]
-    float2* h0s = data + RP * 2 * NF * SEQ;   // [RP*2][N]
+    float2* data = smem;                                   // sequences of rows (j, r), fields f
+    float4* data4 = reinterpret_cast<float4*>(smem);       // the same as pairs (j, r, f / 2)
+    float2* h0s = data + RP * 2 * NF * seq_f2<LOG_N, TC>();  // [RP*2][N]
 
     OceanConsts cst;
     const float2* geom;
@@ -105,6 +147,24 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         return r ? N - p : p;
     };
 
+    // The geometry of this thread's cells is loaded before the h0 rows, so
+    // both loads' latencies overlap ahead of the one barrier.
+    constexpr int CELLS = RP * 2 * N;
+    constexpr int ITER = (CELLS + NT - 1) / NT;
+    float2 wk_of[ITER];
+    float kx_of[ITER], kz_of[ITER];
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int cell = tid + it * NT;
+        if (cell < CELLS) {
+            const int jr = cell >> LOG_N;
+            const int x = cell & (N - 1);
+            const int row = row_of(jr >> 1, jr & 1);
+            wk_of[it] = __ldg(&geom[static_cast<size_t>(row) * N + x]);
+            kx_of[it] = __ldg(&kvec[x]);
+            kz_of[it] = __ldg(&kvec[row]);
+        }
+    }
     for (int i = tid; i < RP * 2 * (N / 2); i += NT) {
         const int jr = i / (N / 2);
         const int c = i % (N / 2);
@@ -115,17 +175,19 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     __syncthreads();
 
     // Evolve (src/core/evolve.cpp:28-121 and :123-184), one cell at a time.
-    for (int cell = tid; cell < RP * 2 * N; cell += NT) {
+#pragma unroll
+    for (int it = 0; it < ITER; ++it) {
+        const int cell = tid + it * NT;
+        if (cell >= CELLS) break;
         const int jr = cell >> LOG_N;  // j*2 + r
         const int x = cell & (N - 1);
         const int j = jr >> 1, r = jr & 1;
         const int p = group * RP + j;
-        const int row = row_of(j, r);
         const int mr = (p == 0) ? r : 1 - r;  // row holding h0 at -kz
         const float2 av = h0s[jr * N + x];
         const float2 bm = h0s[(j * 2 + mr) * N + ((N - x) & (N - 1))];
         const float b_re = bm.x, b_im = -bm.y;
-        const float2 wk = geom[static_cast<size_t>(row) * N + x];
+        const float2 wk = wk_of[it];
 
         float s, c;
         sincos_poly(fold_phase(wk.x, top), s, c);
@@ -135,8 +197,8 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         const float bwd_im = b_im * c - b_re * s;
         const float hr = fwd_re + bwd_re;
         const float hi = fwd_im + bwd_im;
-        const float kx = kvec[x];
-        const float kz = kvec[row];
+        const float kx = kx_of[it];
+        const float kz = kz_of[it];
         const float ki = wk.y;
         const float sx = kx * ki;
         const float sz = kz * ki;
@@ -149,11 +211,11 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         const float jzz_re = jzz * hr, jzz_im = jzz * hi;
         const float jxz_re = jxz * hr, jxz_im = jxz * hi;
 
-        float2* base = data + (jr * NF) * SEQ + pad_idx(x);
-        base[0 * SEQ] = make_float2(hr - dx_im, hi + dx_re);
-        base[1 * SEQ] = make_float2(dz_re - hx_im, dz_im + hx_re);
-        base[2 * SEQ] = make_float2(hz_re - jxx_im, hz_im + jxx_re);
-        base[3 * SEQ] = make_float2(jzz_re - jxz_im, jzz_im + jxz_re);
+        const float2 p0 = make_float2(hr - dx_im, hi + dx_re);
+        const float2 p1 = make_float2(dz_re - hx_im, dz_im + hx_re);
+        const float2 p2 = make_float2(hz_re - jxx_im, hz_im + jxx_re);
+        const float2 p3 = make_float2(jzz_re - jxz_im, jzz_im + jxz_re);
+        float2 p4 = make_float2(0.0f, 0.0f), p5 = p4;
         if constexpr (NF == 6) {
             const float dr = fwd_re - bwd_re;
             const float di = fwd_im - bwd_im;
@@ -162,19 +224,34 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
             const float ux_re = -wsx * dr, ux_im = -wsx * di;
             const float uz_re = -wsz * dr, uz_im = -wsz * di;
             const float uy_re = -w * di, uy_im = w * dr;
-            base[4 * SEQ] = make_float2(ux_re - uy_im, ux_im + uy_re);
-            base[5 * SEQ] = make_float2(uz_re, uz_im);
+            p4 = make_float2(ux_re - uy_im, ux_im + uy_re);
+            p5 = make_float2(uz_re, uz_im);
+        }
+        if constexpr (TC) {
+            float2* base = data + (jr * NF) * SEQ + pad_idx(x);
+            base[0 * SEQ] = p0;
+            base[1 * SEQ] = p1;
+            base[2 * SEQ] = p2;
+            base[3 * SEQ] = p3;
+            if constexpr (NF == 6) {
+                base[4 * SEQ] = p4;
+                base[5 * SEQ] = p5;
+            }
+        } else {
+            float4* base = data4 + (jr * Q) * SEQ4 + pad4(x);
+            base[0] = make_float4(p0.x, p1.x, p0.y, p1.y);
+            base[SEQ4] = make_float4(p2.x, p3.x, p2.y, p3.y);
+            if constexpr (NF == 6) base[2 * SEQ4] = make_float4(p4.x, p5.x, p4.y, p5.y);
         }
     }
     __syncthreads();
 
-    transform_all<LOG_N, G, FAST, TC, RP * 2 * NF, SEQ>(data, tws, tid, eng, error);
+    transform_all<LOG_N, FAST, TC, RP * 2 * NF>(data, tws, tid, eng, error);
     __syncthreads();
 
     // Write the rows cell-major: inter[row][x][f], NF/2 float4 per cell.
     // NT is a multiple of Q, so each thread keeps one field pair fp and walks
     // cells with a constant stride (no division in the loop).
-    constexpr int Q = NF / 2;
     constexpr int CSTEP = NT / Q;
     float4* inter = reinterpret_cast<float4*>(inter_slot);
     const int fp = tid % Q;
@@ -183,9 +260,16 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         const int jr = cell >> LOG_N;
         const int x = cell & (N - 1);
         const int row = row_of(jr >> 1, jr & 1);
-        const float2 v0 = data[(jr * NF + 2 * fp) * SEQ + pad_idx(x)];
-        const float2 v1 = data[(jr * NF + 2 * fp + 1) * SEQ + pad_idx(x)];
-        inter[(static_cast<size_t>(row) * N + x) * Q + fp] = make_float4(v0.x, v0.y, v1.x, v1.y);
+        float4 o;
+        if constexpr (TC) {
+            const float2 v0 = data[(jr * NF + 2 * fp) * SEQ + pad_idx(x)];
+            const float2 v1 = data[(jr * NF + 2 * fp + 1) * SEQ + pad_idx(x)];
+            o = make_float4(v0.x, v0.y, v1.x, v1.y);
+        } else {
+            const float4 v = data4[(jr * Q + fp) * SEQ4 + pad4(x)];
+            o = make_float4(v.x, v.z, v.y, v.w);
+        }
+        inter[(static_cast<size_t>(row) * N + x) * Q + fp] = o;
     }
 }
 
@@ -193,23 +277,60 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
 // Column task helpers
 // ---------------------------------------------------------------------------
 
-// Periodic bilinear fetch from one channel grid (src/foam.cpp:22-41).
-__device__ __forceinline__ float foam_sample_wrap(const float* f, float u, float v, int n)
+// Periodic bilinear fetch from one channel grid (src/foam.cpp:22-41), split
+// into the four tap loads and the blend so that a thread can have the taps of
+// several cells in flight at once.
+struct FoamTaps {
+    float fa, fb, fc, fd, tu, tv;
+};
+
+__device__ __forceinline__ FoamTaps foam_fetch(const float* f, float u, float v, int n)
 {
+    FoamTaps t;
     const float fu = floorf(u), fv = floorf(v);
-    const float tu = u - fu, tv = v - fv;
+    t.tu = u - fu;
+    t.tv = v - fv;
     int x0 = __float2int_rz(fu) % n;
     if (x0 < 0) x0 += n;
     int z0 = __float2int_rz(fv) % n;
     if (z0 < 0) z0 += n;
     const int x1 = (x0 + 1) % n;
     const int z1 = (z0 + 1) % n;
-    const float fa = f[static_cast<size_t>(z0) * n + x0];
-    const float fb = f[static_cast<size_t>(z0) * n + x1];
-    const float fc = f[static_cast<size_t>(z1) * n + x0];
-    const float fd = f[static_cast<size_t>(z1) * n + x1];
-    return fa * (1.0f - tu) * (1.0f - tv) + fb * tu * (1.0f - tv) + fc * (1.0f - tu) * tv +
-           fd * tu * tv;
+    t.fa = f[static_cast<size_t>(z0) * n + x0];
+    t.fb = f[static_cast<size_t>(z0) * n + x1];
+    t.fc = f[static_cast<size_t>(z1) * n + x0];
+    t.fd = f[static_cast<size_t>(z1) * n + x1];
+    return t;
+}
+
+__device__ __forceinline__ float foam_blend(const FoamTaps& t)
+{
+    const float tu = t.tu, tv = t.tv;
+    return t.fa * (1.0f - tu) * (1.0f - tv) + t.fb * tu * (1.0f - tv) + t.fc * (1.0f - tu) * tv +
+           t.fd * tu * tv;
+}
+
+// The backtraced sample point of cell (x, z) and the taps there
+// (src/foam.cpp:89-139, first half).
+__device__ __forceinline__ FoamTaps foam_taps(const float* cur, int n, int x, int z, float velx, float velz,
+                                              float dt, float scale, float drift_x, float drift_z,
+                                              float inv_cell)
+{
+    const float vx = velx * scale + drift_x;
+    const float vz = velz * scale + drift_z;
+    const float su = static_cast<float>(x) - vx * dt * inv_cell;
+    const float sv = static_cast<float>(z) - vz * dt * inv_cell;
+    return foam_fetch(cur, su, sv, n);
+}
+
+// Decay, source and clamp of the sampled foam (second half).
+__device__ __forceinline__ float foam_finish(const FoamTaps& t, float src, float decay, float gain)
+{
+    float f = foam_blend(t);
+    f = f * decay + src * gain;
+    if (f > 1.0f) f = 1.0f;
+    if (f < 0.0f) f = 0.0f;
+    return f;
 }
 
 // One persistent-foam substep for cell (x, z) (src/foam.cpp:89-139).
@@ -218,15 +339,8 @@ __device__ __forceinline__ float foam_cell(const float* cur, int n, int x, int z
                                            float gain, float scale, float drift_x,
                                            float drift_z, float inv_cell)
 {
-    const float vx = velx * scale + drift_x;
-    const float vz = velz * scale + drift_z;
-    const float su = static_cast<float>(x) - vx * dt * inv_cell;
-    const float sv = static_cast<float>(z) - vz * dt * inv_cell;
-    float f = foam_sample_wrap(cur, su, sv, n);
-    f = f * decay + src * gain;
-    if (f > 1.0f) f = 1.0f;
-    if (f < 0.0f) f = 0.0f;
-    return f;
+    return foam_finish(foam_taps(cur, n, x, z, velx, velz, dt, scale, drift_x, drift_z, inv_cell), src,
+                       decay, gain);
 }
 
 // ---------------------------------------------------------------------------
@@ -241,27 +355,49 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
                                          unsigned* error = nullptr)
 {
     using S = Shape<LOG_N>;
-    constexpr int N = S::N, G = S::G, SEQ = S::SEQ;
+    constexpr int N = S::N, G = S::G, SEQ = S::SEQ, SEQ4 = S::SEQ4;
     constexpr int NT = NF * W * G;
     constexpr int Q = NF / 2;
-    float2* data = smem;  // [NF*W][SEQ], sequence = f*W + w
+    float2* data = smem;                             // TC: sequence f*W + w
+    float4* data4 = reinterpret_cast<float4*>(smem); // pairs: pair p*W + w holds fields 2p, 2p+1
     const int x0 = strip * W;
 
     const float4* inter = reinterpret_cast<const float4*>(inter_slot);
     constexpr int CSTEP = NT / Q;  // NT is a multiple of Q
     const int fp = tid % Q;
-#pragma unroll 4
-    for (int cw = tid / Q; cw < N * W; cw += CSTEP) {
-        const int y = cw / W;
-        const int w = cw % W;
-        const float4* src = inter + (static_cast<size_t>(y) * N + x0 + w) * Q + fp;
-        const float4 v = CG ? __ldcg(src) : *src;
-        data[((2 * fp) * W + w) * SEQ + pad_idx(y)] = make_float2(v.x, v.y);
-        data[((2 * fp + 1) * W + w) * SEQ + pad_idx(y)] = make_float2(v.z, v.w);
+    // Up to 8 loads per thread in flight before the first shared store.
+    constexpr int LIT = (N * W + CSTEP - 1) / CSTEP;
+    constexpr int LB = LIT < 8 ? LIT : 8;
+#pragma unroll 1
+    for (int b0 = 0; b0 < LIT; b0 += LB) {
+        float4 buf[LB];
+#pragma unroll
+        for (int k = 0; k < LB; ++k) {
+            const int cw = tid / Q + (b0 + k) * CSTEP;
+            if (cw < N * W) {
+                const float4* src = inter + (static_cast<size_t>(cw / W) * N + x0 + cw % W) * Q + fp;
+                buf[k] = CG ? __ldcg(src) : *src;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < LB; ++k) {
+            const int cw = tid / Q + (b0 + k) * CSTEP;
+            if (cw < N * W) {
+                const int y = cw / W;
+                const int w = cw % W;
+                const float4 v = buf[k];
+                if constexpr (TC) {
+                    data[((2 * fp) * W + w) * SEQ + pad_idx(y)] = make_float2(v.x, v.y);
+                    data[((2 * fp + 1) * W + w) * SEQ + pad_idx(y)] = make_float2(v.z, v.w);
+                } else {
+                    data4[(fp * W + w) * SEQ4 + pad4(y)] = make_float4(v.x, v.z, v.y, v.w);
+                }
+            }
+        }
     }
     __syncthreads();
 
-    transform_all<LOG_N, G, FAST, TC, NF * W, SEQ>(data, tws, tid, eng, error);
+    transform_all<LOG_N, FAST, TC, NF * W>(data, tws, tid, eng, error);
     __syncthreads();
 
     const size_t base = static_cast<size_t>(ocean) * N * N;
@@ -282,15 +418,46 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
         out_vel = a.velocity + base;
     }
     const float lambda = cst.lambda;
-    for (int i = tid; i < N * W; i += NT) {
+    // The cells of this thread, unrolled, so that with persistent foam the
+    // four taps of every cell are in flight together; the foam values are
+    // finished and stored in a second pass.
+    constexpr int FC = N * W;
+    constexpr int FIT = (FC + NT - 1) / NT;
+    constexpr bool FSTEP = NF == 6 && FOAM;
+    FoamTaps taps[FSTEP ? FIT : 1];
+    float fsrc[FSTEP ? FIT : 1];
+#pragma unroll
+    for (int it = 0; it < FIT; ++it) {
+        const int i = tid + it * NT;
+        if (i >= FC) break;
         const int y = i / W;
         const int w = i % W;
         const int x = x0 + w;
-        const int sy = pad_idx(y);
-        const float2 f0 = data[(0 * W + w) * SEQ + sy];
-        const float2 f1 = data[(1 * W + w) * SEQ + sy];
-        const float2 f2 = data[(2 * W + w) * SEQ + sy];
-        const float2 f3 = data[(3 * W + w) * SEQ + sy];
+        float2 f0, f1, f2, f3, f4, f5;
+        if constexpr (TC) {
+            const int sy = pad_idx(y);
+            f0 = data[(0 * W + w) * SEQ + sy];
+            f1 = data[(1 * W + w) * SEQ + sy];
+            f2 = data[(2 * W + w) * SEQ + sy];
+            f3 = data[(3 * W + w) * SEQ + sy];
+            if constexpr (NF == 6) {
+                f4 = data[(4 * W + w) * SEQ + sy];
+                f5 = data[(5 * W + w) * SEQ + sy];
+            }
+        } else {
+            const int sy = pad4(y);
+            const float4 q0 = data4[(0 * W + w) * SEQ4 + sy];
+            const float4 q1 = data4[(1 * W + w) * SEQ4 + sy];
+            f0 = make_float2(q0.x, q0.z);
+            f1 = make_float2(q0.y, q0.w);
+            f2 = make_float2(q1.x, q1.z);
+            f3 = make_float2(q1.y, q1.w);
+            if constexpr (NF == 6) {
+                const float4 q2 = data4[(2 * W + w) * SEQ4 + sy];
+                f4 = make_float2(q2.x, q2.z);
+                f5 = make_float2(q2.y, q2.w);
+            }
+        }
         const float h = f0.x, d_x = f0.y, d_z = f1.x, hx = f1.y;
         const float hz = f2.x, jxx = f2.y, jzz = f3.x, jxz = f3.y;
 
@@ -316,16 +483,21 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
         __stcs(&out_disp[idx], make_float4(disp_x, h, disp_z, foam));
         __stcs(&out_normal[idx], make_float4(nx, ny, nz, jac));
         if constexpr (NF == 6) {
-            const float2 f4 = data[(4 * W + w) * SEQ + sy];
-            const float2 f5 = data[(5 * W + w) * SEQ + sy];
             __stcs(&out_vel[idx], make_float4(f4.x, f4.y, f5.x, 0.0f));
-            if constexpr (FOAM) {
-                const float* cur = a.foam_cur + base;
-                __stcs(&a.foam_next[base + idx],
-                       foam_cell(cur, N, x, y, f4.x, f5.x, foam, a.foam_dt, a.foam_decay,
-                                 a.foam_gain, a.foam_scale, a.foam_drift_x, a.foam_drift_z,
-                                 a.foam_inv_cell));
+            if constexpr (FSTEP) {
+                taps[it] = foam_taps(a.foam_cur + base, N, x, y, f4.x, f5.x, a.foam_dt, a.foam_scale,
+                                     a.foam_drift_x, a.foam_drift_z, a.foam_inv_cell);
+                fsrc[it] = foam;
             }
+        }
+    }
+    if constexpr (FSTEP) {
+#pragma unroll
+        for (int it = 0; it < FIT; ++it) {
+            const int i = tid + it * NT;
+            if (i >= FC) break;
+            const size_t idx = static_cast<size_t>(i / W) * N + x0 + i % W;
+            __stcs(&a.foam_next[base + idx], foam_finish(taps[it], fsrc[it], a.foam_decay, a.foam_gain));
         }
     }
 }
@@ -342,8 +514,8 @@ row_pass_kernel(FrameArgs a)
     constexpr int NT = S::RP * 2 * NF * S::G;
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
-    float2* tws = smem + S::RP * 2 * NF * S::SEQ + S::RP * 2 * S::N;
-    for (int i = threadIdx.x; i < S::N - 1; i += NT) tws[i] = a.twiddles[i];
+    float2* tws = smem + S::RP * 2 * NF * S::SEQ4 + S::RP * 2 * S::N;
+    load_twiddles<LOG_N, false>(tws, a.twiddles, threadIdx.x, NT);
     const int o = blockIdx.y;
     row_task<LOG_N, NF, FAST>(a, a.ocean_base + o, blockIdx.x,
                               a.inter + static_cast<size_t>(o) * S::N * S::N * NF, smem, tws,
@@ -358,8 +530,8 @@ col_pass_kernel(FrameArgs a)
     constexpr int NT = NF * S::W * S::G;
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
-    float2* tws = smem + NF * S::W * S::SEQ;
-    for (int i = threadIdx.x; i < S::N - 1; i += NT) tws[i] = a.twiddles[i];
+    float2* tws = smem + NF * S::W * S::SEQ4;
+    load_twiddles<LOG_N, false>(tws, a.twiddles, threadIdx.x, NT);
     const int o = blockIdx.y;
     col_task<LOG_N, NF, FAST, FOAM, S::W, false>(
         a, a.ocean_base + o, blockIdx.x, a.inter + static_cast<size_t>(o) * S::N * S::N * NF,
@@ -426,19 +598,19 @@ constexpr int frame_min_blocks()
 
 // Shared floats (float2 units) of the persistent kernel's data area, and the
 // byte offset of the tensor-core engine's area behind the twiddles.
-template <int LOG_N, int NF>
+template <int LOG_N, int NF, bool TC>
 __host__ __device__ constexpr size_t frame_data_float2()
 {
     using S = Shape<LOG_N>;
-    constexpr size_t row = S::RP * 2 * NF * S::SEQ + S::RP * 2 * S::N;
-    constexpr size_t col = NF * S::PW * S::SEQ;
+    constexpr size_t row = S::RP * 2 * NF * seq_f2<LOG_N, TC>() + S::RP * 2 * S::N;
+    constexpr size_t col = NF * S::PW * seq_f2<LOG_N, TC>();
     return row > col ? row : col;
 }
 
 template <int LOG_N, int NF>
 __host__ __device__ constexpr size_t frame_engine_offset()
 {
-    return ((frame_data_float2<LOG_N, NF>() + (size_t(1) << LOG_N)) * sizeof(float2) + 127) / 128 * 128;
+    return ((frame_data_float2<LOG_N, NF, true>() + (size_t(1) << LOG_N)) * sizeof(float2) + 127) / 128 * 128;
 }
 
 template <int LOG_N, int NF, bool FAST, bool FOAM, bool TC = false>
@@ -451,7 +623,7 @@ frame_kernel(FrameArgs a, QueueArgs q)
     constexpr int NT = S::RP * 2 * NF * S::G;
     constexpr int RT = (N / 2) / S::RP;  // row tasks per ocean
     constexpr int CT = N / S::PW;        // column tasks per ocean
-    constexpr size_t kDataFloat2 = frame_data_float2<LOG_N, NF>();
+    constexpr size_t kDataFloat2 = frame_data_float2<LOG_N, NF, TC>();
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
     float2* tws = smem + kDataFloat2;
@@ -459,7 +631,7 @@ frame_kernel(FrameArgs a, QueueArgs q)
     __shared__ int s_ok;
 
     const int tid = threadIdx.x;
-    for (int i = tid; i < N - 1; i += NT) tws[i] = a.twiddles[i];
+    load_twiddles<LOG_N, TC>(tws, a.twiddles, tid, NT);
     tc::Engine eng{reinterpret_cast<unsigned char*>(smem4) + frame_engine_offset<LOG_N, NF>(), 0};
     if constexpr (TC) {
         static_assert(NT >= tc::kThreads, "the tensor-core engine needs 8 warps");
@@ -633,13 +805,13 @@ template <int LOG_N, int NF>
 constexpr size_t row_smem_bytes()
 {
     using S = Shape<LOG_N>;
-    return sizeof(float2) * (S::RP * 2 * NF * S::SEQ + S::RP * 2 * S::N + (S::N - 1));
+    return sizeof(float2) * (S::RP * 2 * NF * S::SEQ4 + S::RP * 2 * S::N + twiddle_f2<LOG_N, false>());
 }
 template <int LOG_N, int NF>
 constexpr size_t col_smem_bytes()
 {
     using S = Shape<LOG_N>;
-    return sizeof(float2) * (NF * S::W * S::SEQ + (S::N - 1));
+    return sizeof(float2) * (NF * S::W * S::SEQ4 + twiddle_f2<LOG_N, false>());
 }
 
 template <int LOG_N, int NF, bool FAST>
@@ -675,7 +847,7 @@ constexpr size_t frame_smem_bytes()
 {
     using S = Shape<LOG_N>;
     if (TC) return frame_engine_offset<LOG_N, NF>() + tc::kSmemBytes;
-    return sizeof(float2) * (frame_data_float2<LOG_N, NF>() + (S::N - 1));
+    return sizeof(float2) * (frame_data_float2<LOG_N, NF, false>() + twiddle_f2<LOG_N, false>());
 }
 
 template <int LOG_N, int NF, bool FAST, bool FOAM, bool TC = false>

@@ -178,4 +178,172 @@ __host__ __device__ constexpr int lanes_for(int log_n)
     return (log_n - 4) >= 5 ? 32 : (1 << (log_n - 4 < 0 ? 0 : log_n - 4));
 }
 
+// ---------------------------------------------------------------------------
+// Paired sequences: two sequences A and B of the same length transformed in
+// lockstep, each register and shared-memory slot holding the same index of
+// both. Shared memory holds a pair as float4 (A.re, B.re, A.im, B.im) per
+// index, one float4 of padding after every 8; in registers (A.re, B.re) and
+// (A.im, B.im) are each one 64-bit f32x2 operand. Blackwell's packed FP32
+// instructions (add/sub/mul.rn.f32x2) do the two sequences' operations in one
+// instruction, each lane rounded exactly as the scalar instruction rounds, so
+// the results are bit-identical to transforming A and B one at a time.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int pad4(int i) { return i + (i >> 3); }
+__host__ __device__ constexpr int padded_len4(int n) { return n + n / 8; }
+
+// Lanes per sequence pair: twice the single-sequence count, so a pair of
+// sequences takes as many threads as the two sequences alone, each lane
+// keeping 8 indices (16 at N = 1024) of both.
+__host__ __device__ constexpr int pair_lanes(int log_n) { return 2 * lanes_for(log_n); }
+
+using f32x2 = unsigned long long;  // two floats, low word first
+
+__device__ __forceinline__ f32x2 px_add(f32x2 a, f32x2 b)
+{
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 px_sub(f32x2 a, f32x2 b)
+{
+    f32x2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 px_mul(f32x2 a, f32x2 b)
+{
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 px_fma(f32x2 a, f32x2 b, f32x2 c)
+{
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ f32x2 px_pack(float lo, float hi)
+{
+    f32x2 d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+    return d;
+}
+__device__ __forceinline__ void px_unpack(f32x2 v, float& lo, float& hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+// The radix-2 butterfly of `butterfly` on a pair: (ar, ai) and (br, bi) hold
+// the real and imaginary parts of both sequences, (wx, wy) the twiddle's
+// parts duplicated. EXACT: a' = a + b; b' = (dr wx - di wy, dr wy + di wx),
+// every product rounded before the add. The assembler contracts a packed
+// multiply into a packed add or subtract that consumes it (one fused
+// multiply-add, rounded once) even with contraction disabled, so the four
+// products are packed multiplies and the two sums that combine them are
+// scalar adds of their halves. FAST fuses as `butterfly<true>` does.
+template <bool FAST>
+__device__ __forceinline__ void butterfly_pair(f32x2& ar, f32x2& ai, f32x2& br, f32x2& bi, f32x2 wx, f32x2 wy)
+{
+    const f32x2 dr = px_sub(ar, br);
+    const f32x2 di = px_sub(ai, bi);
+    ar = px_add(ar, br);
+    ai = px_add(ai, bi);
+    if (FAST) {
+        const f32x2 nwy = wy ^ 0x8000000080000000ull;
+        br = px_fma(dr, wx, px_mul(di, nwy));
+        bi = px_fma(dr, wy, px_mul(di, wx));
+    } else {
+        float rx0, rx1, iy0, iy1, ry0, ry1, ix0, ix1;
+        px_unpack(px_mul(dr, wx), rx0, rx1);
+        px_unpack(px_mul(di, wy), iy0, iy1);
+        px_unpack(px_mul(dr, wy), ry0, ry1);
+        px_unpack(px_mul(di, wx), ix0, ix1);
+        br = px_pack(__fsub_rn(rx0, iy0), __fsub_rn(rx1, iy1));
+        bi = px_pack(__fadd_rn(ry0, ix0), __fadd_rn(ry1, ix1));
+    }
+}
+
+// Barrier over the G2 lanes of one pair: the warp when the pair fits in one,
+// else named barrier `id` (1 + the pair's index in the CTA) over its warps.
+template <int G2>
+__device__ __forceinline__ void pair_sync(int id)
+{
+    if constexpr (G2 <= 32) {
+        __syncwarp();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(G2) : "memory");
+    }
+}
+
+// StageBlock's r stages on a pair of sequences (same index algebra, lane
+// ownership and twiddles; `tw` holds the twiddle table as
+// (wx, wx, wy, wy) per entry).
+template <int LOG_N, int G2, int L0, bool FAST>
+struct PairBlock {
+    static constexpr int N = 1 << LOG_N;
+    static constexpr int E = N / G2;
+    static constexpr int RMAX = ilog2c(E);
+    static constexpr int r = cmin(RMAX, LOG_N - L0);
+    static constexpr int RR = 1 << r;
+    static constexpr int C = (N >> r) / G2;
+    static constexpr int w = LOG_N - r - L0;
+
+    __device__ __forceinline__ static void run(ulonglong2* seq, const ulonglong2* tw, int lane, int bar_id)
+    {
+        f32x2 re[C][RR], im[C][RR];
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const int c = lane + G2 * k;
+#pragma unroll
+            for (int t = 0; t < RR; ++t) {
+                const ulonglong2 v = seq[pad4((t << (LOG_N - r)) | c)];
+                re[k][t] = v.x;
+                im[k][t] = v.y;
+            }
+        }
+        pair_sync<G2>(bar_id);
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const int c = lane + G2 * k;
+            const int P = c >> L0;
+#pragma unroll
+            for (int s = 0; s < r; ++s) {
+                const int half = RR >> (s + 1);
+                const int l = L0 + s;
+                const ulonglong2* twl = tw + (N - (N >> l));
+#pragma unroll
+                for (int S = 0; S < RR; ++S) {
+                    if (S & half) continue;
+                    const int Rk = S & (half - 1);
+                    const ulonglong2 wv = twl[(Rk << w) | P];
+                    butterfly_pair<FAST>(re[k][S], im[k][S], re[k][S + half], im[k][S + half], wv.x, wv.y);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const int c = lane + G2 * k;
+            const int P = c >> L0;
+            const int q = c & ((1 << L0) - 1);
+#pragma unroll
+            for (int S = 0; S < RR; ++S) {
+                const int out = (P << (L0 + r)) | (bitrev<r>(S) << L0) | q;
+                seq[pad4(out)] = make_ulonglong2(re[k][S], im[k][S]);
+            }
+        }
+        pair_sync<G2>(bar_id);
+        if constexpr (L0 + r < LOG_N) PairBlock<LOG_N, G2, L0 + r, FAST>::run(seq, tw, lane, bar_id);
+    }
+};
+
+// The unnormalised inverse transforms of the pair at `seq`.
+template <int LOG_N, int G2, bool FAST>
+__device__ __forceinline__ void fft_pair(ulonglong2* seq, const ulonglong2* tw, int lane, int bar_id)
+{
+    PairBlock<LOG_N, G2, 0, FAST>::run(seq, tw, lane, bar_id);
+}
+
+// Twiddle entry of the pair table: (wx, wx, wy, wy).
+__device__ __forceinline__ float4 pair_twiddle(float2 w) { return make_float4(w.x, w.x, w.y, w.y); }
+
 }  // namespace ocean_b200
