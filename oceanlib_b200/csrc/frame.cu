@@ -64,6 +64,19 @@ __host__ __device__ constexpr int twiddle_f2()
     return TC ? (1 << LOG_N) - 1 : 2 * ((1 << LOG_N) - 1);
 }
 
+// Foam window of a column task over W columns: columns x0 - 1 .. x0 + W of
+// every row (WW floats per row), and its size in float2.
+template <int W>
+__host__ __device__ constexpr int foam_window()
+{
+    return W + 2;
+}
+template <int LOG_N, int W>
+__host__ __device__ constexpr int foam_window_f2()
+{
+    return (1 << LOG_N) * foam_window<W>() / 2;
+}
+
 // Fill the twiddle table at `tws` (layout of the form) from the FP32 table.
 template <int LOG_N, bool TC>
 __device__ __forceinline__ void load_twiddles(float2* tws, const float2* __restrict__ src, int tid, int nt)
@@ -277,14 +290,15 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
 // Column task helpers
 // ---------------------------------------------------------------------------
 
-// Periodic bilinear fetch from one channel grid (src/foam.cpp:22-41), split
-// into the four tap loads and the blend so that a thread can have the taps of
-// several cells in flight at once.
+// Periodic bilinear fetch from one channel grid (src/foam.cpp:22-41): the
+// four taps come from `get(z, x)`, so a caller can serve them from a staged
+// shared-memory window or from global memory with the same arithmetic.
 struct FoamTaps {
     float fa, fb, fc, fd, tu, tv;
 };
 
-__device__ __forceinline__ FoamTaps foam_fetch(const float* f, float u, float v, int n)
+template <typename Get>
+__device__ __forceinline__ FoamTaps foam_fetch(float u, float v, int n, Get&& get)
 {
     FoamTaps t;
     const float fu = floorf(u), fv = floorf(v);
@@ -296,10 +310,10 @@ __device__ __forceinline__ FoamTaps foam_fetch(const float* f, float u, float v,
     if (z0 < 0) z0 += n;
     const int x1 = (x0 + 1) % n;
     const int z1 = (z0 + 1) % n;
-    t.fa = f[static_cast<size_t>(z0) * n + x0];
-    t.fb = f[static_cast<size_t>(z0) * n + x1];
-    t.fc = f[static_cast<size_t>(z1) * n + x0];
-    t.fd = f[static_cast<size_t>(z1) * n + x1];
+    t.fa = get(z0, x0);
+    t.fb = get(z0, x1);
+    t.fc = get(z1, x0);
+    t.fd = get(z1, x1);
     return t;
 }
 
@@ -312,15 +326,15 @@ __device__ __forceinline__ float foam_blend(const FoamTaps& t)
 
 // The backtraced sample point of cell (x, z) and the taps there
 // (src/foam.cpp:89-139, first half).
-__device__ __forceinline__ FoamTaps foam_taps(const float* cur, int n, int x, int z, float velx, float velz,
-                                              float dt, float scale, float drift_x, float drift_z,
-                                              float inv_cell)
+template <typename Get>
+__device__ __forceinline__ FoamTaps foam_taps(int n, int x, int z, float velx, float velz, float dt, float scale,
+                                              float drift_x, float drift_z, float inv_cell, Get&& get)
 {
     const float vx = velx * scale + drift_x;
     const float vz = velz * scale + drift_z;
     const float su = static_cast<float>(x) - vx * dt * inv_cell;
     const float sv = static_cast<float>(z) - vz * dt * inv_cell;
-    return foam_fetch(cur, su, sv, n);
+    return foam_fetch(su, sv, n, get);
 }
 
 // Decay, source and clamp of the sampled foam (second half).
@@ -339,8 +353,9 @@ __device__ __forceinline__ float foam_cell(const float* cur, int n, int x, int z
                                            float gain, float scale, float drift_x,
                                            float drift_z, float inv_cell)
 {
-    return foam_finish(foam_taps(cur, n, x, z, velx, velz, dt, scale, drift_x, drift_z, inv_cell), src,
-                       decay, gain);
+    auto get = [&](int zz, int xx) { return cur[static_cast<size_t>(zz) * n + xx]; };
+    return foam_finish(foam_taps(n, x, z, velx, velz, dt, scale, drift_x, drift_z, inv_cell, get), src, decay,
+                       gain);
 }
 
 // ---------------------------------------------------------------------------
@@ -361,6 +376,23 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     float2* data = smem;                             // TC: sequence f*W + w
     float4* data4 = reinterpret_cast<float4*>(smem); // pairs: pair p*W + w holds fields 2p, 2p+1
     const int x0 = strip * W;
+    constexpr bool FSTEP = NF == 6 && FOAM;
+    constexpr int WW = foam_window<W>();
+
+    const size_t base = static_cast<size_t>(ocean) * N * N;
+    // With persistent foam: the previous foam state in columns x0 - 1 ..
+    // x0 + W of every row, [y][WW] behind the sequences (foam_window_f2
+    // float2 the caller reserves), loaded with the intermediate so the taps
+    // of the foam step (within a cell of the strip for any velocity up to
+    // cell / dt) come from shared memory.
+    float* fwin = reinterpret_cast<float*>(smem + NF * W * seq_f2<LOG_N, TC>());
+    if constexpr (FSTEP) {
+        const float* cur = a.foam_cur + base;
+        for (int k = tid; k < N * WW; k += NT) {
+            const int xc = (x0 - 1 + k % WW) & (N - 1);
+            fwin[k] = __ldg(&cur[static_cast<size_t>(k / WW) * N + xc]);
+        }
+    }
 
     const float4* inter = reinterpret_cast<const float4*>(inter_slot);
     constexpr int CSTEP = NT / Q;  // NT is a multiple of Q
@@ -400,7 +432,6 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     transform_all<LOG_N, FAST, TC, NF * W>(data, tws, tid, eng, error);
     __syncthreads();
 
-    const size_t base = static_cast<size_t>(ocean) * N * N;
     OceanConsts cst;
     float4* out_disp;
     float4* out_normal;
@@ -418,14 +449,14 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
         out_vel = a.velocity + base;
     }
     const float lambda = cst.lambda;
-    // The cells of this thread, unrolled, so that with persistent foam the
-    // four taps of every cell are in flight together; the foam values are
-    // finished and stored in a second pass.
     constexpr int FC = N * W;
     constexpr int FIT = (FC + NT - 1) / NT;
-    constexpr bool FSTEP = NF == 6 && FOAM;
-    FoamTaps taps[FSTEP ? FIT : 1];
-    float fsrc[FSTEP ? FIT : 1];
+    const float* cur = a.foam_cur + base;
+    // A tap in the window is read from shared memory, any other from global.
+    auto foam_get = [&](int zz, int xx) {
+        const int j = (xx - x0 + 1) & (N - 1);
+        return j < WW ? fwin[zz * WW + j] : __ldg(&cur[static_cast<size_t>(zz) * N + xx]);
+    };
 #pragma unroll
     for (int it = 0; it < FIT; ++it) {
         const int i = tid + it * NT;
@@ -485,19 +516,10 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
         if constexpr (NF == 6) {
             __stcs(&out_vel[idx], make_float4(f4.x, f4.y, f5.x, 0.0f));
             if constexpr (FSTEP) {
-                taps[it] = foam_taps(a.foam_cur + base, N, x, y, f4.x, f5.x, a.foam_dt, a.foam_scale,
-                                     a.foam_drift_x, a.foam_drift_z, a.foam_inv_cell);
-                fsrc[it] = foam;
+                const FoamTaps t = foam_taps(N, x, y, f4.x, f5.x, a.foam_dt, a.foam_scale, a.foam_drift_x,
+                                             a.foam_drift_z, a.foam_inv_cell, foam_get);
+                __stcs(&a.foam_next[base + idx], foam_finish(t, foam, a.foam_decay, a.foam_gain));
             }
-        }
-    }
-    if constexpr (FSTEP) {
-#pragma unroll
-        for (int it = 0; it < FIT; ++it) {
-            const int i = tid + it * NT;
-            if (i >= FC) break;
-            const size_t idx = static_cast<size_t>(i / W) * N + x0 + i % W;
-            __stcs(&a.foam_next[base + idx], foam_finish(taps[it], fsrc[it], a.foam_decay, a.foam_gain));
         }
     }
 }
@@ -530,7 +552,7 @@ col_pass_kernel(FrameArgs a)
     constexpr int NT = NF * S::W * S::G;
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
-    float2* tws = smem + NF * S::W * S::SEQ4;
+    float2* tws = smem + NF * S::W * S::SEQ4 + foam_window_f2<LOG_N, S::W>();  // behind the foam window
     load_twiddles<LOG_N, false>(tws, a.twiddles, threadIdx.x, NT);
     const int o = blockIdx.y;
     col_task<LOG_N, NF, FAST, FOAM, S::W, false>(
@@ -557,6 +579,13 @@ __device__ __forceinline__ unsigned long long global_ns()
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+
+// Release add at GPU scope: every write that happens before it (the CTA's,
+// through the preceding barrier) is visible to an acquirer that sees the sum.
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
@@ -624,6 +653,8 @@ frame_kernel(FrameArgs a, QueueArgs q)
     constexpr int RT = (N / 2) / S::RP;  // row tasks per ocean
     constexpr int CT = N / S::PW;        // column tasks per ocean
     constexpr size_t kDataFloat2 = frame_data_float2<LOG_N, NF, TC>();
+    static_assert(size_t(NF) * S::PW * seq_f2<LOG_N, TC>() + foam_window_f2<LOG_N, S::PW>() <= kDataFloat2,
+                  "the column task's foam window fits in the data area");
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
     float2* tws = smem + kDataFloat2;
@@ -657,22 +688,26 @@ frame_kernel(FrameArgs a, QueueArgs q)
         }
     };
 
-    // Thread 0 publishes the previous task (the barrier above it orders every
-    // thread's writes before its fence + atomic, the pattern grid-wide
-    // barriers use), then takes the next ticket and waits for that task's
-    // inputs; one barrier hands the ticket to the CTA.
+    // Thread 0 publishes the previous task with a release add (the barrier
+    // above it orders every thread's writes before it, the pattern grid-wide
+    // barriers use), then waits for the inputs of the ticket it drew one
+    // task earlier and draws the following one, whose round trip overlaps
+    // the task; one barrier hands the ticket to the CTA. The publish comes
+    // before the wait: the next task may depend on the one just finished. A
+    // drawn ticket T runs right after the CTA's current task (< T), which
+    // waits on nothing later, so the queue stays deadlock-free.
     unsigned* publish = nullptr;
+    unsigned t_next = 0;
+    if (tid == 0) t_next = atomicAdd(q.ticket, 1u);
     while (true) {
         __syncthreads();  // previous task's writes issued; shared memory free
         if (tid == 0) {
-            if (publish != nullptr) {
-                __threadfence();
-                atomicAdd(publish, 1u);
-            }
-            const unsigned t = atomicAdd(q.ticket, 1u);
+            if (publish != nullptr) red_release_add(publish, 1u);
+            const unsigned t = t_next;
             int ok = 1;
             publish = nullptr;
             if (t < total) {
+                t_next = atomicAdd(q.ticket, 1u);
                 bool row;
                 unsigned ocean, idx;
                 decode(t, row, ocean, idx);
@@ -811,7 +846,7 @@ template <int LOG_N, int NF>
 constexpr size_t col_smem_bytes()
 {
     using S = Shape<LOG_N>;
-    return sizeof(float2) * (NF * S::W * S::SEQ4 + twiddle_f2<LOG_N, false>());
+    return sizeof(float2) * (NF * S::W * S::SEQ4 + foam_window_f2<LOG_N, S::W>() + twiddle_f2<LOG_N, false>());
 }
 
 template <int LOG_N, int NF, bool FAST>
