@@ -64,6 +64,24 @@ __host__ __device__ constexpr int twiddle_f2()
     return TC ? (1 << LOG_N) - 1 : 2 * ((1 << LOG_N) - 1);
 }
 
+// Column tasks over 2 columns shift their sequence pairs (pair s = field
+// pair * W + column) by a few float4 so that the intermediate's stores (lanes
+// walking field pair, column, row) and the finalize's reads (column, row)
+// spread over the shared-memory banks: the shifts minimise the 16-byte
+// wavefronts of both patterns together over a strip (a search over all
+// shifts mod 8 with the padding of pad4 modelled).
+template <int NF, int W>
+__host__ __device__ constexpr int col_pair_shift(int s)
+{
+    return W != 2 ? 0 : (NF == 6 ? (s + 1) / 2 : s % 2);
+}
+// float2 the shifts add behind the last pair.
+template <int NF, int W>
+__host__ __device__ constexpr int col_shift_f2()
+{
+    return 2 * col_pair_shift<NF, W>(NF * W / 2 - 1);
+}
+
 // Foam window of a column task over W columns: columns x0 - 1 .. x0 + W of
 // every row (WW floats per row), and its size in float2.
 template <int W>
@@ -94,7 +112,7 @@ __device__ __forceinline__ void load_twiddles(float2* tws, const float2* __restr
 // on sequence pairs (one lane group of G2 per pair, named barrier 1 + pair
 // where a pair spans two warps), or with TC the tensor-core four-step DFT,
 // 8 sequences per engine call (N = 512).
-template <int LOG_N, bool FAST, bool TC, int COUNT>
+template <int LOG_N, bool FAST, bool TC, int COUNT, int COLW = 0>
 __device__ __forceinline__ void transform_all(float2* data, const float2* tws, int tid, tc::Engine* eng,
                                               unsigned* error)
 {
@@ -110,7 +128,8 @@ __device__ __forceinline__ void transform_all(float2* data, const float2* tws, i
         static_assert(COUNT % 2 == 0, "sequences come in pairs");
         static_assert(S::G2 <= 32 || (COUNT / 2) < 16, "one named barrier per pair");
         const int pair = tid / S::G2;
-        fft_pair<LOG_N, S::G2, FAST>(reinterpret_cast<ulonglong2*>(data) + pair * S::SEQ4,
+        const int shift = COLW != 0 ? col_pair_shift<COUNT / (COLW != 0 ? COLW : 1), COLW>(pair) : 0;
+        fft_pair<LOG_N, S::G2, FAST>(reinterpret_cast<ulonglong2*>(data) + pair * S::SEQ4 + shift,
                                      reinterpret_cast<const ulonglong2*>(tws), tid % S::G2, 1 + pair);
     }
 }
@@ -385,7 +404,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     // float2 the caller reserves), loaded with the intermediate so the taps
     // of the foam step (within a cell of the strip for any velocity up to
     // cell / dt) come from shared memory.
-    float* fwin = reinterpret_cast<float*>(smem + NF * W * seq_f2<LOG_N, TC>());
+    float* fwin = reinterpret_cast<float*>(smem + NF * W * seq_f2<LOG_N, TC>() + (TC ? 0 : col_shift_f2<NF, W>()));
     if constexpr (FSTEP) {
         const float* cur = a.foam_cur + base;
         for (int k = tid; k < N * WW; k += NT) {
@@ -422,14 +441,15 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
                     data[((2 * fp) * W + w) * SEQ + pad_idx(y)] = make_float2(v.x, v.y);
                     data[((2 * fp + 1) * W + w) * SEQ + pad_idx(y)] = make_float2(v.z, v.w);
                 } else {
-                    data4[(fp * W + w) * SEQ4 + pad4(y)] = make_float4(v.x, v.z, v.y, v.w);
+                    data4[(fp * W + w) * SEQ4 + col_pair_shift<NF, W>(fp * W + w) + pad4(y)] =
+                        make_float4(v.x, v.z, v.y, v.w);
                 }
             }
         }
     }
     __syncthreads();
 
-    transform_all<LOG_N, FAST, TC, NF * W>(data, tws, tid, eng, error);
+    transform_all<LOG_N, FAST, TC, NF * W, W>(data, tws, tid, eng, error);
     __syncthreads();
 
     OceanConsts cst;
@@ -477,14 +497,14 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
             }
         } else {
             const int sy = pad4(y);
-            const float4 q0 = data4[(0 * W + w) * SEQ4 + sy];
-            const float4 q1 = data4[(1 * W + w) * SEQ4 + sy];
+            const float4 q0 = data4[(0 * W + w) * SEQ4 + col_pair_shift<NF, W>(0 * W + w) + sy];
+            const float4 q1 = data4[(1 * W + w) * SEQ4 + col_pair_shift<NF, W>(1 * W + w) + sy];
             f0 = make_float2(q0.x, q0.z);
             f1 = make_float2(q0.y, q0.w);
             f2 = make_float2(q1.x, q1.z);
             f3 = make_float2(q1.y, q1.w);
             if constexpr (NF == 6) {
-                const float4 q2 = data4[(2 * W + w) * SEQ4 + sy];
+                const float4 q2 = data4[(2 * W + w) * SEQ4 + col_pair_shift<NF, W>(2 * W + w) + sy];
                 f4 = make_float2(q2.x, q2.z);
                 f5 = make_float2(q2.y, q2.w);
             }
@@ -552,7 +572,7 @@ col_pass_kernel(FrameArgs a)
     constexpr int NT = NF * S::W * S::G;
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
-    float2* tws = smem + NF * S::W * S::SEQ4 + foam_window_f2<LOG_N, S::W>();  // behind the foam window
+    float2* tws = smem + NF * S::W * S::SEQ4 + col_shift_f2<NF, S::W>() + foam_window_f2<LOG_N, S::W>();
     load_twiddles<LOG_N, false>(tws, a.twiddles, threadIdx.x, NT);
     const int o = blockIdx.y;
     col_task<LOG_N, NF, FAST, FOAM, S::W, false>(
@@ -632,7 +652,8 @@ __host__ __device__ constexpr size_t frame_data_float2()
 {
     using S = Shape<LOG_N>;
     constexpr size_t row = S::RP * 2 * NF * seq_f2<LOG_N, TC>() + S::RP * 2 * S::N;
-    constexpr size_t col = NF * S::PW * seq_f2<LOG_N, TC>();
+    constexpr size_t col = NF * S::PW * seq_f2<LOG_N, TC>() + (TC ? 0 : col_shift_f2<NF, S::PW>()) +
+                           foam_window_f2<LOG_N, S::PW>();
     return row > col ? row : col;
 }
 
@@ -653,7 +674,8 @@ frame_kernel(FrameArgs a, QueueArgs q)
     constexpr int RT = (N / 2) / S::RP;  // row tasks per ocean
     constexpr int CT = N / S::PW;        // column tasks per ocean
     constexpr size_t kDataFloat2 = frame_data_float2<LOG_N, NF, TC>();
-    static_assert(size_t(NF) * S::PW * seq_f2<LOG_N, TC>() + foam_window_f2<LOG_N, S::PW>() <= kDataFloat2,
+    static_assert(size_t(NF) * S::PW * seq_f2<LOG_N, TC>() + (TC ? 0 : col_shift_f2<NF, S::PW>()) +
+                          foam_window_f2<LOG_N, S::PW>() <= kDataFloat2,
                   "the column task's foam window fits in the data area");
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
@@ -846,7 +868,8 @@ template <int LOG_N, int NF>
 constexpr size_t col_smem_bytes()
 {
     using S = Shape<LOG_N>;
-    return sizeof(float2) * (NF * S::W * S::SEQ4 + foam_window_f2<LOG_N, S::W>() + twiddle_f2<LOG_N, false>());
+    return sizeof(float2) *
+           (NF * S::W * S::SEQ4 + col_shift_f2<NF, S::W>() + foam_window_f2<LOG_N, S::W>() + twiddle_f2<LOG_N, false>());
 }
 
 template <int LOG_N, int NF, bool FAST>
