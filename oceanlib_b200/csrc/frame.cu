@@ -558,6 +558,7 @@ row_pass_kernel(FrameArgs a)
     float2* smem = reinterpret_cast<float2*>(smem4);
     float2* tws = smem + S::RP * 2 * NF * S::SEQ4 + S::RP * 2 * S::N;
     load_twiddles<LOG_N, false>(tws, a.twiddles, threadIdx.x, NT);
+    __syncthreads();  // the twiddles are complete before any transform reads them
     const int o = blockIdx.y;
     row_task<LOG_N, NF, FAST>(a, a.ocean_base + o, blockIdx.x,
                               a.inter + static_cast<size_t>(o) * S::N * S::N * NF, smem, tws,
@@ -574,6 +575,7 @@ col_pass_kernel(FrameArgs a)
     float2* smem = reinterpret_cast<float2*>(smem4);
     float2* tws = smem + NF * S::W * S::SEQ4 + col_shift_f2<NF, S::W>() + foam_window_f2<LOG_N, S::W>();
     load_twiddles<LOG_N, false>(tws, a.twiddles, threadIdx.x, NT);
+    __syncthreads();  // the twiddles are complete before any transform reads them
     const int o = blockIdx.y;
     col_task<LOG_N, NF, FAST, FOAM, S::W, false>(
         a, a.ocean_base + o, blockIdx.x, a.inter + static_cast<size_t>(o) * S::N * S::N * NF,
@@ -589,10 +591,9 @@ col_pass_kernel(FrameArgs a)
 // b % slots and first waits until C(b - slots) finished reading it. Every
 // awaited task holds an earlier ticket, so it is already running on some CTA
 // and never waits on a later one: the queue cannot deadlock, co-resident or
-// not. Waits are bounded (kWaitNs); a CTA that gives up sets the error word
+// not. Waits are bounded (QueueArgs::wait_ns); a CTA that gives up sets the error word
 // and leaves, and the others give up in turn.
 // ---------------------------------------------------------------------------
-constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
 
 __device__ __forceinline__ unsigned long long global_ns()
 {
@@ -615,7 +616,7 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
     return v;
 }
 
-// Spin until *counter >= target or the error word is set or kWaitNs passes.
+// Spin until *counter >= target or the error word is set or limit_ns passes.
 // Returns false on timeout / abort.
 __device__ bool wait_at_least(const unsigned* counter, unsigned target, unsigned* error,
                               unsigned long long limit_ns)
