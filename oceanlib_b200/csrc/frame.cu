@@ -34,7 +34,6 @@ template <int LOG_N>
 struct Shape {
     static constexpr int N = 1 << LOG_N;
     static constexpr int G = lanes_for(LOG_N);                       // lanes / sequence
-    static constexpr int G2 = pair_lanes(LOG_N);                     // lanes / sequence pair
     static constexpr int SEQ = padded_len(N) + kPad;                 // sequence stride (float2)
     static constexpr int SEQ4 = padded_len4(N) + kPad4;              // pair stride (float4)
     static constexpr int RP = cmin(N / 2, 32 / G > 1 ? 32 / G : 1); // row pairs / CTA
@@ -47,21 +46,41 @@ struct Shape {
     static constexpr int PW = 2 * RP;
 };
 
-// Shared-memory layouts of the sequences a task transforms. The FP32 forms
-// keep fields 2p and 2p+1 of a row or column as one pair (float4 per index,
-// stride SEQ4 float4 = 2 SEQ4 float2 per pair, so SEQ4 float2 per sequence);
-// the tensor-core form keeps every sequence on its own (float2 per index,
-// stride SEQ). Twiddles follow the data: float4 (wx, wx, wy, wy) entries for
-// the pairs, float2 for the tensor-core form.
+// Shared-memory layouts of the sequences a task transforms. Paired: fields
+// 2p and 2p+1 of a row or column as one pair (float4 per index, stride SEQ4
+// float4 = 2 SEQ4 float2 per pair, so SEQ4 float2 per sequence), transformed
+// with packed f32x2 arithmetic. Single: every sequence on its own (float2 per
+// index, stride SEQ). A lane keeps half as many indices of each sequence in
+// a pair (it holds two), so pairs are used where that adds no pass through
+// shared memory: N = 32, 64, 512. N = 16, 128, 256 and 1024 (one pass fewer
+// with 16 or 32 values of one sequence per lane) and the tensor-core form
+// use single sequences. Twiddles follow the data: float4 (wx, wx, wy, wy)
+// entries for pairs, float2 otherwise.
+template <int LOG_N>
+__host__ __device__ constexpr int lane_log_values()
+{
+    return ilog2c((1 << LOG_N) / lanes_for(LOG_N));
+}
+template <int LOG_N>
+__host__ __device__ constexpr bool pairs_pay()
+{
+    return (LOG_N + lane_log_values<LOG_N>() - 1) / lane_log_values<LOG_N>() ==
+           (LOG_N + lane_log_values<LOG_N>() - 2) / (lane_log_values<LOG_N>() - 1);
+}
+template <int LOG_N, bool TC>
+__host__ __device__ constexpr bool paired()
+{
+    return !TC && pairs_pay<LOG_N>();
+}
 template <int LOG_N, bool TC>
 __host__ __device__ constexpr int seq_f2()
 {
-    return TC ? Shape<LOG_N>::SEQ : Shape<LOG_N>::SEQ4;
+    return paired<LOG_N, TC>() ? Shape<LOG_N>::SEQ4 : Shape<LOG_N>::SEQ;
 }
 template <int LOG_N, bool TC>
 __host__ __device__ constexpr int twiddle_f2()
 {
-    return TC ? (1 << LOG_N) - 1 : 2 * ((1 << LOG_N) - 1);
+    return paired<LOG_N, TC>() ? 2 * ((1 << LOG_N) - 1) : (1 << LOG_N) - 1;
 }
 
 // Column tasks over 2 columns shift their sequence pairs (pair s = field
@@ -82,6 +101,13 @@ __host__ __device__ constexpr int col_shift_f2()
     return 2 * col_pair_shift<NF, W>(NF * W / 2 - 1);
 }
 
+// The shifts' float2 for a task of layout (LOG_N, TC) (none for single sequences).
+template <int LOG_N, int NF, int W, bool TC>
+__host__ __device__ constexpr int col_shift_f2_of()
+{
+    return paired<LOG_N, TC>() ? col_shift_f2<NF, W>() : 0;
+}
+
 // Foam window of a column task over W columns: columns x0 - 1 .. x0 + W of
 // every row (WW floats per row), and its size in float2.
 template <int W>
@@ -100,7 +126,7 @@ template <int LOG_N, bool TC>
 __device__ __forceinline__ void load_twiddles(float2* tws, const float2* __restrict__ src, int tid, int nt)
 {
     constexpr int N = 1 << LOG_N;
-    if constexpr (TC) {
+    if constexpr (!paired<LOG_N, TC>()) {
         for (int i = tid; i < N - 1; i += nt) tws[i] = src[i];
     } else {
         float4* t4 = reinterpret_cast<float4*>(tws);
@@ -124,13 +150,16 @@ __device__ __forceinline__ void transform_all(float2* data, const float2* tws, i
         for (int s0 = 0; s0 < COUNT; s0 += tc::kSeq)
             eng->dft512(data + s0 * S::SEQ, S::SEQ, COUNT - s0 < tc::kSeq ? COUNT - s0 : tc::kSeq, tws, tid,
                         error);
+    } else if constexpr (!paired<LOG_N, TC>()) {
+        fft_sequence<LOG_N, S::G, FAST>(data + (tid / S::G) * S::SEQ, tws, tid % S::G);
     } else {
+        constexpr int G2 = pair_lanes(LOG_N);  // lanes per sequence pair
         static_assert(COUNT % 2 == 0, "sequences come in pairs");
-        static_assert(S::G2 <= 32 || (COUNT / 2) < 16, "one named barrier per pair");
-        const int pair = tid / S::G2;
+        static_assert(G2 <= 32 || (COUNT / 2) < 16, "one named barrier per pair");
+        const int pair = tid / G2;
         const int shift = COLW != 0 ? col_pair_shift<COUNT / (COLW != 0 ? COLW : 1), COLW>(pair) : 0;
-        fft_pair<LOG_N, S::G2, FAST>(reinterpret_cast<ulonglong2*>(data) + pair * S::SEQ4 + shift,
-                                     reinterpret_cast<const ulonglong2*>(tws), tid % S::G2, 1 + pair);
+        fft_pair<LOG_N, G2, FAST>(reinterpret_cast<ulonglong2*>(data) + pair * S::SEQ4 + shift,
+                                     reinterpret_cast<const ulonglong2*>(tws), tid % G2, 1 + pair);
     }
 }
 
@@ -149,6 +178,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     constexpr int N = S::N, G = S::G, SEQ = S::SEQ, SEQ4 = S::SEQ4, RP = S::RP;
     constexpr int NT = RP * 2 * NF * G;
     constexpr int Q = NF / 2;
+    constexpr bool PAIRED = paired<LOG_N, TC>();
 
     float2* data = smem;                                   // sequences of rows (j, r), fields f
     float4* data4 = reinterpret_cast<float4*>(smem);       // the same as pairs (j, r, f / 2)
@@ -259,7 +289,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
             p4 = make_float2(ux_re - uy_im, ux_im + uy_re);
             p5 = make_float2(uz_re, uz_im);
         }
-        if constexpr (TC) {
+        if constexpr (!PAIRED) {
             float2* base = data + (jr * NF) * SEQ + pad_idx(x);
             base[0 * SEQ] = p0;
             base[1 * SEQ] = p1;
@@ -293,7 +323,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         const int x = cell & (N - 1);
         const int row = row_of(jr >> 1, jr & 1);
         float4 o;
-        if constexpr (TC) {
+        if constexpr (!PAIRED) {
             const float2 v0 = data[(jr * NF + 2 * fp) * SEQ + pad_idx(x)];
             const float2 v1 = data[(jr * NF + 2 * fp + 1) * SEQ + pad_idx(x)];
             o = make_float4(v0.x, v0.y, v1.x, v1.y);
@@ -392,6 +422,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     constexpr int N = S::N, G = S::G, SEQ = S::SEQ, SEQ4 = S::SEQ4;
     constexpr int NT = NF * W * G;
     constexpr int Q = NF / 2;
+    constexpr bool PAIRED = paired<LOG_N, TC>();
     float2* data = smem;                             // TC: sequence f*W + w
     float4* data4 = reinterpret_cast<float4*>(smem); // pairs: pair p*W + w holds fields 2p, 2p+1
     const int x0 = strip * W;
@@ -404,7 +435,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     // float2 the caller reserves), loaded with the intermediate so the taps
     // of the foam step (within a cell of the strip for any velocity up to
     // cell / dt) come from shared memory.
-    float* fwin = reinterpret_cast<float*>(smem + NF * W * seq_f2<LOG_N, TC>() + (TC ? 0 : col_shift_f2<NF, W>()));
+    float* fwin = reinterpret_cast<float*>(smem + NF * W * seq_f2<LOG_N, TC>() + col_shift_f2_of<LOG_N, NF, W, TC>());
     if constexpr (FSTEP) {
         const float* cur = a.foam_cur + base;
         for (int k = tid; k < N * WW; k += NT) {
@@ -437,7 +468,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
                 const int y = cw / W;
                 const int w = cw % W;
                 const float4 v = buf[k];
-                if constexpr (TC) {
+                if constexpr (!PAIRED) {
                     data[((2 * fp) * W + w) * SEQ + pad_idx(y)] = make_float2(v.x, v.y);
                     data[((2 * fp + 1) * W + w) * SEQ + pad_idx(y)] = make_float2(v.z, v.w);
                 } else {
@@ -485,7 +516,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
         const int w = i % W;
         const int x = x0 + w;
         float2 f0, f1, f2, f3, f4, f5;
-        if constexpr (TC) {
+        if constexpr (!PAIRED) {
             const int sy = pad_idx(y);
             f0 = data[(0 * W + w) * SEQ + sy];
             f1 = data[(1 * W + w) * SEQ + sy];
@@ -556,7 +587,7 @@ row_pass_kernel(FrameArgs a)
     constexpr int NT = S::RP * 2 * NF * S::G;
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
-    float2* tws = smem + S::RP * 2 * NF * S::SEQ4 + S::RP * 2 * S::N;
+    float2* tws = smem + S::RP * 2 * NF * seq_f2<LOG_N, false>() + S::RP * 2 * S::N;
     load_twiddles<LOG_N, false>(tws, a.twiddles, threadIdx.x, NT);
     __syncthreads();  // the twiddles are complete before any transform reads them
     const int o = blockIdx.y;
@@ -573,7 +604,8 @@ col_pass_kernel(FrameArgs a)
     constexpr int NT = NF * S::W * S::G;
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
-    float2* tws = smem + NF * S::W * S::SEQ4 + col_shift_f2<NF, S::W>() + foam_window_f2<LOG_N, S::W>();
+    float2* tws = smem + NF * S::W * seq_f2<LOG_N, false>() + col_shift_f2_of<LOG_N, NF, S::W, false>() +
+                  foam_window_f2<LOG_N, S::W>();
     load_twiddles<LOG_N, false>(tws, a.twiddles, threadIdx.x, NT);
     __syncthreads();  // the twiddles are complete before any transform reads them
     const int o = blockIdx.y;
@@ -653,7 +685,7 @@ __host__ __device__ constexpr size_t frame_data_float2()
 {
     using S = Shape<LOG_N>;
     constexpr size_t row = S::RP * 2 * NF * seq_f2<LOG_N, TC>() + S::RP * 2 * S::N;
-    constexpr size_t col = NF * S::PW * seq_f2<LOG_N, TC>() + (TC ? 0 : col_shift_f2<NF, S::PW>()) +
+    constexpr size_t col = NF * S::PW * seq_f2<LOG_N, TC>() + col_shift_f2_of<LOG_N, NF, S::PW, TC>() +
                            foam_window_f2<LOG_N, S::PW>();
     return row > col ? row : col;
 }
@@ -675,7 +707,7 @@ frame_kernel(FrameArgs a, QueueArgs q)
     constexpr int RT = (N / 2) / S::RP;  // row tasks per ocean
     constexpr int CT = N / S::PW;        // column tasks per ocean
     constexpr size_t kDataFloat2 = frame_data_float2<LOG_N, NF, TC>();
-    static_assert(size_t(NF) * S::PW * seq_f2<LOG_N, TC>() + (TC ? 0 : col_shift_f2<NF, S::PW>()) +
+    static_assert(size_t(NF) * S::PW * seq_f2<LOG_N, TC>() + col_shift_f2_of<LOG_N, NF, S::PW, TC>() +
                           foam_window_f2<LOG_N, S::PW>() <= kDataFloat2,
                   "the column task's foam window fits in the data area");
     extern __shared__ float4 smem4[];
@@ -683,6 +715,11 @@ frame_kernel(FrameArgs a, QueueArgs q)
     float2* tws = smem + kDataFloat2;
     __shared__ unsigned s_ticket;
     __shared__ int s_ok;
+    // Thread 0's queue state between tasks, kept in shared memory so that it
+    // takes no registers in the task code that every thread runs.
+    __shared__ unsigned* s_publish;
+    __shared__ unsigned s_next;
+    __shared__ int s_have_next;
 
     const int tid = threadIdx.x;
     load_twiddles<LOG_N, TC>(tws, a.twiddles, tid, NT);
@@ -713,24 +750,34 @@ frame_kernel(FrameArgs a, QueueArgs q)
 
     // Thread 0 publishes the previous task with a release add (the barrier
     // above it orders every thread's writes before it, the pattern grid-wide
-    // barriers use), then waits for the inputs of the ticket it drew one
-    // task earlier and draws the following one, whose round trip overlaps
-    // the task; one barrier hands the ticket to the CTA. The publish comes
-    // before the wait: the next task may depend on the one just finished. A
-    // drawn ticket T runs right after the CTA's current task (< T), which
-    // waits on nothing later, so the queue stays deadlock-free.
-    unsigned* publish = nullptr;
-    unsigned t_next = 0;
-    if (tid == 0) t_next = atomicAdd(q.ticket, 1u);
+    // barriers use), then takes its next ticket and waits for that task's
+    // inputs; one barrier hands the ticket to the CTA. The publish comes
+    // before the wait: the next task may depend on the one just finished.
+    // Far from the end of the queue the following ticket is drawn one task
+    // ahead; near the end tickets are drawn when a CTA is free, since a
+    // ticket held by a CTA whose current task still waits would idle others
+    // (in a short queue, e.g. 3 x 256^2 cascade levels on 296 CTAs, drawing
+    // ahead cost 8 us per frame). A drawn ticket T runs right after the
+    // CTA's current task (< T), which waits on nothing later, so the queue
+    // stays deadlock-free.
+    if (tid == 0) {
+        s_publish = nullptr;
+        s_next = atomicAdd(q.ticket, 1u);
+        s_have_next = 1;
+    }
     while (true) {
         __syncthreads();  // previous task's writes issued; shared memory free
         if (tid == 0) {
-            if (publish != nullptr) red_release_add(publish, 1u);
-            const unsigned t = t_next;
+            if (s_publish != nullptr) red_release_add(s_publish, 1u);
+            const unsigned t = s_have_next ? s_next : atomicAdd(q.ticket, 1u);
+            s_have_next = 0;
             int ok = 1;
-            publish = nullptr;
+            unsigned* publish = nullptr;
             if (t < total) {
-                t_next = atomicAdd(q.ticket, 1u);
+                if (t + 2u * gridDim.x < total) {
+                    s_next = atomicAdd(q.ticket, 1u);
+                    s_have_next = 1;
+                }
                 bool row;
                 unsigned ocean, idx;
                 decode(t, row, ocean, idx);
@@ -742,6 +789,7 @@ frame_kernel(FrameArgs a, QueueArgs q)
                 }
                 publish = row ? q.rows_done + ocean : q.cols_done + ocean;
             }
+            s_publish = publish;
             s_ticket = t;
             s_ok = ok;
         }
@@ -863,14 +911,15 @@ template <int LOG_N, int NF>
 constexpr size_t row_smem_bytes()
 {
     using S = Shape<LOG_N>;
-    return sizeof(float2) * (S::RP * 2 * NF * S::SEQ4 + S::RP * 2 * S::N + twiddle_f2<LOG_N, false>());
+    return sizeof(float2) * (S::RP * 2 * NF * seq_f2<LOG_N, false>() + S::RP * 2 * S::N + twiddle_f2<LOG_N, false>());
 }
 template <int LOG_N, int NF>
 constexpr size_t col_smem_bytes()
 {
     using S = Shape<LOG_N>;
     return sizeof(float2) *
-           (NF * S::W * S::SEQ4 + col_shift_f2<NF, S::W>() + foam_window_f2<LOG_N, S::W>() + twiddle_f2<LOG_N, false>());
+           (NF * S::W * seq_f2<LOG_N, false>() + col_shift_f2_of<LOG_N, NF, S::W, false>() +
+            foam_window_f2<LOG_N, S::W>() + twiddle_f2<LOG_N, false>());
 }
 
 template <int LOG_N, int NF, bool FAST>
