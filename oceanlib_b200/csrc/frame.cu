@@ -5,9 +5,10 @@
 //   row pass   (grid: row-pair groups x oceans)
 //     h0 rows y and N-y -> shared memory; evolve every cell of both rows into
 //     NF packed complex fields (src/core/evolve.cpp:28-184); 2*NF row FFTs in
-//     shared memory, one lane group per sequence; write the rows to the
-//     intermediate, cell-major [y][x][field] so the column pass reads whole
-//     128-byte lines.
+//     shared memory, one lane group per sequence or per pair of sequences
+//     (packed f32x2 arithmetic, at the sizes where pairs cost no extra pass);
+//     write the rows to the intermediate, cell-major [y][x][field] so the
+//     column pass reads whole 128-byte lines.
 //
 //   column pass (grid: W-column strips x oceans)
 //     gather the strip's NF*W columns; column FFTs; finalize every cell
