@@ -285,6 +285,31 @@ def test_persistent_and_chunked_schedules_are_bit_identical():
             assert np.array_equal(bits(a), bits(b))
 
 
+def test_chunked_schedule_matches_persistent_at_every_size():
+    # The chunked row / column kernels lay out shared memory by size (field
+    # pairs at N = 32, 64, 512, single sequences elsewhere) and stage a wider
+    # foam window (up to 16 columns a strip); every size, with and without
+    # velocity and persistent foam, gives the persistent kernel's bits.
+    for n in (16, 32, 64, 128, 256, 512, 1024):
+        for vel in (False, True):
+            descs = [ob.OceanDesc(size=n, patch_length=2.5 * n, wind_speed=11.0 + k, wind_direction=0.7,
+                                  choppiness=1.2, seed=3 * n + k, compute_velocity=vel) for k in range(2)]
+            foam = W.foam_desc() if vel else None
+            cells = n * n
+            got = []
+            for schedule in (abi.OCEAN_SCHEDULE_PERSISTENT, abi.OCEAN_SCHEDULE_CHUNKED):
+                batch = ob.OceanBatch(descs, foam=foam, schedule=schedule)
+                d = np.empty((2, cells, 4), np.float32)
+                nn, v = np.empty_like(d), (np.empty_like(d) if vel else None)
+                f = np.empty((2, cells), np.float32) if vel else None
+                for k in range(2):  # the second frame advects the first frame's foam
+                    batch.update_host([(k + 1) / 60.0 + 20.0], 1.0 / 60.0 if vel else 0.0, d, nn, v, f)
+                got.append([a.copy() for a in (d, nn, v, f) if a is not None])
+                batch.close()
+            for a, b in zip(got[0], got[1]):
+                assert np.array_equal(bits(a), bits(b)), (n, vel)
+
+
 def test_single_ocean_update_uses_persistent_frame_and_matches_oracle():
     desc = W.foam_patch_512(seed=3)
     oc = ob.Ocean(desc)
