@@ -208,7 +208,19 @@ __device__ __forceinline__ uint32_t pack2(uint16_t a, uint16_t b)
 
 // Read back, level D_L of a row with fixed-point exponent e weighs
 // 2^(48 - 8 L - 30 - e) = 2^(18 - 8 L - e); the levels are added largest
-// first.
+// first. A level is an exact integer below 2^22 and its weight a power of
+// two, so each weighted level is exact and a fused multiply-add rounds the
+// running sum exactly as a multiply followed by an add would: the same
+// bits in fewer instructions.
+__device__ __forceinline__ float level_sum(uint32_t l0, uint32_t l1, int e)
+{
+    return __fmaf_rn(__uint_as_float(l1), pow2f(10 - e), __uint_as_float(l0) * pow2f(18 - e));
+}
+__device__ __forceinline__ float level_add(float acc, uint32_t l2, uint32_t l3, int e)
+{
+    return __fmaf_rn(__uint_as_float(l3), pow2f(-6 - e), __fmaf_rn(__uint_as_float(l2), pow2f(2 - e), acc));
+}
+
 struct Engine {
     unsigned char* smem;  // kSmemBytes, 128-byte aligned
     uint32_t tmem;        // tensor-memory base (lane 0, column 0)
@@ -380,7 +392,7 @@ struct Engine {
                 tmem_wait_ld();
 #pragma unroll
                 for (int j = 0; j < 32; ++j)
-                    y[j] = __uint_as_float(r0[j]) * pow2f(18 - e1) + __uint_as_float(r1[j]) * pow2f(10 - e1);
+                    y[j] = level_sum(r0[j], r1[j], e1);
             }
             {
                 uint32_t r2[32], r3[32];
@@ -389,7 +401,7 @@ struct Engine {
                 tmem_wait_ld();
 #pragma unroll
                 for (int j = 0; j < 32; ++j)
-                    y[j] = (y[j] + __uint_as_float(r2[j]) * pow2f(2 - e1)) + __uint_as_float(r3[j]) * pow2f(-6 - e1);
+                    y[j] = level_add(y[j], r2[j], r3[j], e1);
             }
             // Z staged as FP32, stage-3 row (s, k1) at zbuf + (s * 16 + k1) *
             // kZStride, K = (p, n2), in the sequences' own buffer: every
@@ -479,7 +491,7 @@ struct Engine {
                 tmem_wait_ld();
 #pragma unroll
                 for (int j = 0; j < 32; ++j)
-                    x[j] = __uint_as_float(r0[j]) * pow2f(18 - e) + __uint_as_float(r1[j]) * pow2f(10 - e);
+                    x[j] = level_sum(r0[j], r1[j], e);
             }
             {
                 uint32_t r2[32], r3[32];
@@ -488,7 +500,7 @@ struct Engine {
                 tmem_wait_ld();
 #pragma unroll
                 for (int j = 0; j < 32; ++j)
-                    x[j] = (x[j] + __uint_as_float(r2[j]) * pow2f(2 - e)) + __uint_as_float(r3[j]) * pow2f(-6 - e);
+                    x[j] = level_add(x[j], r2[j], r3[j], e);
             }
             const int s = row >> 4, k1 = row & 15;
             if (s < count) {
