@@ -206,6 +206,33 @@ __device__ __forceinline__ uint32_t pack2(uint16_t a, uint16_t b)
     return static_cast<uint32_t>(a) | (static_cast<uint32_t>(b) << 16);
 }
 
+// The operand form of digits4: signed digits of rint(x), |x| < 2^30, as
+// floats, rint(x) = t0 2^24 + t1 2^16 + t2 2^8 + t3 with |t_i| <= 128 (so
+// every digit product is at most 2^14 and a level of 256 terms at most
+// 2^22, still exact in FP32). Each digit rounds the remaining value at its
+// weight to the nearest integer ((y + 1.5 2^23) - 1.5 2^23 does so for
+// |y| < 2^22) and each residual is exact, all in full-rate FP32 operations;
+// the last digit rounds the fraction, so the digits sum to rint(x). Only
+// ties may split between digits differently from digits4 (same sum).
+__device__ __forceinline__ void digits4f(float x, float (&t)[4])
+{
+    constexpr float M = 12582912.0f;  // 1.5 * 2^23
+    t[0] = __fadd_rn(__fmaf_rn(x, 0x1p-24f, M), -M);
+    const float x1 = __fmaf_rn(t[0], -0x1p24f, x);
+    t[1] = __fadd_rn(__fmaf_rn(x1, 0x1p-16f, M), -M);
+    const float x2 = __fmaf_rn(t[1], -0x1p16f, x1);
+    t[2] = __fadd_rn(__fmaf_rn(x2, 0x1p-8f, M), -M);
+    const float x3 = __fmaf_rn(t[2], -0x1p8f, x2);
+    t[3] = __fadd_rn(__fadd_rn(x3, M), -M);
+}
+
+// Two digits as one FP16 pair (a in the low half), one conversion.
+__device__ __forceinline__ uint32_t half2_bits(float a, float b)
+{
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
 // Read back, level D_L of a row with fixed-point exponent e weighs
 // 2^(48 - 8 L - 30 - e) = 2^(18 - 8 L - e); the levels are added largest
 // first. A level is an exact integer below 2^22 and its weight a power of
@@ -347,15 +374,15 @@ struct Engine {
             const float sc = pow2f(e1);
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
-                uint16_t d[8][4];
+                float d[8][4];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) digits4(__float2int_rn(v[8 * c + q] * sc), d[q]);
+                for (int q = 0; q < 8; ++q) digits4f(v[8 * c + q] * sc, d[q]);
                 const int off = kmajor(tid, 8 * c, kK1);
 #pragma unroll
                 for (int g = 0; g < kDigits; ++g)
                     *reinterpret_cast<uint4*>(a0p + g * kAHalves + off) =
-                        make_uint4(pack2(d[0][g], d[1][g]), pack2(d[2][g], d[3][g]), pack2(d[4][g], d[5][g]),
-                                   pack2(d[6][g], d[7][g]));
+                        make_uint4(half2_bits(d[0][g], d[1][g]), half2_bits(d[2][g], d[3][g]),
+                                   half2_bits(d[4][g], d[5][g]), half2_bits(d[6][g], d[7][g]));
             }
         }
         fence_proxy_async();
@@ -446,15 +473,15 @@ struct Engine {
             const float sc = pow2f(ex3);
 #pragma unroll
             for (int c = 0; c < 4; ++c) {
-                uint16_t d[8][4];
+                float d[8][4];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) digits4(__float2int_rn(v[8 * c + q] * sc), d[q]);
+                for (int q = 0; q < 8; ++q) digits4f(v[8 * c + q] * sc, d[q]);
                 const int off = kmajor(row, half_k * 32 + 8 * c, kK3);
 #pragma unroll
                 for (int g = 0; g < kDigits; ++g)
                     *reinterpret_cast<uint4*>(a0p + g * kAHalves + off) =
-                        make_uint4(pack2(d[0][g], d[1][g]), pack2(d[2][g], d[3][g]), pack2(d[4][g], d[5][g]),
-                                   pack2(d[6][g], d[7][g]));
+                        make_uint4(half2_bits(d[0][g], d[1][g]), half2_bits(d[2][g], d[3][g]),
+                                   half2_bits(d[4][g], d[5][g]), half2_bits(d[6][g], d[7][g]));
             }
             if (half_k == 0) e3()[row] = ex3;
         }
