@@ -448,8 +448,13 @@ struct Engine {
         }
         __syncthreads();
         // ---- stage 3 operand: two threads per row (s, k1), each 32 of its K ----
+        // Warp w takes sequence w's 16 rows; a quarter warp takes 8 rows and
+        // one half of K, so its float4 reads of the staged Z (row stride 68
+        // floats) and its 16-byte digit stores (8 rows of one core matrix)
+        // each touch 8 distinct bank groups. The row's other half sits 8
+        // lanes away.
         if (worker) {
-            const int row = tid >> 1, half_k = tid & 1;
+            const int row = warp * 16 + (lane & 7) + 8 * (lane >> 4), half_k = (lane >> 3) & 1;
             const int s = row >> 4;
             float v[32];
             float m = 0.0f;
@@ -468,7 +473,7 @@ struct Engine {
 #pragma unroll
                 for (int k = 0; k < 32; ++k) v[k] = 0.0f;
             }
-            m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 1));
+            m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, 8));
             const int ex3 = row_exp(m);
             const float sc = pow2f(ex3);
 #pragma unroll
