@@ -206,24 +206,29 @@ __device__ __forceinline__ uint32_t pack2(uint16_t a, uint16_t b)
     return static_cast<uint32_t>(a) | (static_cast<uint32_t>(b) << 16);
 }
 
-// The operand form of digits4: signed digits of rint(x), |x| < 2^30, as
-// floats, rint(x) = t0 2^24 + t1 2^16 + t2 2^8 + t3 with |t_i| <= 128 (so
-// every digit product is at most 2^14 and a level of 256 terms at most
-// 2^22, still exact in FP32). Each digit rounds the remaining value at its
-// weight to the nearest integer ((y + 1.5 2^23) - 1.5 2^23 does so for
-// |y| < 2^22) and each residual is exact, all in full-rate FP32 operations;
-// the last digit rounds the fraction, so the digits sum to rint(x). Only
-// ties may split between digits differently from digits4 (same sum).
-__device__ __forceinline__ void digits4f(float x, float (&t)[4])
+// The operand form of digits4: signed digits of x, |x| < 2^30, as floats,
+// x rounded to the nearest integer = t0 2^24 + t1 2^16 + t2 2^8 + t3 with
+// |t_i| <= 128 (so every digit product is at most 2^14 and a level of 256
+// terms at most 2^22, still exact in FP32). Each digit is the remaining value
+// at its weight rounded to the nearest integer, halves up as digits4 rounds
+// them (floor(y + 1/2): y + 1/2 by one rounding, then a round-down add onto
+// the integer grid of 1.5 2^23), and each residual is exact: full-rate FP32
+// operations only. Rounding halves to even instead measurably raised the
+// worst-cell error of the frame's normals at late times.
+__device__ __forceinline__ float nearest_half_up(float x, float scale)
 {
     constexpr float M = 12582912.0f;  // 1.5 * 2^23
-    t[0] = __fadd_rn(__fmaf_rn(x, 0x1p-24f, M), -M);
+    return __fadd_rn(__fmaf_rd(__fmaf_rn(x, scale, 0.5f), 1.0f, M), -M);
+}
+__device__ __forceinline__ void digits4f(float x, float (&t)[4])
+{
+    t[0] = nearest_half_up(x, 0x1p-24f);
     const float x1 = __fmaf_rn(t[0], -0x1p24f, x);
-    t[1] = __fadd_rn(__fmaf_rn(x1, 0x1p-16f, M), -M);
+    t[1] = nearest_half_up(x1, 0x1p-16f);
     const float x2 = __fmaf_rn(t[1], -0x1p16f, x1);
-    t[2] = __fadd_rn(__fmaf_rn(x2, 0x1p-8f, M), -M);
+    t[2] = nearest_half_up(x2, 0x1p-8f);
     const float x3 = __fmaf_rn(t[2], -0x1p8f, x2);
-    t[3] = __fadd_rn(__fadd_rn(x3, M), -M);
+    t[3] = nearest_half_up(x3, 1.0f);
 }
 
 // Two digits as one FP16 pair (a in the low half), one conversion.
