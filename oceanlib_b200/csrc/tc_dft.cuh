@@ -231,6 +231,19 @@ __device__ __forceinline__ void digits4f(float x, float (&t)[4])
     t[3] = nearest_half_up(x3, 1.0f);
 }
 
+// a b - c d with about one rounding (Kahan: the rounding error of c d is
+// recovered exactly by a fused multiply-add and added back). The twiddle
+// step Z = Y W uses it: rounding each product and the sum separately (three
+// roundings) was the largest of the FP32 errors between the two exact GEMMs,
+// and with it the frame's late-time normals stayed above 2e-6 of FP64.
+__device__ __forceinline__ float diff_of_products(float a, float b, float c, float d)
+{
+    const float w = __fmul_rn(c, d);
+    const float e = __fmaf_rn(-c, d, w);
+    const float f = __fmaf_rn(a, b, -w);
+    return __fadd_rn(f, e);
+}
+
 // Two digits as one FP16 pair (a in the low half), one conversion.
 __device__ __forceinline__ uint32_t half2_bits(float a, float b)
 {
@@ -446,8 +459,8 @@ struct Engine {
                     float2 w = tws[e & 255];
                     if (e & 256) w = make_float2(-w.x, -w.y);
                     float* zrow = zbuf + (s_row * 16 + k1) * kZStride;
-                    zrow[n2] = y[k1] * w.x - y[16 + k1] * w.y;
-                    zrow[32 + n2] = y[k1] * w.y + y[16 + k1] * w.x;
+                    zrow[n2] = diff_of_products(y[k1], w.x, y[16 + k1], w.y);
+                    zrow[32 + n2] = diff_of_products(y[k1], w.y, -y[16 + k1], w.x);
                 }
             }
         }

@@ -4,9 +4,9 @@ Per output channel: max |e| / RMS of the FP64 frame (oracle.fp64_frame: the
 reference's FP32 spectra, an FP64 2-D inverse transform and an FP64
 finalize). The foam channel (a clamp of the Jacobian, mostly zero) is held
 to an absolute bound instead. The FP32 form is the reference's own
-arithmetic, so its errors are the accuracy the reference delivers; the
-tensor-core form must stay within TC_TOL of FP64 on every channel the FP32
-form itself meets 2e-6 on, and within 2x the FP32 form's error elsewhere."""
+arithmetic, so its errors are the accuracy the reference delivers (above
+2e-6 on some normals); the tensor-core form must stay within TC_TOL of FP64
+on every channel."""
 import numpy as np
 import pytest
 
@@ -71,10 +71,10 @@ def test_tensor_form_frame_against_fp64(case):
     for k in e32:
         if k.endswith("(abs)"):
             assert etc[k] <= FOAM_ABS_TOL, (k, etc[k])
-        elif e32[k] <= TC_TOL:
-            assert etc[k] <= TC_TOL, (k, etc[k], e32[k])
         else:
-            assert etc[k] <= 2.0 * e32[k], (k, etc[k], e32[k])
+            # every channel within 2e-6 of FP64, including those (normals at
+            # late times, with velocity) where the FP32 form is not
+            assert etc[k] <= TC_TOL, (k, etc[k], e32[k])
 
 
 def test_tensor_form_batch_is_per_ocean_independent():
