@@ -57,7 +57,7 @@ dft_tc512_kernel(const float2* __restrict__ in, float2* __restrict__ out, int co
     const int tid = threadIdx.x;
     for (int i = tid; i < N - 1; i += NT) tws[i] = tw[i];
     tc::Engine eng{eng_smem, 0};
-    eng.init(tid, NT);
+    eng.init(tid, NT, tw);
     for (int base = blockIdx.x * 8; base < count; base += gridDim.x * 8) {
         const int k = min(8, count - base);
         __syncthreads();
@@ -66,7 +66,7 @@ dft_tc512_kernel(const float2* __restrict__ in, float2* __restrict__ out, int co
             data[s * SEQ + pad_idx(n)] = in[static_cast<size_t>(base + s) * N + n];
         }
         __syncthreads();
-        eng.dft512(data, SEQ, k, tws, tid, error);
+        eng.dft512(data, SEQ, k, tid, error);
         for (int i = tid; i < k * N; i += NT) {
             const int s = i >> 9, n = i & (N - 1);
             out[static_cast<size_t>(base + s) * N + n] = data[s * SEQ + pad_idx(n)];

@@ -136,9 +136,10 @@ __device__ __forceinline__ void load_twiddles(float2* tws, const float2* __restr
 }
 
 // The inverse DFT of the COUNT sequences of a task: the radix-2 Stockham FFT
-// on sequence pairs (one lane group of G2 per pair, named barrier 1 + pair
-// where a pair spans two warps), or with TC the tensor-core four-step DFT,
-// 8 sequences per engine call (N = 512).
+// on single sequences (one lane group of G per sequence) or on sequence pairs
+// (one lane group of G2 per pair, named barrier 1 + pair where a pair spans
+// two warps), or with TC the tensor-core four-step DFT, 8 sequences per
+// engine call (N = 512; its twiddles live in the engine).
 template <int LOG_N, bool FAST, bool TC, int COUNT, int COLW = 0>
 __device__ __forceinline__ void transform_all(float2* data, const float2* tws, int tid, tc::Engine* eng,
                                               unsigned* error)
@@ -149,8 +150,7 @@ __device__ __forceinline__ void transform_all(float2* data, const float2* tws, i
         static_assert(S::SEQ * 2 >= 16 * tc::kZStride, "a sequence's space must hold its staged stage-3 rows");
 #pragma unroll 1
         for (int s0 = 0; s0 < COUNT; s0 += tc::kSeq)
-            eng->dft512(data + s0 * S::SEQ, S::SEQ, COUNT - s0 < tc::kSeq ? COUNT - s0 : tc::kSeq, tws, tid,
-                        error);
+            eng->dft512(data + s0 * S::SEQ, S::SEQ, COUNT - s0 < tc::kSeq ? COUNT - s0 : tc::kSeq, tid, error);
     } else if constexpr (!paired<LOG_N, TC>()) {
         fft_sequence<LOG_N, S::G, FAST>(data + (tid / S::G) * S::SEQ, tws, tid % S::G);
     } else {
@@ -723,11 +723,11 @@ frame_kernel(FrameArgs a, QueueArgs q)
     __shared__ int s_have_next;
 
     const int tid = threadIdx.x;
-    load_twiddles<LOG_N, TC>(tws, a.twiddles, tid, NT);
+    if constexpr (!TC) load_twiddles<LOG_N, TC>(tws, a.twiddles, tid, NT);
     tc::Engine eng{reinterpret_cast<unsigned char*>(smem4) + frame_engine_offset<LOG_N, NF>(), 0};
     if constexpr (TC) {
         static_assert(NT >= tc::kThreads, "the tensor-core engine needs 8 warps");
-        eng.init(tid, NT);
+        eng.init(tid, NT, a.twiddles);
     }
 
     const unsigned count = static_cast<unsigned>(q.count);

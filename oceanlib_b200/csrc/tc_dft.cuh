@@ -70,7 +70,8 @@ constexpr int kOffA = 0;                                       // [digit][8192]
 constexpr int kOffB1 = kOffA + kDigits * kAHalves * 2;          // [digit][32*32]
 constexpr int kOffB3 = kOffB1 + kDigits * kN1 * kK1 * 2;        // [digit][64*64]
 constexpr int kOffE3 = kOffB3 + kDigits * kN3 * kK3 * 2;        // int[kRows3]
-constexpr int kOffBar = kOffE3 + kRows3 * 4;                    // uint64 mbarrier
+constexpr int kOffTw3 = kOffE3 + kRows3 * 4;                    // float2[16][32]: W^(n2 k1)
+constexpr int kOffBar = kOffTw3 + 16 * 32 * 8;                  // uint64 mbarrier
 constexpr int kOffTmem = kOffBar + 8;                           // uint32 tmem base
 constexpr int kSmemBytes = kOffTmem + 8;
 
@@ -277,10 +278,22 @@ struct Engine {
     __device__ int* e3() const { return reinterpret_cast<int*>(smem + kOffE3); }
     __device__ uint32_t bar() const { return smem_u32(smem + kOffBar); }
 
-    // Once per kernel, all threads: the DFT matrices' digits, the mbarrier,
-    // and (warp 0) the tensor-memory allocation.
-    __device__ void init(int tid, int nthreads)
+    __device__ const float2* tw3() const { return reinterpret_cast<const float2*>(smem + kOffTw3); }
+
+    // Once per kernel, all threads: the DFT matrices' digits, the twiddles
+    // of the middle step as [k1][n2] = W^(n2 k1) from the FP32 table `tw`
+    // (W^p, p < 256, W = e^(2 pi i / 512); W^(p + 256) = -W^p), so a warp's
+    // 32 lanes (n2) read 32 consecutive entries, the mbarrier, and (warp 0)
+    // the tensor-memory allocation.
+    __device__ void init(int tid, int nthreads, const float2* __restrict__ tw)
     {
+        float2* t3 = reinterpret_cast<float2*>(smem + kOffTw3);
+        for (int i = tid; i < 16 * 32; i += nthreads) {
+            const int e = (i & 31) * (i >> 5);  // n2 * k1 < 512
+            float2 w = tw[e & 255];
+            if (e & 256) w = make_float2(-w.x, -w.y);
+            t3[i] = w;
+        }
         uint16_t* b1 = reinterpret_cast<uint16_t*>(smem + kOffB1);
         uint16_t* b3 = reinterpret_cast<uint16_t*>(smem + kOffB3);
         const double scale = static_cast<double>(1ll << kBExp);
@@ -357,11 +370,10 @@ struct Engine {
     }
 
     // In-place inverse DFT of sequences s < count (<= 8) of length 512 at
-    // data + s * seq_stride, element n at pad_idx(n). `tws` holds the FP32
-    // twiddles W^p, p < 256 (W = e^(2 pi i / 512)). All threads of the CTA
+    // data + s * seq_stride, element n at pad_idx(n). All threads of the CTA
     // call it (the first 256 do the work); data must be complete on entry,
     // and is complete on return.
-    __device__ void dft512(float2* data, int seq_stride, int count, const float2* tws, int tid, unsigned* error)
+    __device__ void dft512(float2* data, int seq_stride, int count, int tid, unsigned* error)
     {
         const int warp = tid >> 5, lane = tid & 31;
         const bool worker = tid < kThreads;
@@ -455,9 +467,7 @@ struct Engine {
             if (s_row < count) {
 #pragma unroll
                 for (int k1 = 0; k1 < 16; ++k1) {
-                    const int e = n2 * k1;  // < 512
-                    float2 w = tws[e & 255];
-                    if (e & 256) w = make_float2(-w.x, -w.y);
+                    const float2 w = tw3()[k1 * 32 + n2];
                     float* zrow = zbuf + (s_row * 16 + k1) * kZStride;
                     zrow[n2] = diff_of_products(y[k1], w.x, y[16 + k1], w.y);
                     zrow[32 + n2] = diff_of_products(y[k1], w.y, -y[16 + k1], w.x);
