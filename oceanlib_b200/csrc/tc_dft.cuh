@@ -167,6 +167,16 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, unsigned
         : "r"(taddr)                                                                                    \
         : "memory")
 
+#define OCEAN_TMEM_LD16(taddr, r)                                                                       \
+    asm volatile(                                                                                       \
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "                                                       \
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"                               \
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),          \
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),      \
+          "=r"(r[14]), "=r"(r[15])                                                                      \
+        : "r"(taddr)                                                                                    \
+        : "memory")
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // 2^e as a float, e clamped to the normal range.
@@ -537,36 +547,47 @@ struct Engine {
         bar_wait(bar(), 1u, error);
         fence_after_sync();
 
-        // ---- read X: warps 0-3 the real parts, warps 4-7 the imaginary ----
+        // ---- read X: row (s, k1) in lane quadrant warp & 3; warps 0-3 take
+        // k2 < 16, warps 4-7 k2 >= 16, each both parts (level L's real parts
+        // in columns 64 L + k2, imaginary ones 32 further), so every output
+        // is one float2 store and a half warp writes 128 contiguous bytes ----
         if (worker) {
-            const int part = warp >> 2;
-            const uint32_t col = tmem + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + part * 32;
+            const int half = warp >> 2;
+            const uint32_t col = tmem + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + half * 16;
             const int row = 32 * (warp & 3) + lane;  // (s, k1)
             const int e = e3()[row];
-            float x[32];
+            float xr[16], xi[16];
             {
-                uint32_t r0[32], r1[32];
-                OCEAN_TMEM_LD32(col, r0);
-                OCEAN_TMEM_LD32(col + 64, r1);
+                uint32_t r0[16], i0[16], r1[16], i1[16];
+                OCEAN_TMEM_LD16(col, r0);
+                OCEAN_TMEM_LD16(col + 32, i0);
+                OCEAN_TMEM_LD16(col + 64, r1);
+                OCEAN_TMEM_LD16(col + 96, i1);
                 tmem_wait_ld();
 #pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    x[j] = level_sum(r0[j], r1[j], e);
+                for (int j = 0; j < 16; ++j) {
+                    xr[j] = level_sum(r0[j], r1[j], e);
+                    xi[j] = level_sum(i0[j], i1[j], e);
+                }
             }
             {
-                uint32_t r2[32], r3[32];
-                OCEAN_TMEM_LD32(col + 128, r2);
-                OCEAN_TMEM_LD32(col + 192, r3);
+                uint32_t r2[16], i2[16], r3[16], i3[16];
+                OCEAN_TMEM_LD16(col + 128, r2);
+                OCEAN_TMEM_LD16(col + 160, i2);
+                OCEAN_TMEM_LD16(col + 192, r3);
+                OCEAN_TMEM_LD16(col + 224, i3);
                 tmem_wait_ld();
 #pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    x[j] = level_add(x[j], r2[j], r3[j], e);
+                for (int j = 0; j < 16; ++j) {
+                    xr[j] = level_add(xr[j], r2[j], r3[j], e);
+                    xi[j] = level_add(xi[j], i2[j], i3[j], e);
+                }
             }
             const int s = row >> 4, k1 = row & 15;
             if (s < count) {
-                float* seq = reinterpret_cast<float*>(data + s * seq_stride);
+                float2* seq = data + s * seq_stride;
 #pragma unroll
-                for (int k2 = 0; k2 < 32; ++k2) seq[2 * pad_idx(k1 + 16 * k2) + part] = x[k2];
+                for (int j = 0; j < 16; ++j) seq[pad_idx(k1 + 16 * (half * 16 + j))] = make_float2(xr[j], xi[j]);
             }
         }
         fence_before_sync();
