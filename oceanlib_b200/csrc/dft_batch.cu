@@ -42,11 +42,13 @@ dft_fp32_kernel(const float2* __restrict__ in, float2* __restrict__ out, int cou
     }
 }
 
-__global__ void __launch_bounds__(tc::kThreads)
+using BatchEngine = tc::Engine<8>;  // 8 sequences per engine call
+
+__global__ void __launch_bounds__(BatchEngine::Lay::kThreads)
 dft_tc512_kernel(const float2* __restrict__ in, float2* __restrict__ out, int count,
                  const float2* __restrict__ tw, unsigned* error)
 {
-    constexpr int N = 512, NT = tc::kThreads;
+    constexpr int N = 512, NT = BatchEngine::Lay::kThreads;
     constexpr int SEQ = padded_len(N) + kSeqPad;
     static_assert(SEQ * 2 >= 16 * tc::kZStride, "a sequence's space must hold its staged stage-3 rows");
     extern __shared__ float4 smem4[];
@@ -56,7 +58,7 @@ dft_tc512_kernel(const float2* __restrict__ in, float2* __restrict__ out, int co
                               ((8 * SEQ + N) * sizeof(float2) + 127) / 128 * 128;
     const int tid = threadIdx.x;
     for (int i = tid; i < N - 1; i += NT) tws[i] = tw[i];
-    tc::Engine eng{eng_smem, 0};
+    BatchEngine eng{eng_smem, 0};
     eng.init(tid, NT, tw);
     for (int base = blockIdx.x * 8; base < count; base += gridDim.x * 8) {
         const int k = min(8, count - base);
@@ -93,7 +95,7 @@ cudaError_t fp32_launch(bool fast, const float2* in, float2* out, int count, con
 size_t tc_dft_smem_bytes()
 {
     constexpr int N = 512;
-    return ((8 * (padded_len(N) + kSeqPad) + N) * sizeof(float2) + 127) / 128 * 128 + tc::kSmemBytes;
+    return ((8 * (padded_len(N) + kSeqPad) + N) * sizeof(float2) + 127) / 128 * 128 + BatchEngine::Lay::kSmemBytes;
 }
 
 cudaError_t launch_dft_batch(int log_n, int form, const float2* in, float2* out, int count, const float2* tw,
@@ -106,7 +108,7 @@ cudaError_t launch_dft_batch(int log_n, int form, const float2* in, float2* out,
         cudaError_t e = cudaFuncSetAttribute(dft_tc512_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              static_cast<int>(smem));
         if (e != cudaSuccess) return e;
-        dft_tc512_kernel<<<grid, tc::kThreads, smem, st>>>(in, out, count, tw, error);
+        dft_tc512_kernel<<<grid, BatchEngine::Lay::kThreads, smem, st>>>(in, out, count, tw, error);
         return cudaGetLastError();
     }
     const bool fast = form == 1;

@@ -122,6 +122,11 @@ __host__ __device__ constexpr int foam_window_f2()
     return (1 << LOG_N) * foam_window<W>() / 2;
 }
 
+// The tensor-core engine of a task's 2 NF sequences (one row pair or two
+// columns: 8 without velocity, 12 with): one engine call per transform.
+template <int NF>
+using TcEngine = tc::Engine<2 * NF>;
+
 // Fill the twiddle table at `tws` (layout of the form) from the FP32 table.
 template <int LOG_N, bool TC>
 __device__ __forceinline__ void load_twiddles(float2* tws, const float2* __restrict__ src, int tid, int nt)
@@ -140,17 +145,16 @@ __device__ __forceinline__ void load_twiddles(float2* tws, const float2* __restr
 // (one lane group of G2 per pair, named barrier 1 + pair where a pair spans
 // two warps), or with TC the tensor-core four-step DFT, 8 sequences per
 // engine call (N = 512; its twiddles live in the engine).
-template <int LOG_N, bool FAST, bool TC, int COUNT, int COLW = 0>
-__device__ __forceinline__ void transform_all(float2* data, const float2* tws, int tid, tc::Engine* eng,
+template <int LOG_N, bool FAST, bool TC, int COUNT, int COLW = 0, class Eng = tc::Engine<8>>
+__device__ __forceinline__ void transform_all(float2* data, const float2* tws, int tid, Eng* eng,
                                               unsigned* error)
 {
     using S = Shape<LOG_N>;
     if constexpr (TC) {
         static_assert(LOG_N == 9, "the tensor-core form is built for N = 512");
         static_assert(S::SEQ * 2 >= 16 * tc::kZStride, "a sequence's space must hold its staged stage-3 rows");
-#pragma unroll 1
-        for (int s0 = 0; s0 < COUNT; s0 += tc::kSeq)
-            eng->dft512(data + s0 * S::SEQ, S::SEQ, COUNT - s0 < tc::kSeq ? COUNT - s0 : tc::kSeq, tid, error);
+        static_assert(COUNT == Eng::Lay::kThreads / 32, "one engine call holds the task's sequences");
+        eng->dft512(data, S::SEQ, COUNT, tid, error);
     } else if constexpr (!paired<LOG_N, TC>()) {
         fft_sequence<LOG_N, S::G, FAST>(data + (tid / S::G) * S::SEQ, tws, tid % S::G);
     } else {
@@ -172,7 +176,7 @@ __device__ __forceinline__ void transform_all(float2* data, const float2* tws, i
 template <int LOG_N, int NF, bool FAST, bool TC = false>
 __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int group,
                                          float2* __restrict__ inter_slot, float2* smem,
-                                         const float2* tws, int tid, tc::Engine* eng = nullptr,
+                                         const float2* tws, int tid, TcEngine<NF>* eng = nullptr,
                                          unsigned* error = nullptr)
 {
     using S = Shape<LOG_N>;
@@ -416,7 +420,7 @@ __device__ __forceinline__ float foam_cell(const float* cur, int n, int x, int z
 template <int LOG_N, int NF, bool FAST, bool FOAM, int W, bool CG, bool TC = false>
 __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int strip,
                                          const float2* __restrict__ inter_slot, float2* smem,
-                                         const float2* tws, int tid, tc::Engine* eng = nullptr,
+                                         const float2* tws, int tid, TcEngine<NF>* eng = nullptr,
                                          unsigned* error = nullptr)
 {
     using S = Shape<LOG_N>;
@@ -724,9 +728,9 @@ frame_kernel(FrameArgs a, QueueArgs q)
 
     const int tid = threadIdx.x;
     if constexpr (!TC) load_twiddles<LOG_N, TC>(tws, a.twiddles, tid, NT);
-    tc::Engine eng{reinterpret_cast<unsigned char*>(smem4) + frame_engine_offset<LOG_N, NF>(), 0};
+    TcEngine<NF> eng{reinterpret_cast<unsigned char*>(smem4) + frame_engine_offset<LOG_N, NF>(), 0};
     if constexpr (TC) {
-        static_assert(NT >= tc::kThreads, "the tensor-core engine needs 8 warps");
+        static_assert(NT == TcEngine<NF>::Lay::kThreads, "the engine works with the task's threads");
         eng.init(tid, NT, a.twiddles);
     }
 
@@ -955,7 +959,7 @@ template <int LOG_N, int NF, bool TC = false>
 constexpr size_t frame_smem_bytes()
 {
     using S = Shape<LOG_N>;
-    if (TC) return frame_engine_offset<LOG_N, NF>() + tc::kSmemBytes;
+    if (TC) return frame_engine_offset<LOG_N, NF>() + TcEngine<NF>::Lay::kSmemBytes;
     return sizeof(float2) * (frame_data_float2<LOG_N, NF, false>() + twiddle_f2<LOG_N, false>());
 }
 
@@ -978,7 +982,7 @@ struct FrameLaunch {
                                                           frame_smem_bytes<LOG_N, NF, TC>()) != cudaSuccess)
             return 0;
         // The tensor-core engine's tensor memory bounds its residency.
-        if (TC && n * tc::kTmemCols > 512) n = 512 / tc::kTmemCols;
+        if (TC && n * TcEngine<NF>::Lay::kTmemCols > 512) n = 512 / TcEngine<NF>::Lay::kTmemCols;
         return n;
     }
 
@@ -992,7 +996,7 @@ struct FrameLaunch {
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<LOG_N, NF, FAST, FOAM, TC>,
                                                               threads(), frame_smem_bytes<LOG_N, NF, TC>());
             if (e != cudaSuccess) return e;
-            if (n * tc::kTmemCols > 512) return cudaErrorInvalidConfiguration;
+            if (n * TcEngine<NF>::Lay::kTmemCols > 512) return cudaErrorInvalidConfiguration;
         }
         frame_kernel<LOG_N, NF, FAST, FOAM, TC><<<grid, threads(), frame_smem_bytes<LOG_N, NF, TC>(), st>>>(a, q);
         return cudaGetLastError();

@@ -45,35 +45,49 @@
 namespace ocean_b200 {
 namespace tc {
 
-constexpr int kSeq = 8;          // sequences per engine call
-constexpr int kRows1 = 256;      // stage 1 rows: 8 x 32
 constexpr int kK1 = 32;          // stage 1 K (16 complex)
 constexpr int kN1 = 32;          // stage 1 N (16 complex)
-constexpr int kRows3 = 128;      // stage 3 rows: 8 x 16
 constexpr int kK3 = 64;          // stage 3 K (32 complex)
 constexpr int kN3 = 64;          // stage 3 N (32 complex)
 constexpr int kDigits = 4;       // signed 8-bit digits per value
 constexpr int kLevels = 4;       // digit-pair levels kept (i + j < 4)
-// Accumulators (FP32 columns), one per level: stage 1 tile t, level L at
-// 128 t + 32 L; stage 3 level L at 64 L. All 256 columns.
-constexpr int kTmemCols = 256;
-constexpr int kThreads = 256;    // the engine's working threads (8 warps)
 constexpr int kZStride = 68;     // floats per staged stage-3 row (64 + 4 against bank conflicts)
 constexpr int kFixExp = 29;      // row max scaled into [2^29, 2^30)
 constexpr int kBExp = 30;        // DFT matrices scaled by 2^30
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
 
-// Shared-memory layout of the engine (bytes, all 128-byte aligned).
-constexpr int kAHalves = kRows1 * kK1;  // == kRows3 * kK3 = 8192 halves per digit
-static_assert(kRows1 * kK1 == kRows3 * kK3, "stage operands share one buffer");
-constexpr int kOffA = 0;                                       // [digit][8192]
-constexpr int kOffB1 = kOffA + kDigits * kAHalves * 2;          // [digit][32*32]
-constexpr int kOffB3 = kOffB1 + kDigits * kN1 * kK1 * 2;        // [digit][64*64]
-constexpr int kOffE3 = kOffB3 + kDigits * kN3 * kK3 * 2;        // int[kRows3]
-constexpr int kOffTw3 = kOffE3 + kRows3 * 4;                    // float2[16][32]: W^(n2 k1)
-constexpr int kOffBar = kOffTw3 + 16 * 32 * 8;                  // uint64 mbarrier
-constexpr int kOffTmem = kOffBar + 8;                           // uint32 tmem base
-constexpr int kSmemBytes = kOffTmem + 8;
+// An engine call transforms SEQS sequences (8, or 12: a frame task's 2 rows
+// x 6 fields) with SEQS x 32 threads. Stage 1 has SEQS x 32 rows (SEQS / 4
+// tiles of M = 128); stage 3 has SEQS x 16 rows, one tile or two, the second
+// holding rows 128..191 (its MMA also reads the 64 rows behind them, which
+// lie inside the engine's shared memory and land in tensor-memory lanes that
+// are never read). Accumulators (FP32 columns), one per level: stage 1 tile
+// t, level L at 128 t + 32 L; stage 3 tile t, level L at 256 t + 64 L.
+// Shared-memory layout in bytes, all offsets 128-byte aligned.
+template <int SEQS>
+struct Layout {
+    static_assert(SEQS == 8 || SEQS == 12, "8 or 12 sequences per engine call");
+    static constexpr int kRows1 = SEQS * 32;
+    static constexpr int kTiles1 = kRows1 / 128;
+    static constexpr int kRows3 = SEQS * 16;
+    static constexpr int kTiles3 = (kRows3 + 127) / 128;
+    static constexpr int kThreads = SEQS * 32;
+    static constexpr int kTmemCols = kTiles3 > 1 ? 512 : 256;
+    static constexpr int kAHalves = kRows1 * kK1;  // halves per digit plane (== kRows3 * kK3)
+    static_assert(kRows1 * kK1 == kRows3 * kK3, "stage operands share one buffer");
+    static constexpr int kOffA = 0;                                 // [digit][kAHalves]
+    static constexpr int kOffB1 = kOffA + kDigits * kAHalves * 2;    // [digit][32*32]
+    static constexpr int kOffB3 = kOffB1 + kDigits * kN1 * kK1 * 2;  // [digit][64*64]
+    static constexpr int kOffE3 = kOffB3 + kDigits * kN3 * kK3 * 2;  // int[kRows3]
+    static constexpr int kOffTw3 = kOffE3 + kRows3 * 4;              // float2[16][32]: W^(n2 k1)
+    static constexpr int kOffBar = kOffTw3 + 16 * 32 * 8;            // uint64 mbarrier
+    static constexpr int kOffTmem = kOffBar + 8;                     // uint32 tmem base
+    static constexpr int kSmemBytes = kOffTmem + 8;
+    // The second stage-3 tile's MMA reads rows 128..255 of each digit plane;
+    // for the last plane those end inside B1.
+    static_assert(kTiles3 == 1 || kOffA + (kDigits - 1) * kAHalves * 2 + 256 * kK3 * 2 <= kOffB3,
+                  "stage-3 tile reads stay inside the engine's shared memory");
+};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -277,18 +291,20 @@ __device__ __forceinline__ float level_add(float acc, uint32_t l2, uint32_t l3, 
     return __fmaf_rn(__uint_as_float(l3), pow2f(-6 - e), __fmaf_rn(__uint_as_float(l2), pow2f(2 - e), acc));
 }
 
+template <int SEQS>
 struct Engine {
-    unsigned char* smem;  // kSmemBytes, 128-byte aligned
+    using Lay = Layout<SEQS>;
+    unsigned char* smem;  // Lay::kSmemBytes, 128-byte aligned
     uint32_t tmem;        // tensor-memory base (lane 0, column 0)
 
     __device__ uint16_t* a(int digit) const
     {
-        return reinterpret_cast<uint16_t*>(smem + kOffA) + digit * kAHalves;
+        return reinterpret_cast<uint16_t*>(smem + Lay::kOffA) + digit * Lay::kAHalves;
     }
-    __device__ int* e3() const { return reinterpret_cast<int*>(smem + kOffE3); }
-    __device__ uint32_t bar() const { return smem_u32(smem + kOffBar); }
+    __device__ int* e3() const { return reinterpret_cast<int*>(smem + Lay::kOffE3); }
+    __device__ uint32_t bar() const { return smem_u32(smem + Lay::kOffBar); }
 
-    __device__ const float2* tw3() const { return reinterpret_cast<const float2*>(smem + kOffTw3); }
+    __device__ const float2* tw3() const { return reinterpret_cast<const float2*>(smem + Lay::kOffTw3); }
 
     // Once per kernel, all threads: the DFT matrices' digits, the twiddles
     // of the middle step as [k1][n2] = W^(n2 k1) from the FP32 table `tw`
@@ -297,15 +313,15 @@ struct Engine {
     // the tensor-memory allocation.
     __device__ void init(int tid, int nthreads, const float2* __restrict__ tw)
     {
-        float2* t3 = reinterpret_cast<float2*>(smem + kOffTw3);
+        float2* t3 = reinterpret_cast<float2*>(smem + Lay::kOffTw3);
         for (int i = tid; i < 16 * 32; i += nthreads) {
             const int e = (i & 31) * (i >> 5);  // n2 * k1 < 512
             float2 w = tw[e & 255];
             if (e & 256) w = make_float2(-w.x, -w.y);
             t3[i] = w;
         }
-        uint16_t* b1 = reinterpret_cast<uint16_t*>(smem + kOffB1);
-        uint16_t* b3 = reinterpret_cast<uint16_t*>(smem + kOffB3);
+        uint16_t* b1 = reinterpret_cast<uint16_t*>(smem + Lay::kOffB1);
+        uint16_t* b3 = reinterpret_cast<uint16_t*>(smem + Lay::kOffB3);
         const double scale = static_cast<double>(1ll << kBExp);
         // B1[j][k]: j = (q, k1) output, k = (p, n1) input, angle 2 pi n1 k1 / 16
         for (int i = tid; i < kN1 * kK1; i += nthreads) {
@@ -334,9 +350,9 @@ struct Engine {
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
         if (tid < 32) {
-            const uint32_t slot = smem_u32(smem + kOffTmem);
+            const uint32_t slot = smem_u32(smem + Lay::kOffTmem);
             asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
-                         "r"(kTmemCols)
+                         "r"(Lay::kTmemCols)
                          : "memory");
             asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
         }
@@ -344,7 +360,7 @@ struct Engine {
         fence_before_sync();
         __syncthreads();
         fence_after_sync();
-        tmem = *reinterpret_cast<volatile uint32_t*>(smem + kOffTmem);
+        tmem = *reinterpret_cast<volatile uint32_t*>(smem + Lay::kOffTmem);
     }
 
     // Once per kernel, all threads, after the last engine call.
@@ -354,7 +370,7 @@ struct Engine {
         __syncthreads();
         fence_after_sync();
         if (tid < 32)
-            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Lay::kTmemCols)
                          : "memory");
     }
 
@@ -379,17 +395,19 @@ struct Engine {
         }
     }
 
-    // In-place inverse DFT of sequences s < count (<= 8) of length 512 at
+    // In-place inverse DFT of sequences s < count (<= SEQS) of length 512 at
     // data + s * seq_stride, element n at pad_idx(n). All threads of the CTA
-    // call it (the first 256 do the work); data must be complete on entry,
-    // and is complete on return.
+    // call it (the first SEQS x 32 do the work); data must be complete on
+    // entry, and is complete on return.
     __device__ void dft512(float2* data, int seq_stride, int count, int tid, unsigned* error)
     {
         const int warp = tid >> 5, lane = tid & 31;
-        const bool worker = tid < kThreads;
+        const bool worker = tid < Lay::kThreads;
         uint16_t* a0p = a(0);
-        // Stage-1 tile 1 holds sequences 4..7: skipped when there are none.
-        const int tiles1 = count > 4 ? 2 : 1;
+        // Stage-1 tile t holds sequences 4t..4t+3, stage-3 tile t sequences
+        // 8t..8t+7: tiles without sequences are skipped.
+        const int tiles1 = (count + 3) / 4;
+        const int tiles3 = (count + 7) / 8;
 
         // ---- stage 1 operand: row r = (s, n2), 16 complex x[32 n1 + n2] ----
         int e1 = 0;
@@ -420,7 +438,7 @@ struct Engine {
                 const int off = kmajor(tid, 8 * c, kK1);
 #pragma unroll
                 for (int g = 0; g < kDigits; ++g)
-                    *reinterpret_cast<uint4*>(a0p + g * kAHalves + off) =
+                    *reinterpret_cast<uint4*>(a0p + g * Lay::kAHalves + off) =
                         make_uint4(half2_bits(d[0][g], d[1][g]), half2_bits(d[2][g], d[3][g]),
                                    half2_bits(d[4][g], d[5][g]), half2_bits(d[6][g], d[7][g]));
             }
@@ -432,14 +450,14 @@ struct Engine {
 
         // ---- stage 1 MMAs: tiles1 tiles x 2 K steps x 10 digit pairs ----
         if (tid == 0) {
-            const uint32_t abase = smem_u32(a0p), bbase = smem_u32(smem + kOffB1);
+            const uint32_t abase = smem_u32(a0p), bbase = smem_u32(smem + Lay::kOffB1);
             constexpr uint32_t sbo = kK1 * 16;
             constexpr uint32_t idesc = instr_desc(128, kN1);
 #pragma unroll 1
             for (int t = 0; t < tiles1; ++t)
 #pragma unroll 1
                 for (int ks = 0; ks < kK1 / 16; ++ks)
-                    issue_levels(tmem + t * 128, kN1, abase, bbase, kAHalves * 2, kN1 * kK1 * 2, ks * 256,
+                    issue_levels(tmem + t * 128, kN1, abase, bbase, Lay::kAHalves * 2, kN1 * kK1 * 2, ks * 256,
                                  t * 16 * sbo, sbo, sbo, idesc, ks == 0);
             mma_commit(bar());
         }
@@ -522,7 +540,7 @@ struct Engine {
                 const int off = kmajor(row, half_k * 32 + 8 * c, kK3);
 #pragma unroll
                 for (int g = 0; g < kDigits; ++g)
-                    *reinterpret_cast<uint4*>(a0p + g * kAHalves + off) =
+                    *reinterpret_cast<uint4*>(a0p + g * Lay::kAHalves + off) =
                         make_uint4(half2_bits(d[0][g], d[1][g]), half2_bits(d[2][g], d[3][g]),
                                    half2_bits(d[4][g], d[5][g]), half2_bits(d[6][g], d[7][g]));
             }
@@ -533,61 +551,74 @@ struct Engine {
         __syncthreads();
         fence_after_sync();
 
-        // ---- stage 3 MMAs: 1 tile x 4 K steps x 10 digit pairs ----
+        // ---- stage 3 MMAs: tiles3 tiles x 4 K steps x 10 digit pairs ----
         if (tid == 0) {
-            const uint32_t abase = smem_u32(a0p), bbase = smem_u32(smem + kOffB3);
+            const uint32_t abase = smem_u32(a0p), bbase = smem_u32(smem + Lay::kOffB3);
             constexpr uint32_t sbo = kK3 * 16;
             constexpr uint32_t idesc = instr_desc(128, kN3);
 #pragma unroll 1
-            for (int ks = 0; ks < kK3 / 16; ++ks)
-                issue_levels(tmem, kN3, abase, bbase, kAHalves * 2, kN3 * kK3 * 2, ks * 256, 0u, sbo, sbo, idesc,
-                             ks == 0);
+            for (int t = 0; t < tiles3; ++t)
+#pragma unroll 1
+                for (int ks = 0; ks < kK3 / 16; ++ks)
+                    issue_levels(tmem + t * 256, kN3, abase, bbase, Lay::kAHalves * 2, kN3 * kK3 * 2, ks * 256,
+                                 t * 16 * sbo, sbo, sbo, idesc, ks == 0);
             mma_commit(bar());
         }
         bar_wait(bar(), 1u, error);
         fence_after_sync();
 
-        // ---- read X: row (s, k1) in lane quadrant warp & 3; warps 0-3 take
-        // k2 < 16, warps 4-7 k2 >= 16, each both parts (level L's real parts
-        // in columns 64 L + k2, imaginary ones 32 further), so every output
-        // is one float2 store and a half warp writes 128 contiguous bytes ----
+        // ---- read X: row (s, k1) of stage-3 tile t in lane quadrant (row &
+        // 127) / 32, where warp w may read quadrant w & 3. Tile 0: warps 0-3
+        // take k2 < 16 and warps 4-7 k2 >= 16; tile 1 (rows 128..191, lanes
+        // 0..63): warps 8 and 9, both halves. Each reads both parts (level
+        // L's real parts in columns 256 t + 64 L + k2, imaginary ones 32
+        // further), so every output is one float2 store and a half warp
+        // writes 128 contiguous bytes ----
         if (worker) {
-            const int half = warp >> 2;
-            const uint32_t col = tmem + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + half * 16;
-            const int row = 32 * (warp & 3) + lane;  // (s, k1)
-            const int e = e3()[row];
-            float xr[16], xi[16];
-            {
-                uint32_t r0[16], i0[16], r1[16], i1[16];
-                OCEAN_TMEM_LD16(col, r0);
-                OCEAN_TMEM_LD16(col + 32, i0);
-                OCEAN_TMEM_LD16(col + 64, r1);
-                OCEAN_TMEM_LD16(col + 96, i1);
-                tmem_wait_ld();
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    xr[j] = level_sum(r0[j], r1[j], e);
-                    xi[j] = level_sum(i0[j], i1[j], e);
-                }
-            }
-            {
-                uint32_t r2[16], i2[16], r3[16], i3[16];
-                OCEAN_TMEM_LD16(col + 128, r2);
-                OCEAN_TMEM_LD16(col + 160, i2);
-                OCEAN_TMEM_LD16(col + 192, r3);
-                OCEAN_TMEM_LD16(col + 224, i3);
-                tmem_wait_ld();
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    xr[j] = level_add(xr[j], r2[j], r3[j], e);
-                    xi[j] = level_add(xi[j], i2[j], i3[j], e);
-                }
-            }
-            const int s = row >> 4, k1 = row & 15;
-            if (s < count) {
+            const bool second = warp >= 8;
+            const int t = second ? 1 : 0;
+            if (!second || (t < tiles3 && warp < 10)) {
+                const int row = 128 * t + 32 * (warp & 3) + lane;  // (s, k1)
+                const int e = e3()[row];
+                const int s = row >> 4, k1 = row & 15;
                 float2* seq = data + s * seq_stride;
+                const int h0 = second ? 0 : (warp >> 2), h1 = second ? 2 : h0 + 1;
+#pragma unroll 1
+                for (int half = h0; half < h1; ++half) {
+                    const uint32_t col = tmem + (static_cast<uint32_t>(32 * (warp & 3)) << 16) + 256 * t + half * 16;
+                    float xr[16], xi[16];
+                    {
+                        uint32_t r0[16], i0[16], r1[16], i1[16];
+                        OCEAN_TMEM_LD16(col, r0);
+                        OCEAN_TMEM_LD16(col + 32, i0);
+                        OCEAN_TMEM_LD16(col + 64, r1);
+                        OCEAN_TMEM_LD16(col + 96, i1);
+                        tmem_wait_ld();
 #pragma unroll
-                for (int j = 0; j < 16; ++j) seq[pad_idx(k1 + 16 * (half * 16 + j))] = make_float2(xr[j], xi[j]);
+                        for (int j = 0; j < 16; ++j) {
+                            xr[j] = level_sum(r0[j], r1[j], e);
+                            xi[j] = level_sum(i0[j], i1[j], e);
+                        }
+                    }
+                    {
+                        uint32_t r2[16], i2[16], r3[16], i3[16];
+                        OCEAN_TMEM_LD16(col + 128, r2);
+                        OCEAN_TMEM_LD16(col + 160, i2);
+                        OCEAN_TMEM_LD16(col + 192, r3);
+                        OCEAN_TMEM_LD16(col + 224, i3);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            xr[j] = level_add(xr[j], r2[j], r3[j], e);
+                            xi[j] = level_add(xi[j], i2[j], i3[j], e);
+                        }
+                    }
+                    if (s < count) {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                            seq[pad_idx(k1 + 16 * (half * 16 + j))] = make_float2(xr[j], xi[j]);
+                    }
+                }
             }
         }
         fence_before_sync();
