@@ -226,11 +226,6 @@ __device__ __forceinline__ void digits4(int v, uint16_t (&d)[4])
     d[3] = __half_as_ushort(__int2half_rn(d3));
 }
 
-__device__ __forceinline__ uint32_t pack2(uint16_t a, uint16_t b)
-{
-    return static_cast<uint32_t>(a) | (static_cast<uint32_t>(b) << 16);
-}
-
 // The operand form of digits4: signed digits of x, |x| < 2^30, as floats,
 // x rounded to the nearest integer = t0 2^24 + t1 2^16 + t2 2^8 + t3 with
 // |t_i| <= 128 (so every digit product is at most 2^14 and a level of 256
