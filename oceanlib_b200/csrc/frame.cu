@@ -20,6 +20,7 @@
 // Pairing rows y and N-y means h0(-k) - the conjugate-mirror table the
 // reference stores separately (src/core/spectrum.cpp:329-338) - is read from
 // the other row already in shared memory, so h0 is read from HBM once.
+#include "frame_cells.cuh"
 #include "ocean_device.cuh"
 #include "query_device.cuh"
 #include "spectrum.h"
@@ -253,62 +254,17 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         const int mr = (p == 0) ? r : 1 - r;  // row holding h0 at -kz
         const float2 av = h0s[jr * N + x];
         const float2 bm = h0s[(j * 2 + mr) * N + ((N - x) & (N - 1))];
-        const float b_re = bm.x, b_im = -bm.y;
-        const float2 wk = wk_of[it];
-
-        float s, c;
-        sincos_poly(fold_phase(wk.x, top), s, c);
-        const float fwd_re = av.x * c - av.y * s;
-        const float fwd_im = av.x * s + av.y * c;
-        const float bwd_re = b_re * c + b_im * s;
-        const float bwd_im = b_im * c - b_re * s;
-        const float hr = fwd_re + bwd_re;
-        const float hi = fwd_im + bwd_im;
-        const float kx = kx_of[it];
-        const float kz = kz_of[it];
-        const float ki = wk.y;
-        const float sx = kx * ki;
-        const float sz = kz * ki;
-        const float dx_re = sx * hi, dx_im = -sx * hr;
-        const float dz_re = sz * hi, dz_im = -sz * hr;
-        const float hx_re = -kx * hi, hx_im = kx * hr;
-        const float hz_re = -kz * hi, hz_im = kz * hr;
-        const float jxx = kx * sx, jzz = kz * sz, jxz = kx * sz;
-        const float jxx_re = jxx * hr, jxx_im = jxx * hi;
-        const float jzz_re = jzz * hr, jzz_im = jzz * hi;
-        const float jxz_re = jxz * hr, jxz_im = jxz * hi;
-
-        const float2 p0 = make_float2(hr - dx_im, hi + dx_re);
-        const float2 p1 = make_float2(dz_re - hx_im, dz_im + hx_re);
-        const float2 p2 = make_float2(hz_re - jxx_im, hz_im + jxx_re);
-        const float2 p3 = make_float2(jzz_re - jxz_im, jzz_im + jxz_re);
-        float2 p4 = make_float2(0.0f, 0.0f), p5 = p4;
-        if constexpr (NF == 6) {
-            const float dr = fwd_re - bwd_re;
-            const float di = fwd_im - bwd_im;
-            const float w = wk.x;
-            const float wsx = w * sx, wsz = w * sz;
-            const float ux_re = -wsx * dr, ux_im = -wsx * di;
-            const float uz_re = -wsz * dr, uz_im = -wsz * di;
-            const float uy_re = -w * di, uy_im = w * dr;
-            p4 = make_float2(ux_re - uy_im, ux_im + uy_re);
-            p5 = make_float2(uz_re, uz_im);
-        }
+        float2 pv[NF];
+        evolve_cell<NF>(av, bm, wk_of[it], kx_of[it], kz_of[it], top, pv);
         if constexpr (!PAIRED) {
             float2* base = data + (jr * NF) * SEQ + pad_idx(x);
-            base[0 * SEQ] = p0;
-            base[1 * SEQ] = p1;
-            base[2 * SEQ] = p2;
-            base[3 * SEQ] = p3;
-            if constexpr (NF == 6) {
-                base[4 * SEQ] = p4;
-                base[5 * SEQ] = p5;
-            }
+#pragma unroll
+            for (int f = 0; f < NF; ++f) base[f * SEQ] = pv[f];
         } else {
             float4* base = data4 + (jr * Q) * SEQ4 + pad4(x);
-            base[0] = make_float4(p0.x, p1.x, p0.y, p1.y);
-            base[SEQ4] = make_float4(p2.x, p3.x, p2.y, p3.y);
-            if constexpr (NF == 6) base[2 * SEQ4] = make_float4(p4.x, p5.x, p4.y, p5.y);
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+                base[q * SEQ4] = make_float4(pv[2 * q].x, pv[2 * q + 1].x, pv[2 * q].y, pv[2 * q + 1].y);
         }
     }
     __syncthreads();
@@ -338,78 +294,6 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         }
         inter[(static_cast<size_t>(row) * N + x) * Q + fp] = o;
     }
-}
-
-// ---------------------------------------------------------------------------
-// Column task helpers
-// ---------------------------------------------------------------------------
-
-// Periodic bilinear fetch from one channel grid (src/foam.cpp:22-41): the
-// four taps come from `get(z, x)`, so a caller can serve them from a staged
-// shared-memory window or from global memory with the same arithmetic.
-struct FoamTaps {
-    float fa, fb, fc, fd, tu, tv;
-};
-
-template <typename Get>
-__device__ __forceinline__ FoamTaps foam_fetch(float u, float v, int n, Get&& get)
-{
-    FoamTaps t;
-    const float fu = floorf(u), fv = floorf(v);
-    t.tu = u - fu;
-    t.tv = v - fv;
-    int x0 = __float2int_rz(fu) % n;
-    if (x0 < 0) x0 += n;
-    int z0 = __float2int_rz(fv) % n;
-    if (z0 < 0) z0 += n;
-    const int x1 = (x0 + 1) % n;
-    const int z1 = (z0 + 1) % n;
-    t.fa = get(z0, x0);
-    t.fb = get(z0, x1);
-    t.fc = get(z1, x0);
-    t.fd = get(z1, x1);
-    return t;
-}
-
-__device__ __forceinline__ float foam_blend(const FoamTaps& t)
-{
-    const float tu = t.tu, tv = t.tv;
-    return t.fa * (1.0f - tu) * (1.0f - tv) + t.fb * tu * (1.0f - tv) + t.fc * (1.0f - tu) * tv +
-           t.fd * tu * tv;
-}
-
-// The backtraced sample point of cell (x, z) and the taps there
-// (src/foam.cpp:89-139, first half).
-template <typename Get>
-__device__ __forceinline__ FoamTaps foam_taps(int n, int x, int z, float velx, float velz, float dt, float scale,
-                                              float drift_x, float drift_z, float inv_cell, Get&& get)
-{
-    const float vx = velx * scale + drift_x;
-    const float vz = velz * scale + drift_z;
-    const float su = static_cast<float>(x) - vx * dt * inv_cell;
-    const float sv = static_cast<float>(z) - vz * dt * inv_cell;
-    return foam_fetch(su, sv, n, get);
-}
-
-// Decay, source and clamp of the sampled foam (second half).
-__device__ __forceinline__ float foam_finish(const FoamTaps& t, float src, float decay, float gain)
-{
-    float f = foam_blend(t);
-    f = f * decay + src * gain;
-    if (f > 1.0f) f = 1.0f;
-    if (f < 0.0f) f = 0.0f;
-    return f;
-}
-
-// One persistent-foam substep for cell (x, z) (src/foam.cpp:89-139).
-__device__ __forceinline__ float foam_cell(const float* cur, int n, int x, int z, float velx,
-                                           float velz, float src, float dt, float decay,
-                                           float gain, float scale, float drift_x,
-                                           float drift_z, float inv_cell)
-{
-    auto get = [&](int zz, int xx) { return cur[static_cast<size_t>(zz) * n + xx]; };
-    return foam_finish(foam_taps(n, x, z, velx, velz, dt, scale, drift_x, drift_z, inv_cell, get), src, decay,
-                       gain);
 }
 
 // ---------------------------------------------------------------------------
@@ -545,36 +429,16 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
                 f5 = make_float2(q2.y, q2.w);
             }
         }
-        const float h = f0.x, d_x = f0.y, d_z = f1.x, hx = f1.y;
-        const float hz = f2.x, jxx = f2.y, jzz = f3.x, jxz = f3.y;
-
-        const float disp_x = lambda * d_x;
-        const float disp_z = lambda * d_z;
-        const float axx = 1.0f + lambda * jxx;
-        const float azz = 1.0f + lambda * jzz;
-        const float axz = lambda * jxz;
-        const float jac = axx * azz - axz * axz;
-        float nx = -(hx * azz - axz * hz);
-        float ny = jac;
-        float nz = -(axx * hz - hx * axz);
-        const float len2 = nx * nx + ny * ny + nz * nz;
-        const float inv_len = (len2 > 0.0f) ? 1.0f / sqrtf(len2) : 0.0f;
-        nx *= inv_len;
-        ny *= inv_len;
-        nz *= inv_len;
-        float foam = (cst.foam_threshold - jac) * cst.inv_threshold;
-        if (foam < 0.0f) foam = 0.0f;
-        if (foam > 1.0f) foam = 1.0f;
-
+        const CellOut c = finalize_cell(f0, f1, f2, f3, lambda, cst.foam_threshold, cst.inv_threshold);
         const size_t idx = static_cast<size_t>(y) * N + x;
-        __stcs(&out_disp[idx], make_float4(disp_x, h, disp_z, foam));
-        __stcs(&out_normal[idx], make_float4(nx, ny, nz, jac));
+        __stcs(&out_disp[idx], c.disp);
+        __stcs(&out_normal[idx], c.normal);
         if constexpr (NF == 6) {
             __stcs(&out_vel[idx], make_float4(f4.x, f4.y, f5.x, 0.0f));
             if constexpr (FSTEP) {
                 const FoamTaps t = foam_taps(N, x, y, f4.x, f5.x, a.foam_dt, a.foam_scale, a.foam_drift_x,
                                              a.foam_drift_z, a.foam_inv_cell, foam_get);
-                __stcs(&a.foam_next[base + idx], foam_finish(t, foam, a.foam_decay, a.foam_gain));
+                __stcs(&a.foam_next[base + idx], foam_finish(t, c.disp.w, a.foam_decay, a.foam_gain));
             }
         }
     }

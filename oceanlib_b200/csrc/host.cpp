@@ -77,14 +77,11 @@ bool copy_desc(const ocean_desc* src, ocean_desc& dst)
     return true;
 }
 
-constexpr uint32_t kMaxSize = 1024;  // largest N the frame kernels are built for
-
 void validate(const ocean_desc& d)
 {
     const uint32_t n = d.size;
     const bool pow2 = n != 0 && (n & (n - 1)) == 0;
     if (!pow2 || n < 16 || n > 4096) throw std::invalid_argument("size");
-    if (n > kMaxSize) throw std::invalid_argument("size above the built kernel range");
     if (!(d.patch_length > 0.0f)) throw std::invalid_argument("patch_length");
     if (!(d.spectrum.gravity > 0.0f)) throw std::invalid_argument("gravity");
     if (!(d.spectrum.fetch > 0.0f)) throw std::invalid_argument("fetch");
@@ -198,6 +195,7 @@ public:
             if (!velocity_) throw std::invalid_argument("foam needs compute_velocity");
         }
         form_ = form;
+        if (n_ > kMaxPersistentSize) persistent_ = false;
         // The tensor-core DFT is built for N = 512 and runs in the persistent kernel.
         if (form_ == OCEAN_FFT_TENSOR && (n_ != 512 || !persistent_))
             throw std::invalid_argument("the tensor-core form needs N = 512 and the persistent schedule");
@@ -249,7 +247,11 @@ public:
         top_ = DevBuf<double>(count_ * kTimeSlots);
         top_host_ = HostBuf<double>(count_ * kTimeSlots);
         slots_ = static_cast<int>(std::min<uint32_t>(count_, 3));
-        inter_ = DevBuf<float2>(cells_ * nf_ * std::max<uint32_t>(chunk_, static_cast<uint32_t>(slots_)));
+        // The persistent kernel's ring needs `slots_` oceans; the row/column
+        // passes one per chunk ocean (all a batch above N = 1024 ever uses).
+        const uint32_t inter_oceans =
+            large() ? chunk_ : std::max<uint32_t>(chunk_, static_cast<uint32_t>(slots_));
+        inter_ = DevBuf<float2>(cells_ * nf_ * inter_oceans);
         queue_ = DevBuf<unsigned>(1 + 2 * size_t(count_));
         error_ = DevBuf<unsigned>(1);
         check(cudaMemsetAsync(error_.p, 0, sizeof(unsigned), stream_), "memset");
@@ -560,7 +562,7 @@ public:
     // launches with (1 = the whole GPU).
     void set_grid_share(double s) { grid_share_ = std::min(1.0, std::max(1e-3, s)); }
     double grid_share() const { return grid_share_; }
-    void set_persistent(bool p) { persistent_ = p; }
+    void set_persistent(bool p) { persistent_ = p && !large(); }
     bool persistent() const { return persistent_; }
 
 private:
@@ -595,9 +597,17 @@ private:
         prof_used_ = 0;
     }
 
+    // Sizes above the persistent kernel's range (N = 2048, 4096).
+    bool large() const { return n_ > kMaxPersistentSize; }
+
     void run_row(const FrameArgs& a, cudaStream_t st)
     {
-        timed(0, st, [&] { check(launch_row_pass(log_n_, nf_, form_ == OCEAN_FFT_FAST, a, st), "row pass"); });
+        const bool fast = form_ == OCEAN_FFT_FAST;
+        if (large()) {
+            timed(0, st, [&] { check(launch_large_rows(log_n_, nf_, fast, a, st), "row pass"); });
+            return;
+        }
+        timed(0, st, [&] { check(launch_row_pass(log_n_, nf_, fast, a, st), "row pass"); });
     }
 
     // One persistent launch for oceans [base, base + k) (csrc/frame.cu
@@ -628,9 +638,13 @@ private:
 
     void run_col(const FrameArgs& a, cudaStream_t st, bool foam)
     {
-        timed(1, st, [&] {
-            check(launch_col_pass(log_n_, nf_, form_ == OCEAN_FFT_FAST, foam, a, st), "column pass");
-        });
+        const bool fast = form_ == OCEAN_FFT_FAST;
+        if (large()) {
+            timed(1, st, [&] { check(launch_large_cols(log_n_, nf_, fast, a, st), "column pass"); });
+            timed(1, st, [&] { check(launch_large_finalize(log_n_, nf_, foam, a, st), "finalize"); });
+            return;
+        }
+        timed(1, st, [&] { check(launch_col_pass(log_n_, nf_, fast, foam, a, st), "column pass"); });
     }
     static constexpr double kInvTwoPi = 0.159154943091895335769;
 
@@ -652,7 +666,10 @@ public:
     // t / 2 pi as every frame hoists it (src/core/evolve.cpp:33).
     static double time_over_2pi(double t) { return t * kInvTwoPi; }
     // Settles the launch shapes, so a capture issues launches only.
-    void prime_shapes() { (void)frame_grid(false); }
+    void prime_shapes()
+    {
+        if (persistent_) (void)frame_grid(false);
+    }
 
 private:
 

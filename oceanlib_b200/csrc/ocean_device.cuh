@@ -97,7 +97,9 @@ __device__ __forceinline__ void butterfly(float2& a, float2& b, float2 w)
 // ---------------------------------------------------------------------------
 // One block of r consecutive radix-2 Stockham stages, L0 .. L0+r-1, on a
 // sequence of N = 2^LOG_N points held (swizzled) in shared memory and worked
-// on by a group of G lanes.
+// on by a group of G lanes. A group of one warp or less synchronises with
+// __syncwarp; a sequence spanning several warps (G > 32) uses the CTA
+// barrier, so every thread of the CTA must run the same transforms.
 //
 // Index algebra. At stage L0 an element index is [T : r bits][P : w bits]
 // [q : L0 bits] with w = LOG_N - r - L0. The r stages pair the elements that
@@ -110,6 +112,17 @@ __device__ __forceinline__ void butterfly(float2& a, float2& b, float2 w)
 // the reference's stage loop (src/core/fft.cpp:70-74) with the same operands
 // and twiddles, so the EXACT form is bit-identical to it.
 // ---------------------------------------------------------------------------
+// Barrier for the lanes of one sequence group (see StageBlock).
+template <int G>
+__device__ __forceinline__ void group_sync()
+{
+    if constexpr (G > 32) {
+        __syncthreads();
+    } else {
+        __syncwarp();
+    }
+}
+
 template <int LOG_N, int G, int L0, bool FAST>
 struct StageBlock {
     static constexpr int N = 1 << LOG_N;
@@ -129,7 +142,7 @@ struct StageBlock {
 #pragma unroll
             for (int t = 0; t < RR; ++t) v[k][t] = seq[pad_idx((t << (LOG_N - r)) | c)];
         }
-        __syncwarp();
+        group_sync<G>();
 #pragma unroll
         for (int k = 0; k < C; ++k) {
             const int c = lane + G * k;
@@ -159,7 +172,7 @@ struct StageBlock {
                 seq[pad_idx(out)] = v[k][S];
             }
         }
-        __syncwarp();
+        group_sync<G>();
         if constexpr (L0 + r < LOG_N) StageBlock<LOG_N, G, L0 + r, FAST>::run(seq, tw, lane);
     }
 };

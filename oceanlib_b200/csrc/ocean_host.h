@@ -16,8 +16,11 @@ void desc_defaults(ocean_desc* d);
 // struct_size-aware copy (src/c_api.cpp:46-60); false for a bad struct_size.
 bool copy_desc(const ocean_desc* src, ocean_desc& dst);
 // Throws std::invalid_argument as the reference's constructor would
-// (src/ocean.cpp:28-59), and for N above the built kernel range.
+// (src/ocean.cpp:28-59): N a power of two in [16, 4096], and so on.
 void validate(const ocean_desc& d);
+// Largest N of the persistent frame kernel (frame.cu); 2048 and 4096 run
+// the three-pass schedule of frame_large.cu.
+constexpr uint32_t kMaxPersistentSize = 1024;
 int ilog2u(uint32_t v);
 // Per-stage inverse twiddles, N - 1 entries (src/core/fft.cpp:24-33).
 std::vector<float2> stage_twiddles(uint32_t n);

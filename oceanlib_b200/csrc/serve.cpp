@@ -303,6 +303,8 @@ public:
     {
         ocean_desc od = od_in;
         validate(od);
+        // The dispatcher batches sessions into persistent frame launches.
+        if (od.size > kMaxPersistentSize) throw std::invalid_argument("session size above 1024");
         ocean_interaction_desc fd{};
         if (fd_in != nullptr) {
             fd = *fd_in;

@@ -96,6 +96,16 @@ cudaError_t launch_row_pass(int log_n, int nf, bool fast, const FrameArgs& args,
 cudaError_t launch_col_pass(int log_n, int nf, bool fast, bool fuse_foam,
                             const FrameArgs& args, cudaStream_t stream);
 
+// The frame at N = 2048 and 4096 (log_n 11, 12; frame_large.cu), for
+// `args.chunk` oceans from args.ocean_base, in three launches: rows (evolve +
+// row FFTs), column FFTs in place, finalize (+ the first foam substep when
+// fuse_foam; nf = 6). The intermediate is field-major: field f of chunk ocean
+// o at args.inter + (o * nf + f) * N * N. args.table must be null.
+cudaError_t launch_large_rows(int log_n, int nf, bool fast, const FrameArgs& args, cudaStream_t stream);
+cudaError_t launch_large_cols(int log_n, int nf, bool fast, const FrameArgs& args, cudaStream_t stream);
+cudaError_t launch_large_finalize(int log_n, int nf, bool fuse_foam, const FrameArgs& args,
+                                  cudaStream_t stream);
+
 // Stand-alone foam substep for oceans [0, count) (used for substeps after the
 // first in one update).
 cudaError_t launch_foam_step(int n, int count, const float4* disp, const float4* velocity,

@@ -2,12 +2,13 @@
 (oracle/_ref/libocean_ref.so, compiled from the reference's own sources by
 oracle/Makefile). Run here, where the reference sources exist:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py           # every fixture
+    python tests/golden/make_golden.py hashes    # only the named ones
 
 Outputs
   ref_small.npz    full tables and frame outputs for small grids (N <= 64)
   ref_hashes.json  sha256 of the reference's output bytes at full sizes,
-                   so GPU tests can check bit-exactness at N = 256 / 512 / 1024
+                   so GPU tests can check bit-exactness at N = 128 ... 4096
                    without storing the arrays
   ref_queries.npz  reference sample_at results for seeded query points
   ref_cascade.npz  reference CascadeStack::sample_at results (3 levels)
@@ -175,17 +176,20 @@ def pack() -> None:
     (HERE / "ref_pack.json").write_text(json.dumps(out, indent=1))
 
 
+PARTS = {"small": small, "hashes": hashes, "queries": queries, "cascades": cascades,
+         "interaction": interaction, "pack": pack, "abi_layout": abi_layout}
+
+
 def main() -> None:
     if not O.ref_available():
         raise SystemExit("the reference library could not be built (reference sources absent)")
     O.ref().oref_c_force_simd_level(None)
-    small()
-    hashes()
-    queries()
-    cascades()
-    interaction()
-    pack()
-    abi_layout()
+    names = sys.argv[1:] or list(PARTS)
+    unknown = [n for n in names if n not in PARTS]
+    if unknown:
+        raise SystemExit(f"unknown fixture(s) {unknown}; choose from {list(PARTS)}")
+    for name in names:
+        PARTS[name]()
     print("golden fixtures written to", HERE)
 
 

@@ -47,7 +47,11 @@ def _exact_level(cuda_device):
 
 
 def test_device_h0_tables_are_bit_exact():
+    # N = 4096 tables are checked against the reference's digests in
+    # test_gpu_large (the oracle takes seconds per table there).
     for desc, _ in HASH_CASES + SMALL_CASES:
+        if desc.size > 2048:
+            continue
         batch = ob.OceanBatch([desc])
         h0, wk = batch.read_spectrum(0)
         tables = O.spectrum(desc)

@@ -66,9 +66,13 @@ def test_choppiness_zero_gives_unit_jacobian():
 
 
 def test_oracle_matches_reference_hashes_full_size():
+    # Sizes up to 2048 (a 4096^2 oracle frame takes tens of seconds; the GPU
+    # suite checks those digests against the device directly).
     golden = json.loads((GOLDEN / "ref_hashes.json").read_text())
     for case in golden["cases"]:
         desc = desc_from_json(case["desc"])
+        if desc.size > 2048:
+            continue
         tables = O.spectrum(desc)
         assert sha(np.stack([tables[0], tables[1]], axis=1)) == case["h0"], desc
         for fr in case["frames"]:
@@ -99,7 +103,9 @@ class FoamAccumulator:
         return s
 
 
-def run_oracle_foam(desc, foam, frames, dt):
+def run_oracle_foam(desc, foam, frames):
+    """The oracle's foam state after each (t, dt) frame, stepped as the
+    reference's FoamField is (fixed substeps from an accumulator)."""
     n = desc.size
     tables = O.spectrum(desc)
     cur = np.zeros(n * n, np.float32)
@@ -109,8 +115,8 @@ def run_oracle_foam(desc, foam, frames, dt):
     gain = np.float32(np.float32(foam.source_gain) * fdt)
     cell = np.float32(np.float32(desc.patch_length) / np.float32(n))
     out = []
-    for k in range(frames):
-        d, _, v = O.update(desc, (k + 1) * dt, tables)
+    for t, dt in frames:
+        d, _, v = O.update(desc, t, tables)
         for _ in range(acc.steps(dt)):
             cur = O.foam_step(n, cell, fdt, decay, gain, foam.advect_scale, foam.wind_drift_x,
                               foam.wind_drift_z, d, v, cur)
@@ -122,7 +128,7 @@ def test_oracle_foam_matches_reference():
     golden = json.loads((GOLDEN / "ref_hashes.json").read_text())["foam"]
     desc, foam, frames, dt = FOAM_CASE
     # 24 frames keep the CPU suite fast; the GPU test checks all of them.
-    got = run_oracle_foam(desc, foam, 24, dt)
+    got = run_oracle_foam(desc, foam, [((k + 1) * dt, dt) for k in range(24)])
     for k in range(24):
         assert sha(got[k]) == golden["hashes"][k], k
 

@@ -41,6 +41,13 @@ HASH_CASES = [
                compute_velocity=True), (5.0,)),
     (OceanDesc(size=1024, patch_length=1000.0, wind_speed=25.0, wind_direction=2.0, choppiness=1.2,
                seed=5), (42.0,)),
+    # Above the persistent kernel's range: the three-pass schedule.
+    (OceanDesc(size=2048, patch_length=2000.0, wind_speed=18.0, wind_direction=0.9, choppiness=1.4,
+               seed=2048, compute_velocity=True), (7.5, 1e4)),
+    (OceanDesc(size=4096, patch_length=4000.0, wind_speed=10.0, wind_direction=2.6, choppiness=0.9,
+               seed=4096, compute_velocity=True), (3.0,)),
+    (OceanDesc(size=4096, patch_length=600.0, wind_speed=21.0, wind_direction=-1.2, depth=40.0,
+               seed=77), (250.0,)),
 ]
 
 # Persistent foam on the foam patch: 120 frames at 60 Hz.
