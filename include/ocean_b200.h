@@ -298,12 +298,15 @@ typedef enum ocean_fft_form {
     OCEAN_FFT_EXACT = 0, /* radix-2 Stockham in the reference's operation order,
                             no FMA: bit-identical to the reference           */
     OCEAN_FFT_FAST  = 1, /* same dataflow with fused multiply-adds           */
-    OCEAN_FFT_TENSOR = 2 /* four-step DFT on the tensor cores (tcgen05), FP16
-                            hi + lo operands with FP32 accumulation; N = 512 */
+    OCEAN_FFT_TENSOR = 2 /* four-step DFT on the tensor cores (tcgen05):
+                            operands cut into four signed 8-bit digits held
+                            as FP16, exact digit products, levels combined
+                            in FP32; N = 512 */
 } ocean_fft_form;
 
 /* `count` unnormalised inverse DFTs (sign +, as src/core/fft.cpp) of
- * complex sequences of length `size`, in the given form. `input` and
+ * complex sequences of length `size` (a power of two in [16, 1024]; 512 for
+ * the tensor form), in the given form. `input` and
  * `output` are DEVICE arrays of count * size interleaved (re, im) floats;
  * the call waits for the result. For accuracy checks of the forms. */
 OCEAN_API ocean_status ocean_dft_batch(uint32_t size, uint32_t count, int32_t form, const float* input,
@@ -430,7 +433,8 @@ OCEAN_API ocean_status ocean_batch_read_spectrum(const ocean_batch* batch, uint3
 typedef struct ocean_ensemble ocean_ensemble;
 
 /* Groups the oceans by size; each frame forks one stream per size and runs
- * that size's persistent kernel on it. With autotune != 0 the schedule
+ * that size's persistent kernel on it (the three-pass schedule at N = 2048
+ * and 4096). With autotune != 0 the schedule
  * (sizes in sequence, or concurrently with SM shares by estimated or by
  * measured cost) is chosen by timing each candidate on this GPU at creation. */
 OCEAN_API ocean_ensemble* ocean_ensemble_create(const ocean_desc* oceans, uint32_t count,

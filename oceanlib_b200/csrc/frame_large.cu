@@ -38,6 +38,10 @@ struct Large {
     static constexpr int ROW_T = 2 * G;            // threads: two sequences
     static constexpr int COL_T = W * G;            // threads: W sequences
     static constexpr int ROW_TASKS = 4;            // tasks per row CTA
+    // Resident row CTAs per SM the registers are capped for: two at N = 4096
+    // (512 threads, 102 KB each; 7% faster than one), three at 2048 (256
+    // threads, 51 KB each).
+    static constexpr int ROW_BLOCKS = LOG_N >= 12 ? 2 : 3;
     static constexpr int COL_TASKS = 2;            // tasks per column CTA
     static constexpr size_t ROW_SMEM = sizeof(float2) * (2 * SEQ + N - 1);
     static constexpr size_t COL_SMEM = sizeof(float2) * (W * SEQ + N - 1);
@@ -45,7 +49,8 @@ struct Large {
 };
 
 template <int LOG_N, int NF, bool FAST>
-__global__ void __launch_bounds__(Large<LOG_N>::ROW_T) large_row_kernel(FrameArgs a)
+__global__ void __launch_bounds__(Large<LOG_N>::ROW_T, Large<LOG_N>::ROW_BLOCKS)
+large_row_kernel(FrameArgs a)
 {
     using S = Large<LOG_N>;
     constexpr int N = S::N, NT = S::ROW_T, SEQ = S::SEQ, G = S::G;
