@@ -416,6 +416,32 @@ OCEAN_API ocean_status ocean_batch_get_device_buffers(const ocean_batch* batch, 
 /* Number of foam substeps the last update ran (0..max_substeps). */
 OCEAN_API uint32_t ocean_batch_last_foam_substeps(const ocean_batch* batch);
 
+/* The rest of ocean::FoamField (include/ocean/foam.hpp:88-142) for a batch
+ * with persistent foam; OCEAN_ERROR_INVALID_ARG without it. These are ordered
+ * after the work queued on the batch's own stream; updates queued on another
+ * stream must be complete first. */
+/* FoamField::clear (src/foam.cpp:254-260): every ocean's foam to zero and the
+ * substep accumulator reset (after a seek). Returns when done. */
+OCEAN_API ocean_status ocean_batch_foam_clear(ocean_batch* batch);
+/* FoamField::set_desc (src/foam.cpp:266-283): decay, source_gain,
+ * advect_scale and the wind drift apply from the next update on; fixed_dt
+ * and max_substeps keep the values the batch was created with. The stored
+ * foam is untouched. */
+OCEAN_API ocean_status ocean_batch_foam_set_desc(ocean_batch* batch, const ocean_foam_desc* desc);
+/* FoamField::desc(): the descriptor in effect. */
+OCEAN_API ocean_status ocean_batch_foam_get_desc(const ocean_batch* batch, ocean_foam_desc* out);
+/* FoamField::foam_at (src/foam.cpp:291-305) at `count` world points of ocean
+ * `index`: the same displacement inversion as ocean_sample_at, then the
+ * periodic bilinear foam fetch. xz (count (x, z) pairs) and out (count
+ * floats) are HOST arrays; returns when out is written. Bit-identical to the
+ * reference point by point. */
+OCEAN_API ocean_status ocean_batch_foam_at_many(const ocean_batch* batch, uint32_t index, const float* xz,
+                                                uint64_t count, float* out);
+/* FoamField::coverage (src/foam.cpp:307-313): mean foam of ocean `index`,
+ * summed in double on the device in a fixed order (the reference sums in
+ * index order; the two differ by double rounding only). */
+OCEAN_API ocean_status ocean_batch_foam_coverage(const ocean_batch* batch, uint32_t index, double* out);
+
 /* Waits for all work queued on the batch's own stream. Returns
  * OCEAN_ERROR_TIMEOUT (once) if a bounded device wait of the persistent
  * frame kernel gave up since the last check. */

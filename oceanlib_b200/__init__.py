@@ -332,6 +332,36 @@ class OceanBatch:
     def launch_count(self) -> int:
         return lib().ocean_batch_launch_count(self._h)
 
+    # The rest of ocean::FoamField (persistent foam batches only).
+    def foam_clear(self) -> None:
+        """FoamField::clear: every ocean's foam to zero, accumulator reset."""
+        _check(lib().ocean_batch_foam_clear(self._h), "ocean_batch_foam_clear")
+
+    def set_foam_desc(self, foam: "FoamDesc") -> None:
+        """FoamField::set_desc: decay, gain, advect scale and drift from the
+        next update on (fixed_dt and max_substeps stay as created)."""
+        f = foam.to_c()
+        _check(lib().ocean_batch_foam_set_desc(self._h, C.byref(f)), "ocean_batch_foam_set_desc")
+
+    def foam_desc(self) -> FoamDescC:
+        f = FoamDescC()
+        _check(lib().ocean_batch_foam_get_desc(self._h, C.byref(f)), "ocean_batch_foam_get_desc")
+        return f
+
+    def foam_at_many(self, index: int, xz: np.ndarray) -> np.ndarray:
+        """FoamField::foam_at at world points xz (count x 2 float32)."""
+        pts = np.ascontiguousarray(xz, dtype=np.float32).reshape(-1, 2)
+        out = np.empty(pts.shape[0], np.float32)
+        _check(lib().ocean_batch_foam_at_many(self._h, index, pts.ctypes.data, pts.shape[0], out.ctypes.data),
+               "ocean_batch_foam_at_many")
+        return out
+
+    def foam_coverage(self, index: int = 0) -> float:
+        """FoamField::coverage: mean foam over the patch."""
+        v = C.c_double(0.0)
+        _check(lib().ocean_batch_foam_coverage(self._h, index, C.byref(v)), "ocean_batch_foam_coverage")
+        return v.value
+
     def read_spectrum(self, index: int):
         n = self.size
         h0 = np.empty((n * n, 2), dtype=np.float32)

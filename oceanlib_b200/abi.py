@@ -257,6 +257,11 @@ SIGNATURES = {
     "ocean_batch_last_foam_substeps": (C.c_uint32, [C.c_void_p]),
     "ocean_batch_synchronize": (C.c_int, [C.c_void_p]),
     "ocean_batch_read_spectrum": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "ocean_batch_foam_clear": (C.c_int, [C.c_void_p]),
+    "ocean_batch_foam_set_desc": (C.c_int, [C.c_void_p, C.POINTER(FoamDescC)]),
+    "ocean_batch_foam_get_desc": (C.c_int, [C.c_void_p, C.POINTER(FoamDescC)]),
+    "ocean_batch_foam_at_many": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint64, C.c_void_p]),
+    "ocean_batch_foam_coverage": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_double)]),
     "ocean_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "ocean_batch_read_profile": (C.c_int, [C.c_void_p, C.POINTER(PassProfile)]),
     "ocean_batch_launch_count": (C.c_uint64, [C.c_void_p]),

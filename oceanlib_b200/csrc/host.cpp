@@ -312,6 +312,70 @@ public:
     const ocean_desc& desc(uint32_t i) const { return descs_[i]; }
     cudaStream_t stream() const { return stream_; }
     uint32_t last_foam_substeps() const { return foam_last_; }
+
+    // FoamField::clear (src/foam.cpp:254-260): no foam anywhere, substep
+    // accumulator reset. Ordered after the work on the batch's own stream;
+    // returns when the field is cleared.
+    void foam_clear()
+    {
+        if (!foam_on_) throw std::invalid_argument("no persistent foam");
+        const size_t bytes = cells_ * count_ * sizeof(float);
+        check(cudaMemsetAsync(foam_a_.p, 0, bytes, stream_), "memset");
+        check(cudaMemsetAsync(foam_b_.p, 0, bytes, stream_), "memset");
+        check(cudaStreamSynchronize(stream_), "foam clear");
+        foam_accum_ = 0.0;
+    }
+
+    // FoamField::set_desc (src/foam.cpp:266-283): retunes decay, gain, advect
+    // scale and drift from the next update on. The substep length and count
+    // stay what the batch was created with; the stored foam is untouched.
+    void foam_set_desc(const ocean_foam_desc& d)
+    {
+        if (!foam_on_) throw std::invalid_argument("no persistent foam");
+        validate_foam(d);
+        const float keep_dt = foam_.fixed_dt;
+        const uint32_t keep_steps = foam_.max_substeps;
+        foam_ = d;
+        foam_.fixed_dt = keep_dt;
+        foam_.max_substeps = keep_steps;
+    }
+    const ocean_foam_desc& foam_desc() const { return foam_; }
+
+    // FoamField::foam_at (src/foam.cpp:291-305) at `count` world points of
+    // ocean i: xz and out are host arrays. Ordered after the work on the
+    // batch's own stream; returns when `out` is written.
+    void foam_at_many(uint32_t i, const float* xz, uint64_t count, float* out) const
+    {
+        if (!foam_on_) throw std::invalid_argument("no persistent foam");
+        if (count == 0) return;
+        std::lock_guard<std::mutex> lock(query_mutex_);
+        if (q_in_.n < count) {
+            q_in_ = DevBuf<float2>(count);
+            q_out_ = DevBuf<float>(count);
+        }
+        const float cell = descs_[i].patch_length / static_cast<float>(n_);
+        const float inv_cell = static_cast<float>(n_) / descs_[i].patch_length;
+        check(cudaMemcpyAsync(q_in_.p, xz, count * sizeof(float2), cudaMemcpyHostToDevice, stream_), "query");
+        check(launch_foam_at(static_cast<int>(n_), inv_cell, cell, disp(i), normal(i), foam_ptr(i), q_in_.p,
+                             count, q_out_.p, stream_), "foam_at kernel");
+        check(cudaMemcpyAsync(out, q_out_.p, count * sizeof(float), cudaMemcpyDeviceToHost, stream_), "query");
+        check(cudaStreamSynchronize(stream_), "query");
+    }
+
+    // FoamField::coverage (src/foam.cpp:307-313) of ocean i, computed on the
+    // device in a fixed order (equal to the reference's sequential sum up to
+    // double rounding).
+    double foam_coverage(uint32_t i) const
+    {
+        if (!foam_on_) throw std::invalid_argument("no persistent foam");
+        std::lock_guard<std::mutex> lock(query_mutex_);
+        if (q_sum_.n == 0) q_sum_ = DevBuf<double>(1);
+        check(launch_foam_coverage(foam_ptr(i), cells_, q_sum_.p, stream_), "coverage kernel");
+        double v = 0.0;
+        check(cudaMemcpyAsync(&v, q_sum_.p, sizeof(double), cudaMemcpyDeviceToHost, stream_), "coverage");
+        check(cudaStreamSynchronize(stream_), "coverage");
+        return v;
+    }
     size_t cells() const { return cells_; }
 
     float4* disp(uint32_t i) const { return disp_.p + i * cells_; }
@@ -795,6 +859,11 @@ private:
     ocean_foam_desc foam_{};
     double foam_accum_ = 0.0;
     uint32_t foam_last_ = 0;
+    // Scratch of the foam queries (allocated on first use).
+    mutable std::mutex query_mutex_;
+    mutable DevBuf<float2> q_in_;
+    mutable DevBuf<float> q_out_;
+    mutable DevBuf<double> q_sum_;
 };
 
 // ---------------------------------------------------------------------------
@@ -1688,6 +1757,45 @@ ocean_status ocean_batch_read_spectrum(const ocean_batch* batch, uint32_t index,
     return guarded([&] {
         batch->impl.read_spectrum(index, h0, omega_kinv);
     });
+}
+
+ocean_status ocean_batch_foam_clear(ocean_batch* batch)
+{
+    if (batch == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { batch->impl.foam_clear(); });
+}
+
+ocean_status ocean_batch_foam_set_desc(ocean_batch* batch, const ocean_foam_desc* desc)
+{
+    if (batch == nullptr || desc == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    if (desc->struct_size == 0 || desc->struct_size > sizeof(ocean_foam_desc)) return OCEAN_ERROR_INVALID_ARG;
+    ocean_foam_desc d;
+    ocean_b200::foam_desc_defaults(&d);
+    std::memcpy(&d, desc, desc->struct_size);
+    d.struct_size = sizeof(ocean_foam_desc);
+    return guarded([&] { batch->impl.foam_set_desc(d); });
+}
+
+ocean_status ocean_batch_foam_get_desc(const ocean_batch* batch, ocean_foam_desc* out)
+{
+    if (batch == nullptr || out == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    if (!batch->impl.foam_on()) return OCEAN_ERROR_INVALID_ARG;
+    *out = batch->impl.foam_desc();
+    return OCEAN_OK;
+}
+
+ocean_status ocean_batch_foam_at_many(const ocean_batch* batch, uint32_t index, const float* xz, uint64_t count,
+                                      float* out)
+{
+    if (batch == nullptr || index >= batch->impl.count()) return OCEAN_ERROR_INVALID_ARG;
+    if (count > 0 && (xz == nullptr || out == nullptr)) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { batch->impl.foam_at_many(index, xz, count, out); });
+}
+
+ocean_status ocean_batch_foam_coverage(const ocean_batch* batch, uint32_t index, double* out)
+{
+    if (batch == nullptr || out == nullptr || index >= batch->impl.count()) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { *out = batch->impl.foam_coverage(index); });
 }
 
 ocean_status ocean_batch_set_profiling(ocean_batch* batch, int32_t enable)

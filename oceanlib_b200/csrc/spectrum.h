@@ -113,6 +113,16 @@ cudaError_t launch_foam_step(int n, int count, const float4* disp, const float4*
                              float scale, float drift_x, float drift_z, float inv_cell,
                              cudaStream_t stream);
 
+// FoamField::foam_at (src/foam.cpp:291-305) at `count` world points of one
+// ocean: the displacement inversion, then the periodic bilinear foam fetch.
+// inv_cell = N / patch_length (the inversion's), cell = patch_length / N.
+cudaError_t launch_foam_at(int n, float inv_cell, float cell, const float4* disp, const float4* normal,
+                           const float* foam, const float2* xz, uint64_t count, float* out,
+                           cudaStream_t stream);
+// FoamField::coverage (src/foam.cpp:307-313): mean of `cells` floats, in
+// double, deterministic (fixed partial sums and tree).
+cudaError_t launch_foam_coverage(const float* foam, uint64_t cells, double* out, cudaStream_t stream);
+
 // Batched world queries (src/ocean.cpp:375-452), one thread per point.
 struct SurfaceEx {
     float height, offset_x, offset_z, normal_x, normal_y, normal_z, foam;

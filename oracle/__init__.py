@@ -84,6 +84,7 @@ def oracle() -> C.CDLL:
             "or_update": (None, [C.POINTER(OrDesc), _P, C.c_double, _P, _P, _P, _P]),
             "or_sample_many": (None, [C.c_uint32, C.c_float, _P, _P, _P, _P, C.c_uint64, _P]),
             "or_foam_step": (None, [C.c_uint32] + [C.c_float] * 7 + [_P, _P, _P, _P]),
+            "or_foam_at_many": (None, [C.c_uint32, C.c_float, _P, _P, _P, _P, C.c_uint64, _P]),
             "or_dft2d_points": (None, [C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P, _P]),
             "or_dft2d_full": (None, [C.c_uint32, _P, _P, _P, _P]),
         }
@@ -146,6 +147,7 @@ def ref() -> C.CDLL:
             "oref_foam_coverage": (C.c_double, [_P]),
             "oref_foam_at": (C.c_float, [_P, C.c_float, C.c_float]),
             "oref_foam_clear": (None, [_P]),
+            "oref_foam_set_desc": (C.c_int, [_P, C.POINTER(OrefFoamDesc)]),
             "oref_cascade_create": (_P, [_P, C.c_uint32, C.POINTER(C.c_int)]),
             "oref_cascade_destroy": (None, [_P]),
             "oref_cascade_update": (None, [_P, C.c_double]),
@@ -282,6 +284,18 @@ def foam_step(n, cell, dt, decay, gain, scale, drift_x, drift_z, disp, vel, cur)
                           vel.ctypes.data, np.ascontiguousarray(cur, np.float32).ctypes.data,
                           nxt.ctypes.data)
     return nxt
+
+
+def foam_at_many(n: int, patch_length: float, disp, normal, foam, xz: np.ndarray) -> np.ndarray:
+    """FoamField::foam_at (src/foam.cpp:291-305) at the points xz (count x 2)."""
+    pts = np.ascontiguousarray(xz, dtype=np.float32).reshape(-1, 2)
+    d = np.ascontiguousarray(disp, np.float32)
+    nm = np.ascontiguousarray(normal, np.float32)
+    f = np.ascontiguousarray(foam, np.float32)
+    out = np.empty(pts.shape[0], np.float32)
+    oracle().or_foam_at_many(n, patch_length, d.ctypes.data, nm.ctypes.data, f.ctypes.data, pts.ctypes.data,
+                             pts.shape[0], out.ctypes.data)
+    return out
 
 
 def dft_points(re: np.ndarray, im: np.ndarray, xs, ys):
@@ -448,6 +462,24 @@ class RefFoam:
     @property
     def last_substeps(self) -> int:
         return ref().oref_foam_last_substeps(self.h)
+
+    def coverage(self) -> float:
+        return ref().oref_foam_coverage(self.h)
+
+    def foam_at_many(self, xz: np.ndarray) -> np.ndarray:
+        pts = np.ascontiguousarray(xz, dtype=np.float32).reshape(-1, 2)
+        return np.array([ref().oref_foam_at(self.h, float(x), float(z)) for x, z in pts], np.float32)
+
+    def clear(self) -> None:
+        ref().oref_foam_clear(self.h)
+
+    def set_desc(self, foam_desc) -> None:
+        d = OrefFoamDesc()
+        for k in ("decay", "source_gain", "advect_scale", "wind_drift_x", "wind_drift_z", "fixed_dt"):
+            setattr(d, k, getattr(foam_desc, k))
+        d.max_substeps = foam_desc.max_substeps
+        if ref().oref_foam_set_desc(self.h, C.byref(d)) != 0:
+            raise ValueError("reference FoamField::set_desc rejected the descriptor")
 
     def close(self):
         if self.h:

@@ -622,6 +622,21 @@ static float sample_wrap(const float* f, float u, float v, int n)
            d * tu * tv;
 }
 
+void or_foam_at_many(uint32_t n, float patch_length, const float* disp, const float* normal,
+                     const float* foam, const float* xz, uint64_t count, float* out)
+{
+    /* src/foam.cpp:291-305: the ocean's inversion, then the wrapped fetch */
+    const float cell = patch_length / (float)n;
+    float s[10];
+    for (uint64_t i = 0; i < count; ++i) {
+        const float x = xz[2 * i], z = xz[2 * i + 1];
+        or_sample_at(n, patch_length, disp, normal, NULL, x, z, s);
+        const float u = (x - s[1]) / cell;
+        const float v = (z - s[2]) / cell;
+        out[i] = sample_wrap(foam, u, v, (int)n);
+    }
+}
+
 void or_foam_step(uint32_t n, float cell, float dt, float decay, float gain, float scale,
                   float drift_x, float drift_z, const float* disp, const float* velocity,
                   const float* cur, float* next)

@@ -66,6 +66,10 @@ void or_sample_at(uint32_t n, float patch_length, const float* disp, const float
 void or_sample_many(uint32_t n, float patch_length, const float* disp, const float* normal,
                     const float* velocity, const float* xz, uint64_t count, float* out);
 
+/* FoamField::foam_at at `count` world points: out[i] for (xz[2i], xz[2i+1]). */
+void or_foam_at_many(uint32_t n, float patch_length, const float* disp, const float* normal,
+                     const float* foam, const float* xz, uint64_t count, float* out);
+
 /* One persistent-foam substep (FoamField step_rows). `decay` is the already
  * evaluated expf(-decay_rate * dt), as the reference computes it on the host. */
 void or_foam_step(uint32_t n, float cell, float dt, float decay, float gain, float scale,

@@ -262,6 +262,24 @@ OREF_API float oref_foam_at(void* f, float x, float z)
     return static_cast<ocean::FoamField*>(f)->foam_at(x, z);
 }
 OREF_API void oref_foam_clear(void* f) { static_cast<ocean::FoamField*>(f)->clear(); }
+OREF_API int oref_foam_set_desc(void* f, const OrefFoamDesc* d)
+{
+    ocean::FoamDesc fd;
+    fd.decay = d->decay;
+    fd.source_gain = d->source_gain;
+    fd.advect_scale = d->advect_scale;
+    fd.wind_drift_x = d->wind_drift_x;
+    fd.wind_drift_z = d->wind_drift_z;
+    fd.fixed_dt = d->fixed_dt;
+    fd.max_substeps = d->max_substeps;
+    fd.thread_count = d->thread_count;
+    try {
+        static_cast<ocean::FoamField*>(f)->set_desc(fd);
+        return 0;
+    } catch (...) {
+        return 1;
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Cascades (C++ only in the reference).

@@ -13,6 +13,7 @@ Outputs
   ref_queries.npz  reference sample_at results for seeded query points
   ref_cascade.npz  reference CascadeStack::sample_at results (3 levels)
   ref_pack.json    sha256 of the viewer's RGBA16F pack over seeded bit patterns
+  ref_foam.json    FoamField::foam_at / coverage / set_desc / clear on the foam patch
   abi_layout.json  offsets/sizes of the reference's C structs (include/ocean/ocean.h)
 """
 from __future__ import annotations
@@ -32,7 +33,8 @@ sys.path.insert(0, str(ROOT))
 import oracle as O  # noqa: E402
 from oceanlib_b200.abi import OceanDescC  # noqa: E402
 from tests.workloads import (SMALL_CASES, HASH_CASES, FOAM_CASE, QUERY_CASE, CASCADE_CASE,  # noqa: E402
-                             desc_to_json, query_points, cascade_points, pack_patterns)
+                             FOAM_QUERY_FRAMES, FOAM_RETUNE, desc_to_json, query_points, cascade_points,
+                             pack_patterns)
 
 HERE = Path(__file__).resolve().parent
 
@@ -176,8 +178,35 @@ def pack() -> None:
     (HERE / "ref_pack.json").write_text(json.dumps(out, indent=1))
 
 
+def foam_queries() -> None:
+    desc, foam, _, dt = FOAM_CASE
+    first, second = FOAM_QUERY_FRAMES
+    ro = O.RefOcean(desc)
+    rf = O.RefFoam(ro, foam)
+    for k in range(first):
+        ro.update((k + 1) * dt)
+        rf.update(dt)
+    xz = query_points(desc, 4096)
+    out = {"desc": desc_to_json(desc), "dt": dt, "frames": [first, second],
+           "at": sha(rf.foam_at_many(xz)), "coverage": rf.coverage(), "field": sha(rf.data())}
+    rf.set_desc(FOAM_RETUNE)
+    retuned = []
+    for k in range(first, first + second):
+        ro.update((k + 1) * dt)
+        rf.update(dt)
+        retuned.append({"field": sha(rf.data()), "substeps": rf.last_substeps})
+    out["retuned"] = retuned
+    out["coverage_retuned"] = rf.coverage()
+    rf.clear()
+    out["coverage_cleared"] = rf.coverage()
+    ro.update((first + second + 1) * dt)
+    rf.update(dt)
+    out["after_clear"] = sha(rf.data())
+    (HERE / "ref_foam.json").write_text(json.dumps(out, indent=1))
+
+
 PARTS = {"small": small, "hashes": hashes, "queries": queries, "cascades": cascades,
-         "interaction": interaction, "pack": pack, "abi_layout": abi_layout}
+         "interaction": interaction, "pack": pack, "abi_layout": abi_layout, "foam_queries": foam_queries}
 
 
 def main() -> None:

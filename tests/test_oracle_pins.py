@@ -15,8 +15,8 @@ import pytest
 
 import oracle as O
 from oceanlib_b200 import workloads as W
-from tests.workloads import (FOAM_CASE, HASH_CASES, QUERY_CASE, SMALL_CASES, desc_from_json,
-                             query_points)
+from tests.workloads import (FOAM_CASE, FOAM_QUERY_FRAMES, HASH_CASES, QUERY_CASE, SMALL_CASES,
+                             desc_from_json, query_points)
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
@@ -131,6 +131,21 @@ def test_oracle_foam_matches_reference():
     got = run_oracle_foam(desc, foam, [((k + 1) * dt, dt) for k in range(24)])
     for k in range(24):
         assert sha(got[k]) == golden["hashes"][k], k
+
+
+def test_oracle_foam_at_and_coverage_match_reference():
+    # FoamField::foam_at (src/foam.cpp:291-305) and coverage (:307-313) after
+    # 30 frames of the foam patch, against the reference's own results.
+    g = json.loads((GOLDEN / "ref_foam.json").read_text())
+    desc, foam, _, dt = FOAM_CASE
+    first, _ = FOAM_QUERY_FRAMES
+    field = run_oracle_foam(desc, foam, [((k + 1) * dt, dt) for k in range(first)])[-1]
+    assert sha(field) == g["field"]
+    d, n, _ = O.update(desc, first * dt)
+    at = O.foam_at_many(desc.size, desc.patch_length, d, n, field, query_points(desc, 4096))
+    assert sha(at) == g["at"]
+    # The reference sums in index order; any other order differs by rounding.
+    assert abs(float(field.astype(np.float64).mean()) - g["coverage"]) <= 1e-12 * g["coverage"]
 
 
 def test_oracle_queries_match_reference():

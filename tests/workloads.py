@@ -53,6 +53,14 @@ HASH_CASES = [
 # Persistent foam on the foam patch: 120 frames at 60 Hz.
 FOAM_CASE = (W.foam_patch_512(), W.foam_desc(), 120, 1.0 / 60.0)
 
+# The rest of FoamField on the foam patch: foam_at and coverage after 30
+# frames, then set_desc to FOAM_RETUNE for 20 more frames (fixed_dt and
+# max_substeps given here differ from the field's and must be ignored), then
+# clear() and one more frame.
+FOAM_QUERY_FRAMES = (30, 20)
+FOAM_RETUNE = FoamDesc(decay=1.2, source_gain=0.5, advect_scale=0.5, wind_drift_x=3.0, wind_drift_z=-2.0,
+                       fixed_dt=1.0 / 30.0, max_substeps=1)
+
 # World queries on the single 256 patch at t = 10.
 QUERY_CASE = (_s256, _t256, 4096)
 
