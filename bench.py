@@ -173,17 +173,31 @@ def profile_traffic():
 # ---------------------------------------------------------------------------
 # Reference CPU implementation (the reference compiled from its own sources)
 # ---------------------------------------------------------------------------
-def reference_rate(seconds: float, warm: int = 2):
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), as the reference's
+    bench_update prints it beside its figures."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_rate(seconds: float, warm: int = 2, threads: int = 0):
     """Updates/s of the reference's own Ocean + FoamField on this host's cores
     for the same workload, sequential frames of one ocean with its built-in
-    thread pool over all hardware threads (the reference's threaded path)."""
+    thread pool over all hardware threads (threads = 0, the reference's
+    threaded path) or over `threads` threads."""
     import oracle as O
     from oceanlib_b200 import workloads as W
 
     desc = W.foam_patch_512()
+    desc.thread_count = threads
     ro = O.RefOcean(desc)
-    rf = O.RefFoam(ro, W.foam_desc())
-    cores = int(O.ref().oref_hardware_concurrency())
+    rf = O.RefFoam(ro, W.foam_desc(), thread_count=threads)
+    cores = threads if threads > 0 else int(O.ref().oref_hardware_concurrency())
     dt = W.FOAM_DT
     frame = 0
     for _ in range(warm):
@@ -862,11 +876,19 @@ def main():
                                           f"{srv['offered_rps']:.0f} requests/s offered over 256 sessions"}
         if not args.no_cpu_baseline and world == 1:
             try:
+                import oracle as O
+
                 rate, cores, frames = reference_rate(args.cpu_seconds)
+                rate1, _, frames1 = reference_rate(min(args.cpu_seconds, 4.0), threads=1)
                 line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference",
                                         "sample": f"{frames} sequential frames of one 512^2 ocean "
                                                   f"(reference Ocean + FoamField, its thread pool "
-                                                  f"over {cores} hardware threads)"}
+                                                  f"over {cores} hardware threads)",
+                                        "cpu_model": cpu_model(),
+                                        "simd_level": O.ref().oref_c_simd_level().decode(),
+                                        "single_thread": {"value": rate1, "unit": UNIT, "cores": 1,
+                                                          "sample": f"{frames1} sequential frames, "
+                                                                    "thread_count = 1"}}
             except Exception as e:  # the checker is optional on a box without it
                 line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                                         "sample": f"unavailable: {e}"}

@@ -124,6 +124,14 @@ def test_null_handles_are_tolerated():
     assert lib.ocean_batch_count(None) == 0
     assert lib.ocean_batch_update(None, None, 0, 0.0, None) == abi.OCEAN_ERROR_INVALID_ARG
     assert lib.ocean_get_device_buffers(None, None) == abi.OCEAN_ERROR_INVALID_ARG
+    # the FoamField members of a batch
+    inval = abi.OCEAN_ERROR_INVALID_ARG
+    assert lib.ocean_batch_foam_clear(None) == inval
+    assert lib.ocean_batch_foam_set_desc(None, None) == inval
+    assert lib.ocean_batch_foam_get_desc(None, None) == inval
+    assert lib.ocean_batch_foam_at_many(None, 0, None, 0, None) == inval
+    v = C.c_double(-1.0)
+    assert lib.ocean_batch_foam_coverage(None, 0, C.byref(v)) == inval and v.value == -1.0
 
 
 def test_force_simd_level_semantics():
