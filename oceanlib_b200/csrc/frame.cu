@@ -174,11 +174,76 @@ __device__ __forceinline__ void transform_all(float2* data, const float2* tws, i
 // intermediate slot `inter_slot` (N*N*NF float2). `tws` already holds the
 // twiddles in shared memory.
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// h0 rows by bulk asynchronous copy (TMA, untiled). A row task's h0 rows are
+// contiguous in global memory and land unchanged in shared memory, so thread
+// 0 copies each with one cp.async.bulk completing on an mbarrier and the CTA
+// waits on it, instead of every thread moving 16-byte pieces through its
+// registers (the shared-memory pipe is the frame's busiest unit). The other
+// transfers of the frame change layout on the way (rows to cell-major, strips
+// to padded sequences, transposes), which a TMA copy cannot do.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kH0WaitNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Once per CTA (thread 0), before the CTA's first barrier.
+__device__ __forceinline__ void h0_bar_init(uint64_t* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Thread 0: `rows` copies of row_f2 float2 each, src(r) -> dst + r * row_f2,
+// all completing on `bar`. Addresses and sizes are multiples of 16 bytes.
+template <typename RowSrc>
+__device__ __forceinline__ void h0_rows_issue(uint64_t* bar, float2* dst, int rows, int row_f2, RowSrc src)
+{
+    const uint32_t b = smem_addr(bar);
+    const unsigned bytes = static_cast<unsigned>(row_f2 * sizeof(float2));
+    // The previous task accessed this memory through the generic proxy.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes * rows) : "memory");
+    for (int r = 0; r < rows; ++r) {
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_addr(dst + r * row_f2)),
+                     "l"(src(r)), "r"(bytes), "r"(b)
+                     : "memory");
+    }
+}
+
+// Every thread: wait for phase `parity` of `bar`, for at most kH0WaitNs;
+// then the error word is set (when there is one) and the task goes on.
+__device__ __forceinline__ void h0_rows_wait(uint64_t* bar, uint32_t parity, unsigned* error)
+{
+    const uint32_t b = smem_addr(bar);
+    unsigned long long t0 = 0;
+    for (int spin = 0;; ++spin) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P;\n\t}\n"
+            : "=r"(done)
+            : "r"(b), "r"(parity)
+            : "memory");
+        if (done) return;
+        if (spin == 0) t0 = tc::now_ns();
+        if ((spin & 63) == 63 && tc::now_ns() - t0 > kH0WaitNs) {
+            if (error != nullptr) atomicCAS(error, 0u, 1u);
+            return;
+        }
+    }
+}
+
 template <int LOG_N, int NF, bool FAST, bool TC = false>
 __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int group,
                                          float2* __restrict__ inter_slot, float2* smem,
-                                         const float2* tws, int tid, TcEngine<NF>* eng = nullptr,
-                                         unsigned* error = nullptr)
+                                         const float2* tws, int tid, uint64_t* h0_bar, uint32_t h0_parity,
+                                         TcEngine<NF>* eng = nullptr, unsigned* error = nullptr)
 {
     using S = Shape<LOG_N>;
     constexpr int N = S::N, G = S::G, SEQ = S::SEQ, SEQ4 = S::SEQ4, RP = S::RP;
@@ -215,8 +280,13 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         return r ? N - p : p;
     };
 
-    // The geometry of this thread's cells is loaded before the h0 rows, so
-    // both loads' latencies overlap ahead of the one barrier.
+    // The h0 rows go first (bulk copies), then every thread loads the
+    // geometry of its cells, so both latencies overlap ahead of the wait.
+    static_assert((RP * 2 * NF * seq_f2<LOG_N, TC>() * sizeof(float2)) % 16 == 0 && (N * sizeof(float2)) % 16 == 0,
+                  "the h0 rows start and end on 16-byte boundaries in shared memory");
+    if (tid == 0) {
+        h0_rows_issue(h0_bar, h0s, RP * 2, N, [&](int jr) { return h0 + static_cast<size_t>(row_of(jr >> 1, jr & 1)) * N; });
+    }
     constexpr int CELLS = RP * 2 * N;
     constexpr int ITER = (CELLS + NT - 1) / NT;
     float2 wk_of[ITER];
@@ -233,13 +303,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
             kz_of[it] = __ldg(&kvec[row]);
         }
     }
-    for (int i = tid; i < RP * 2 * (N / 2); i += NT) {
-        const int jr = i / (N / 2);
-        const int c = i % (N / 2);
-        const int row = row_of(jr >> 1, jr & 1);
-        reinterpret_cast<float4*>(h0s + jr * N)[c] =
-            __ldcs(reinterpret_cast<const float4*>(h0 + static_cast<size_t>(row) * N) + c);
-    }
+    h0_rows_wait(h0_bar, h0_parity, error);
     __syncthreads();
 
     // Evolve (src/core/evolve.cpp:28-121 and :123-184), one cell at a time.
@@ -457,12 +521,14 @@ row_pass_kernel(FrameArgs a)
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
     float2* tws = smem + S::RP * 2 * NF * seq_f2<LOG_N, false>() + S::RP * 2 * S::N;
+    __shared__ uint64_t h0_bar;
+    if (threadIdx.x == 0) h0_bar_init(&h0_bar);
     load_twiddles<LOG_N, false>(tws, a.twiddles, threadIdx.x, NT);
-    __syncthreads();  // the twiddles are complete before any transform reads them
+    __syncthreads();  // the twiddles are complete before any transform reads them; the barrier is set up
     const int o = blockIdx.y;
     row_task<LOG_N, NF, FAST>(a, a.ocean_base + o, blockIdx.x,
                               a.inter + static_cast<size_t>(o) * S::N * S::N * NF, smem, tws,
-                              threadIdx.x);
+                              threadIdx.x, &h0_bar, 0u, nullptr, a.error);
 }
 
 template <int LOG_N, int NF, bool FAST, bool FOAM>
@@ -589,6 +655,8 @@ frame_kernel(FrameArgs a, QueueArgs q)
     __shared__ unsigned* s_publish;
     __shared__ unsigned s_next;
     __shared__ int s_have_next;
+    __shared__ uint64_t h0_bar;   // the row tasks' h0 copies; phase k = k-th row task
+    uint32_t h0_parity = 0;
 
     const int tid = threadIdx.x;
     if constexpr (!TC) load_twiddles<LOG_N, TC>(tws, a.twiddles, tid, NT);
@@ -630,6 +698,7 @@ frame_kernel(FrameArgs a, QueueArgs q)
     // CTA's current task (< T), which waits on nothing later, so the queue
     // stays deadlock-free.
     if (tid == 0) {
+        h0_bar_init(&h0_bar);
         s_publish = nullptr;
         s_next = atomicAdd(q.ticket, 1u);
         s_have_next = 1;
@@ -672,7 +741,8 @@ frame_kernel(FrameArgs a, QueueArgs q)
         const int abs_ocean = a.ocean_base + static_cast<int>(ocean);
         if (row) {
             row_task<LOG_N, NF, FAST, TC>(a, abs_ocean, static_cast<int>(idx), a.inter + slot * slot_f2,
-                                          smem, tws, tid, &eng, q.error);
+                                          smem, tws, tid, &h0_bar, h0_parity, &eng, q.error);
+            h0_parity ^= 1u;
         } else {
             col_task<LOG_N, NF, FAST, FOAM, S::PW, true, TC>(a, abs_ocean, static_cast<int>(idx),
                                                              a.inter + slot * slot_f2, smem, tws, tid,

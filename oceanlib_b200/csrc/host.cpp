@@ -750,6 +750,7 @@ private:
         a.disp = disp_.p;
         a.normal = normal_.p;
         a.velocity = velocity_buf_.p;
+        a.error = error_.p;
         return a;
     }
 

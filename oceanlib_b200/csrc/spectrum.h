@@ -63,6 +63,9 @@ struct FrameArgs {
     // constants) and the batch arrays above are unused, except t_over_2pi
     // (indexed by i) and the intermediate. No persistent foam in this form.
     const OceanSlot* table;
+    // Sticky error word of the row / column passes (a bounded wait that gave
+    // up sets it); may be null. The persistent kernel uses QueueArgs::error.
+    unsigned* error;
 };
 
 // Work queue of the persistent frame kernel. `ticket`, `rows_done[count]` and
