@@ -311,6 +311,59 @@ def bench_cascade(torch, queries: int = 1_000_000, frames: int = 50):
     return res
 
 
+def bench_large_sizes(torch, frames: int = 10):
+    """N = 2048 and 4096, the reference's largest sizes (three launches per
+    frame): device time per update with velocity on, oceans resident in HBM,
+    frames back to back."""
+    import oceanlib_b200 as ob
+
+    res = {}
+    stream = torch.cuda.Stream()
+    sh = stream.cuda_stream
+    for n, count in ((2048, 4), (4096, 1)):
+        descs = [ob.OceanDesc(size=n, patch_length=0.8 * n, wind_speed=15.0, seed=9 + k, compute_velocity=True)
+                 for k in range(count)]
+        b = ob.OceanBatch(descs)
+        for k in range(3):
+            b.update([1.0 + k / 60.0], stream=sh)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(frames):
+            b.update([2.0 + k / 60.0], stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / frames
+        alg = 56 * n * n  # h0 in; displacement, normal and velocity out
+        res[str(n)] = {"workload": f"{count} x {n}^2, L = {0.8 * n:.0f} m, U = 15 m/s, velocity on",
+                       "updates_per_s": count * 1000.0 / ms, "ms_per_frame": ms,
+                       "gpu_launches_per_frame": 3, "alg_bytes_per_update": alg,
+                       "achieved_gbs": alg * count / (ms / 1000.0) / 1e9}
+        b.close()
+    return res
+
+
+def bench_large_reference(seconds: float = 2.0):
+    """The reference Ocean at the same large descriptors, its thread pool over
+    all hardware threads."""
+    import oracle as O
+    from oceanlib_b200 import OceanDesc
+
+    res = {}
+    for n in (2048, 4096):
+        ro = O.RefOcean(OceanDesc(size=n, patch_length=0.8 * n, wind_speed=15.0, seed=9, compute_velocity=True))
+        ro.update(1.0)
+        t0 = time.perf_counter()
+        k = 0
+        while time.perf_counter() - t0 < seconds / 2 or k < 2:
+            ro.update(2.0 + k / 60.0)
+            k += 1
+        res[str(n)] = {"updates_per_s": k / (time.perf_counter() - t0), "frames": k,
+                       "threads": int(O.ref().oref_hardware_concurrency())}
+        ro.close()
+    return res
+
+
 def bench_ensemble(torch, frames: int = 30):
     """64 seeded sea states of uneven N (64..1024), schedule picked by the
     autotuner; one frame = every ocean advanced once."""
@@ -859,13 +912,15 @@ def main():
             plain_cpu = 0.0 if args.no_cpu_baseline else 4.0
             for name, fn in (("bench_update_512", lambda: bench_plain_update(torch, cpu_seconds=plain_cpu)),
                              ("cascade", lambda: bench_cascade(torch)), ("iwave", bench_iwave),
-                             ("ensemble", lambda: bench_ensemble(torch)), ("serving", bench_serving)):
+                             ("ensemble", lambda: bench_ensemble(torch)), ("serving", bench_serving),
+                             ("large_sizes", lambda: bench_large_sizes(torch))):
                 try:
                     extra[name] = fn()
                 except Exception as e:  # report, do not lose the headline line
                     extra[name] = {"error": str(e)}
             if not args.no_cpu_baseline:
-                for name, fn in (("cascade", bench_cascade_reference), ("iwave", bench_iwave_reference)):
+                for name, fn in (("cascade", bench_cascade_reference), ("iwave", bench_iwave_reference),
+                                 ("large_sizes", bench_large_reference)):
                     try:
                         extra[name]["reference_cpu"] = fn()
                     except Exception as e:
