@@ -718,10 +718,11 @@ OCEAN_API ocean_status ocean_frame_static_scratch(uint32_t size, float patch_len
                                                   float* displacement, float* normal,
                                                   float* velocity, void* stream);
 
-/* Runs the persistent kernel's bounded wait on a counter that nothing
- * increments, with the given limit, and reports OCEAN_ERROR_TIMEOUT when the
- * wait gave up and returned (the expected outcome) - a self-test of the
- * timeout path that leaves the device usable. */
+/* Runs the frame kernels' bounded waits with the given limit on things that
+ * never complete - the work queue's wait on a counter nothing increments and
+ * the h0 copy's wait on an mbarrier nothing arrives at - and reports
+ * OCEAN_ERROR_TIMEOUT when both gave up and returned (the expected outcome):
+ * a self-test of the timeout paths that leaves the device usable. */
 OCEAN_API ocean_status ocean_check_bounded_wait(uint32_t timeout_ms);
 
 /* Synchronous copy of `bytes` from a device pointer this library handed out

@@ -215,9 +215,10 @@ __device__ __forceinline__ void h0_rows_issue(uint64_t* bar, float2* dst, int ro
     }
 }
 
-// Every thread: wait for phase `parity` of `bar`, for at most kH0WaitNs;
+// Every thread: wait for phase `parity` of `bar`, for at most limit_ns;
 // then the error word is set (when there is one) and the task goes on.
-__device__ __forceinline__ void h0_rows_wait(uint64_t* bar, uint32_t parity, unsigned* error)
+__device__ __forceinline__ void h0_rows_wait(uint64_t* bar, uint32_t parity, unsigned* error,
+                                             unsigned long long limit_ns = kH0WaitNs)
 {
     const uint32_t b = smem_addr(bar);
     unsigned long long t0 = 0;
@@ -232,7 +233,7 @@ __device__ __forceinline__ void h0_rows_wait(uint64_t* bar, uint32_t parity, uns
             : "memory");
         if (done) return;
         if (spin == 0) t0 = tc::now_ns();
-        if ((spin & 63) == 63 && tc::now_ns() - t0 > kH0WaitNs) {
+        if ((spin & 63) == 63 && tc::now_ns() - t0 > limit_ns) {
             if (error != nullptr) atomicCAS(error, 0u, 1u);
             return;
         }
@@ -752,12 +753,20 @@ frame_kernel(FrameArgs a, QueueArgs q)
     if constexpr (TC) eng.release(tid);
 }
 
-// A single bounded wait on a counter that nothing increments: exercises the
-// timeout path of wait_at_least on its own.
+// Bounded waits that nothing completes, each of which must give up after
+// limit_ns and set its error word: the queue's wait on a counter nothing
+// increments (wait_at_least), and the h0 copy's wait on an mbarrier no
+// thread arrives at and no copy targets (h0_rows_wait).
 __global__ void wait_probe_kernel(const unsigned* counter, unsigned target, unsigned* error,
-                                  unsigned long long limit_ns)
+                                  unsigned* bar_error, unsigned long long limit_ns)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0) wait_at_least(counter, target, error, limit_ns);
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) h0_bar_init(&bar);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        wait_at_least(counter, target, error, limit_ns);
+        h0_rows_wait(&bar, 0u, bar_error, limit_ns);
+    }
 }
 
 __global__ void foam_step_kernel(int n, int count, const float4* __restrict__ disp,
@@ -1005,10 +1014,10 @@ cudaError_t launch_frame(int log_n, int nf, int form, bool fuse_foam, const Fram
                           [&](auto L) { return decltype(L)::launch(a, q, grid, st); });
 }
 
-cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned* error,
+cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned* error, unsigned* bar_error,
                               unsigned long long limit_ns, cudaStream_t stream)
 {
-    wait_probe_kernel<<<1, 32, 0, stream>>>(counter, target, error, limit_ns);
+    wait_probe_kernel<<<1, 32, 0, stream>>>(counter, target, error, bar_error, limit_ns);
     return cudaGetLastError();
 }
 

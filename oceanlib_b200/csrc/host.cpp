@@ -1925,15 +1925,17 @@ ocean_status ocean_check_bounded_wait(uint32_t timeout_ms)
 {
     return guarded([&] {
         unsigned* d = nullptr;
-        ocean_b200::check(cudaMalloc(&d, 2 * sizeof(unsigned)), "cudaMalloc");
-        unsigned h[2] = {0, 0};
-        cudaError_t e = cudaMemset(d, 0, 2 * sizeof(unsigned));
+        ocean_b200::check(cudaMalloc(&d, 3 * sizeof(unsigned)), "cudaMalloc");
+        unsigned h[3] = {0, 0, 0};
+        cudaError_t e = cudaMemset(d, 0, 3 * sizeof(unsigned));
         if (e == cudaSuccess)
-            e = ocean_b200::launch_wait_probe(d, 1u, d + 1, uint64_t(timeout_ms) * 1000000ull, nullptr);
+            e = ocean_b200::launch_wait_probe(d, 1u, d + 1, d + 2, uint64_t(timeout_ms) * 1000000ull, nullptr);
         if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
         cudaFree(d);
         ocean_b200::check(e, "wait probe");
-        if (h[1] != 0) throw ocean_b200::TimeoutError();
+        // Both waits must give up: the timeout status is the expected outcome.
+        if (h[1] != 0 && h[2] != 0) throw ocean_b200::TimeoutError();
+        if (h[1] != 0 || h[2] != 0) throw std::runtime_error("only one bounded wait gave up");
     });
 }
 

@@ -87,8 +87,10 @@ cudaError_t launch_frame(int log_n, int nf, int form, bool fuse_foam, const Fram
                          const QueueArgs& q, int grid, cudaStream_t stream);
 // Resident CTAs per SM of the persistent frame kernel (0: no such variant).
 int frame_blocks_per_sm(int log_n, int nf, int form, bool fuse_foam);
-// A bounded wait on `counter` that nothing increments (tests the timeout path).
-cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned* error,
+// Bounded waits that nothing completes (tests the timeout paths): on
+// `counter`, which nothing increments, setting *error, and on an mbarrier
+// nothing arrives at, setting *bar_error.
+cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned* error, unsigned* bar_error,
                               unsigned long long limit_ns, cudaStream_t stream);
 
 // Row pass (evolve + row FFTs) and column pass (column FFTs + finalize, with

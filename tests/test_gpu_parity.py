@@ -325,8 +325,9 @@ def test_single_ocean_update_uses_persistent_frame_and_matches_oracle():
 
 
 def test_bounded_wait_gives_up_and_device_stays_usable():
-    # The persistent kernel's waits are bounded: a wait on a counter nothing
-    # increments returns after its limit with a timeout status ...
+    # The frame kernels' waits are bounded: a wait on a counter nothing
+    # increments and one on an mbarrier nothing arrives at both return after
+    # their limit, with a timeout status ...
     assert ob.lib().ocean_check_bounded_wait(50) == abi.OCEAN_ERROR_TIMEOUT
     # ... and the context is still healthy afterwards.
     desc = ob.OceanDesc(size=64, seed=5)
