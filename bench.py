@@ -865,6 +865,10 @@ def main():
                     "traffic": None if traffic is None else traffic.get("frame_bytes_per_launch"),
                     "frame": {"achieved": frame_achieved, "frac": frame_achieved / peak,
                               "alg_bytes_per_update": ALG_BYTES_PER_CELL * CELLS}}
+            # The unit that bounds this kernel, from the committed ncu capture of
+            # the same kernel and workload (HBM is not it).
+            if traffic is not None and "binding_unit" in traffic:
+                roof["binding_unit"] = traffic["binding_unit"]
         else:
             col_launch_ms = prof["col_ms"] / max(1, prof["col_launches"])
             row_launch_ms = prof["row_ms"] / max(1, prof["row_launches"])
