@@ -1,7 +1,9 @@
 """The C-ABI library without a GPU: it loads, exports every symbol the header
 declares, keeps the reference's struct layouts, and its host-side behaviour
 (status codes, NULL tolerance, struct_size versioning, level forcing) matches
-the reference's C ABI tests (tests/test_c_api.cpp). No device work is done."""
+the reference's C ABI tests (tests/test_c_api.cpp). No device work is done
+without a GPU: a descriptor that passes the checks then fails to create. Where
+a GPU is present, the valid-size test does create, then destroy, its oceans."""
 import ctypes as C
 import json
 import re
@@ -75,6 +77,20 @@ def test_desc_init_defaults_match_reference():
     assert abs(d.spectrum.gravity - 9.81) < 1e-6 and d.spectrum.small_wave_cutoff == 0.5
     assert d.choppiness == 1.0 and d.foam_threshold == 0.5 and d.seed == 1337
     assert d.water_depth == 0.0 and d.compute_velocity == 0 and not d.parallel_for
+
+
+@pytest.mark.parametrize("size", [16, 1024, 2048, 4096])
+def test_every_reference_size_passes_validation(size):
+    # src/ocean.cpp:28-59: N is a power of two in [16, 4096]. Past the
+    # descriptor checks, a create without a GPU fails on the device instead.
+    d = abi.OceanDescC()
+    ob.lib().ocean_desc_init(C.byref(d))
+    d.size = size
+    st = C.c_int(-1)
+    h = ob.lib().ocean_create(C.byref(d), C.byref(st))
+    assert st.value != abi.OCEAN_ERROR_INVALID_ARG
+    if h:
+        ob.lib().ocean_destroy(h)
 
 
 @pytest.mark.parametrize("mutate", [
