@@ -212,8 +212,10 @@ def test_foam_substep_clamp_and_zero_steps():
     batch.close()
 
 
-def test_parallel_for_hook_called_four_times_per_frame():
-    # tests/test_c_api.cpp:370-392
+@pytest.mark.parametrize("size", [64, 2048])
+def test_parallel_for_hook_called_four_times_per_frame(size):
+    # tests/test_c_api.cpp:370-392; at 2048 the stages are the three-pass
+    # schedule's launches.
     calls = []
 
     @abi.PARALLEL_FOR_FN
@@ -222,7 +224,7 @@ def test_parallel_for_hook_called_four_times_per_frame():
         for i in range(count):
             task(ctx, i)
 
-    desc = ob.OceanDesc(size=64, seed=9)
+    desc = ob.OceanDesc(size=size, patch_length=3.0 * size, seed=9)
     cd = desc.to_c()
     cd.parallel_for = C.cast(hook, C.c_void_p)
     oc = ob.Ocean(cd)
