@@ -217,6 +217,9 @@ def reference_rate(seconds: float, warm: int = 2, threads: int = 0):
     return done / el, cores, done
 
 
+REF_TIMED_S = 2.5  # seconds the reference arm's timed steps span together
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -231,12 +234,22 @@ def run_reference_arm(args, rank, world):
     rf = O.RefFoam(ro, W.foam_desc())
     cores = int(O.ref().oref_hardware_concurrency())
     dt = W.FOAM_DT
-    per_step = 4  # frames of one ocean per step: a bounded sample of the batch frame
+    # Warm-up: at least W x 4 frames and 0.5 s, so the reference's thread pool
+    # is running at speed; its rate sets the frames per step.
     frame = 0
-    for _ in range(args.warmup * per_step):
+    t0 = time.perf_counter()
+    while True:
         frame += 1
         ro.update(frame * dt)
         rf.update(dt)
+        el = time.perf_counter() - t0
+        if frame >= args.warmup * 4 and el >= 0.5:
+            break
+    rate = frame / el
+    # Frames of one ocean per step (a bounded sample of the batch frame):
+    # enough for the K timed steps to span about REF_TIMED_S seconds, so the
+    # figure is a steady rate and not a start-up transient.
+    per_step = max(4, int(np.ceil(rate * REF_TIMED_S / max(1, args.steps))))
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()

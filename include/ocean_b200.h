@@ -710,13 +710,34 @@ OCEAN_API uint64_t ocean_batch_launch_count(const ocean_batch* batch);
  * is limited to 16..512; larger N returns OCEAN_ERROR_INVALID_ARG. All calls
  * on a device share that array: calls whose GPU work overlaps (e.g. on two
  * streams) race and corrupt each other. The first call on a device looks up
- * the array's device address, so make it before any stream capture. Work is
- * queued on `stream` (a cudaStream_t, NULL = legacy default stream). */
+ * the array's device address (a CUDA runtime query), so make that first call
+ * before any stream capture begins. Work is queued on `stream` (a
+ * cudaStream_t, NULL = legacy default stream). A buffer that is NULL (other
+ * than velocity) or not 16-byte aligned returns OCEAN_ERROR_INVALID_ARG
+ * before anything is queued. The call returns once the work is queued; a
+ * bounded device wait that gave up during the frame is reported by
+ * ocean_frame_static_scratch_status. */
 OCEAN_API ocean_status ocean_frame_static_scratch(uint32_t size, float patch_length, double time,
                                                   float choppiness, float foam_threshold,
                                                   const float* h0, const float* omega_kinv,
                                                   float* displacement, float* normal,
                                                   float* velocity, void* stream);
+
+/* Status of the last ocean_frame_static_scratch call on the current device:
+ * waits for `stream` (the stream that call used), then returns OCEAN_OK, or
+ * OCEAN_ERROR_TIMEOUT if a bounded wait of that frame gave up (its outputs
+ * are then not valid). The word lives in the same static array and each
+ * frame call clears it, so read it before the next call. Allocates nothing.
+ * No counterpart in the reference. */
+OCEAN_API ocean_status ocean_frame_static_scratch_status(void* stream);
+
+/* Self-test of that status word: runs the frame's bounded mbarrier wait
+ * (the h0 copy's wait) on a barrier nothing arrives at, with the static
+ * array's status word as its error word, for `timeout_ms`, then returns what
+ * ocean_frame_static_scratch_status reads: OCEAN_ERROR_TIMEOUT is the
+ * expected outcome. Leaves the device usable; the next frame call clears
+ * the word. */
+OCEAN_API ocean_status ocean_check_static_scratch_status(uint32_t timeout_ms);
 
 /* Runs the frame kernels' bounded waits with the given limit on things that
  * never complete - the work queue's wait on a counter nothing increments and

@@ -268,6 +268,8 @@ SIGNATURES = {
     "ocean_frame_static_scratch": (C.c_int, [C.c_uint32, C.c_float, C.c_double, C.c_float,
                                              C.c_float, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ocean_frame_static_scratch_status": (C.c_int, [C.c_void_p]),
+    "ocean_check_static_scratch_status": (C.c_int, [C.c_uint32]),
     "ocean_ensemble_create": (C.c_void_p, [C.POINTER(OceanDescC), C.c_uint32, C.c_int32,
                                            C.POINTER(C.c_int)]),
     "ocean_ensemble_destroy": (None, [C.c_void_p]),

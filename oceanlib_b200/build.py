@@ -25,7 +25,7 @@ LIB = PKG / "libocean_b200.so"
 INCLUDE = PKG.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-prec-div=true",
+COMMON = ["-O3", "-std=c++20", "-lineinfo", "-fmad=false", "-prec-div=true",
           "-prec-sqrt=true", "-ftz=false", "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off",
           f"-I{INCLUDE}", f"-I{CSRC}"]
 

@@ -15,12 +15,20 @@
 // process exits. All calls on one device share it: two calls whose work
 // overlaps on the GPU (for example on two different streams) race on it and
 // corrupt each other's results. Nothing in it needs to start at zero: each
-// call rewrites the whole header and the row pass overwrites every
-// intermediate value before the column pass reads it.
+// call rewrites the whole header (its status word included, cleared to zero)
+// and the row pass overwrites every intermediate value before the column
+// pass reads it.
+//
+// The status word: the row pass's h0 copy completes on an mbarrier whose
+// wait is bounded (1 s). A wait that gives up sets the word, and the frame's
+// outputs are then not to be trusted. The call itself cannot see that (it
+// returns when the work is queued), so ocean_frame_static_scratch_status
+// waits for the stream and reads the word.
 #include "../../include/ocean_b200.h"
 #include "spectrum.h"
 
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <mutex>
 
@@ -29,6 +37,9 @@ namespace {
 // Layout of the static array (bytes):
 //   [0, 16)        OceanConsts of the frame
 //   [16, 24)       t / (2 pi)
+//   [24, 28)       status word: 0, or 1 once a bounded wait gave up
+//   [28, 32)       zero (the self-test's counter that nothing increments)
+//   [32, 36)       the self-test's scratch error word
 //   [256, 8448)    per-stage twiddles, N - 1 float2 (N <= 1024 fits)
 //   [8448, 12544)  signed wavenumbers, N floats
 //   [12544, ...)   row-pass intermediate, N * N * fields float2
@@ -81,7 +92,28 @@ int log2_exact(uint32_t v)
 struct Header {
     ocean_b200::OceanConsts consts;
     double t_over_2pi;
+    unsigned status;
+    unsigned zero;
 };
+static_assert(offsetof(Header, status) == 24 && sizeof(Header) == 32, "header layout");
+constexpr size_t kProbeErrorOffset = 32;
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Waits for `stream` and reads the status word of the current device's array.
+ocean_status read_status(cudaStream_t st)
+{
+    unsigned char* scratch = nullptr;
+    if (scratch_address(&scratch) != cudaSuccess) return OCEAN_ERROR_DEVICE;
+    unsigned word = 0;
+    // A device-to-pageable copy returns once it has been made, after the
+    // stream's earlier work; the synchronise also surfaces any launch error.
+    if (cudaMemcpyAsync(&word, scratch + offsetof(Header, status), sizeof(word), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return OCEAN_ERROR_DEVICE;
+    return word != 0 ? OCEAN_ERROR_TIMEOUT : OCEAN_OK;
+}
 
 }  // namespace
 
@@ -94,6 +126,12 @@ extern "C" OCEAN_API ocean_status ocean_frame_static_scratch(
     if (!pow2 || size < 16 || size > kMaxStaticSize) return OCEAN_ERROR_INVALID_ARG;
     if (!(patch_length > 0.0f) || !(choppiness >= 0.0f)) return OCEAN_ERROR_INVALID_ARG;
     if (h0 == nullptr || omega_kinv == nullptr || displacement == nullptr || normal == nullptr)
+        return OCEAN_ERROR_INVALID_ARG;
+    // h0 rows arrive by bulk copies (16-byte aligned sources) and the outputs
+    // are written as float4: a misaligned buffer is refused here, before any
+    // work is queued, instead of faulting on the device.
+    if (!aligned16(h0) || !aligned16(omega_kinv) || !aligned16(displacement) || !aligned16(normal) ||
+        (velocity != nullptr && !aligned16(velocity)))
         return OCEAN_ERROR_INVALID_ARG;
     const int nf = velocity != nullptr ? 6 : 4;
     const size_t inter_bytes = size_t(size) * size * nf * sizeof(float2);
@@ -113,6 +151,8 @@ extern "C" OCEAN_API ocean_status ocean_frame_static_scratch(
     hdr.consts.inv_threshold = (foam_threshold > 1e-6f) ? (1.0f / foam_threshold) : 0.0f;
     hdr.consts.geom = 0;
     hdr.t_over_2pi = time * 0.159154943091895335769;
+    hdr.status = 0;
+    hdr.zero = 0;
 
     float2 base[kMaxStaticSize / 2];
     float2 tw[kMaxStaticSize];
@@ -155,8 +195,31 @@ extern "C" OCEAN_API ocean_status ocean_frame_static_scratch(
     a.velocity = reinterpret_cast<float4*>(velocity);
     a.ocean_base = 0;
     a.chunk = 1;
+    a.error = reinterpret_cast<unsigned*>(scratch + offsetof(Header, status));
     if (ocean_b200::launch_row_pass(log_n, nf, false, a, st) != cudaSuccess) return OCEAN_ERROR_DEVICE;
     if (ocean_b200::launch_col_pass(log_n, nf, false, false, a, st) != cudaSuccess)
         return OCEAN_ERROR_DEVICE;
     return OCEAN_OK;
+}
+
+extern "C" OCEAN_API ocean_status ocean_frame_static_scratch_status(void* stream)
+{
+    return read_status(static_cast<cudaStream_t>(stream));
+}
+
+extern "C" OCEAN_API ocean_status ocean_check_static_scratch_status(uint32_t timeout_ms)
+{
+    unsigned char* scratch = nullptr;
+    if (scratch_address(&scratch) != cudaSuccess) return OCEAN_ERROR_DEVICE;
+    // The probe's counter is the header's zero word (nothing increments it)
+    // and its mbarrier wait reports into the status word.
+    unsigned* status = reinterpret_cast<unsigned*>(scratch + offsetof(Header, status));
+    if (cudaMemset(status, 0, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(scratch + kProbeErrorOffset, 0, sizeof(unsigned)) != cudaSuccess)
+        return OCEAN_ERROR_DEVICE;
+    if (ocean_b200::launch_wait_probe(reinterpret_cast<const unsigned*>(scratch + offsetof(Header, zero)), 1u,
+                                      reinterpret_cast<unsigned*>(scratch + kProbeErrorOffset), status,
+                                      uint64_t(timeout_ms) * 1000000ull, nullptr) != cudaSuccess)
+        return OCEAN_ERROR_DEVICE;
+    return read_status(nullptr);
 }

@@ -24,7 +24,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libocean_ref.so"
-REF_SRC = Path(os.environ.get("OCEAN_REF_SRC", "/root/reference"))
+# The reference checkout: $OCEAN_REF_SRC, else a "reference" directory beside
+# this repository.
+REF_SRC = Path(os.environ.get("OCEAN_REF_SRC", str(HERE.parent.parent / "reference")))
 
 
 class OrDesc(C.Structure):

@@ -27,8 +27,18 @@ def _bits(a):
     return np.ascontiguousarray(a).view(np.uint32)
 
 
-@pytest.mark.parametrize("make", [W.foam_patch_512, lambda: W.single_patch_256()[0]],
-                         ids=["512_velocity", "256_plain"])
+def _small(size, velocity):
+    return lambda: ob.OceanDesc(size=size, patch_length=40.0 * size / 16, wind_speed=11.0,
+                                choppiness=1.3, seed=900 + size, compute_velocity=velocity)
+
+
+# 16 and 64 take other stage offsets and lane layouts than 256 and 512
+# (single sequences vs pairs, one or several stage blocks).
+@pytest.mark.parametrize("make", [W.foam_patch_512, lambda: W.single_patch_256()[0],
+                                  _small(16, True), _small(16, False), _small(64, True),
+                                  _small(64, False)],
+                         ids=["512_velocity", "256_plain", "16_velocity", "16_plain",
+                              "64_velocity", "64_plain"])
 def test_static_scratch_frame_matches_batch_entry_point(cuda_device, make):
     import torch
 
@@ -55,6 +65,8 @@ def test_static_scratch_frame_matches_batch_entry_point(cuda_device, make):
             h0_d.data_ptr(), wk_d.data_ptr(), disp_d.data_ptr(), nrm_d.data_ptr(),
             None if vel_d is None else vel_d.data_ptr(), C.c_void_p(stream.cuda_stream))
         assert st == abi.OCEAN_OK, ob.status_string(st)
+        st = ob.lib().ocean_frame_static_scratch_status(C.c_void_p(stream.cuda_stream))
+        assert st == abi.OCEAN_OK, ob.status_string(st)
         torch.cuda.synchronize()
         batch.update_host([t], 0.0, want_d, want_n, want_v)
         assert np.array_equal(_bits(disp_d.cpu().numpy()), _bits(want_d)), t
@@ -71,3 +83,34 @@ def test_static_scratch_rejects_sizes_beyond_its_array(cuda_device):
         assert st == abi.OCEAN_ERROR_INVALID_ARG, bad
     st = lib.ocean_frame_static_scratch(256, 100.0, 1.0, 1.0, 0.5, None, 16, 16, 16, None, None)
     assert st == abi.OCEAN_ERROR_INVALID_ARG
+    # Buffers off a 16-byte boundary are refused before anything is queued
+    # (the values are never dereferenced: the call returns first).
+    for k in range(5):
+        ptrs = [4096, 4096, 4096, 4096, 4096]
+        ptrs[k] += 8
+        st = lib.ocean_frame_static_scratch(256, 100.0, 1.0, 1.0, 0.5, *ptrs, None)
+        assert st == abi.OCEAN_ERROR_INVALID_ARG, k
+
+
+def test_static_scratch_status_reports_a_bounded_wait_that_gave_up(cuda_device):
+    """The frame's h0-copy wait, run on an mbarrier nothing arrives at with the
+    static array's status word as its error word, gives up after 50 ms; the
+    status query then reports OCEAN_ERROR_TIMEOUT, the device stays usable,
+    and the next frame call clears the word."""
+    import torch
+
+    lib = ob.lib()
+    assert lib.ocean_check_static_scratch_status(50) == abi.OCEAN_ERROR_TIMEOUT
+    assert lib.ocean_frame_static_scratch_status(None) == abi.OCEAN_ERROR_TIMEOUT
+    desc = _small(16, False)()
+    batch = ob.OceanBatch([desc])
+    h0, wk = batch.read_spectrum(0)
+    h0_d = torch.from_numpy(h0).cuda()
+    wk_d = torch.from_numpy(wk).cuda()
+    out = torch.empty((2, 16 * 16, 4), dtype=torch.float32, device="cuda")
+    st = lib.ocean_frame_static_scratch(16, desc.patch_length, 1.0, desc.choppiness, desc.foam_threshold,
+                                        h0_d.data_ptr(), wk_d.data_ptr(), out[0].data_ptr(),
+                                        out[1].data_ptr(), None, None)
+    assert st == abi.OCEAN_OK
+    assert lib.ocean_frame_static_scratch_status(None) == abi.OCEAN_OK
+    batch.close()
