@@ -528,6 +528,21 @@ OCEAN_API const float* ocean_interaction_device_field(const ocean_interaction* f
 OCEAN_API uint32_t ocean_interaction_last_substeps(const ocean_interaction* field);
 OCEAN_API int32_t ocean_interaction_last_clamped(const ocean_interaction* field);
 
+/* The whole-cell shift the last ocean_interaction_recenter applied (both 0
+ * when it did not move): InteractionField::last_shift_x / last_shift_z,
+ * include/ocean/interaction.hpp:300-301. */
+OCEAN_API void ocean_interaction_last_shift(const ocean_interaction* field, int32_t* dx, int32_t* dz);
+
+/* The obstruction tables the last ocean_interaction_set_obstruction (or
+ * recentre) built on the device: the solid cells in index order
+ * (*solid_count of them; `solid` holds up to N*N entries) and, per cell, the
+ * index of the fluid cell a solid cell copies under the Neumann condition
+ * (itself for fluid cells, 0xFFFFFFFF where no fluid is reachable), as the
+ * reference's multi-source BFS assigns them (src/interaction.cpp:255-292).
+ * Either array may be NULL; *solid_count is 0 without an obstruction. */
+OCEAN_API ocean_status ocean_interaction_obstruction_tables(const ocean_interaction* field, uint32_t* solid,
+                                                            uint32_t* nearest, uint32_t* solid_count);
+
 /* Discrete energy the undamped leapfrog conserves (InteractionField::energy,
  * src/interaction.cpp:803-846), evaluated on the device. */
 OCEAN_API double ocean_interaction_energy(const ocean_interaction* field);

@@ -304,6 +304,8 @@ SIGNATURES = {
     "ocean_interaction_dispersion_error": (C.c_float, [C.c_void_p]),
     "ocean_sample_combined": (None, [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.POINTER(SurfaceEx)]),
     "ocean_interaction_device_field": (C.c_void_p, [C.c_void_p]),
+    "ocean_interaction_obstruction_tables": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]),
+    "ocean_interaction_last_shift": (None, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "ocean_interaction_last_substeps": (C.c_uint32, [C.c_void_p]),
     "ocean_interaction_last_clamped": (C.c_int32, [C.c_void_p]),
     "ocean_interaction_energy": (C.c_double, [C.c_void_p]),

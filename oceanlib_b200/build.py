@@ -42,7 +42,8 @@ def sources() -> list[Path]:
 
 
 def headers() -> list[Path]:
-    return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h")))
+    return sorted(list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h")) +
+                  list(INCLUDE.glob("ocean/*")))
 
 
 def _compile(src: Path, force: bool, verbose: bool) -> Path:

@@ -43,10 +43,35 @@ struct Shape {
     // rows of the intermediate); 2 at N = 1024, where 32 values per lane
     // leave room for fewer threads only.
     static constexpr int W = LOG_N >= 10 ? 2 : cmin(N, (128 / G) > 4 ? 128 / G : 4);
-    // columns / task of the persistent kernel: 2*RP, so a row task and a
-    // column task use the same thread count (2 * NF * G * RP).
-    static constexpr int PW = 2 * RP;
 };
+
+// Which rows a row task owns. Paired (ROWS = 2 RP): RP row pairs (p, N-p),
+// each row's h0(-k) read from the other row of its pair, already staged
+// (rows 0 and N/2 are their own mirrors). Single (ROWS = RP): RP rows, each
+// staged with a copy of its mirror row (N - y) mod N beside it - twice the h0
+// reads (the second from L2: the mirror row's own task is the neighbouring
+// ticket) for half the CTA. At N = 512 and 1024 a row pair fills a whole
+// 384-thread CTA (256 without velocity); single rows make the persistent
+// kernel's CTAs half that size, so twice as many independent CTAs share each
+// SM and one CTA's barriers and load waits idle fewer warps. Column tasks
+// cover PW = ROWS columns, so both task kinds have the same thread count.
+template <int LOG_N, bool SINGLE_ROWS>
+struct RowSched {
+    static constexpr bool SINGLE = SINGLE_ROWS;
+    static constexpr int ROWS = SINGLE ? Shape<LOG_N>::RP : 2 * Shape<LOG_N>::RP;  // rows per row task
+    static constexpr int H0ROWS = SINGLE ? 2 * ROWS : ROWS;                         // h0 rows staged
+    static constexpr int PW = ROWS;                                                  // columns per column task
+    static constexpr int RT = (1 << LOG_N) / ROWS;                                   // row tasks per ocean
+};
+// The persistent kernel's choice: single rows at N >= 512 (FP32 forms; the
+// tensor-core engine is built for a row pair's sequences).
+template <int LOG_N, bool TC>
+__host__ __device__ constexpr bool single_rows()
+{
+    return !TC && LOG_N >= 9;
+}
+template <int LOG_N, bool TC>
+using FrameSched = RowSched<LOG_N, single_rows<LOG_N, TC>()>;
 
 // Shared-memory layouts of the sequences a task transforms. Paired: fields
 // 2p and 2p+1 of a row or column as one pair (float4 per index, stride SEQ4
@@ -240,21 +265,21 @@ __device__ __forceinline__ void h0_rows_wait(uint64_t* bar, uint32_t parity, uns
     }
 }
 
-template <int LOG_N, int NF, bool FAST, bool TC = false>
+template <int LOG_N, int NF, bool FAST, bool TC = false, class D = RowSched<LOG_N, false>>
 __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int group,
                                          float2* __restrict__ inter_slot, float2* smem,
                                          const float2* tws, int tid, uint64_t* h0_bar, uint32_t h0_parity,
                                          TcEngine<NF>* eng = nullptr, unsigned* error = nullptr)
 {
     using S = Shape<LOG_N>;
-    constexpr int N = S::N, G = S::G, SEQ = S::SEQ, SEQ4 = S::SEQ4, RP = S::RP;
-    constexpr int NT = RP * 2 * NF * G;
+    constexpr int N = S::N, G = S::G, SEQ = S::SEQ, SEQ4 = S::SEQ4, ROWS = D::ROWS;
+    constexpr int NT = ROWS * NF * G;
     constexpr int Q = NF / 2;
     constexpr bool PAIRED = paired<LOG_N, TC>();
 
-    float2* data = smem;                                   // sequences of rows (j, r), fields f
-    float4* data4 = reinterpret_cast<float4*>(smem);       // the same as pairs (j, r, f / 2)
-    float2* h0s = data + RP * 2 * NF * seq_f2<LOG_N, TC>();  // [RP*2][N]
+    float2* data = smem;                                   // sequences of rows jr, fields f
+    float4* data4 = reinterpret_cast<float4*>(smem);       // the same as pairs (jr, f / 2)
+    float2* h0s = data + ROWS * NF * seq_f2<LOG_N, TC>();  // [H0ROWS][N]
 
     OceanConsts cst;
     const float2* geom;
@@ -274,21 +299,47 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     }
     const double top = a.t_over_2pi[ocean];
 
-    // Rows handled by pair slot j: (p, N-p), or (0, N/2) for p = 0.
-    auto row_of = [&](int j, int r) -> int {
-        const int p = group * RP + j;
+    // Row of slot jr: pair p = (jr's pair index) covers (p, N-p), or (0, N/2)
+    // for p = 0. Paired tasks hold whole pairs (slot jr = 2 j + r); single-row
+    // tasks take consecutive rows of that order, so a row and its mirror are
+    // neighbouring tasks.
+    auto row_of = [&](int jr) -> int {
+        int p, r;
+        if constexpr (D::SINGLE) {
+            const int idx = group * ROWS + jr;
+            p = idx >> 1;
+            r = idx & 1;
+        } else {
+            p = group * S::RP + (jr >> 1);
+            r = jr & 1;
+        }
         if (p == 0) return r ? N / 2 : 0;
         return r ? N - p : p;
+    };
+    // Staged h0 row holding h0(-k) for slot jr's row: single rows keep a copy
+    // of the mirror row in slot ROWS + jr; a pair's other row is the mirror
+    // (rows 0 and N/2 mirror themselves).
+    auto mirror_slot = [&](int jr) -> int {
+        if constexpr (D::SINGLE) {
+            return ROWS + jr;
+        } else {
+            const int p = group * S::RP + (jr >> 1);
+            const int r = jr & 1;
+            return (jr & ~1) + ((p == 0) ? r : 1 - r);
+        }
     };
 
     // The h0 rows go first (bulk copies), then every thread loads the
     // geometry of its cells, so both latencies overlap ahead of the wait.
-    static_assert((RP * 2 * NF * seq_f2<LOG_N, TC>() * sizeof(float2)) % 16 == 0 && (N * sizeof(float2)) % 16 == 0,
+    static_assert((ROWS * NF * seq_f2<LOG_N, TC>() * sizeof(float2)) % 16 == 0 && (N * sizeof(float2)) % 16 == 0,
                   "the h0 rows start and end on 16-byte boundaries in shared memory");
     if (tid == 0) {
-        h0_rows_issue(h0_bar, h0s, RP * 2, N, [&](int jr) { return h0 + static_cast<size_t>(row_of(jr >> 1, jr & 1)) * N; });
+        h0_rows_issue(h0_bar, h0s, D::H0ROWS, N, [&](int k) {
+            const int row = k < ROWS ? row_of(k) : ((N - row_of(k - ROWS)) & (N - 1));
+            return h0 + static_cast<size_t>(row) * N;
+        });
     }
-    constexpr int CELLS = RP * 2 * N;
+    constexpr int CELLS = ROWS * N;
     constexpr int ITER = (CELLS + NT - 1) / NT;
     float2 wk_of[ITER];
     float kx_of[ITER], kz_of[ITER];
@@ -298,7 +349,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         if (cell < CELLS) {
             const int jr = cell >> LOG_N;
             const int x = cell & (N - 1);
-            const int row = row_of(jr >> 1, jr & 1);
+            const int row = row_of(jr);
             wk_of[it] = __ldg(&geom[static_cast<size_t>(row) * N + x]);
             kx_of[it] = __ldg(&kvec[x]);
             kz_of[it] = __ldg(&kvec[row]);
@@ -312,13 +363,10 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     for (int it = 0; it < ITER; ++it) {
         const int cell = tid + it * NT;
         if (cell >= CELLS) break;
-        const int jr = cell >> LOG_N;  // j*2 + r
+        const int jr = cell >> LOG_N;
         const int x = cell & (N - 1);
-        const int j = jr >> 1, r = jr & 1;
-        const int p = group * RP + j;
-        const int mr = (p == 0) ? r : 1 - r;  // row holding h0 at -kz
         const float2 av = h0s[jr * N + x];
-        const float2 bm = h0s[(j * 2 + mr) * N + ((N - x) & (N - 1))];
+        const float2 bm = h0s[mirror_slot(jr) * N + ((N - x) & (N - 1))];
         float2 pv[NF];
         evolve_cell<NF>(av, bm, wk_of[it], kx_of[it], kz_of[it], top, pv);
         if constexpr (!PAIRED) {
@@ -334,7 +382,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     }
     __syncthreads();
 
-    transform_all<LOG_N, FAST, TC, RP * 2 * NF>(data, tws, tid, eng, error);
+    transform_all<LOG_N, FAST, TC, ROWS * NF>(data, tws, tid, eng, error);
     __syncthreads();
 
     // Write the rows cell-major: inter[row][x][f], NF/2 float4 per cell.
@@ -344,10 +392,10 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     float4* inter = reinterpret_cast<float4*>(inter_slot);
     const int fp = tid % Q;
 #pragma unroll 4
-    for (int cell = tid / Q; cell < RP * 2 * N; cell += CSTEP) {
+    for (int cell = tid / Q; cell < ROWS * N; cell += CSTEP) {
         const int jr = cell >> LOG_N;
         const int x = cell & (N - 1);
-        const int row = row_of(jr >> 1, jr & 1);
+        const int row = row_of(jr);
         float4 o;
         if constexpr (!PAIRED) {
             const float2 v0 = data[(jr * NF + 2 * fp) * SEQ + pad_idx(x)];
@@ -603,15 +651,17 @@ __device__ bool wait_at_least(const unsigned* counter, unsigned target, unsigned
 }
 
 // Resident CTAs the persistent kernel is compiled for: 768 threads per SM
-// (one CTA at N = 1024, whose 32 values per lane need the registers).
+// (at N = 1024, whose 32 values per lane need the registers, two CTAs of
+// single rows).
 // (The tensor-core form needs about 150-170 KB of shared memory per CTA:
 // one CTA per SM, which also bounds its tensor memory to 256 columns.)
 template <int LOG_N, int NF, bool TC = false>
 constexpr int frame_min_blocks()
 {
-    constexpr int nt = Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G;
+    constexpr int nt = FrameSched<LOG_N, TC>::ROWS * NF * Shape<LOG_N>::G;
     if (TC) return 1;
-    return LOG_N >= 10 ? 1 : (768 / nt < 1 ? 1 : (768 / nt > 16 ? 16 : 768 / nt));
+    if (LOG_N >= 10) return 768 / nt >= 2 ? 2 : 1;
+    return 768 / nt < 1 ? 1 : (768 / nt > 16 ? 16 : 768 / nt);
 }
 
 // Shared floats (float2 units) of the persistent kernel's data area, and the
@@ -620,9 +670,10 @@ template <int LOG_N, int NF, bool TC>
 __host__ __device__ constexpr size_t frame_data_float2()
 {
     using S = Shape<LOG_N>;
-    constexpr size_t row = S::RP * 2 * NF * seq_f2<LOG_N, TC>() + S::RP * 2 * S::N;
-    constexpr size_t col = NF * S::PW * seq_f2<LOG_N, TC>() + col_shift_f2_of<LOG_N, NF, S::PW, TC>() +
-                           foam_window_f2<LOG_N, S::PW>();
+    using D = FrameSched<LOG_N, TC>;
+    constexpr size_t row = D::ROWS * NF * seq_f2<LOG_N, TC>() + D::H0ROWS * S::N;
+    constexpr size_t col = NF * D::PW * seq_f2<LOG_N, TC>() + col_shift_f2_of<LOG_N, NF, D::PW, TC>() +
+                           foam_window_f2<LOG_N, D::PW>();
     return row > col ? row : col;
 }
 
@@ -633,18 +684,19 @@ __host__ __device__ constexpr size_t frame_engine_offset()
 }
 
 template <int LOG_N, int NF, bool FAST, bool FOAM, bool TC = false>
-__global__ void __launch_bounds__(Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G,
+__global__ void __launch_bounds__(FrameSched<LOG_N, TC>::ROWS * NF * Shape<LOG_N>::G,
                                   frame_min_blocks<LOG_N, NF, TC>())
 frame_kernel(FrameArgs a, QueueArgs q)
 {
     using S = Shape<LOG_N>;
+    using D = FrameSched<LOG_N, TC>;
     constexpr int N = S::N;
-    constexpr int NT = S::RP * 2 * NF * S::G;
-    constexpr int RT = (N / 2) / S::RP;  // row tasks per ocean
-    constexpr int CT = N / S::PW;        // column tasks per ocean
+    constexpr int NT = D::ROWS * NF * S::G;
+    constexpr int RT = D::RT;       // row tasks per ocean
+    constexpr int CT = N / D::PW;   // column tasks per ocean
     constexpr size_t kDataFloat2 = frame_data_float2<LOG_N, NF, TC>();
-    static_assert(size_t(NF) * S::PW * seq_f2<LOG_N, TC>() + col_shift_f2_of<LOG_N, NF, S::PW, TC>() +
-                          foam_window_f2<LOG_N, S::PW>() <= kDataFloat2,
+    static_assert(size_t(NF) * D::PW * seq_f2<LOG_N, TC>() + col_shift_f2_of<LOG_N, NF, D::PW, TC>() +
+                          foam_window_f2<LOG_N, D::PW>() <= kDataFloat2,
                   "the column task's foam window fits in the data area");
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
@@ -741,11 +793,11 @@ frame_kernel(FrameArgs a, QueueArgs q)
         const unsigned slot = ocean % static_cast<unsigned>(q.slots);
         const int abs_ocean = a.ocean_base + static_cast<int>(ocean);
         if (row) {
-            row_task<LOG_N, NF, FAST, TC>(a, abs_ocean, static_cast<int>(idx), a.inter + slot * slot_f2,
-                                          smem, tws, tid, &h0_bar, h0_parity, &eng, q.error);
+            row_task<LOG_N, NF, FAST, TC, D>(a, abs_ocean, static_cast<int>(idx), a.inter + slot * slot_f2,
+                                             smem, tws, tid, &h0_bar, h0_parity, &eng, q.error);
             h0_parity ^= 1u;
         } else {
-            col_task<LOG_N, NF, FAST, FOAM, S::PW, true, TC>(a, abs_ocean, static_cast<int>(idx),
+            col_task<LOG_N, NF, FAST, FOAM, D::PW, true, TC>(a, abs_ocean, static_cast<int>(idx),
                                                              a.inter + slot * slot_f2, smem, tws, tid,
                                                              &eng, q.error);
         }
@@ -908,7 +960,7 @@ constexpr size_t frame_smem_bytes()
 
 template <int LOG_N, int NF, bool FAST, bool FOAM, bool TC = false>
 struct FrameLaunch {
-    static constexpr int threads() { return Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G; }
+    static constexpr int threads() { return FrameSched<LOG_N, TC>::ROWS * NF * Shape<LOG_N>::G; }
 
     static cudaError_t prepare()
     {

@@ -54,6 +54,7 @@ public:
         queue_.reset(d.max_sources);
         solid_dev_ = DevBuf<uint32_t>(cells_);
         nearest_dev_ = DevBuf<uint32_t>(cells_);
+        mask_dev_ = DevBuf<uint8_t>(cells_);
         mask_.assign(cells_, 0);
         const std::vector<float>& taps = setup_.stencil.taps;
         taps_dev_ = DevBuf<float>(taps.size());
@@ -172,6 +173,19 @@ public:
         rebuild_mask_tables();
     }
 
+    // The tables as the device holds them (host arrays of cells entries).
+    void read_tables(uint32_t* solid, uint32_t* nearest, uint32_t* count)
+    {
+        *count = has_mask_ ? solid_count_ : 0;
+        if (has_mask_ && solid != nullptr && solid_count_ > 0)
+            check(cudaMemcpyAsync(solid, solid_dev_.p, solid_count_ * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                  stream_), "tables");
+        if (has_mask_ && nearest != nullptr)
+            check(cudaMemcpyAsync(nearest, nearest_dev_.p, cells_ * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                  stream_), "tables");
+        check(cudaStreamSynchronize(stream_), "tables");
+    }
+
     void sample(float x, float z, ocean_interaction_sample* out)
     {
         std::lock_guard<std::mutex> lock(query_mutex_);
@@ -237,6 +251,8 @@ public:
     uint32_t last_substeps() const { return clock_.last_steps; }
     bool last_clamped() const { return clock_.clamped; }
     bool moved() const { return moved_; }
+    int32_t shift_x() const { return shift_x_; }
+    int32_t shift_z() const { return shift_z_; }
     const std::vector<float>& taps() const { return setup_.stencil.taps; }
 
 private:
@@ -309,44 +325,19 @@ private:
         check(cudaStreamSynchronize(stream_), "damping");
     }
 
-    // Multi-source BFS from every fluid cell (src/interaction.cpp:255-292).
+    // The obstruction tables (src/interaction.cpp:255-292), built on the
+    // device from the mask by a level-synchronous BFS that reproduces the
+    // reference's queue order (obstruction.cu).
     void rebuild_mask_tables()
     {
         solid_count_ = 0;
         if (!has_mask_) return;
-        std::vector<uint32_t> nearest(cells_), solid, q;
-        q.reserve(cells_);
-        for (size_t i = 0; i < cells_; ++i) {
-            if (mask_[i] == 0) {
-                nearest[i] = static_cast<uint32_t>(i);
-                q.push_back(static_cast<uint32_t>(i));
-            } else {
-                nearest[i] = 0xFFFFFFFFu;
-                solid.push_back(static_cast<uint32_t>(i));
-            }
-        }
-        for (size_t head = 0; head < q.size(); ++head) {
-            const uint32_t i = q[head];
-            const int x = static_cast<int>(i % n_), z = static_cast<int>(i / n_);
-            static const int ddx[4] = {1, -1, 0, 0};
-            static const int ddz[4] = {0, 0, 1, -1};
-            for (int e = 0; e < 4; ++e) {
-                const int nx = x + ddx[e], nz = z + ddz[e];
-                if (nx < 0 || nz < 0 || nx >= static_cast<int>(n_) || nz >= static_cast<int>(n_)) continue;
-                const uint32_t j = static_cast<uint32_t>(nz) * n_ + static_cast<uint32_t>(nx);
-                if (nearest[j] == 0xFFFFFFFFu) {
-                    nearest[j] = nearest[i];
-                    q.push_back(j);
-                }
-            }
-        }
-        solid_count_ = static_cast<uint32_t>(solid.size());
-        if (solid_count_ > 0)
-            check(cudaMemcpyAsync(solid_dev_.p, solid.data(), solid.size() * sizeof(uint32_t),
-                                  cudaMemcpyHostToDevice, stream_), "mask");
-        check(cudaMemcpyAsync(nearest_dev_.p, nearest.data(), cells_ * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                              stream_), "mask");
-        check(cudaStreamSynchronize(stream_), "mask");
+        check(cudaMemcpyAsync(mask_dev_.p, mask_.data(), cells_, cudaMemcpyHostToDevice, stream_), "mask");
+        uint32_t count = 0;
+        check(build_obstruction_tables(mask_dev_.p, static_cast<int>(n_), solid_dev_.p, nearest_dev_.p, &count,
+                                       stream_),
+              "obstruction tables");
+        solid_count_ = count;
     }
 
     void copy_plane_out(int b, float* dst)
@@ -387,6 +378,7 @@ private:
     bool has_mask_ = false;
     uint32_t solid_count_ = 0;
     DevBuf<uint32_t> solid_dev_, nearest_dev_;
+    DevBuf<uint8_t> mask_dev_;
     std::mutex query_mutex_;
     DevBuf<float2> q_in_;
     DevBuf<float4> q_out_;
@@ -449,6 +441,21 @@ int32_t ocean_interaction_recenter(ocean_interaction* field, float world_x, floa
     bool moved = false;
     guarded([&] { moved = field->impl.recenter(world_x, world_z); });
     return moved ? 1 : 0;
+}
+
+void ocean_interaction_last_shift(const ocean_interaction* field, int32_t* dx, int32_t* dz)
+{
+    // InteractionField::recentered / last_shift_x / last_shift_z
+    // (src/interaction.cpp:707-709): zero for a NULL handle.
+    if (dx != nullptr) *dx = field == nullptr ? 0 : field->impl.shift_x();
+    if (dz != nullptr) *dz = field == nullptr ? 0 : field->impl.shift_z();
+}
+
+ocean_status ocean_interaction_obstruction_tables(const ocean_interaction* field, uint32_t* solid,
+                                                  uint32_t* nearest, uint32_t* solid_count)
+{
+    if (field == nullptr || solid_count == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { const_cast<ocean_interaction*>(field)->impl.read_tables(solid, nearest, solid_count); });
 }
 
 void ocean_interaction_set_obstruction(ocean_interaction* field, const uint8_t* mask)

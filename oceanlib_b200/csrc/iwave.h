@@ -60,6 +60,12 @@ cudaError_t launch_interaction_sample(const float4* out, int n, float cell, floa
                                       float4* res, cudaStream_t st);
 cudaError_t launch_combine(const SurfaceEx* ocean_s, const float4* e, uint64_t count, SurfaceEx* out,
                            cudaStream_t st);
+// The obstruction tables from a device mask of n*n bytes (non-zero =
+// solid): solid cells in index order and the nearest-fluid index of every
+// cell, as the reference's multi-source BFS assigns them
+// (src/interaction.cpp:255-292). Waits for the stream; *solid_count is host.
+cudaError_t build_obstruction_tables(const uint8_t* mask, int n, uint32_t* solid, uint32_t* nearest,
+                                     uint32_t* solid_count, cudaStream_t st);
 cudaError_t launch_energy_rows(const IWaveField& f, const float* taps, int p, double* row_kin,
                                double* row_pot, cudaStream_t st);
 

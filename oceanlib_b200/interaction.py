@@ -156,6 +156,17 @@ class InteractionField:
         _check(lib().ocean_interaction_kernel_taps(self._h, t.ctypes.data), "ocean_interaction_kernel_taps")
         return t
 
+    def obstruction_tables(self):
+        """(solid cells in index order, nearest-fluid index per cell) as the
+        device built them for the current obstruction."""
+        n = self.size
+        solid = np.empty(n * n, np.uint32)
+        nearest = np.empty(n * n, np.uint32)
+        count = C.c_uint32(0)
+        _check(lib().ocean_interaction_obstruction_tables(self._h, solid.ctypes.data, nearest.ctypes.data,
+                                                          C.byref(count)), "ocean_interaction_obstruction_tables")
+        return solid[:count.value].copy(), nearest
+
     def get_state(self):
         n = self.size
         cur = np.empty(n * n, np.float32)

@@ -85,6 +85,8 @@ def oracle() -> C.CDLL:
             "or_finalize": (None, [C.POINTER(OrDesc), _P, _P, _P, _P]),
             "or_update": (None, [C.POINTER(OrDesc), _P, C.c_double, _P, _P, _P, _P]),
             "or_sample_many": (None, [C.c_uint32, C.c_float, _P, _P, _P, _P, C.c_uint64, _P]),
+            "or_cascade_sample_many": (None, [C.c_uint32, _P, _P, _P, _P, _P, _P, C.c_uint64, C.c_int,
+                                              C.c_float, _P]),
             "or_foam_step": (None, [C.c_uint32] + [C.c_float] * 7 + [_P, _P, _P, _P]),
             "or_foam_at_many": (None, [C.c_uint32, C.c_float, _P, _P, _P, _P, C.c_uint64, _P]),
             "or_dft2d_points": (None, [C.c_uint32, _P, _P, C.c_uint32, _P, _P, _P, _P]),
@@ -277,6 +279,25 @@ def sample_many(n: int, patch_length: float, disp, normal, vel, xz: np.ndarray) 
     out = np.empty((xz.shape[0], 10), dtype=np.float32)
     oracle().or_sample_many(n, patch_length, disp.ctypes.data, normal.ctypes.data, _ptr(vel),
                             xz.ctypes.data, xz.shape[0], out.ctypes.data)
+    return out
+
+
+def cascade_sample_many(levels, frames, xz: np.ndarray, iterations: int = 4,
+                        tolerance: float = 0.0) -> np.ndarray:
+    """CascadeStack::sample_at (src/cascade.cpp:80-153) at the points xz
+    (count x 2) over `levels` (descriptors) with their frames [(disp, normal,
+    velocity or None)], each level inverted with `iterations` fixed-point
+    steps stopping once both coordinates move by <= tolerance (0: never).
+    iterations=4, tolerance=0 is the reference. (count, 10) float32."""
+    k = len(levels)
+    pts = np.ascontiguousarray(xz, dtype=np.float32).reshape(-1, 2)
+    keep = [tuple(np.ascontiguousarray(a, np.float32) if a is not None else None for a in f) for f in frames]
+    ns = (C.c_uint32 * k)(*[d.size for d in levels])
+    ls = (C.c_float * k)(*[d.patch_length for d in levels])
+    arr = lambda j: (C.c_void_p * k)(*[(f[j].ctypes.data if f[j] is not None else None) for f in keep])
+    out = np.empty((pts.shape[0], 10), dtype=np.float32)
+    oracle().or_cascade_sample_many(k, ns, ls, arr(0), arr(1), arr(2), pts.ctypes.data, pts.shape[0],
+                                    int(iterations), float(tolerance), out.ctypes.data)
     return out
 
 

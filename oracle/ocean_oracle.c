@@ -549,16 +549,23 @@ static float fetch(const float* b, const tap_t* t, int c)
            b[t->i11 + c] * t->w11;
 }
 
-void or_sample_at(uint32_t n, float patch_length, const float* disp, const float* normal,
-                  const float* velocity, float x, float z, float* out)
+void or_sample_at_iter(uint32_t n, float patch_length, const float* disp, const float* normal,
+                       const float* velocity, float x, float z, int iters, float tol, float* out)
 {
-    /* src/ocean.cpp:375-452 */
+    /* src/ocean.cpp:375-452, with the fixed-point step count (the reference's
+     * kInversionSteps = 4, src/ocean.cpp:366) as a parameter and an optional
+     * stop once both parameter coordinates move by <= tol (tol = 0: never).
+     * The step taken last is kept, as when the loop runs to its count. */
     const float inv_cell = (float)n / patch_length;
     float u = x, v = z;
-    for (int it = 0; it < 4; ++it) {
+    for (int it = 0; it < iters; ++it) {
         tap_t t = make_tap(u, v, n, inv_cell);
-        u = x - fetch(disp, &t, 0);
-        v = z - fetch(disp, &t, 2);
+        const float un = x - fetch(disp, &t, 0);
+        const float vn = z - fetch(disp, &t, 2);
+        const int done = tol > 0.0f && fabsf(un - u) <= tol && fabsf(vn - v) <= tol;
+        u = un;
+        v = vn;
+        if (done) break;
     }
     tap_t t = make_tap(u, v, n, inv_cell);
     out[1] = fetch(disp, &t, 0);
@@ -588,6 +595,62 @@ void or_sample_at(uint32_t n, float patch_length, const float* disp, const float
         out[9] = fetch(velocity, &t, 2);
     } else {
         out[7] = out[8] = out[9] = 0.0f;
+    }
+}
+
+void or_sample_at(uint32_t n, float patch_length, const float* disp, const float* normal,
+                  const float* velocity, float x, float z, float* out)
+{
+    or_sample_at_iter(n, patch_length, disp, normal, velocity, x, z, 4, 0.0f, out);
+}
+
+void or_cascade_sample_many(uint32_t levels, const uint32_t* n, const float* patch_length,
+                            const float* const* disp, const float* const* normal,
+                            const float* const* velocity, const float* xz, uint64_t count, int iters,
+                            float tol, float* out)
+{
+    /* src/cascade.cpp:80-153: levels visited in order, each with its own
+     * inversion; height, offsets and velocity summed, normals summed then
+     * renormalised, foam as 1 - prod(1 - foam_i). */
+    float s[10];
+    for (uint64_t i = 0; i < count; ++i) {
+        const float x = xz[2 * i], z = xz[2 * i + 1];
+        float height = 0.0f, offset_x = 0.0f, offset_z = 0.0f;
+        float normal_x = 0.0f, normal_y = 0.0f, normal_z = 0.0f;
+        float transparency = 1.0f;
+        float vx = 0.0f, vy = 0.0f, vz = 0.0f;
+        for (uint32_t l = 0; l < levels; ++l) {
+            or_sample_at_iter(n[l], patch_length[l], disp[l], normal[l], velocity[l], x, z, iters, tol, s);
+            height += s[0];
+            offset_x += s[1];
+            offset_z += s[2];
+            normal_x += s[3];
+            normal_y += s[4];
+            normal_z += s[5];
+            vx += s[7];
+            vy += s[8];
+            vz += s[9];
+            transparency *= (1.0f - s[6]);
+        }
+        float* o = out + 10 * i;
+        o[0] = height;
+        o[1] = offset_x;
+        o[2] = offset_z;
+        o[6] = 1.0f - transparency;
+        o[7] = vx;
+        o[8] = vy;
+        o[9] = vz;
+        const float len2 = normal_x * normal_x + normal_y * normal_y + normal_z * normal_z;
+        if (len2 > 0.0f) {
+            const float inv = 1.0f / sqrtf(len2);
+            o[3] = normal_x * inv;
+            o[4] = normal_y * inv;
+            o[5] = normal_z * inv;
+        } else {
+            o[3] = 0.0f;
+            o[4] = 1.0f;
+            o[5] = 0.0f;
+        }
     }
 }
 

@@ -66,6 +66,18 @@ void or_sample_at(uint32_t n, float patch_length, const float* disp, const float
 void or_sample_many(uint32_t n, float patch_length, const float* disp, const float* normal,
                     const float* velocity, const float* xz, uint64_t count, float* out);
 
+/* Ocean::sample_at with `iters` fixed-point steps (4 = the reference) that
+ * stop early once both parameter coordinates move by <= tol (0 = never). */
+void or_sample_at_iter(uint32_t n, float patch_length, const float* disp, const float* normal,
+                       const float* velocity, float x, float z, int iters, float tol, float* out);
+
+/* CascadeStack::sample_at over `levels` oceans at `count` points, each level
+ * inverted with (iters, tol); out is count x 10 as or_sample_at. */
+void or_cascade_sample_many(uint32_t levels, const uint32_t* n, const float* patch_length,
+                            const float* const* disp, const float* const* normal,
+                            const float* const* velocity, const float* xz, uint64_t count, int iters,
+                            float tol, float* out);
+
 /* FoamField::foam_at at `count` world points: out[i] for (xz[2i], xz[2i+1]). */
 void or_foam_at_many(uint32_t n, float patch_length, const float* disp, const float* normal,
                      const float* foam, const float* xz, uint64_t count, float* out);

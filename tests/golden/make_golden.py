@@ -14,6 +14,9 @@ Outputs
   ref_cascade.npz  reference CascadeStack::sample_at results (3 levels)
   ref_pack.json    sha256 of the viewer's RGBA16F pack over seeded bit patterns
   ref_foam.json    FoamField::foam_at / coverage / set_desc / clear on the foam patch
+  ref_foam_long.json  the foam patch's FoamField over 1000 frames at 60 Hz:
+                   sha256 of the foam plane, coverage and plane statistics
+                   at the checkpoint frames
   abi_layout.json  offsets/sizes of the reference's C structs (include/ocean/ocean.h)
 """
 from __future__ import annotations
@@ -33,8 +36,8 @@ sys.path.insert(0, str(ROOT))
 import oracle as O  # noqa: E402
 from oceanlib_b200.abi import OceanDescC  # noqa: E402
 from tests.workloads import (SMALL_CASES, HASH_CASES, FOAM_CASE, QUERY_CASE, CASCADE_CASE,  # noqa: E402
-                             FOAM_QUERY_FRAMES, FOAM_RETUNE, desc_to_json, query_points, cascade_points,
-                             pack_patterns)
+                             FOAM_QUERY_FRAMES, FOAM_RETUNE, FOAM_LONG_CASE, FOAM_LONG_CHECKPOINTS,
+                             desc_to_json, query_points, cascade_points, pack_patterns)
 
 HERE = Path(__file__).resolve().parent
 
@@ -205,7 +208,23 @@ def foam_queries() -> None:
     (HERE / "ref_foam.json").write_text(json.dumps(out, indent=1))
 
 
-PARTS = {"small": small, "hashes": hashes, "queries": queries, "cascades": cascades,
+def foam_long() -> None:
+    desc, foam, frames, dt = FOAM_LONG_CASE
+    ro = O.RefOcean(desc)
+    rf = O.RefFoam(ro, foam)
+    checks = {}
+    for k in range(1, frames + 1):
+        ro.update(k * dt)
+        rf.update(dt)
+        if k in FOAM_LONG_CHECKPOINTS:
+            f = rf.data()
+            checks[str(k)] = {"sha": sha(f), "coverage": rf.coverage(), "max": float(f.max()),
+                              "nonzero": int(np.count_nonzero(f)), "substeps": rf.last_substeps}
+    out = {"desc": desc_to_json(desc), "frames": frames, "dt": dt, "checkpoints": checks}
+    (HERE / "ref_foam_long.json").write_text(json.dumps(out, indent=1))
+
+
+PARTS = {"foam_long": foam_long, "small": small, "hashes": hashes, "queries": queries, "cascades": cascades,
          "interaction": interaction, "pack": pack, "abi_layout": abi_layout, "foam_queries": foam_queries}
 
 

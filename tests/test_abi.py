@@ -185,3 +185,15 @@ def test_batch_descriptor_validation_is_host_side():
     bd.persistent_foam = 1
     assert not lib.ocean_batch_create(C.byref(bd), C.byref(st))
     assert st.value == abi.OCEAN_ERROR_INVALID_ARG
+
+
+def test_reference_header_paths_compile_and_link():
+    # include/ocean/ocean.h as C99 (-pedantic -Werror) and include/ocean/*.hpp
+    # as C++20, each in a program linked against libocean_b200.so: C and C++
+    # code written against the reference's headers builds and links here.
+    # (The GPU test runs both programs.)
+    from tests.native.build_native import build
+
+    exes = build()
+    for path in exes.values():
+        assert path.exists()

@@ -91,6 +91,24 @@ def test_converged_inversion_reaches_one_micrometre():
     cs.close()
 
 
+def test_config3_million_queries_match_the_oracle_four_step_and_converged():
+    # Config 3: 1,000,000 summed queries uniform over the 800 m tile, with the
+    # reference's 4 fixed-point steps and with the inversion run until both
+    # parameter coordinates move by <= 1e-6 m (at most 64 steps). Both are
+    # bit-identical to the oracle's restatement (or_cascade_sample_many),
+    # which at 4 steps is pinned to the reference's CascadeStack records.
+    levels, t, _ = CASCADE_CASE
+    cs = ob.CascadeStack(levels)
+    cs.update(t)
+    frames = [O.update(d, t) for d in levels]
+    xz = W.cascade_query_points(1_000_000)
+    for iters, tol in ((4, 0.0), (64, 1e-6)):
+        got = cs.sample_many(xz, iterations=iters, tolerance=tol)
+        want = O.cascade_sample_many(levels, frames, xz, iterations=iters, tolerance=tol)
+        assert np.array_equal(bits(got), bits(want)), (iters, tol)
+    cs.close()
+
+
 def test_cascade_rejects_bad_input():
     with pytest.raises(ValueError):
         ob.CascadeStack([])

@@ -251,3 +251,51 @@ def test_pack_rgba16_matches_reference_viewer_pack():
     assert src.shape[0] == golden["texels"]
     assert sha(O.pack_rgba16(src)) == golden["plain"]
     assert sha(O.pack_rgba16(src, alpha)) == golden["alpha"]
+
+
+def test_oracle_cascade_restatement_matches_reference():
+    # The C restatement of CascadeStack::sample_at (or_cascade_sample_many)
+    # at the reference's 4 fixed-point steps: the reference's own records.
+    from tests.workloads import CASCADE_CASE
+
+    g = np.load(GOLDEN / "ref_cascade.npz")
+    levels, t, count = CASCADE_CASE
+    frames = [O.update(d, t) for d in levels]
+    got = O.cascade_sample_many(levels, frames, g["xz"], iterations=4, tolerance=0.0)
+    assert np.array_equal(bits(got), bits(g["out"]))
+
+
+def test_oracle_converged_inversion_is_a_fixed_point():
+    # Config 3's converged mode (steps until both parameter coordinates move
+    # by <= 1e-6 m, at most 64): where the surface has not folded the
+    # iteration is a contraction, so 200 steps no longer move the answer
+    # (float32 rounding aside), while 4 steps (the reference) still differ.
+    from tests.workloads import CASCADE_CASE
+
+    levels, t, _ = CASCADE_CASE
+    frames = [O.update(d, t) for d in levels]
+    xz = W.cascade_query_points(20_000)
+    conv = O.cascade_sample_many(levels, frames, xz, iterations=64, tolerance=1e-6)
+    more = O.cascade_sample_many(levels, frames, xz, iterations=200, tolerance=0.0)
+    four = O.cascade_sample_many(levels, frames, xz, iterations=4, tolerance=0.0)
+    dh = np.abs(conv[:, 0].astype(np.float64) - more[:, 0])
+    assert np.quantile(dh, 0.999) < 1e-5
+    assert np.abs(four[:, 0] - conv[:, 0]).max() > 0.0
+
+
+def test_fp64_foam_run_tracks_the_fp32_foam():
+    # The FP64 foam yardstick (oracle/fp64_foam.py) against the oracle's FP32
+    # FoamField on a small choppy patch: the two stay within a few 1e-6.
+    import oceanlib_b200 as ob
+    from oracle.fp64_foam import fp64_foam_run
+
+    desc = ob.OceanDesc(size=64, patch_length=60.0, wind_speed=20.0, choppiness=1.6, seed=21,
+                        compute_velocity=True)
+    foam = W.foam_desc()
+    dt = 1.0 / 60.0
+    f64 = fp64_foam_run(desc, foam, 40, dt, [10, 40], device="cpu", threads=4)
+    f32 = run_oracle_foam(desc, foam, [((k + 1) * dt, dt) for k in range(40)])
+    for k in (10, 40):
+        err = np.abs(f32[k - 1].astype(np.float64) - f64[k])
+        assert err.max() < 2e-5, (k, err.max())
+        assert f32[k - 1].max() > 0.1  # the patch does foam

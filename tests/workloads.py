@@ -53,6 +53,11 @@ HASH_CASES = [
 # Persistent foam on the foam patch: 120 frames at 60 Hz.
 FOAM_CASE = (W.foam_patch_512(), W.foam_desc(), 120, 1.0 / 60.0)
 
+# Config 2's full run: 1000 frames at 60 Hz from t = 0 (frame k at t = k/60,
+# then FoamField::update(1/60)), foam checked at these frames.
+FOAM_LONG_CASE = (W.foam_patch_512(), W.foam_desc(), 1000, 1.0 / 60.0)
+FOAM_LONG_CHECKPOINTS = (250, 500, 1000)
+
 # The rest of FoamField on the foam patch: foam_at and coverage after 30
 # frames, then set_desc to FOAM_RETUNE for 20 more frames (fixed_dt and
 # max_substeps given here differ from the field's and must be ignored), then
