@@ -63,12 +63,14 @@ struct RowSched {
     static constexpr int PW = ROWS;                                                  // columns per column task
     static constexpr int RT = (1 << LOG_N) / ROWS;                                   // row tasks per ocean
 };
-// The persistent kernel's choice: single rows at N >= 512 (FP32 forms; the
-// tensor-core engine is built for a row pair's sequences).
+// The persistent kernel's choice: row pairs. Single rows were measured at
+// N = 512 (64 oceans, velocity and persistent foam): 1.336 ms per frame
+// against 1.117 ms with row pairs - the second h0 read and twice the tasks
+// cost more than the smaller CTAs recover.
 template <int LOG_N, bool TC>
 __host__ __device__ constexpr bool single_rows()
 {
-    return !TC && LOG_N >= 9;
+    return false;
 }
 template <int LOG_N, bool TC>
 using FrameSched = RowSched<LOG_N, single_rows<LOG_N, TC>()>;
