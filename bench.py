@@ -420,6 +420,17 @@ def bench_ensemble(torch, frames: int = 30):
            "schedule": ens.schedule,
            "cuda_graph": {"ms_per_frame": ms, "host_us_per_update": host_graph},
            "per_call_launches": {"ms_per_frame": ms_calls, "host_us_per_update": host_calls}}
+    # Every schedule forced in turn (graph replay), beside the autotuner's pick.
+    per = {}
+    for name, kind in (("sequential", ob.OceanEnsemble.SEQUENTIAL),
+                       ("concurrent_work_shares", ob.OceanEnsemble.CONCURRENT),
+                       ("one_launch", ob.OceanEnsemble.ONE_LAUNCH)):
+        try:
+            ens.set_schedule(kind)
+        except ValueError:
+            continue
+        per[name] = timed(True)[0]
+    res["schedules_ms_per_frame"] = per
     ens.close()
     return res
 

@@ -458,11 +458,13 @@ OCEAN_API ocean_status ocean_batch_read_spectrum(const ocean_batch* batch, uint3
 
 typedef struct ocean_ensemble ocean_ensemble;
 
-/* Groups the oceans by size; each frame forks one stream per size and runs
- * that size's persistent kernel on it (the three-pass schedule at N = 2048
- * and 4096). With autotune != 0 the schedule
- * (sizes in sequence, or concurrently with SM shares by estimated or by
- * measured cost) is chosen by timing each candidate on this GPU at creation. */
+/* Groups the oceans by size. Schedules of a frame: the sizes in sequence,
+ * each size's persistent kernel on its own stream concurrently with SM shares
+ * (by estimated or by measured cost; the three-pass schedule at N = 2048 and
+ * 4096), or - when every size is 32..1024, all with the same velocity flag,
+ * in an FP32 form - one persistent launch whose work queue holds every
+ * size's tasks. With autotune != 0 the schedule is chosen by timing each
+ * candidate on this GPU at creation; otherwise it is the concurrent one. */
 OCEAN_API ocean_ensemble* ocean_ensemble_create(const ocean_desc* oceans, uint32_t count,
                                                 int32_t autotune, ocean_status* out_status);
 OCEAN_API void ocean_ensemble_destroy(ocean_ensemble* ensemble);
@@ -470,7 +472,15 @@ OCEAN_API uint32_t ocean_ensemble_count(const ocean_ensemble* ensemble);
 /* All oceans to absolute time `time`, asynchronously on `stream` (NULL = the
  * ensemble's stream). */
 OCEAN_API ocean_status ocean_ensemble_update(ocean_ensemble* ensemble, double time, void* stream);
+/* Waits for the ensemble's stream; OCEAN_ERROR_TIMEOUT (once) if a bounded
+ * device wait of the one-launch schedule gave up. */
 OCEAN_API ocean_status ocean_ensemble_synchronize(ocean_ensemble* ensemble);
+/* Forces a schedule: 0 sizes in sequence, 1 concurrent with SM shares by the
+ * work estimate, 2 one launch for every size (OCEAN_ERROR_INVALID_ARG where
+ * the sizes do not qualify). */
+OCEAN_API ocean_status ocean_ensemble_set_schedule(ocean_ensemble* ensemble, int32_t schedule);
+/* The schedule in use: 0, 1 or 2 as above (-1 for NULL). */
+OCEAN_API int32_t ocean_ensemble_schedule(const ocean_ensemble* ensemble);
 /* With enable != 0 (the default) each update replays one CUDA graph of the
  * whole frame - the time upload, the fork onto one stream per size, every
  * size's persistent launch and the join - captured at the first update under
@@ -707,6 +717,19 @@ OCEAN_API ocean_status ocean_batch_set_profiling(ocean_batch* batch, int32_t ena
 
 /* Waits for the batch's work, returns the accumulated profile and resets it. */
 OCEAN_API ocean_status ocean_batch_read_profile(ocean_batch* batch, ocean_pass_profile* out);
+
+/* Task plans of the batch's persistent kernel (no reference counterpart):
+ * plan 0 is the default; N = 256 and 512 also have single-row tasks (plan
+ * 1), N = 1024 sequences over 64 lanes with single-row tasks (plan 1). Every
+ * plan gives the same bits. plan_count is 1 or 2; set_plan returns
+ * OCEAN_ERROR_INVALID_ARG for a plan the batch does not have.
+ * ocean_batch_autotune_plan times a few frames of each plan on the batch's
+ * stream (advancing any persistent foam), keeps the fastest and writes the
+ * median milliseconds per plan to `ms` (plan_count entries; may be NULL). */
+OCEAN_API ocean_status ocean_batch_set_plan(ocean_batch* batch, int32_t plan);
+OCEAN_API int32_t ocean_batch_plan(const ocean_batch* batch);
+OCEAN_API int32_t ocean_batch_plan_count(const ocean_batch* batch);
+OCEAN_API ocean_status ocean_batch_autotune_plan(ocean_batch* batch, double* ms);
 
 /* Kernels this batch has launched (all kinds) since it was created. */
 OCEAN_API uint64_t ocean_batch_launch_count(const ocean_batch* batch);

@@ -329,6 +329,27 @@ class OceanBatch:
         return {k: getattr(p, k) for k, _ in abi.PassProfile._fields_}
 
     @property
+    def plan_count(self) -> int:
+        return lib().ocean_batch_plan_count(self._h)
+
+    @property
+    def plan(self) -> int:
+        return lib().ocean_batch_plan(self._h)
+
+    def set_plan(self, plan: int) -> None:
+        """Pick the persistent kernel's task plan (0 default, 1 the alternative)."""
+        st = lib().ocean_batch_set_plan(self._h, int(plan))
+        if st == abi.OCEAN_ERROR_INVALID_ARG:
+            raise ValueError(f"plan {plan} is not available for this batch")
+        _check(st, "ocean_batch_set_plan")
+
+    def autotune_plan(self) -> list:
+        """Time every plan, keep the fastest; median ms per plan."""
+        ms = np.zeros(max(1, self.plan_count), np.float64)
+        _check(lib().ocean_batch_autotune_plan(self._h, ms.ctypes.data), "ocean_batch_autotune_plan")
+        return list(ms[: self.plan_count]) if self.plan_count > 1 else []
+
+    @property
     def launch_count(self) -> int:
         return lib().ocean_batch_launch_count(self._h)
 
@@ -406,6 +427,20 @@ class OceanEnsemble:
 
     def synchronize(self) -> None:
         _check(lib().ocean_ensemble_synchronize(self._h), "ocean_ensemble_synchronize")
+
+    SEQUENTIAL, CONCURRENT, ONE_LAUNCH = 0, 1, 2
+
+    def set_schedule(self, schedule: int) -> None:
+        """Force a schedule: SEQUENTIAL, CONCURRENT (SM shares by work) or
+        ONE_LAUNCH (every size in one persistent launch)."""
+        st = lib().ocean_ensemble_set_schedule(self._h, int(schedule))
+        if st == abi.OCEAN_ERROR_INVALID_ARG:
+            raise ValueError(f"schedule {schedule} is not available for these oceans")
+        _check(st, "ocean_ensemble_set_schedule")
+
+    @property
+    def schedule_kind(self) -> int:
+        return lib().ocean_ensemble_schedule(self._h)
 
     def device_buffers(self, index: int) -> DeviceBuffers:
         d = DeviceBuffers()

@@ -265,6 +265,10 @@ SIGNATURES = {
     "ocean_batch_set_profiling": (C.c_int, [C.c_void_p, C.c_int32]),
     "ocean_batch_read_profile": (C.c_int, [C.c_void_p, C.POINTER(PassProfile)]),
     "ocean_batch_launch_count": (C.c_uint64, [C.c_void_p]),
+    "ocean_batch_set_plan": (C.c_int, [C.c_void_p, C.c_int32]),
+    "ocean_batch_plan": (C.c_int32, [C.c_void_p]),
+    "ocean_batch_plan_count": (C.c_int32, [C.c_void_p]),
+    "ocean_batch_autotune_plan": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ocean_frame_static_scratch": (C.c_int, [C.c_uint32, C.c_float, C.c_double, C.c_float,
                                              C.c_float, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -276,6 +280,8 @@ SIGNATURES = {
     "ocean_ensemble_count": (C.c_uint32, [C.c_void_p]),
     "ocean_ensemble_update": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
     "ocean_ensemble_synchronize": (C.c_int, [C.c_void_p]),
+    "ocean_ensemble_set_schedule": (C.c_int, [C.c_void_p, C.c_int32]),
+    "ocean_ensemble_schedule": (C.c_int32, [C.c_void_p]),
     "ocean_ensemble_set_graph": (C.c_int, [C.c_void_p, C.c_int32]),
     "ocean_ensemble_device_buffers": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(DeviceBuffers)]),
     "ocean_ensemble_describe": (C.c_uint64, [C.c_void_p, C.c_char_p, C.c_uint64]),

@@ -32,85 +32,101 @@ namespace {
 constexpr int kPad = 4;   // float2 padding between sequences in shared memory
 constexpr int kPad4 = 3;  // float4 padding between sequence pairs (stride = 3 mod 8 float4)
 
+// Columns per CTA of the per-chunk column kernel: 4 at N = 512 (128-byte rows
+// of the intermediate); 2 at N = 1024, where 32 values per lane leave room
+// for fewer threads only.
 template <int LOG_N>
 struct Shape {
     static constexpr int N = 1 << LOG_N;
-    static constexpr int G = lanes_for(LOG_N);                       // lanes / sequence
-    static constexpr int SEQ = padded_len(N) + kPad;                 // sequence stride (float2)
-    static constexpr int SEQ4 = padded_len4(N) + kPad4;              // pair stride (float4)
-    static constexpr int RP = cmin(N / 2, 32 / G > 1 ? 32 / G : 1); // row pairs / CTA
-    // columns / CTA of the per-chunk column kernel: 4 at N = 512 (128-byte
-    // rows of the intermediate); 2 at N = 1024, where 32 values per lane
-    // leave room for fewer threads only.
+    static constexpr int G = lanes_for(LOG_N);
     static constexpr int W = LOG_N >= 10 ? 2 : cmin(N, (128 / G) > 4 ? 128 / G : 4);
 };
 
-// Which rows a row task owns. Paired (ROWS = 2 RP): RP row pairs (p, N-p),
-// each row's h0(-k) read from the other row of its pair, already staged
-// (rows 0 and N/2 are their own mirrors). Single (ROWS = RP): RP rows, each
-// staged with a copy of its mirror row (N - y) mod N beside it - twice the h0
-// reads (the second from L2: the mirror row's own task is the neighbouring
-// ticket) for half the CTA. At N = 512 and 1024 a row pair fills a whole
-// 384-thread CTA (256 without velocity); single rows make the persistent
-// kernel's CTAs half that size, so twice as many independent CTAs share each
-// SM and one CTA's barriers and load waits idle fewer warps. Column tasks
-// cover PW = ROWS columns, so both task kinds have the same thread count.
-template <int LOG_N, bool SINGLE_ROWS>
-struct RowSched {
+// The plan of one size's tasks: how a sequence spreads over lanes, how the
+// sequences sit in shared memory, and which rows a row task owns.
+//
+//   G lanes per sequence, each keeping N / G values (2^LANE_LOG): one stage
+//   block of LANE_LOG radix-2 stages per pass through shared memory. The
+//   default G (lanes_for) gives 16 values a lane (32 at N = 1024) within one
+//   warp; a plan may take more lanes (N = 1024 over 64 lanes: 16 values, a
+//   pass more, half the registers).
+//
+//   Paired: fields 2p and 2p+1 of a row or column as one pair (float4 per
+//   index, stride SEQ4 float4 = 2 SEQ4 float2 per pair, so SEQ4 float2 per
+//   sequence), transformed with packed f32x2 arithmetic over G2 = 2 G lanes.
+//   Single: every sequence on its own (float2 per index, stride SEQ). A lane
+//   keeps half as many indices of each sequence in a pair (it holds two), so
+//   pairs are used where that adds no pass through shared memory (with the
+//   default lanes: N = 32, 64, 512). The tensor-core form uses single
+//   sequences. Twiddles follow the data: float4 (wx, wx, wy, wy) entries for
+//   pairs, float2 otherwise.
+//
+//   Row pairs (ROWS = 2 RP): RP row pairs (p, N-p), each row's h0(-k) read
+//   from the other row of its pair, already staged (rows 0 and N/2 are their
+//   own mirrors). Single rows (ROWS = RP): RP rows, each staged with a copy of
+//   its mirror row (N - y) mod N beside it - twice the h0 reads (the second
+//   from L2: the mirror row's task is the neighbouring ticket) for half the
+//   threads. Column tasks of the persistent kernels cover PW = ROWS columns,
+//   so both task kinds have the same thread count, ROWS * NF * G.
+template <int LOG_N_, int G_, bool TC_, bool SINGLE_ROWS>
+struct Plan {
+    static constexpr int LOG_N = LOG_N_;
+    static constexpr int N = 1 << LOG_N;
+    static constexpr int G = G_;
+    static constexpr bool TC = TC_;
+    static constexpr int SEQ = padded_len(N) + kPad;                  // sequence stride (float2)
+    static constexpr int SEQ4 = padded_len4(N) + kPad4;               // pair stride (float4)
+    static constexpr int RP = cmin(N / 2, 32 / G > 1 ? 32 / G : 1);  // row pairs / task
+    static constexpr int LANE_LOG = ilog2c(N / G);
+    static_assert(LANE_LOG >= 2, "a lane keeps at least four values");
+    static constexpr bool PAIRED =
+        !TC && (LOG_N + LANE_LOG - 1) / LANE_LOG == (LOG_N + LANE_LOG - 2) / (LANE_LOG - 1);
+    static constexpr int G2 = 2 * G;                                  // lanes per sequence pair
+    static constexpr int SEQF2 = PAIRED ? SEQ4 : SEQ;                 // float2 per sequence
+    static constexpr int TWF2 = PAIRED ? 2 * (N - 1) : N - 1;         // float2 of the twiddle table
     static constexpr bool SINGLE = SINGLE_ROWS;
-    static constexpr int ROWS = SINGLE ? Shape<LOG_N>::RP : 2 * Shape<LOG_N>::RP;  // rows per row task
-    static constexpr int H0ROWS = SINGLE ? 2 * ROWS : ROWS;                         // h0 rows staged
-    static constexpr int PW = ROWS;                                                  // columns per column task
-    static constexpr int RT = (1 << LOG_N) / ROWS;                                   // row tasks per ocean
+    static constexpr int ROWS = SINGLE ? RP : 2 * RP;                 // rows per row task
+    static constexpr int H0ROWS = SINGLE ? 2 * ROWS : ROWS;           // h0 rows staged
+    static constexpr int PW = ROWS;                                   // columns per column task
+    static constexpr int RT = N / ROWS;                               // row tasks per ocean
+    template <int NF>
+    __host__ __device__ static constexpr int threads()
+    {
+        return ROWS * NF * G;
+    }
 };
-// The persistent kernel's choice: row pairs. Single rows were measured at
-// N = 512 (64 oceans, velocity and persistent foam): 1.336 ms per frame
-// against 1.117 ms with row pairs - the second h0 read and twice the tasks
-// cost more than the smaller CTAs recover.
-template <int LOG_N, bool TC>
-__host__ __device__ constexpr bool single_rows()
-{
-    return false;
-}
-template <int LOG_N, bool TC>
-using FrameSched = RowSched<LOG_N, single_rows<LOG_N, TC>()>;
 
-// Shared-memory layouts of the sequences a task transforms. Paired: fields
-// 2p and 2p+1 of a row or column as one pair (float4 per index, stride SEQ4
-// float4 = 2 SEQ4 float2 per pair, so SEQ4 float2 per sequence), transformed
-// with packed f32x2 arithmetic. Single: every sequence on its own (float2 per
-// index, stride SEQ). A lane keeps half as many indices of each sequence in
-// a pair (it holds two), so pairs are used where that adds no pass through
-// shared memory: N = 32, 64, 512. N = 16, 128, 256 and 1024 (one pass fewer
-// with 16 or 32 values of one sequence per lane) and the tensor-core form
-// use single sequences. Twiddles follow the data: float4 (wx, wx, wy, wy)
-// entries for pairs, float2 otherwise.
+// The persistent kernel's plan: default lanes, row pairs. Single rows were
+// measured at N = 512 (64 oceans, velocity and persistent foam): 1.336 ms per
+// frame against 1.117 ms with row pairs - the second h0 read and twice the
+// tasks cost more than the smaller CTAs recover.
+template <int LOG_N, bool TC>
+using FramePlan = Plan<LOG_N, lanes_for(LOG_N), TC, false>;
+// The per-chunk kernels' plan.
 template <int LOG_N>
-__host__ __device__ constexpr int lane_log_values()
-{
-    return ilog2c((1 << LOG_N) / lanes_for(LOG_N));
-}
+using ChunkPlan = Plan<LOG_N, lanes_for(LOG_N), false, false>;
+
+// The persistent kernel's alternative plans, one per size that has them, for
+// a batch's autotuner to time against the default (plan 0):
+//   N = 256, 512  single rows (half the threads a task, twice the h0 reads);
+//   N = 1024      64 lanes a sequence (16 values a lane: three passes
+//                 instead of two, about half the registers, so two CTAs of
+//                 single rows per SM instead of one of row pairs).
 template <int LOG_N>
-__host__ __device__ constexpr bool pairs_pay()
+__host__ __device__ constexpr int frame_plan_count(bool tc)
 {
-    return (LOG_N + lane_log_values<LOG_N>() - 1) / lane_log_values<LOG_N>() ==
-           (LOG_N + lane_log_values<LOG_N>() - 2) / (lane_log_values<LOG_N>() - 1);
+    return (!tc && LOG_N >= 8 && LOG_N <= 10) ? 2 : 1;
 }
-template <int LOG_N, bool TC>
-__host__ __device__ constexpr bool paired()
-{
-    return !TC && pairs_pay<LOG_N>();
-}
-template <int LOG_N, bool TC>
-__host__ __device__ constexpr int seq_f2()
-{
-    return paired<LOG_N, TC>() ? Shape<LOG_N>::SEQ4 : Shape<LOG_N>::SEQ;
-}
-template <int LOG_N, bool TC>
-__host__ __device__ constexpr int twiddle_f2()
-{
-    return paired<LOG_N, TC>() ? 2 * ((1 << LOG_N) - 1) : (1 << LOG_N) - 1;
-}
+template <int LOG_N, int V, bool TC>
+struct PlanOfT {
+    using type = FramePlan<LOG_N, TC>;
+};
+template <int LOG_N>
+struct PlanOfT<LOG_N, 1, false> {
+    using type = Plan<LOG_N, (LOG_N >= 10 ? 64 : lanes_for(LOG_N)), false, true>;
+};
+template <int LOG_N, int V, bool TC>
+using PlanOf = typename PlanOfT<LOG_N, V, TC>::type;
 
 // Column tasks over 2 columns shift their sequence pairs (pair s = field
 // pair * W + column) by a few float4 so that the intermediate's stores (lanes
@@ -130,11 +146,11 @@ __host__ __device__ constexpr int col_shift_f2()
     return 2 * col_pair_shift<NF, W>(NF * W / 2 - 1);
 }
 
-// The shifts' float2 for a task of layout (LOG_N, TC) (none for single sequences).
-template <int LOG_N, int NF, int W, bool TC>
+// The shifts' float2 for a task of plan P (none for single sequences).
+template <class P, int NF, int W>
 __host__ __device__ constexpr int col_shift_f2_of()
 {
-    return paired<LOG_N, TC>() ? col_shift_f2<NF, W>() : 0;
+    return P::PAIRED ? col_shift_f2<NF, W>() : 0;
 }
 
 // Foam window of a column task over W columns: columns x0 - 1 .. x0 + W of
@@ -156,11 +172,11 @@ template <int NF>
 using TcEngine = tc::Engine<2 * NF>;
 
 // Fill the twiddle table at `tws` (layout of the form) from the FP32 table.
-template <int LOG_N, bool TC>
+template <class P>
 __device__ __forceinline__ void load_twiddles(float2* tws, const float2* __restrict__ src, int tid, int nt)
 {
-    constexpr int N = 1 << LOG_N;
-    if constexpr (!paired<LOG_N, TC>()) {
+    constexpr int N = P::N;
+    if constexpr (!P::PAIRED) {
         for (int i = tid; i < N - 1; i += nt) tws[i] = src[i];
     } else {
         float4* t4 = reinterpret_cast<float4*>(tws);
@@ -173,25 +189,24 @@ __device__ __forceinline__ void load_twiddles(float2* tws, const float2* __restr
 // (one lane group of G2 per pair, named barrier 1 + pair where a pair spans
 // two warps), or with TC the tensor-core four-step DFT, 8 sequences per
 // engine call (N = 512; its twiddles live in the engine).
-template <int LOG_N, bool FAST, bool TC, int COUNT, int COLW = 0, class Eng = tc::Engine<8>>
+template <class P, bool FAST, int COUNT, int COLW = 0, class Eng = tc::Engine<8>>
 __device__ __forceinline__ void transform_all(float2* data, const float2* tws, int tid, Eng* eng,
                                               unsigned* error)
 {
-    using S = Shape<LOG_N>;
-    if constexpr (TC) {
-        static_assert(LOG_N == 9, "the tensor-core form is built for N = 512");
-        static_assert(S::SEQ * 2 >= 16 * tc::kZStride, "a sequence's space must hold its staged stage-3 rows");
+    if constexpr (P::TC) {
+        static_assert(P::LOG_N == 9, "the tensor-core form is built for N = 512");
+        static_assert(P::SEQ * 2 >= 16 * tc::kZStride, "a sequence's space must hold its staged stage-3 rows");
         static_assert(COUNT == Eng::Lay::kThreads / 32, "one engine call holds the task's sequences");
-        eng->dft512(data, S::SEQ, COUNT, tid, error);
-    } else if constexpr (!paired<LOG_N, TC>()) {
-        fft_sequence<LOG_N, S::G, FAST>(data + (tid / S::G) * S::SEQ, tws, tid % S::G);
+        eng->dft512(data, P::SEQ, COUNT, tid, error);
+    } else if constexpr (!P::PAIRED) {
+        fft_sequence<P::LOG_N, P::G, FAST>(data + (tid / P::G) * P::SEQ, tws, tid % P::G);
     } else {
-        constexpr int G2 = pair_lanes(LOG_N);  // lanes per sequence pair
+        constexpr int G2 = P::G2;
         static_assert(COUNT % 2 == 0, "sequences come in pairs");
         static_assert(G2 <= 32 || (COUNT / 2) < 16, "one named barrier per pair");
         const int pair = tid / G2;
         const int shift = COLW != 0 ? col_pair_shift<COUNT / (COLW != 0 ? COLW : 1), COLW>(pair) : 0;
-        fft_pair<LOG_N, G2, FAST>(reinterpret_cast<ulonglong2*>(data) + pair * S::SEQ4 + shift,
+        fft_pair<P::LOG_N, G2, FAST>(reinterpret_cast<ulonglong2*>(data) + pair * P::SEQ4 + shift,
                                      reinterpret_cast<const ulonglong2*>(tws), tid % G2, 1 + pair);
     }
 }
@@ -267,21 +282,22 @@ __device__ __forceinline__ void h0_rows_wait(uint64_t* bar, uint32_t parity, uns
     }
 }
 
-template <int LOG_N, int NF, bool FAST, bool TC = false, class D = RowSched<LOG_N, false>>
+template <class P, int NF, bool FAST>
 __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int group,
                                          float2* __restrict__ inter_slot, float2* smem,
                                          const float2* tws, int tid, uint64_t* h0_bar, uint32_t h0_parity,
                                          TcEngine<NF>* eng = nullptr, unsigned* error = nullptr)
 {
-    using S = Shape<LOG_N>;
-    constexpr int N = S::N, G = S::G, SEQ = S::SEQ, SEQ4 = S::SEQ4, ROWS = D::ROWS;
+    using D = P;
+    constexpr int LOG_N = P::LOG_N;
+    constexpr int N = P::N, G = P::G, SEQ = P::SEQ, SEQ4 = P::SEQ4, ROWS = P::ROWS;
     constexpr int NT = ROWS * NF * G;
     constexpr int Q = NF / 2;
-    constexpr bool PAIRED = paired<LOG_N, TC>();
+    constexpr bool PAIRED = P::PAIRED;
 
     float2* data = smem;                                   // sequences of rows jr, fields f
     float4* data4 = reinterpret_cast<float4*>(smem);       // the same as pairs (jr, f / 2)
-    float2* h0s = data + ROWS * NF * seq_f2<LOG_N, TC>();  // [H0ROWS][N]
+    float2* h0s = data + ROWS * NF * P::SEQF2;             // [H0ROWS][N]
 
     OceanConsts cst;
     const float2* geom;
@@ -312,7 +328,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
             p = idx >> 1;
             r = idx & 1;
         } else {
-            p = group * S::RP + (jr >> 1);
+            p = group * P::RP + (jr >> 1);
             r = jr & 1;
         }
         if (p == 0) return r ? N / 2 : 0;
@@ -325,7 +341,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         if constexpr (D::SINGLE) {
             return ROWS + jr;
         } else {
-            const int p = group * S::RP + (jr >> 1);
+            const int p = group * P::RP + (jr >> 1);
             const int r = jr & 1;
             return (jr & ~1) + ((p == 0) ? r : 1 - r);
         }
@@ -333,7 +349,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
 
     // The h0 rows go first (bulk copies), then every thread loads the
     // geometry of its cells, so both latencies overlap ahead of the wait.
-    static_assert((ROWS * NF * seq_f2<LOG_N, TC>() * sizeof(float2)) % 16 == 0 && (N * sizeof(float2)) % 16 == 0,
+    static_assert((ROWS * NF * P::SEQF2 * sizeof(float2)) % 16 == 0 && (N * sizeof(float2)) % 16 == 0,
                   "the h0 rows start and end on 16-byte boundaries in shared memory");
     if (tid == 0) {
         h0_rows_issue(h0_bar, h0s, D::H0ROWS, N, [&](int k) {
@@ -384,7 +400,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     }
     __syncthreads();
 
-    transform_all<LOG_N, FAST, TC, ROWS * NF>(data, tws, tid, eng, error);
+    transform_all<P, FAST, ROWS * NF>(data, tws, tid, eng, error);
     __syncthreads();
 
     // Write the rows cell-major: inter[row][x][f], NF/2 float4 per cell.
@@ -416,17 +432,16 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
 // (column FFTs + finalize + optional foam substep). CG loads read the
 // intermediate from L2: another CTA wrote it during this launch.
 // ---------------------------------------------------------------------------
-template <int LOG_N, int NF, bool FAST, bool FOAM, int W, bool CG, bool TC = false>
+template <class P, int NF, bool FAST, bool FOAM, int W, bool CG>
 __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int strip,
                                          const float2* __restrict__ inter_slot, float2* smem,
                                          const float2* tws, int tid, TcEngine<NF>* eng = nullptr,
                                          unsigned* error = nullptr)
 {
-    using S = Shape<LOG_N>;
-    constexpr int N = S::N, G = S::G, SEQ = S::SEQ, SEQ4 = S::SEQ4;
+    constexpr int N = P::N, G = P::G, SEQ = P::SEQ, SEQ4 = P::SEQ4;
     constexpr int NT = NF * W * G;
     constexpr int Q = NF / 2;
-    constexpr bool PAIRED = paired<LOG_N, TC>();
+    constexpr bool PAIRED = P::PAIRED;
     float2* data = smem;                             // TC: sequence f*W + w
     float4* data4 = reinterpret_cast<float4*>(smem); // pairs: pair p*W + w holds fields 2p, 2p+1
     const int x0 = strip * W;
@@ -439,7 +454,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     // float2 the caller reserves), loaded with the intermediate so the taps
     // of the foam step (within a cell of the strip for any velocity up to
     // cell / dt) come from shared memory.
-    float* fwin = reinterpret_cast<float*>(smem + NF * W * seq_f2<LOG_N, TC>() + col_shift_f2_of<LOG_N, NF, W, TC>());
+    float* fwin = reinterpret_cast<float*>(smem + NF * W * P::SEQF2 + col_shift_f2_of<P, NF, W>());
     if constexpr (FSTEP) {
         const float* cur = a.foam_cur + base;
         for (int k = tid; k < N * WW; k += NT) {
@@ -484,7 +499,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     }
     __syncthreads();
 
-    transform_all<LOG_N, FAST, TC, NF * W, W>(data, tws, tid, eng, error);
+    transform_all<P, FAST, NF * W, W>(data, tws, tid, eng, error);
     __syncthreads();
 
     OceanConsts cst;
@@ -564,22 +579,21 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
 // uses intermediate slot o.
 // ---------------------------------------------------------------------------
 template <int LOG_N, int NF, bool FAST>
-__global__ void __launch_bounds__(Shape<LOG_N>::RP * 2 * NF * Shape<LOG_N>::G)
+__global__ void __launch_bounds__(ChunkPlan<LOG_N>::template threads<NF>())
 row_pass_kernel(FrameArgs a)
 {
-    using S = Shape<LOG_N>;
-    constexpr int NT = S::RP * 2 * NF * S::G;
+    using P = ChunkPlan<LOG_N>;
+    constexpr int NT = P::template threads<NF>();
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
-    float2* tws = smem + S::RP * 2 * NF * seq_f2<LOG_N, false>() + S::RP * 2 * S::N;
+    float2* tws = smem + P::ROWS * NF * P::SEQF2 + P::H0ROWS * P::N;
     __shared__ uint64_t h0_bar;
     if (threadIdx.x == 0) h0_bar_init(&h0_bar);
-    load_twiddles<LOG_N, false>(tws, a.twiddles, threadIdx.x, NT);
+    load_twiddles<P>(tws, a.twiddles, threadIdx.x, NT);
     __syncthreads();  // the twiddles are complete before any transform reads them; the barrier is set up
     const int o = blockIdx.y;
-    row_task<LOG_N, NF, FAST>(a, a.ocean_base + o, blockIdx.x,
-                              a.inter + static_cast<size_t>(o) * S::N * S::N * NF, smem, tws,
-                              threadIdx.x, &h0_bar, 0u, nullptr, a.error);
+    row_task<P, NF, FAST>(a, a.ocean_base + o, blockIdx.x, a.inter + static_cast<size_t>(o) * P::N * P::N * NF,
+                          smem, tws, threadIdx.x, &h0_bar, 0u, nullptr, a.error);
 }
 
 template <int LOG_N, int NF, bool FAST, bool FOAM>
@@ -587,17 +601,17 @@ __global__ void __launch_bounds__(NF * Shape<LOG_N>::W * Shape<LOG_N>::G)
 col_pass_kernel(FrameArgs a)
 {
     using S = Shape<LOG_N>;
+    using P = ChunkPlan<LOG_N>;
     constexpr int NT = NF * S::W * S::G;
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
-    float2* tws = smem + NF * S::W * seq_f2<LOG_N, false>() + col_shift_f2_of<LOG_N, NF, S::W, false>() +
-                  foam_window_f2<LOG_N, S::W>();
-    load_twiddles<LOG_N, false>(tws, a.twiddles, threadIdx.x, NT);
+    float2* tws = smem + NF * S::W * P::SEQF2 + col_shift_f2_of<P, NF, S::W>() + foam_window_f2<LOG_N, S::W>();
+    load_twiddles<P>(tws, a.twiddles, threadIdx.x, NT);
     __syncthreads();  // the twiddles are complete before any transform reads them
     const int o = blockIdx.y;
-    col_task<LOG_N, NF, FAST, FOAM, S::W, false>(
-        a, a.ocean_base + o, blockIdx.x, a.inter + static_cast<size_t>(o) * S::N * S::N * NF,
-        smem, tws, threadIdx.x);
+    col_task<P, NF, FAST, FOAM, S::W, false>(a, a.ocean_base + o, blockIdx.x,
+                                             a.inter + static_cast<size_t>(o) * P::N * P::N * NF, smem, tws,
+                                             threadIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -657,48 +671,46 @@ __device__ bool wait_at_least(const unsigned* counter, unsigned target, unsigned
 // single rows).
 // (The tensor-core form needs about 150-170 KB of shared memory per CTA:
 // one CTA per SM, which also bounds its tensor memory to 256 columns.)
-template <int LOG_N, int NF, bool TC = false>
+template <class P, int NF>
 constexpr int frame_min_blocks()
 {
-    constexpr int nt = FrameSched<LOG_N, TC>::ROWS * NF * Shape<LOG_N>::G;
-    if (TC) return 1;
-    if (LOG_N >= 10) return 768 / nt >= 2 ? 2 : 1;
+    constexpr int nt = P::template threads<NF>();
+    if (P::TC) return 1;
+    if (P::LANE_LOG >= 5) return 1;  // 32 values a lane: the registers allow one CTA
     return 768 / nt < 1 ? 1 : (768 / nt > 16 ? 16 : 768 / nt);
 }
 
-// Shared floats (float2 units) of the persistent kernel's data area, and the
-// byte offset of the tensor-core engine's area behind the twiddles.
-template <int LOG_N, int NF, bool TC>
+// Shared floats (float2 units) of a persistent task's data area (either
+// kind), and the byte offset of the tensor-core engine's area behind the
+// twiddles.
+template <class P, int NF>
 __host__ __device__ constexpr size_t frame_data_float2()
 {
-    using S = Shape<LOG_N>;
-    using D = FrameSched<LOG_N, TC>;
-    constexpr size_t row = D::ROWS * NF * seq_f2<LOG_N, TC>() + D::H0ROWS * S::N;
-    constexpr size_t col = NF * D::PW * seq_f2<LOG_N, TC>() + col_shift_f2_of<LOG_N, NF, D::PW, TC>() +
-                           foam_window_f2<LOG_N, D::PW>();
+    constexpr size_t row = P::ROWS * NF * P::SEQF2 + P::H0ROWS * P::N;
+    constexpr size_t col = NF * P::PW * P::SEQF2 + col_shift_f2_of<P, NF, P::PW>() + foam_window_f2<P::LOG_N, P::PW>();
     return row > col ? row : col;
 }
 
 template <int LOG_N, int NF>
 __host__ __device__ constexpr size_t frame_engine_offset()
 {
-    return ((frame_data_float2<LOG_N, NF, true>() + (size_t(1) << LOG_N)) * sizeof(float2) + 127) / 128 * 128;
+    return ((frame_data_float2<FramePlan<LOG_N, true>, NF>() + (size_t(1) << LOG_N)) * sizeof(float2) + 127) /
+           128 * 128;
 }
 
-template <int LOG_N, int NF, bool FAST, bool FOAM, bool TC = false>
-__global__ void __launch_bounds__(FrameSched<LOG_N, TC>::ROWS * NF * Shape<LOG_N>::G,
-                                  frame_min_blocks<LOG_N, NF, TC>())
+template <class P, int NF, bool FAST, bool FOAM>
+__global__ void __launch_bounds__(P::template threads<NF>(), frame_min_blocks<P, NF>())
 frame_kernel(FrameArgs a, QueueArgs q)
 {
-    using S = Shape<LOG_N>;
-    using D = FrameSched<LOG_N, TC>;
-    constexpr int N = S::N;
-    constexpr int NT = D::ROWS * NF * S::G;
-    constexpr int RT = D::RT;       // row tasks per ocean
-    constexpr int CT = N / D::PW;   // column tasks per ocean
-    constexpr size_t kDataFloat2 = frame_data_float2<LOG_N, NF, TC>();
-    static_assert(size_t(NF) * D::PW * seq_f2<LOG_N, TC>() + col_shift_f2_of<LOG_N, NF, D::PW, TC>() +
-                          foam_window_f2<LOG_N, D::PW>() <= kDataFloat2,
+    constexpr int LOG_N = P::LOG_N;
+    constexpr bool TC = P::TC;
+    constexpr int N = P::N;
+    constexpr int NT = P::template threads<NF>();
+    constexpr int RT = P::RT;       // row tasks per ocean
+    constexpr int CT = N / P::PW;   // column tasks per ocean
+    constexpr size_t kDataFloat2 = frame_data_float2<P, NF>();
+    static_assert(size_t(NF) * P::PW * P::SEQF2 + col_shift_f2_of<P, NF, P::PW>() +
+                          foam_window_f2<LOG_N, P::PW>() <= kDataFloat2,
                   "the column task's foam window fits in the data area");
     extern __shared__ float4 smem4[];
     float2* smem = reinterpret_cast<float2*>(smem4);
@@ -714,7 +726,7 @@ frame_kernel(FrameArgs a, QueueArgs q)
     uint32_t h0_parity = 0;
 
     const int tid = threadIdx.x;
-    if constexpr (!TC) load_twiddles<LOG_N, TC>(tws, a.twiddles, tid, NT);
+    if constexpr (!TC) load_twiddles<P>(tws, a.twiddles, tid, NT);
     TcEngine<NF> eng{reinterpret_cast<unsigned char*>(smem4) + frame_engine_offset<LOG_N, NF>(), 0};
     if constexpr (TC) {
         static_assert(NT == TcEngine<NF>::Lay::kThreads, "the engine works with the task's threads");
@@ -795,17 +807,258 @@ frame_kernel(FrameArgs a, QueueArgs q)
         const unsigned slot = ocean % static_cast<unsigned>(q.slots);
         const int abs_ocean = a.ocean_base + static_cast<int>(ocean);
         if (row) {
-            row_task<LOG_N, NF, FAST, TC, D>(a, abs_ocean, static_cast<int>(idx), a.inter + slot * slot_f2,
-                                             smem, tws, tid, &h0_bar, h0_parity, &eng, q.error);
+            row_task<P, NF, FAST>(a, abs_ocean, static_cast<int>(idx), a.inter + slot * slot_f2, smem, tws, tid,
+                                  &h0_bar, h0_parity, &eng, q.error);
             h0_parity ^= 1u;
         } else {
-            col_task<LOG_N, NF, FAST, FOAM, D::PW, true, TC>(a, abs_ocean, static_cast<int>(idx),
+            col_task<P, NF, FAST, FOAM, P::PW, true>(a, abs_ocean, static_cast<int>(idx),
                                                              a.inter + slot * slot_f2, smem, tws, tid,
                                                              &eng, q.error);
         }
     }
     if constexpr (TC) eng.release(tid);
 }
+
+// ---------------------------------------------------------------------------
+// Mixed-size frame kernel: the frames of several same-size groups of oceans in
+// one persistent launch. Every size runs with 64 * NF threads (384 with
+// velocity, 256 without): the default plans from N = 32 to 512 (row pairs,
+// RP * G = 32), and N = 1024 over 64 lanes a sequence (16 values a lane, three
+// passes, single rows) instead of the persistent kernel's 32 lanes x 32
+// values, whose registers would cap every size at one CTA per SM. The queue
+// holds group after group (each in the persistent kernel's order, with its
+// own counters and intermediate ring), so a CTA picks up whichever size comes
+// next, and the wave's tail is shared by all sizes. Each size's twiddle table
+// sits in shared memory for the whole launch.
+// ---------------------------------------------------------------------------
+constexpr int kMixMinLog = 5;
+constexpr int kMixMaxLog = 10;
+
+template <int L>
+using MixPlan = Plan<L, (L >= 10 ? 64 : lanes_for(L)), false, (L >= 10)>;
+
+template <int NF, int L = kMixMinLog>
+__host__ __device__ constexpr size_t mixed_data_float2()
+{
+    constexpr size_t here = frame_data_float2<MixPlan<L>, NF>();
+    if constexpr (L >= kMixMaxLog) {
+        return here;
+    } else {
+        constexpr size_t rest = mixed_data_float2<NF, L + 1>();
+        return here > rest ? here : rest;
+    }
+}
+
+// float2 of size log_n's twiddle table, rounded up to a 16-byte multiple.
+__host__ __device__ constexpr int mix_twf2(int log_n)
+{
+    const int t = log_n == 5   ? MixPlan<5>::TWF2
+                  : log_n == 6 ? MixPlan<6>::TWF2
+                  : log_n == 7 ? MixPlan<7>::TWF2
+                  : log_n == 8 ? MixPlan<8>::TWF2
+                  : log_n == 9 ? MixPlan<9>::TWF2
+                               : MixPlan<10>::TWF2;
+    return (t + 1) & ~1;
+}
+// Offset of size log_n's table in the twiddle area (float2).
+__host__ __device__ constexpr int mix_tw_offset(int log_n)
+{
+    int off = 0;
+    for (int l = kMixMinLog; l < log_n; ++l) off += mix_twf2(l);
+    return off;
+}
+__host__ __device__ constexpr size_t mixed_smem_bytes(int nf)
+{
+    return sizeof(float2) * ((nf == 4 ? mixed_data_float2<4>() : mixed_data_float2<6>()) +
+                             mix_tw_offset(kMixMaxLog + 1));
+}
+
+template <int L>
+__host__ __device__ constexpr int mix_rt()
+{
+    return MixPlan<L>::RT;
+}
+template <int L>
+__host__ __device__ constexpr int mix_ct()
+{
+    return MixPlan<L>::N / MixPlan<L>::PW;
+}
+// (row tasks, column tasks) per ocean of size log_n.
+__host__ __device__ inline void mix_tasks_per_ocean(int log_n, unsigned& rt, unsigned& ct)
+{
+    switch (log_n) {
+        case 5: rt = mix_rt<5>(), ct = mix_ct<5>(); break;
+        case 6: rt = mix_rt<6>(), ct = mix_ct<6>(); break;
+        case 7: rt = mix_rt<7>(), ct = mix_ct<7>(); break;
+        case 8: rt = mix_rt<8>(), ct = mix_ct<8>(); break;
+        case 9: rt = mix_rt<9>(), ct = mix_ct<9>(); break;
+        default: rt = mix_rt<10>(), ct = mix_ct<10>(); break;
+    }
+}
+
+template <int L, int NF>
+__device__ __forceinline__ void mix_load_twiddles(float2* area, const float2* __restrict__ src, int tid, int nt)
+{
+    load_twiddles<MixPlan<L>>(area + mix_tw_offset(L), src, tid, nt);
+}
+
+template <int L, int NF, bool FAST>
+__device__ __noinline__ void mix_run(const MixedGroup& g, bool row, int ocean, int idx, float2* smem,
+                                        const float2* tw_area, int tid, uint64_t* h0_bar, uint32_t h0_parity,
+                                        unsigned* error)
+{
+    using P = MixPlan<L>;
+    const unsigned slot = static_cast<unsigned>(ocean) % static_cast<unsigned>(g.slots);
+    float2* inter = g.a.inter + static_cast<size_t>(slot) * P::N * P::N * NF;
+    const float2* tws = tw_area + mix_tw_offset(L);
+    if (row) {
+        row_task<P, NF, FAST>(g.a, ocean, idx, inter, smem, tws, tid, h0_bar, h0_parity, nullptr, error);
+    } else {
+        col_task<P, NF, FAST, false, P::PW, true>(g.a, ocean, idx, inter, smem, tws, tid, nullptr, error);
+    }
+}
+
+template <int NF, bool FAST>
+__global__ void __launch_bounds__(64 * NF, 768 / (64 * NF)) mixed_frame_kernel(MixedArgs m)
+{
+    constexpr int NT = 64 * NF;
+    static_assert(MixPlan<5>::template threads<NF>() == NT && MixPlan<6>::template threads<NF>() == NT &&
+                      MixPlan<7>::template threads<NF>() == NT && MixPlan<8>::template threads<NF>() == NT &&
+                      MixPlan<9>::template threads<NF>() == NT && MixPlan<10>::template threads<NF>() == NT,
+                  "every size's tasks take the same threads");
+    extern __shared__ float4 smem4[];
+    float2* smem = reinterpret_cast<float2*>(smem4);
+    float2* tw_area = smem + mixed_data_float2<NF>();
+    __shared__ unsigned s_ticket;
+    __shared__ int s_ok, s_group, s_row, s_ocean, s_idx;
+    __shared__ unsigned* s_publish;
+    __shared__ unsigned s_next;
+    __shared__ int s_have_next;
+    __shared__ uint64_t h0_bar;
+    // The group table in shared memory: tasks index it by a runtime group,
+    // which on the kernel's parameters would take a copy per thread.
+    __shared__ MixedGroup s_groups[kMaxMixedGroups];
+    uint32_t h0_parity = 0;
+    const int tid = threadIdx.x;
+    {
+        const int words = static_cast<int>(m.groups * sizeof(MixedGroup) / sizeof(unsigned));
+        const unsigned* src = reinterpret_cast<const unsigned*>(m.g);
+        unsigned* dst = reinterpret_cast<unsigned*>(s_groups);
+        for (int i = tid; i < words; i += NT) dst[i] = src[i];
+    }
+    static_assert(sizeof(MixedGroup) % sizeof(unsigned) == 0, "the group table copies as words");
+
+    for (int gi = 0; gi < m.groups; ++gi) {
+        const float2* src = m.g[gi].a.twiddles;
+        switch (m.g[gi].log_n) {
+            case 5: mix_load_twiddles<5, NF>(tw_area, src, tid, NT); break;
+            case 6: mix_load_twiddles<6, NF>(tw_area, src, tid, NT); break;
+            case 7: mix_load_twiddles<7, NF>(tw_area, src, tid, NT); break;
+            case 8: mix_load_twiddles<8, NF>(tw_area, src, tid, NT); break;
+            case 9: mix_load_twiddles<9, NF>(tw_area, src, tid, NT); break;
+            default: mix_load_twiddles<10, NF>(tw_area, src, tid, NT); break;
+        }
+    }
+    if (tid == 0) {
+        h0_bar_init(&h0_bar);
+        s_publish = nullptr;
+        s_next = atomicAdd(m.ticket, 1u);
+        s_have_next = 1;
+    }
+    // The persistent kernel's protocol (frame_kernel), with a group lookup:
+    // publish the previous task, take a ticket (one ahead far from the end),
+    // wait for the task's inputs, hand it to the CTA.
+    while (true) {
+        __syncthreads();
+        if (tid == 0) {
+            if (s_publish != nullptr) red_release_add(s_publish, 1u);
+            const unsigned t = s_have_next ? s_next : atomicAdd(m.ticket, 1u);
+            s_have_next = 0;
+            int ok = 1;
+            unsigned* publish = nullptr;
+            if (t < m.total) {
+                if (t + 2u * gridDim.x < m.total) {
+                    s_next = atomicAdd(m.ticket, 1u);
+                    s_have_next = 1;
+                }
+                int gi = m.groups - 1;
+                while (gi > 0 && t < m.g[gi].first) --gi;
+                const MixedGroup& g = m.g[gi];
+                unsigned rt, ct;
+                mix_tasks_per_ocean(g.log_n, rt, ct);
+                const unsigned count = static_cast<unsigned>(g.count);
+                const unsigned lt = t - g.first;
+                bool row;
+                unsigned ocean, idx;
+                if (lt < rt) {
+                    row = true, ocean = 0, idx = lt;
+                } else {
+                    const unsigned u = lt - rt, per = rt + ct, blk = u / per, off = u % per;
+                    if (blk + 1 < count) {
+                        row = off < rt;
+                        ocean = row ? blk + 1 : blk;
+                        idx = row ? off : off - rt;
+                    } else {
+                        row = false, ocean = count - 1, idx = off;
+                    }
+                }
+                if (row) {
+                    if (ocean >= static_cast<unsigned>(g.slots))
+                        ok = wait_at_least(g.cols_done + (ocean - g.slots), ct, m.error, m.wait_ns);
+                } else {
+                    ok = wait_at_least(g.rows_done + ocean, rt, m.error, m.wait_ns);
+                }
+                publish = row ? g.rows_done + ocean : g.cols_done + ocean;
+                s_group = gi;
+                s_row = row ? 1 : 0;
+                s_ocean = static_cast<int>(ocean);
+                s_idx = static_cast<int>(idx);
+            }
+            s_publish = publish;
+            s_ticket = t;
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (s_ticket >= m.total || !s_ok) break;
+        const MixedGroup& g = s_groups[s_group];
+        const bool row = s_row != 0;
+        switch (g.log_n) {
+            case 5: mix_run<5, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
+            case 6: mix_run<6, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
+            case 7: mix_run<7, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
+            case 8: mix_run<8, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
+            case 9: mix_run<9, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
+            default: mix_run<10, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
+        }
+        if (row) h0_parity ^= 1u;
+    }
+}
+
+template <int NF, bool FAST>
+struct MixedLaunch {
+    static constexpr int threads() { return 64 * NF; }
+    static cudaError_t prepare()
+    {
+        return cudaFuncSetAttribute(mixed_frame_kernel<NF, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(mixed_smem_bytes(NF)));
+    }
+    static int blocks_per_sm()
+    {
+        if (prepare() != cudaSuccess) return 0;
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mixed_frame_kernel<NF, FAST>, threads(),
+                                                          mixed_smem_bytes(NF)) != cudaSuccess)
+            return 0;
+        return n;
+    }
+    static cudaError_t launch(const MixedArgs& m, int grid, cudaStream_t st)
+    {
+        cudaError_t e = prepare();
+        if (e != cudaSuccess) return e;
+        mixed_frame_kernel<NF, FAST><<<grid, threads(), mixed_smem_bytes(NF), st>>>(m);
+        return cudaGetLastError();
+    }
+};
 
 // Bounded waits that nothing completes, each of which must give up after
 // limit_ns and set its error word: the queue's wait on a counter nothing
@@ -912,29 +1165,29 @@ __global__ void cascade_sample_kernel(CascadeLevels lv, const float2* __restrict
 template <int LOG_N, int NF>
 constexpr size_t row_smem_bytes()
 {
-    using S = Shape<LOG_N>;
-    return sizeof(float2) * (S::RP * 2 * NF * seq_f2<LOG_N, false>() + S::RP * 2 * S::N + twiddle_f2<LOG_N, false>());
+    using P = ChunkPlan<LOG_N>;
+    return sizeof(float2) * (P::ROWS * NF * P::SEQF2 + P::H0ROWS * P::N + P::TWF2);
 }
 template <int LOG_N, int NF>
 constexpr size_t col_smem_bytes()
 {
     using S = Shape<LOG_N>;
+    using P = ChunkPlan<LOG_N>;
     return sizeof(float2) *
-           (NF * S::W * seq_f2<LOG_N, false>() + col_shift_f2_of<LOG_N, NF, S::W, false>() +
-            foam_window_f2<LOG_N, S::W>() + twiddle_f2<LOG_N, false>());
+           (NF * S::W * P::SEQF2 + col_shift_f2_of<P, NF, S::W>() + foam_window_f2<LOG_N, S::W>() + P::TWF2);
 }
 
 template <int LOG_N, int NF, bool FAST>
 cudaError_t row_launch(const FrameArgs& a, cudaStream_t st)
 {
-    using S = Shape<LOG_N>;
+    using P = ChunkPlan<LOG_N>;
     constexpr size_t smem = row_smem_bytes<LOG_N, NF>();
     auto k = row_pass_kernel<LOG_N, NF, FAST>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    dim3 grid((S::N / 2) / S::RP, a.chunk);
-    k<<<grid, S::RP * 2 * NF * S::G, smem, st>>>(a);
+    dim3 grid(P::RT, a.chunk);
+    k<<<grid, P::template threads<NF>(), smem, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -952,31 +1205,31 @@ cudaError_t col_launch(const FrameArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-template <int LOG_N, int NF, bool TC = false>
+template <class P, int NF>
 constexpr size_t frame_smem_bytes()
 {
-    using S = Shape<LOG_N>;
-    if (TC) return frame_engine_offset<LOG_N, NF>() + TcEngine<NF>::Lay::kSmemBytes;
-    return sizeof(float2) * (frame_data_float2<LOG_N, NF, false>() + twiddle_f2<LOG_N, false>());
+    if (P::TC) return frame_engine_offset<P::LOG_N, NF>() + TcEngine<NF>::Lay::kSmemBytes;
+    return sizeof(float2) * (frame_data_float2<P, NF>() + P::TWF2);
 }
 
-template <int LOG_N, int NF, bool FAST, bool FOAM, bool TC = false>
+template <int LOG_N, int NF, bool FAST, bool FOAM, bool TC = false, int V = 0>
 struct FrameLaunch {
-    static constexpr int threads() { return FrameSched<LOG_N, TC>::ROWS * NF * Shape<LOG_N>::G; }
+    using P = PlanOf<LOG_N, V, TC>;
+    static constexpr int threads() { return P::template threads<NF>(); }
+    static constexpr size_t smem() { return frame_smem_bytes<P, NF>(); }
 
     static cudaError_t prepare()
     {
-        return cudaFuncSetAttribute(frame_kernel<LOG_N, NF, FAST, FOAM, TC>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(frame_smem_bytes<LOG_N, NF, TC>()));
+        return cudaFuncSetAttribute(frame_kernel<P, NF, FAST, FOAM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem()));
     }
 
     static int blocks_per_sm()
     {
         if (prepare() != cudaSuccess) return 0;
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<LOG_N, NF, FAST, FOAM, TC>, threads(),
-                                                          frame_smem_bytes<LOG_N, NF, TC>()) != cudaSuccess)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<P, NF, FAST, FOAM>, threads(), smem()) !=
+            cudaSuccess)
             return 0;
         // The tensor-core engine's tensor memory bounds its residency.
         if (TC && n * TcEngine<NF>::Lay::kTmemCols > 512) n = 512 / TcEngine<NF>::Lay::kTmemCols;
@@ -990,19 +1243,29 @@ struct FrameLaunch {
         if (TC) {
             // Every resident CTA must obtain its tensor memory without waiting.
             int n = 0;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<LOG_N, NF, FAST, FOAM, TC>,
-                                                              threads(), frame_smem_bytes<LOG_N, NF, TC>());
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<P, NF, FAST, FOAM>, threads(), smem());
             if (e != cudaSuccess) return e;
             if (n * TcEngine<NF>::Lay::kTmemCols > 512) return cudaErrorInvalidConfiguration;
         }
-        frame_kernel<LOG_N, NF, FAST, FOAM, TC><<<grid, threads(), frame_smem_bytes<LOG_N, NF, TC>(), st>>>(a, q);
+        frame_kernel<P, NF, FAST, FOAM><<<grid, threads(), smem(), st>>>(a, q);
         return cudaGetLastError();
     }
 };
 
 // form: 0 exact, 1 fast (FMA), 2 tensor cores (N = 512 only).
+template <int LOG_N, int V, typename Fn>
+auto frame_variant_plan(int nf, bool fast, bool foam, Fn&& fn)
+{
+    if (nf == 4) return fast ? fn(FrameLaunch<LOG_N, 4, true, false, false, V>{})
+                             : fn(FrameLaunch<LOG_N, 4, false, false, false, V>{});
+    if (foam) return fast ? fn(FrameLaunch<LOG_N, 6, true, true, false, V>{})
+                          : fn(FrameLaunch<LOG_N, 6, false, true, false, V>{});
+    return fast ? fn(FrameLaunch<LOG_N, 6, true, false, false, V>{})
+                : fn(FrameLaunch<LOG_N, 6, false, false, false, V>{});
+}
+
 template <int LOG_N, typename Fn>
-auto frame_variant(int nf, int form, bool foam, Fn&& fn)
+auto frame_variant(int nf, int form, bool foam, int plan, Fn&& fn)
 {
     if constexpr (LOG_N == 9) {
         if (form == 2) {
@@ -1012,24 +1275,23 @@ auto frame_variant(int nf, int form, bool foam, Fn&& fn)
         }
     }
     const bool fast = form == 1;
-    if (nf == 4) return fast ? fn(FrameLaunch<LOG_N, 4, true, false>{})
-                             : fn(FrameLaunch<LOG_N, 4, false, false>{});
-    if (foam) return fast ? fn(FrameLaunch<LOG_N, 6, true, true>{})
-                          : fn(FrameLaunch<LOG_N, 6, false, true>{});
-    return fast ? fn(FrameLaunch<LOG_N, 6, true, false>{}) : fn(FrameLaunch<LOG_N, 6, false, false>{});
+    if constexpr (frame_plan_count<LOG_N>(false) > 1) {
+        if (plan == 1) return frame_variant_plan<LOG_N, 1>(nf, fast, foam, fn);
+    }
+    return frame_variant_plan<LOG_N, 0>(nf, fast, foam, fn);
 }
 
 template <typename Fn>
-auto frame_dispatch(int log_n, int nf, int form, bool foam, Fn&& fn)
+auto frame_dispatch(int log_n, int nf, int form, bool foam, int plan, Fn&& fn)
 {
     switch (log_n) {
-        case 4: return frame_variant<4>(nf, form, foam, fn);
-        case 5: return frame_variant<5>(nf, form, foam, fn);
-        case 6: return frame_variant<6>(nf, form, foam, fn);
-        case 7: return frame_variant<7>(nf, form, foam, fn);
-        case 8: return frame_variant<8>(nf, form, foam, fn);
-        case 9: return frame_variant<9>(nf, form, foam, fn);
-        default: return frame_variant<10>(nf, form, foam, fn);
+        case 4: return frame_variant<4>(nf, form, foam, plan, fn);
+        case 5: return frame_variant<5>(nf, form, foam, plan, fn);
+        case 6: return frame_variant<6>(nf, form, foam, plan, fn);
+        case 7: return frame_variant<7>(nf, form, foam, plan, fn);
+        case 8: return frame_variant<8>(nf, form, foam, plan, fn);
+        case 9: return frame_variant<9>(nf, form, foam, plan, fn);
+        default: return frame_variant<10>(nf, form, foam, plan, fn);
     }
 }
 
@@ -1052,20 +1314,54 @@ cudaError_t col_dispatch_n(int nf, bool fast, bool foam, const FrameArgs& a, cud
 
 }  // namespace
 
-int frame_blocks_per_sm(int log_n, int nf, int form, bool fuse_foam)
+int frame_plan_count(int log_n, int form)
+{
+    if (log_n < 4 || log_n > 10) return 0;
+    return (form != 2 && log_n >= 8) ? 2 : 1;
+}
+
+int frame_blocks_per_sm(int log_n, int nf, int form, bool fuse_foam, int plan)
 {
     if (log_n < 4 || log_n > 10) return 0;
     if (form == 2 && log_n != 9) return 0;
-    return frame_dispatch(log_n, nf, form, fuse_foam, [](auto L) { return decltype(L)::blocks_per_sm(); });
+    if (plan < 0 || plan >= frame_plan_count(log_n, form)) return 0;
+    return frame_dispatch(log_n, nf, form, fuse_foam, plan, [](auto L) { return decltype(L)::blocks_per_sm(); });
 }
 
 cudaError_t launch_frame(int log_n, int nf, int form, bool fuse_foam, const FrameArgs& a,
-                         const QueueArgs& q, int grid, cudaStream_t st)
+                         const QueueArgs& q, int grid, cudaStream_t st, int plan)
 {
     if (log_n < 4 || log_n > 10) return cudaErrorInvalidValue;
     if (form == 2 && log_n != 9) return cudaErrorInvalidValue;
-    return frame_dispatch(log_n, nf, form, fuse_foam,
+    if (plan < 0 || plan >= frame_plan_count(log_n, form)) return cudaErrorInvalidValue;
+    return frame_dispatch(log_n, nf, form, fuse_foam, plan,
                           [&](auto L) { return decltype(L)::launch(a, q, grid, st); });
+}
+
+
+bool mixed_size_ok(int log_n) { return log_n >= kMixMinLog && log_n <= kMixMaxLog; }
+
+uint32_t mixed_tasks(int log_n, int count)
+{
+    unsigned rt = 0, ct = 0;
+    mix_tasks_per_ocean(log_n, rt, ct);
+    return static_cast<uint32_t>(count) * (rt + ct);
+}
+
+int mixed_blocks_per_sm(int nf, bool fast)
+{
+    if (nf == 4) return fast ? MixedLaunch<4, true>::blocks_per_sm() : MixedLaunch<4, false>::blocks_per_sm();
+    return fast ? MixedLaunch<6, true>::blocks_per_sm() : MixedLaunch<6, false>::blocks_per_sm();
+}
+
+cudaError_t launch_mixed_frame(int nf, bool fast, const MixedArgs& m, int grid, cudaStream_t st)
+{
+    if (m.groups < 1 || m.groups > kMaxMixedGroups) return cudaErrorInvalidValue;
+    for (int g = 0; g < m.groups; ++g)
+        if (!mixed_size_ok(m.g[g].log_n) || m.g[g].a.table != nullptr || m.g[g].count < 1 || m.g[g].slots < 1)
+            return cudaErrorInvalidValue;
+    if (nf == 4) return fast ? MixedLaunch<4, true>::launch(m, grid, st) : MixedLaunch<4, false>::launch(m, grid, st);
+    return fast ? MixedLaunch<6, true>::launch(m, grid, st) : MixedLaunch<6, false>::launch(m, grid, st);
 }
 
 cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned* error, unsigned* bar_error,

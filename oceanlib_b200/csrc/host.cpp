@@ -695,7 +695,7 @@ private:
         const int shared = std::max(1, static_cast<int>(std::lround(grid * grid_share_)));
         const int launch_grid = static_cast<int>(std::min<uint64_t>(shared, uint64_t(k) * n_));
         timed(3, st, [&] {
-            check(launch_frame(log_n_, nf_, form_, foam, a, q, launch_grid, st),
+            check(launch_frame(log_n_, nf_, form_, foam, a, q, launch_grid, st, plan_),
                   "frame kernel");
         });
     }
@@ -715,11 +715,11 @@ private:
     // One wave of resident CTAs of the persistent kernel (computed once).
     int frame_grid(bool foam)
     {
-        int& grid = frame_grid_[foam ? 1 : 0];
+        int& grid = frame_grid_[plan_][foam ? 1 : 0];
         if (grid == 0) {
             int sms = 0;
             check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_), "SM count");
-            const int per_sm = frame_blocks_per_sm(log_n_, nf_, form_, foam);
+            const int per_sm = frame_blocks_per_sm(log_n_, nf_, form_, foam, plan_);
             if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "frame occupancy");
             grid = per_sm * sms;
         }
@@ -729,6 +729,79 @@ private:
 public:
     // t / 2 pi as every frame hoists it (src/core/evolve.cpp:33).
     static double time_over_2pi(double t) { return t * kInvTwoPi; }
+
+    // Task plans of the persistent kernel for this batch, the one in use, and
+    // a choice between them (plan < plan_count()).
+    int plan_count() const { return persistent_ ? frame_plan_count(log_n_, form_) : 1; }
+    int plan() const { return plan_; }
+    void set_plan(int plan)
+    {
+        if (plan < 0 || plan >= plan_count()) throw std::invalid_argument("plan");
+        check(cudaStreamSynchronize(stream_), "sync");
+        plan_ = plan;
+    }
+
+    // The batch's autotuner: times `frames` frames (after two untimed ones)
+    // of every task plan on the batch's own stream, keeps the fastest and
+    // returns the median times in milliseconds, plan by plan. Persistent
+    // foam state advances with the timed frames (a clear() resets it).
+    std::vector<double> autotune_plan(int frames = 5)
+    {
+        std::vector<double> ms;
+        if (plan_count() < 2) return ms;
+        cudaEvent_t e0, e1;
+        check(cudaEventCreate(&e0), "event");
+        check(cudaEventCreate(&e1), "event");
+        for (int v = 0; v < plan_count(); ++v) {
+            set_plan(v);
+            std::vector<float> t;
+            for (int k = 0; k < frames + 2; ++k) {
+                const double time = 1.0 + k / 60.0;
+                check(cudaEventRecord(e0, stream_), "event");
+                update(&time, false, foam_on_ ? foam_.fixed_dt : 0.0f, stream_);
+                check(cudaEventRecord(e1, stream_), "event");
+                check(cudaEventSynchronize(e1), "event");
+                float m = 0.0f;
+                check(cudaEventElapsedTime(&m, e0, e1), "elapsed");
+                if (k >= 2) t.push_back(m);
+            }
+            std::sort(t.begin(), t.end());
+            ms.push_back(t[t.size() / 2]);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        set_plan(static_cast<int>(std::min_element(ms.begin(), ms.end()) - ms.begin()));
+        if (take_error()) throw TimeoutError();
+        return ms;
+    }
+
+    // Whether the batch can be one group of a mixed-size launch
+    // (mixed_frame_kernel): a persistent size from 32 to 1024, an FP32 form,
+    // no persistent foam.
+    bool mixable() const
+    {
+        return persistent_ && !foam_on_ && form_ != OCEAN_FFT_TENSOR && mixed_size_ok(log_n_);
+    }
+    int nf() const { return nf_; }
+    int form() const { return form_; }
+
+    // The batch as one group of a mixed-size launch, with the per-ocean
+    // t / 2 pi at `top` on the device; its queue counters are zeroed on `st`.
+    MixedGroup mixed_group(const double* top, cudaStream_t st)
+    {
+        MixedGroup g{};
+        g.a = frame_args(top);
+        g.a.ocean_base = 0;
+        g.a.chunk = static_cast<int32_t>(count_);
+        check(cudaMemsetAsync(queue_.p, 0, (1 + 2 * size_t(count_)) * sizeof(unsigned), st), "queue reset");
+        g.rows_done = queue_.p + 1;
+        g.cols_done = queue_.p + 1 + count_;
+        g.count = static_cast<int32_t>(count_);
+        g.slots = slots_;
+        g.log_n = log_n_;
+        return g;
+    }
+
     // Settles the launch shapes, so a capture issues launches only.
     void prime_shapes()
     {
@@ -841,7 +914,8 @@ private:
     double prof_ms_[4] = {0.0, 0.0, 0.0, 0.0};
     bool persistent_ = true;
     int slots_ = 1;
-    int frame_grid_[2] = {0, 0};
+    int frame_grid_[2][2] = {{0, 0}, {0, 0}};
+    int plan_ = 0;  // the persistent kernel's task plan (frame_plan_count)
     double grid_share_ = 1.0;
     DevBuf<unsigned> queue_, error_;
     uint64_t launches_ = 0;
@@ -1204,10 +1278,6 @@ public:
             check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
             done_.push_back(e);
         }
-        apply_shares(work_);
-        concurrent_ = true;
-        describe_ = "concurrent, SM shares by work estimate";
-        if (tune) autotune();
         // The frame's times: one pinned block, one device block, batch g's
         // oceans from toff_[g].
         size_t off = 0;
@@ -1218,6 +1288,29 @@ public:
         gtimes_ = HostBuf<double>(off);
         dtimes_ = DevBuf<double>(off);
         check(cudaEventCreateWithFlags(&copied_, cudaEventDisableTiming), "event");
+        // One mixed-size launch can run every size when all groups qualify.
+        mixed_ok_ = batches_.size() <= static_cast<size_t>(kMaxMixedGroups);
+        for (auto& b : batches_)
+            mixed_ok_ = mixed_ok_ && b->mixable() && b->nf() == batches_[0]->nf() && b->form() == batches_[0]->form();
+        if (mixed_ok_) {
+            mix_words_ = DevBuf<unsigned>(2);  // ticket, error word
+            check(cudaMemsetAsync(mix_words_.p, 0, 2 * sizeof(unsigned), stream_), "memset");
+            for (size_t g = 0; g < batches_.size(); ++g) mix_order_.push_back(g);
+            // Largest tasks first, so the short ones fill the wave's tail.
+            std::stable_sort(mix_order_.begin(), mix_order_.end(),
+                             [&](size_t a, size_t b) { return batches_[a]->size() > batches_[b]->size(); });
+            int sms = 0, dev = 0;
+            check(cudaGetDevice(&dev), "cudaGetDevice");
+            check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+            const int per_sm =
+                mixed_blocks_per_sm(batches_[0]->nf(), batches_[0]->form() == OCEAN_FFT_FAST);
+            if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "mixed frame occupancy");
+            mix_grid_ = per_sm * sms;
+        }
+        apply_shares(work_);
+        concurrent_ = true;
+        describe_ = "concurrent, SM shares by work estimate";
+        if (tune) autotune();
         use_graph_ = true;  // after the autotuner, which times per-call launches
     }
 
@@ -1248,6 +1341,11 @@ public:
             check(cudaGraphLaunch(exec_, st), "graph launch");
             return;
         }
+        if (mixed_) {
+            stage_times(t, st);
+            enqueue_mixed(dtimes_.p, st);
+            return;
+        }
         if (!concurrent_) {
             for (auto& b : batches_) b->update(&t, false, 0.0f, st);
             return;
@@ -1272,6 +1370,38 @@ public:
     }
     bool graph() const { return use_graph_; }
 
+    // Forces a schedule: 0 sizes in sequence, 1 concurrently with SM shares
+    // by the work estimate, 2 one mixed-size launch (when every size
+    // qualifies; std::invalid_argument otherwise).
+    void set_schedule(int schedule)
+    {
+        if (schedule < 0 || schedule > 2 || (schedule == 2 && !mixed_ok_)) throw std::invalid_argument("schedule");
+        check(cudaStreamSynchronize(stream_), "sync");
+        drop_graph();
+        mixed_ = schedule == 2;
+        concurrent_ = schedule == 1;
+        if (concurrent_) apply_shares(work_);
+        else full_grids();
+        describe_ = schedule == 2 ? "mixed: every size in one persistent launch (forced)"
+                    : schedule == 1 ? "concurrent, SM shares by work estimate (forced)"
+                                    : "sequential (forced)";
+    }
+    int schedule() const { return mixed_ ? 2 : (concurrent_ ? 1 : 0); }
+
+    // Reports (once) a bounded device wait of the mixed launch that gave up.
+    void take_error()
+    {
+        if (!mixed_ok_) return;
+        unsigned w = 0;
+        check(cudaMemcpyAsync(&w, mix_words_.p + 1, sizeof(w), cudaMemcpyDeviceToHost, stream_), "error word");
+        check(cudaStreamSynchronize(stream_), "error word");
+        if (w != 0) {
+            check(cudaMemsetAsync(mix_words_.p + 1, 0, sizeof(unsigned), stream_), "memset");
+            check(cudaStreamSynchronize(stream_), "error word");
+            throw TimeoutError();
+        }
+    }
+
     uint32_t count() const { return static_cast<uint32_t>(where_.size()); }
     cudaStream_t stream() const { return stream_; }
     const Batch& batch_of(uint32_t i) const { return *batches_[where_[i].first]; }
@@ -1294,7 +1424,9 @@ private:
             // between replays; a plain record inside a capture only orders
             // the capture's own streams.
             check(cudaEventRecordWithFlags(copied_, stream_, cudaEventRecordExternal), "event");
-            if (concurrent_) {
+            if (mixed_) {
+                enqueue_mixed(dtimes_.p, stream_);
+            } else if (concurrent_) {
                 check(cudaEventRecord(fork_, stream_), "event");
                 for (size_t g = 0; g < batches_.size(); ++g) {
                     check(cudaStreamWaitEvent(streams_[g], fork_, 0), "wait");
@@ -1313,6 +1445,42 @@ private:
         }
         check(cudaStreamEndCapture(stream_, &graph_), "end capture");
         check(cudaGraphInstantiate(&exec_, graph_, 0), "graph instantiate");
+    }
+
+    // The host's t / 2 pi for every ocean into the pinned block (once the
+    // previous upload has read it), then uploaded on `st`.
+    void stage_times(double t, cudaStream_t st)
+    {
+        check(cudaEventSynchronize(copied_), "time staging");
+        const double top = Batch::time_over_2pi(t);
+        for (size_t i = 0; i < gtimes_.n; ++i) gtimes_.p[i] = top;
+        check(cudaMemcpyAsync(dtimes_.p, gtimes_.p, gtimes_.n * sizeof(double), cudaMemcpyHostToDevice, st),
+              "times");
+        check(cudaEventRecord(copied_, st), "event");
+    }
+
+    // Every size's frame as one mixed_frame_kernel launch on `st`: the groups'
+    // counters and the ticket reset, then the launch (device work only, so a
+    // capture can hold it).
+    void enqueue_mixed(const double* dtimes, cudaStream_t st)
+    {
+        MixedArgs m{};
+        m.groups = static_cast<int32_t>(mix_order_.size());
+        uint32_t first = 0;
+        for (size_t k = 0; k < mix_order_.size(); ++k) {
+            const size_t g = mix_order_[k];
+            m.g[k] = batches_[g]->mixed_group(dtimes + toff_[g], st);
+            m.g[k].first = first;
+            first += mixed_tasks(m.g[k].log_n, m.g[k].count);
+        }
+        m.total = first;
+        m.ticket = mix_words_.p;
+        m.error = mix_words_.p + 1;
+        m.wait_ns = 1000000000ull;
+        check(cudaMemsetAsync(mix_words_.p, 0, sizeof(unsigned), st), "ticket reset");
+        const int grid = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(mix_grid_), first));
+        check(launch_mixed_frame(batches_[0]->nf(), batches_[0]->form() == OCEAN_FFT_FAST, m, grid, st),
+              "mixed frame kernel");
     }
 
     void drop_graph()
@@ -1366,6 +1534,16 @@ private:
     void autotune()
     {
         const int frames = 5;
+        // Per size: the persistent kernel's task plans, timed alone.
+        std::string plans;
+        for (auto& b : batches_) {
+            const std::vector<double> ms = b->autotune_plan(frames);
+            if (ms.empty()) continue;
+            char pb[128];
+            std::snprintf(pb, sizeof(pb), "%sN=%u plan %d (%.3f / %.3f ms)", plans.empty() ? "" : ", ", b->size(),
+                          b->plan(), ms[0], ms[1]);
+            plans += pb;
+        }
         std::vector<double> alone(batches_.size());
         full_grids();
         for (size_t g = 0; g < batches_.size(); ++g)
@@ -1377,8 +1555,20 @@ private:
         const double t_work = time_frames(frames, [&](double t) { update(t, stream_); });
         apply_shares(alone);
         const double t_meas = time_frames(frames, [&](double t) { update(t, stream_); });
+        double t_mixed = -1.0;
+        if (mixed_ok_) {
+            mixed_ = true;
+            t_mixed = time_frames(frames, [&](double t) { update(t, stream_); });
+            mixed_ = false;
+        }
         char buf[256];
-        if (t_seq <= t_work && t_seq <= t_meas) {
+        if (t_mixed >= 0.0 && t_mixed <= t_seq && t_mixed <= t_work && t_mixed <= t_meas) {
+            mixed_ = true;
+            concurrent_ = false;
+            full_grids();
+            std::snprintf(buf, sizeof(buf), "mixed: every size in one persistent launch (%.3f ms; sequential %.3f, "
+                          "work-share %.3f, measured-share %.3f)", t_mixed, t_seq, t_work, t_meas);
+        } else if (t_seq <= t_work && t_seq <= t_meas) {
             concurrent_ = false;
             full_grids();
             std::snprintf(buf, sizeof(buf), "sequential (%.3f ms; concurrent %.3f / %.3f ms)", t_seq, t_work,
@@ -1392,6 +1582,7 @@ private:
                           "work-share %.3f)", t_meas, t_seq, t_work);
         }
         describe_ = buf;
+        if (!plans.empty()) describe_ += "; task plans: " + plans;
         check(cudaStreamSynchronize(stream_), "autotune");
     }
 
@@ -1403,6 +1594,12 @@ private:
     cudaStream_t stream_ = nullptr;
     cudaEvent_t fork_ = nullptr;
     bool concurrent_ = true;
+    // the mixed-size launch
+    bool mixed_ok_ = false;
+    bool mixed_ = false;
+    int mix_grid_ = 0;
+    std::vector<size_t> mix_order_;
+    DevBuf<unsigned> mix_words_;
     std::string describe_;
     // graph replay of the frame
     bool use_graph_ = false;
@@ -1811,6 +2008,26 @@ ocean_status ocean_batch_read_profile(ocean_batch* batch, ocean_pass_profile* ou
     return guarded([&] { *out = batch->impl.read_profile(); });
 }
 
+ocean_status ocean_batch_set_plan(ocean_batch* batch, int32_t plan)
+{
+    if (batch == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { batch->impl.set_plan(plan); });
+}
+
+int32_t ocean_batch_plan(const ocean_batch* batch) { return batch == nullptr ? -1 : batch->impl.plan(); }
+
+int32_t ocean_batch_plan_count(const ocean_batch* batch) { return batch == nullptr ? 0 : batch->impl.plan_count(); }
+
+ocean_status ocean_batch_autotune_plan(ocean_batch* batch, double* ms)
+{
+    if (batch == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] {
+        const std::vector<double> t = batch->impl.autotune_plan();
+        if (ms != nullptr)
+            for (size_t i = 0; i < t.size(); ++i) ms[i] = t[i];
+    });
+}
+
 uint64_t ocean_batch_launch_count(const ocean_batch* batch)
 {
     return batch ? batch->impl.launch_count() : 0u;
@@ -1844,7 +2061,21 @@ ocean_status ocean_ensemble_set_graph(ocean_ensemble* ensemble, int32_t enable)
 ocean_status ocean_ensemble_synchronize(ocean_ensemble* ensemble)
 {
     if (ensemble == nullptr) return OCEAN_ERROR_INVALID_ARG;
-    return guarded([&] { ocean_b200::check(cudaStreamSynchronize(ensemble->impl.stream()), "sync"); });
+    return guarded([&] {
+        ocean_b200::check(cudaStreamSynchronize(ensemble->impl.stream()), "sync");
+        ensemble->impl.take_error();
+    });
+}
+
+ocean_status ocean_ensemble_set_schedule(ocean_ensemble* ensemble, int32_t schedule)
+{
+    if (ensemble == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { ensemble->impl.set_schedule(schedule); });
+}
+
+int32_t ocean_ensemble_schedule(const ocean_ensemble* ensemble)
+{
+    return ensemble == nullptr ? -1 : ensemble->impl.schedule();
 }
 
 ocean_status ocean_ensemble_device_buffers(const ocean_ensemble* ensemble, uint32_t index,

@@ -83,15 +83,49 @@ struct QueueArgs {
 // One persistent launch for the whole frame of `q.count` oceans (foam fused
 // when fuse_foam). `form` is an ocean_fft_form (the tensor form: N = 512).
 // `grid` = CTAs to launch (0 = one wave of resident CTAs).
+// `plan` picks the task plan (0: the default; 1: the alternative of N = 256,
+// 512 and 1024, see frame_plan_count).
 cudaError_t launch_frame(int log_n, int nf, int form, bool fuse_foam, const FrameArgs& args,
-                         const QueueArgs& q, int grid, cudaStream_t stream);
+                         const QueueArgs& q, int grid, cudaStream_t stream, int plan = 0);
 // Resident CTAs per SM of the persistent frame kernel (0: no such variant).
-int frame_blocks_per_sm(int log_n, int nf, int form, bool fuse_foam);
+int frame_blocks_per_sm(int log_n, int nf, int form, bool fuse_foam, int plan = 0);
+// Task plans the persistent kernel has for a size and form (1 or 2).
+int frame_plan_count(int log_n, int form);
 // Bounded waits that nothing completes (tests the timeout paths): on
 // `counter`, which nothing increments, setting *error, and on an mbarrier
 // nothing arrives at, setting *bar_error.
 cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned* error, unsigned* bar_error,
                               unsigned long long limit_ns, cudaStream_t stream);
+
+// Mixed-size frames: the frames of several same-size groups of oceans (each
+// a batch with its own arrays, counters and intermediate ring) as one
+// persistent launch whose ticket queue holds group after group. Sizes N = 32
+// .. 1024 (log_n 5..10), one field count for all groups, FP32 forms, no
+// persistent foam. Group g's tickets are [first, first + tasks), tasks =
+// mixed_tasks(log_n, count); its rows_done / cols_done (count each) and the
+// ticket must be zero at launch.
+constexpr int kMaxMixedGroups = 6;
+struct MixedGroup {
+    FrameArgs a;          // the group's arrays (ocean_base 0, table null)
+    unsigned* rows_done;  // [count]
+    unsigned* cols_done;  // [count]
+    uint32_t first;       // first ticket of the group
+    int32_t count;        // oceans
+    int32_t slots;        // intermediate ring slots (a.inter holds them)
+    int32_t log_n;
+};
+struct MixedArgs {
+    MixedGroup g[kMaxMixedGroups];
+    int32_t groups;
+    uint32_t total;       // tickets of all groups
+    unsigned* ticket;
+    unsigned* error;      // sticky: set when a bounded wait gives up
+    unsigned long long wait_ns;
+};
+bool mixed_size_ok(int log_n);
+uint32_t mixed_tasks(int log_n, int count);
+int mixed_blocks_per_sm(int nf, bool fast);
+cudaError_t launch_mixed_frame(int nf, bool fast, const MixedArgs& m, int grid, cudaStream_t stream);
 
 // Row pass (evolve + row FFTs) and column pass (column FFTs + finalize, with
 // an optional fused foam substep) for `args.chunk` oceans starting at

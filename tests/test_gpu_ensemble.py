@@ -74,3 +74,70 @@ def test_ensemble_rejects_bad_descriptors():
     bad[2].size = 100
     with pytest.raises(ValueError):
         ob.OceanEnsemble(bad, autotune=False)
+
+
+def _check_against_oracle(ens, descs, t, indices):
+    for i in indices:
+        od, on, ov = O.update(descs[i], t)
+        d, n = ens.read(i)
+        assert np.array_equal(bits(d), bits(od)), (descs[i].size, i)
+        assert np.array_equal(bits(n), bits(on)), (descs[i].size, i)
+
+
+def test_one_launch_schedule_is_bit_exact_per_ocean():
+    # Config 4's 64 sea states (N from 64 to 1024) with every size's tasks in
+    # one persistent launch (N = 1024 over 64 lanes a sequence, single rows):
+    # one ocean of each size equals the oracle, per call and per graph replay.
+    descs = W.ensemble_64()
+    sizes = sorted({d.size for d in descs})
+    pick = [next(i for i, d in enumerate(descs) if d.size == n) for n in sizes]
+    ens = ob.OceanEnsemble(descs, autotune=False)
+    ens.set_schedule(ob.OceanEnsemble.ONE_LAUNCH)
+    assert ens.schedule_kind == ob.OceanEnsemble.ONE_LAUNCH
+    ens.set_graph(False)
+    ens.update(12.5)
+    ens.synchronize()
+    _check_against_oracle(ens, descs, 12.5, pick)
+    ens.set_graph(True)
+    for t in (3.0, 47.25):
+        ens.update(t)
+    ens.synchronize()
+    _check_against_oracle(ens, descs, 47.25, pick)
+    ens.close()
+
+
+@pytest.mark.parametrize("velocity", [False, True])
+def test_one_launch_schedule_small_sizes_and_velocity(velocity):
+    # N = 32 (field pairs, 2 lanes a sequence, 32 rows a task)
+    # up to 1024 in one launch, several oceans a size, velocity off and on.
+    descs = []
+    for k, n in enumerate((32, 64, 128, 256, 512, 1024)):
+        for j in range(2):
+            descs.append(ob.OceanDesc(size=n, patch_length=20.0 + 3.0 * n, wind_speed=9.0 + k + j,
+                                      wind_direction=0.3 * k, choppiness=0.8 + 0.1 * j, seed=100 * k + j,
+                                      compute_velocity=velocity))
+    ens = ob.OceanEnsemble(descs, autotune=False)
+    ens.set_schedule(ob.OceanEnsemble.ONE_LAUNCH)
+    ens.update(7.75)
+    ens.synchronize()
+    for i, d in enumerate(descs):
+        od, on, ov = O.update(d, 7.75)
+        dd, nn = ens.read(i)
+        assert np.array_equal(bits(dd), bits(od)), (d.size, i)
+        assert np.array_equal(bits(nn), bits(on)), (d.size, i)
+        if velocity:
+            db = ens.device_buffers(i)
+            v = np.empty((d.size * d.size, 4), np.float32)
+            assert ob.lib().ocean_copy_to_host(v.ctypes.data, db.velocity, v.nbytes) == 0
+            assert np.array_equal(bits(v), bits(ov)), (d.size, i)
+    ens.close()
+
+
+def test_one_launch_schedule_refused_where_sizes_do_not_qualify():
+    descs = [ob.OceanDesc(size=16, seed=1), ob.OceanDesc(size=64, seed=2)]
+    ens = ob.OceanEnsemble(descs, autotune=False)
+    with pytest.raises(ValueError):
+        ens.set_schedule(ob.OceanEnsemble.ONE_LAUNCH)
+    ens.set_schedule(ob.OceanEnsemble.SEQUENTIAL)
+    assert ens.schedule_kind == ob.OceanEnsemble.SEQUENTIAL
+    ens.close()

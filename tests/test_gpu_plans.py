@@ -1,0 +1,88 @@
+"""The persistent kernel's task plans (0 default; 1 single-row tasks at
+N = 256 and 512, 64 lanes a sequence with single-row tasks at N = 1024):
+every plan gives the reference's bits, with and without velocity and with
+persistent foam, and the batch autotuner keeps a plan that exists."""
+import hashlib
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oceanlib_b200 as ob
+import oracle as O
+from oceanlib_b200 import workloads as W
+from tests.workloads import FOAM_CASE
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.fixture(autouse=True)
+def _device(cuda_device):
+    ob.force_simd_level(None)
+    yield
+
+
+@pytest.mark.parametrize("n", [256, 512, 1024])
+@pytest.mark.parametrize("velocity", [False, True])
+def test_every_plan_is_bit_exact(n, velocity):
+    descs = [ob.OceanDesc(size=n, patch_length=0.6 * n + 40.0, wind_speed=13.0 + k, wind_direction=0.5 * k,
+                          choppiness=1.1, seed=70 + k, compute_velocity=velocity) for k in range(3)]
+    batch = ob.OceanBatch(descs)
+    assert batch.plan_count == 2
+    cells = n * n
+    for plan in (1, 0):
+        batch.set_plan(plan)
+        assert batch.plan == plan
+        disp = np.empty((3 * cells, 4), np.float32)
+        nrm = np.empty_like(disp)
+        vel = np.empty_like(disp) if velocity else None
+        batch.update_host([21.5], 0.0, disp, nrm, vel)
+        for k, d in enumerate(descs):
+            od, on, ov = O.update(d, 21.5)
+            sl = slice(k * cells, (k + 1) * cells)
+            assert np.array_equal(bits(disp[sl]), bits(od)), (n, plan, k)
+            assert np.array_equal(bits(nrm[sl]), bits(on)), (n, plan, k)
+            if velocity:
+                assert np.array_equal(bits(vel[sl]), bits(ov)), (n, plan, k)
+    with pytest.raises(ValueError):
+        batch.set_plan(2)
+    batch.close()
+
+
+def test_single_row_plan_with_persistent_foam_matches_reference_foamfield():
+    # The foam patch's first 24 frames under plan 1 (single-row tasks) give
+    # the reference FoamField's bits, frame by frame.
+    golden = json.loads((GOLDEN / "ref_hashes.json").read_text())["foam"]
+    desc, foam, _, dt = FOAM_CASE
+    cells = desc.size * desc.size
+    batch = ob.OceanBatch([desc], foam=foam)
+    batch.set_plan(1)
+    disp = np.empty((cells, 4), np.float32)
+    nrm = np.empty_like(disp)
+    vel = np.empty_like(disp)
+    fo = np.empty(cells, np.float32)
+    for k in range(24):
+        batch.update_host([(k + 1) * dt], dt, disp, nrm, vel, fo)
+        assert sha(fo) == golden["hashes"][k], k
+    batch.close()
+
+
+def test_batch_autotuner_keeps_an_existing_plan():
+    batch = ob.OceanBatch([W.bench_update_patch(512, seed=1337 + b) for b in range(8)])
+    ms = batch.autotune_plan()
+    assert len(ms) == 2 and all(m > 0 for m in ms)
+    assert batch.plan == int(np.argmin(ms))
+    small = ob.OceanBatch([ob.OceanDesc(size=64, seed=3)])
+    assert small.plan_count == 1 and small.autotune_plan() == []
+    small.close()
+    batch.close()
