@@ -64,6 +64,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--extra", default=None,
+                    choices=["bench_update_512", "cascade", "iwave", "ensemble", "serving", "large_sizes"],
+                    help="run only this secondary workload and print its JSON object")
     return ap.parse_args()
 
 
@@ -731,6 +734,12 @@ def main():
     import torch
 
     torch.cuda.set_device(local)
+    if args.extra is not None:
+        fn = {"bench_update_512": lambda: bench_plain_update(torch), "cascade": lambda: bench_cascade(torch),
+              "iwave": bench_iwave, "ensemble": lambda: bench_ensemble(torch), "serving": bench_serving,
+              "large_sizes": lambda: bench_large_sizes(torch)}[args.extra]
+        print(json.dumps({"extra": args.extra, "result": fn()}))
+        return
     if world > 1:
         import datetime
 

@@ -26,7 +26,9 @@ import numpy as np
 from . import abi
 from .abi import OceanDescC, FoamDescC, BatchDescC, SurfaceEx, DeviceBuffers
 
-_LIB_PATH = Path(__file__).resolve().parent / "libocean_b200.so"
+# The in-tree build; OCEANLIB_B200_LIBRARY names another build of the same
+# library (e.g. one compiled with different flags) to load instead.
+_LIB_PATH = Path(os.environ.get("OCEANLIB_B200_LIBRARY", str(Path(__file__).resolve().parent / "libocean_b200.so")))
 _lib: Optional[C.CDLL] = None
 
 

@@ -58,8 +58,7 @@ struct Shape {
 //   keeps half as many indices of each sequence in a pair (it holds two), so
 //   pairs are used where that adds no pass through shared memory (with the
 //   default lanes: N = 32, 64, 512). The tensor-core form uses single
-//   sequences. Twiddles follow the data: float4 (wx, wx, wy, wy) entries for
-//   pairs, float2 otherwise.
+//   sequences. Both layouts read the same float2 twiddle table.
 //
 //   Row pairs (ROWS = 2 RP): RP row pairs (p, N-p), each row's h0(-k) read
 //   from the other row of its pair, already staged (rows 0 and N/2 are their
@@ -83,7 +82,7 @@ struct Plan {
         !TC && (LOG_N + LANE_LOG - 1) / LANE_LOG == (LOG_N + LANE_LOG - 2) / (LANE_LOG - 1);
     static constexpr int G2 = 2 * G;                                  // lanes per sequence pair
     static constexpr int SEQF2 = PAIRED ? SEQ4 : SEQ;                 // float2 per sequence
-    static constexpr int TWF2 = PAIRED ? 2 * (N - 1) : N - 1;         // float2 of the twiddle table
+    static constexpr int TWF2 = N - 1;                                // float2 of the twiddle table
     static constexpr bool SINGLE = SINGLE_ROWS;
     static constexpr int ROWS = SINGLE ? RP : 2 * RP;                 // rows per row task
     static constexpr int H0ROWS = SINGLE ? 2 * ROWS : ROWS;           // h0 rows staged
@@ -171,17 +170,12 @@ __host__ __device__ constexpr int foam_window_f2()
 template <int NF>
 using TcEngine = tc::Engine<2 * NF>;
 
-// Fill the twiddle table at `tws` (layout of the form) from the FP32 table.
+// Copy the FP32 twiddle table into shared memory at `tws`.
 template <class P>
 __device__ __forceinline__ void load_twiddles(float2* tws, const float2* __restrict__ src, int tid, int nt)
 {
     constexpr int N = P::N;
-    if constexpr (!P::PAIRED) {
-        for (int i = tid; i < N - 1; i += nt) tws[i] = src[i];
-    } else {
-        float4* t4 = reinterpret_cast<float4*>(tws);
-        for (int i = tid; i < N - 1; i += nt) t4[i] = pair_twiddle(src[i]);
-    }
+    for (int i = tid; i < N - 1; i += nt) tws[i] = src[i];
 }
 
 // The inverse DFT of the COUNT sequences of a task: the radix-2 Stockham FFT
@@ -206,8 +200,8 @@ __device__ __forceinline__ void transform_all(float2* data, const float2* tws, i
         static_assert(G2 <= 32 || (COUNT / 2) < 16, "one named barrier per pair");
         const int pair = tid / G2;
         const int shift = COLW != 0 ? col_pair_shift<COUNT / (COLW != 0 ? COLW : 1), COLW>(pair) : 0;
-        fft_pair<P::LOG_N, G2, FAST>(reinterpret_cast<ulonglong2*>(data) + pair * P::SEQ4 + shift,
-                                     reinterpret_cast<const ulonglong2*>(tws), tid % G2, 1 + pair);
+        fft_pair<P::LOG_N, G2, FAST>(reinterpret_cast<ulonglong2*>(data) + pair * P::SEQ4 + shift, tws, tid % G2,
+                                     1 + pair);
     }
 }
 
@@ -456,10 +450,14 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     // cell / dt) come from shared memory.
     float* fwin = reinterpret_cast<float*>(smem + NF * W * P::SEQF2 + col_shift_f2_of<P, NF, W>());
     if constexpr (FSTEP) {
+        // Asynchronous 4-byte copies straight into the window (no register
+        // round trip, nothing to wait for until the finalize below).
         const float* cur = a.foam_cur + base;
         for (int k = tid; k < N * WW; k += NT) {
             const int xc = (x0 - 1 + k % WW) & (N - 1);
-            fwin[k] = __ldg(&cur[static_cast<size_t>(k / WW) * N + xc]);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(fwin + k)),
+                         "l"(cur + static_cast<size_t>(k / WW) * N + xc)
+                         : "memory");
         }
     }
 
@@ -500,6 +498,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     __syncthreads();
 
     transform_all<P, FAST, NF * W, W>(data, tws, tid, eng, error);
+    if constexpr (FSTEP) asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's window copies
     __syncthreads();
 
     OceanConsts cst;
@@ -1358,7 +1357,7 @@ cudaError_t launch_mixed_frame(int nf, bool fast, const MixedArgs& m, int grid, 
 {
     if (m.groups < 1 || m.groups > kMaxMixedGroups) return cudaErrorInvalidValue;
     for (int g = 0; g < m.groups; ++g)
-        if (!mixed_size_ok(m.g[g].log_n) || m.g[g].a.table != nullptr || m.g[g].count < 1 || m.g[g].slots < 1)
+        if (!mixed_size_ok(m.g[g].log_n) || m.g[g].count < 1 || m.g[g].slots < 1)
             return cudaErrorInvalidValue;
     if (nf == 4) return fast ? MixedLaunch<4, true>::launch(m, grid, st) : MixedLaunch<4, false>::launch(m, grid, st);
     return fast ? MixedLaunch<6, true>::launch(m, grid, st) : MixedLaunch<6, false>::launch(m, grid, st);

@@ -289,8 +289,7 @@ __device__ __forceinline__ void pair_sync(int id)
 }
 
 // StageBlock's r stages on a pair of sequences (same index algebra, lane
-// ownership and twiddles; `tw` holds the twiddle table as
-// (wx, wx, wy, wy) per entry).
+// ownership and twiddles; `tw` is the same float2 table as StageBlock's).
 template <int LOG_N, int G2, int L0, bool FAST>
 struct PairBlock {
     static constexpr int N = 1 << LOG_N;
@@ -301,7 +300,7 @@ struct PairBlock {
     static constexpr int C = (N >> r) / G2;
     static constexpr int w = LOG_N - r - L0;
 
-    __device__ __forceinline__ static void run(ulonglong2* seq, const ulonglong2* tw, int lane, int bar_id)
+    __device__ __forceinline__ static void run(ulonglong2* seq, const float2* tw, int lane, int bar_id)
     {
         f32x2 re[C][RR], im[C][RR];
 #pragma unroll
@@ -323,13 +322,17 @@ struct PairBlock {
             for (int s = 0; s < r; ++s) {
                 const int half = RR >> (s + 1);
                 const int l = L0 + s;
-                const ulonglong2* twl = tw + (N - (N >> l));
+                const float2* twl = tw + (N - (N >> l));
 #pragma unroll
                 for (int S = 0; S < RR; ++S) {
                     if (S & half) continue;
                     const int Rk = S & (half - 1);
-                    const ulonglong2 wv = twl[(Rk << w) | P];
-                    butterfly_pair<FAST>(re[k][S], im[k][S], re[k][S + half], im[k][S + half], wv.x, wv.y);
+                    // One 8-byte load, duplicated into both lanes of each
+                    // f32x2 in registers (a 16-byte (wx, wx, wy, wy) table
+                    // entry costs twice the shared-memory wavefronts).
+                    const float2 wv = twl[(Rk << w) | P];
+                    butterfly_pair<FAST>(re[k][S], im[k][S], re[k][S + half], im[k][S + half], px_pack(wv.x, wv.x),
+                                         px_pack(wv.y, wv.y));
                 }
             }
         }
@@ -351,12 +354,10 @@ struct PairBlock {
 
 // The unnormalised inverse transforms of the pair at `seq`.
 template <int LOG_N, int G2, bool FAST>
-__device__ __forceinline__ void fft_pair(ulonglong2* seq, const ulonglong2* tw, int lane, int bar_id)
+__device__ __forceinline__ void fft_pair(ulonglong2* seq, const float2* tw, int lane, int bar_id)
 {
     PairBlock<LOG_N, G2, 0, FAST>::run(seq, tw, lane, bar_id);
 }
 
-// Twiddle entry of the pair table: (wx, wx, wy, wy).
-__device__ __forceinline__ float4 pair_twiddle(float2 w) { return make_float4(w.x, w.x, w.y, w.y); }
 
 }  // namespace ocean_b200

@@ -249,6 +249,7 @@ public:
         uint64_t keep = UINT64_MAX;  // keep freed memory cached in the pool
         check(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep), "pool attribute");
         error_ = DevBuf<unsigned>(1);
+        mix_ticket_ = DevBuf<unsigned>(1);
         check(cudaMemsetAsync(error_.p, 0, sizeof(unsigned), stream_), "memset");
         ctxs_.resize(desc_.max_inflight);
         // Staging for a full batch of query points plus the tables and sources
@@ -907,6 +908,14 @@ private:
         uint32_t kernels = 0;
         check(cudaEventRecord(c->start, stream_), "event");
         if (in_bytes > 0) check(cudaMemcpyAsync(d, h, in_bytes, cudaMemcpyHostToDevice, stream_), "batch upload");
+        // The batch's oceans: one launch for every size when the sizes allow
+        // it (mixed_frame_kernel: N up to 1024, one field count, an FP32
+        // form), else one persistent launch per size.
+        bool one_launch = oparts.size() > 1 && oparts.size() <= static_cast<size_t>(kMaxMixedGroups) &&
+                          desc_.fft_form != OCEAN_FFT_TENSOR;
+        for (const OceanPart& p : oparts)
+            one_launch = one_launch && mixed_size_ok(p.k->log_n) && p.k->nf == oparts[0].k->nf;
+        MixedArgs m{};
         for (const OceanPart& p : oparts) {
             OceanKind* k = p.k;
             const int count = static_cast<int>(p.count);
@@ -918,6 +927,16 @@ private:
             a.table = reinterpret_cast<const OceanSlot*>(d + p.slots);
             a.ocean_base = 0;
             a.chunk = count;
+            if (one_launch) {
+                MixedGroup& g = m.g[m.groups++];
+                g.a = a;
+                g.rows_done = k->queue + 1;
+                g.cols_done = k->queue + 1 + p.count;
+                g.count = count;
+                g.slots = std::min(count, 3);
+                g.log_n = k->log_n;
+                continue;
+            }
             QueueArgs q;
             q.ticket = k->queue;
             q.rows_done = k->queue + 1;
@@ -928,6 +947,31 @@ private:
             q.wait_ns = 1000000000ull;
             const int grid = static_cast<int>(std::min<uint64_t>(k->grid, uint64_t(count) * k->n));
             check(launch_frame(k->log_n, k->nf, desc_.fft_form, false, a, q, grid, stream_), "frame kernel");
+            ++kernels;
+        }
+        if (one_launch) {
+            // Largest sizes first, so the short tasks fill the wave's tail.
+            std::sort(m.g, m.g + m.groups, [](const MixedGroup& x, const MixedGroup& y) { return x.log_n > y.log_n; });
+            uint32_t first = 0;
+            for (int i = 0; i < m.groups; ++i) {
+                m.g[i].first = first;
+                first += mixed_tasks(m.g[i].log_n, m.g[i].count);
+            }
+            m.total = first;
+            m.ticket = mix_ticket_.p;
+            m.error = error_.p;
+            m.wait_ns = 1000000000ull;
+            const int nf = oparts[0].k->nf;
+            const bool fast = desc_.fft_form == OCEAN_FFT_FAST;
+            int& grid = mix_grid_[nf == 6 ? 1 : 0];
+            if (grid == 0) {
+                const int per_sm = mixed_blocks_per_sm(nf, fast);
+                if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "mixed frame occupancy");
+                grid = per_sm * sms_;
+            }
+            check(cudaMemsetAsync(mix_ticket_.p, 0, sizeof(unsigned), stream_), "ticket reset");
+            check(launch_mixed_frame(nf, fast, m, static_cast<int>(std::min<uint64_t>(grid, first)), stream_),
+                  "mixed frame kernel");
             ++kernels;
         }
         const IWaveSource* dev_src = reinterpret_cast<const IWaveSource*>(d + src_off);
@@ -1164,6 +1208,8 @@ private:
     cudaStream_t stream_ = nullptr;
     cudaMemPool_t pool_ = nullptr;
     DevBuf<unsigned> error_;
+    DevBuf<unsigned> mix_ticket_;  // the one-launch frame's ticket
+    int mix_grid_[2] = {0, 0};     // its resident grid, by field count (4, 6)
     std::vector<std::unique_ptr<BatchCtx>> ctxs_;
     std::deque<BatchCtx*> free_ctx_, inflight_;
     std::vector<std::unique_ptr<OceanKind>> ocean_kinds_;

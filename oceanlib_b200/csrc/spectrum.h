@@ -106,7 +106,7 @@ cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned
 // ticket must be zero at launch.
 constexpr int kMaxMixedGroups = 6;
 struct MixedGroup {
-    FrameArgs a;          // the group's arrays (ocean_base 0, table null)
+    FrameArgs a;          // the group's arrays, or its pointer table (ocean_base 0)
     unsigned* rows_done;  // [count]
     unsigned* cols_done;  // [count]
     uint32_t first;       // first ticket of the group
