@@ -141,3 +141,21 @@ def test_one_launch_schedule_refused_where_sizes_do_not_qualify():
     ens.set_schedule(ob.OceanEnsemble.SEQUENTIAL)
     assert ens.schedule_kind == ob.OceanEnsemble.SEQUENTIAL
     ens.close()
+
+
+def test_sharded_ensemble_holds_this_ranks_share():
+    # Rank 1 of 2: the router's share of config 4, advanced on this GPU; its
+    # oceans are the oracle's.
+    from oceanlib_b200 import router
+
+    descs = W.ensemble_64(16)
+    sh = router.ShardedEnsemble(descs, rank=1, world=2, autotune=False)
+    assert sh.indices == router.assign(descs, 2)[1]
+    sh.update(4.5)
+    sh.synchronize()
+    for local in (0, len(sh.indices) - 1):
+        i = sh.indices[local]
+        od, on, _ = O.update(descs[i], 4.5)
+        d, n = sh.ensemble.read(local)
+        assert np.array_equal(bits(d), bits(od)) and np.array_equal(bits(n), bits(on)), i
+    sh.close()
