@@ -722,13 +722,20 @@ OCEAN_API ocean_status ocean_batch_read_profile(ocean_batch* batch, ocean_pass_p
  * plan 0 is the default; N = 256 and 512 also have single-row tasks (plan
  * 1), N = 1024 sequences over 64 lanes with single-row tasks (plan 1). Every
  * plan gives the same bits. plan_count is 1 or 2; set_plan returns
- * OCEAN_ERROR_INVALID_ARG for a plan the batch does not have.
- * ocean_batch_autotune_plan times a few frames of each plan on the batch's
- * stream (advancing any persistent foam), keeps the fastest and writes the
- * median milliseconds per plan to `ms` (plan_count entries; may be NULL). */
+ * OCEAN_ERROR_INVALID_ARG for a plan the batch does not have. The ring
+ * slots are how many oceans' row-pass results may be in flight: 2 or 3 (1
+ * for a batch of one ocean; at most the ocean count); fewer keep a large
+ * size's ring in L2, more overlap an ocean's rows with the previous ones'
+ * columns; same bits. Other values return OCEAN_ERROR_INVALID_ARG.
+ * ocean_batch_autotune_plan times a few frames of every (plan, ring slots)
+ * combination on the batch's stream (advancing any persistent foam), keeps
+ * the fastest and writes each plan's best median milliseconds to `ms`
+ * (plan_count entries; may be NULL). */
 OCEAN_API ocean_status ocean_batch_set_plan(ocean_batch* batch, int32_t plan);
 OCEAN_API int32_t ocean_batch_plan(const ocean_batch* batch);
 OCEAN_API int32_t ocean_batch_plan_count(const ocean_batch* batch);
+OCEAN_API ocean_status ocean_batch_set_ring_slots(ocean_batch* batch, int32_t slots);
+OCEAN_API int32_t ocean_batch_ring_slots(const ocean_batch* batch);
 OCEAN_API ocean_status ocean_batch_autotune_plan(ocean_batch* batch, double* ms);
 
 /* Kernels this batch has launched (all kinds) since it was created. */

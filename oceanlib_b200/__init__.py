@@ -345,11 +345,24 @@ class OceanBatch:
             raise ValueError(f"plan {plan} is not available for this batch")
         _check(st, "ocean_batch_set_plan")
 
+    @property
+    def ring_slots(self) -> int:
+        return lib().ocean_batch_ring_slots(self._h)
+
+    def set_ring_slots(self, slots: int) -> None:
+        """Intermediate ring depth of the persistent kernel: 2 or 3 oceans in
+        flight (as allocated; 1 for a batch of one ocean)."""
+        st = lib().ocean_batch_set_ring_slots(self._h, int(slots))
+        if st == abi.OCEAN_ERROR_INVALID_ARG:
+            raise ValueError(f"{slots} ring slots are not available for this batch")
+        _check(st, "ocean_batch_set_ring_slots")
+
     def autotune_plan(self) -> list:
-        """Time every plan, keep the fastest; median ms per plan."""
-        ms = np.zeros(max(1, self.plan_count), np.float64)
+        """Time every (plan, ring slots) combination, keep the fastest; each
+        plan's best median ms (empty when there is nothing to choose)."""
+        ms = np.full(max(1, self.plan_count), -1.0, np.float64)
         _check(lib().ocean_batch_autotune_plan(self._h, ms.ctypes.data), "ocean_batch_autotune_plan")
-        return list(ms[: self.plan_count]) if self.plan_count > 1 else []
+        return [float(m) for m in ms[: self.plan_count] if m >= 0.0]
 
     @property
     def launch_count(self) -> int:

@@ -247,6 +247,7 @@ public:
         top_ = DevBuf<double>(count_ * kTimeSlots);
         top_host_ = HostBuf<double>(count_ * kTimeSlots);
         slots_ = static_cast<int>(std::min<uint32_t>(count_, 3));
+        max_slots_ = slots_;
         // The persistent kernel's ring needs `slots_` oceans; the row/column
         // passes one per chunk ocean (all a batch above N = 1024 ever uses).
         const uint32_t inter_oceans =
@@ -741,36 +742,67 @@ public:
         plan_ = plan;
     }
 
+    // Intermediate ring slots of the persistent kernel: how many oceans'
+    // row-pass results may be in flight (2 or 3, as allocated; a batch of one
+    // ocean has 1). Fewer slots keep a large size's ring in L2; more let an
+    // ocean's rows overlap the previous oceans' columns. One slot with more
+    // oceans would make R(b + 1) wait for C(b), whose tickets come after it
+    // in the queue: the queue is only deadlock-free from two slots up.
+    int ring_slots() const { return slots_; }
+    int min_ring_slots() const { return std::min(max_slots_, 2); }
+    void set_ring_slots(int slots)
+    {
+        if (slots < min_ring_slots() || slots > max_slots_) throw std::invalid_argument("ring slots");
+        check(cudaStreamSynchronize(stream_), "sync");
+        slots_ = slots;
+    }
+
     // The batch's autotuner: times `frames` frames (after two untimed ones)
-    // of every task plan on the batch's own stream, keeps the fastest and
-    // returns the median times in milliseconds, plan by plan. Persistent
-    // foam state advances with the timed frames (a clear() resets it).
+    // of every task plan with every ring depth (3 and 2 slots, as allocated)
+    // on the batch's own stream, keeps the fastest combination and returns,
+    // plan by plan, the median time in milliseconds of that plan's best ring
+    // depth. Persistent foam state advances with the timed frames (a clear()
+    // resets it). Nothing to choose (one plan, one slot): an empty result.
     std::vector<double> autotune_plan(int frames = 5)
     {
         std::vector<double> ms;
-        if (plan_count() < 2) return ms;
+        if (!persistent_ || (plan_count() < 2 && max_slots_ <= min_ring_slots())) return ms;
         cudaEvent_t e0, e1;
         check(cudaEventCreate(&e0), "event");
         check(cudaEventCreate(&e1), "event");
+        double best = 1e30;
+        int best_plan = 0, best_slots = max_slots_;
         for (int v = 0; v < plan_count(); ++v) {
-            set_plan(v);
-            std::vector<float> t;
-            for (int k = 0; k < frames + 2; ++k) {
-                const double time = 1.0 + k / 60.0;
-                check(cudaEventRecord(e0, stream_), "event");
-                update(&time, false, foam_on_ ? foam_.fixed_dt : 0.0f, stream_);
-                check(cudaEventRecord(e1, stream_), "event");
-                check(cudaEventSynchronize(e1), "event");
-                float m = 0.0f;
-                check(cudaEventElapsedTime(&m, e0, e1), "elapsed");
-                if (k >= 2) t.push_back(m);
+            double plan_best = 1e30;
+            for (int sl = max_slots_; sl >= min_ring_slots(); --sl) {
+                set_plan(v);
+                set_ring_slots(sl);
+                std::vector<float> t;
+                for (int k = 0; k < frames + 2; ++k) {
+                    const double time = 1.0 + k / 60.0;
+                    check(cudaEventRecord(e0, stream_), "event");
+                    update(&time, false, foam_on_ ? foam_.fixed_dt : 0.0f, stream_);
+                    check(cudaEventRecord(e1, stream_), "event");
+                    check(cudaEventSynchronize(e1), "event");
+                    float m = 0.0f;
+                    check(cudaEventElapsedTime(&m, e0, e1), "elapsed");
+                    if (k >= 2) t.push_back(m);
+                }
+                std::sort(t.begin(), t.end());
+                const double med = t[t.size() / 2];
+                plan_best = std::min(plan_best, med);
+                if (med < best) {
+                    best = med;
+                    best_plan = v;
+                    best_slots = sl;
+                }
             }
-            std::sort(t.begin(), t.end());
-            ms.push_back(t[t.size() / 2]);
+            ms.push_back(plan_best);
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        set_plan(static_cast<int>(std::min_element(ms.begin(), ms.end()) - ms.begin()));
+        set_plan(best_plan);
+        set_ring_slots(best_slots);
         if (take_error()) throw TimeoutError();
         return ms;
     }
@@ -913,7 +945,8 @@ private:
     uint64_t prof_n_[4] = {0, 0, 0, 0};
     double prof_ms_[4] = {0.0, 0.0, 0.0, 0.0};
     bool persistent_ = true;
-    int slots_ = 1;
+    int slots_ = 1;      // intermediate ring slots the persistent kernel uses
+    int max_slots_ = 1;  // slots the ring buffer holds
     int frame_grid_[2][2] = {{0, 0}, {0, 0}};
     int plan_ = 0;  // the persistent kernel's task plan (frame_plan_count)
     double grid_share_ = 1.0;
@@ -1540,8 +1573,12 @@ private:
             const std::vector<double> ms = b->autotune_plan(frames);
             if (ms.empty()) continue;
             char pb[128];
-            std::snprintf(pb, sizeof(pb), "%sN=%u plan %d (%.3f / %.3f ms)", plans.empty() ? "" : ", ", b->size(),
-                          b->plan(), ms[0], ms[1]);
+            if (ms.size() > 1)
+                std::snprintf(pb, sizeof(pb), "%sN=%u plan %d, %d ring slots (%.3f / %.3f ms)",
+                              plans.empty() ? "" : ", ", b->size(), b->plan(), b->ring_slots(), ms[0], ms[1]);
+            else
+                std::snprintf(pb, sizeof(pb), "%sN=%u %d ring slots (%.3f ms)", plans.empty() ? "" : ", ",
+                              b->size(), b->ring_slots(), ms[0]);
             plans += pb;
         }
         std::vector<double> alone(batches_.size());
@@ -1556,18 +1593,43 @@ private:
         apply_shares(alone);
         const double t_meas = time_frames(frames, [&](double t) { update(t, stream_); });
         double t_mixed = -1.0;
+        std::vector<int> kept;  // each size's ring depth from its own tuning
         if (mixed_ok_) {
             mixed_ = true;
             t_mixed = time_frames(frames, [&](double t) { update(t, stream_); });
+            // The one launch again with every group at its shallowest ring:
+            // all sizes' intermediates share L2 in this schedule.
+            bool shallower = false;
+            for (auto& b : batches_) {
+                kept.push_back(b->ring_slots());
+                shallower = shallower || b->ring_slots() > b->min_ring_slots();
+            }
+            if (shallower) {
+                for (auto& b : batches_) b->set_ring_slots(b->min_ring_slots());
+                const double t2 = time_frames(frames, [&](double t) { update(t, stream_); });
+                if (t2 < t_mixed) {
+                    t_mixed = t2;
+                    mixed_shallow_ = true;
+                } else {
+                    for (size_t g = 0; g < batches_.size(); ++g) batches_[g]->set_ring_slots(kept[g]);
+                }
+            }
             mixed_ = false;
         }
         char buf[256];
-        if (t_mixed >= 0.0 && t_mixed <= t_seq && t_mixed <= t_work && t_mixed <= t_meas) {
+        const bool mixed_wins = t_mixed >= 0.0 && t_mixed <= t_seq && t_mixed <= t_work && t_mixed <= t_meas;
+        if (!mixed_wins && mixed_shallow_) {
+            // The shallow rings were for the one launch only.
+            for (size_t g = 0; g < batches_.size(); ++g) batches_[g]->set_ring_slots(kept[g]);
+            mixed_shallow_ = false;
+        }
+        if (mixed_wins) {
             mixed_ = true;
             concurrent_ = false;
             full_grids();
-            std::snprintf(buf, sizeof(buf), "mixed: every size in one persistent launch (%.3f ms; sequential %.3f, "
-                          "work-share %.3f, measured-share %.3f)", t_mixed, t_seq, t_work, t_meas);
+            std::snprintf(buf, sizeof(buf), "mixed: every size in one persistent launch%s (%.3f ms; sequential %.3f, "
+                          "work-share %.3f, measured-share %.3f)", mixed_shallow_ ? " at 2 ring slots" : "",
+                          t_mixed, t_seq, t_work, t_meas);
         } else if (t_seq <= t_work && t_seq <= t_meas) {
             concurrent_ = false;
             full_grids();
@@ -1597,6 +1659,7 @@ private:
     // the mixed-size launch
     bool mixed_ok_ = false;
     bool mixed_ = false;
+    bool mixed_shallow_ = false;  // the one launch timed fastest with the shallowest rings
     int mix_grid_ = 0;
     std::vector<size_t> mix_order_;
     DevBuf<unsigned> mix_words_;
@@ -2017,6 +2080,14 @@ ocean_status ocean_batch_set_plan(ocean_batch* batch, int32_t plan)
 int32_t ocean_batch_plan(const ocean_batch* batch) { return batch == nullptr ? -1 : batch->impl.plan(); }
 
 int32_t ocean_batch_plan_count(const ocean_batch* batch) { return batch == nullptr ? 0 : batch->impl.plan_count(); }
+
+ocean_status ocean_batch_set_ring_slots(ocean_batch* batch, int32_t slots)
+{
+    if (batch == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { batch->impl.set_ring_slots(slots); });
+}
+
+int32_t ocean_batch_ring_slots(const ocean_batch* batch) { return batch == nullptr ? 0 : batch->impl.ring_slots(); }
 
 ocean_status ocean_batch_autotune_plan(ocean_batch* batch, double* ms)
 {

@@ -1,7 +1,8 @@
 """The persistent kernel's task plans (0 default; 1 single-row tasks at
-N = 256 and 512, 64 lanes a sequence with single-row tasks at N = 1024):
-every plan gives the reference's bits, with and without velocity and with
-persistent foam, and the batch autotuner keeps a plan that exists."""
+N = 256 and 512, 64 lanes a sequence with single-row tasks at N = 1024) and
+intermediate ring depths (2 or 3 oceans in flight): every combination gives
+the reference's bits, with and without velocity and with persistent foam,
+and the batch autotuner keeps a combination that exists."""
 import hashlib
 import json
 from pathlib import Path
@@ -40,9 +41,10 @@ def test_every_plan_is_bit_exact(n, velocity):
     batch = ob.OceanBatch(descs)
     assert batch.plan_count == 2
     cells = n * n
-    for plan in (1, 0):
+    for plan, slots in ((1, 3), (1, 2), (0, 2), (0, 3)):
         batch.set_plan(plan)
-        assert batch.plan == plan
+        batch.set_ring_slots(slots)
+        assert batch.plan == plan and batch.ring_slots == slots
         disp = np.empty((3 * cells, 4), np.float32)
         nrm = np.empty_like(disp)
         vel = np.empty_like(disp) if velocity else None
@@ -56,6 +58,10 @@ def test_every_plan_is_bit_exact(n, velocity):
                 assert np.array_equal(bits(vel[sl]), bits(ov)), (n, plan, k)
     with pytest.raises(ValueError):
         batch.set_plan(2)
+    with pytest.raises(ValueError):
+        batch.set_ring_slots(4)
+    with pytest.raises(ValueError):
+        batch.set_ring_slots(1)  # one slot: the queue would not be deadlock-free
     batch.close()
 
 
@@ -82,6 +88,7 @@ def test_batch_autotuner_keeps_an_existing_plan():
     ms = batch.autotune_plan()
     assert len(ms) == 2 and all(m > 0 for m in ms)
     assert batch.plan == int(np.argmin(ms))
+    assert batch.ring_slots in (2, 3)
     small = ob.OceanBatch([ob.OceanDesc(size=64, seed=3)])
     assert small.plan_count == 1 and small.autotune_plan() == []
     small.close()
