@@ -939,6 +939,10 @@ def main():
             "clocks": clk,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "api": "ocean_batch_update_host (pinned host buffers)",
+                    # device -> host bytes per second over the end-to-end steps: the
+                    # PCIe link's rate, which bounds this figure (the frame itself
+                    # takes a few per cent of each step)
+                    "d2h_gbs_per_gpu": d2h * e2e_steps / e2e_s / 1e9,
                     "rgba16": e2e_half},
         }
         if tc is not None:
