@@ -727,15 +727,21 @@ OCEAN_API ocean_status ocean_batch_read_profile(ocean_batch* batch, ocean_pass_p
  * for a batch of one ocean; at most the ocean count); fewer keep a large
  * size's ring in L2, more overlap an ocean's rows with the previous ones'
  * columns; same bits. Other values return OCEAN_ERROR_INVALID_ARG.
- * ocean_batch_autotune_plan times a few frames of every (plan, ring slots)
- * combination on the batch's stream (advancing any persistent foam), keeps
- * the fastest and writes each plan's best median milliseconds to `ms`
- * (plan_count entries; may be NULL). */
+ * The deferred publish (1) lets a CTA of the persistent kernel announce a
+ * finished row task only once its next task has staged its inputs, so the
+ * release does not stall it; 0 announces it before the next task. Same
+ * bits; the default is 1 with velocity, 0 without.
+ * ocean_batch_autotune_plan times a few frames of every (plan, ring slots,
+ * publish) combination on the batch's stream (advancing any persistent
+ * foam), keeps the fastest and writes each plan's best median milliseconds
+ * to `ms` (plan_count entries; may be NULL). */
 OCEAN_API ocean_status ocean_batch_set_plan(ocean_batch* batch, int32_t plan);
 OCEAN_API int32_t ocean_batch_plan(const ocean_batch* batch);
 OCEAN_API int32_t ocean_batch_plan_count(const ocean_batch* batch);
 OCEAN_API ocean_status ocean_batch_set_ring_slots(ocean_batch* batch, int32_t slots);
 OCEAN_API int32_t ocean_batch_ring_slots(const ocean_batch* batch);
+OCEAN_API ocean_status ocean_batch_set_deferred_publish(ocean_batch* batch, int32_t defer);
+OCEAN_API int32_t ocean_batch_deferred_publish(const ocean_batch* batch);
 OCEAN_API ocean_status ocean_batch_autotune_plan(ocean_batch* batch, double* ms);
 
 /* Kernels this batch has launched (all kinds) since it was created. */

@@ -357,9 +357,21 @@ class OceanBatch:
             raise ValueError(f"{slots} ring slots are not available for this batch")
         _check(st, "ocean_batch_set_ring_slots")
 
+    @property
+    def deferred_publish(self) -> bool:
+        return lib().ocean_batch_deferred_publish(self._h) == 1
+
+    def set_deferred_publish(self, defer: bool) -> None:
+        """When the persistent kernel announces a finished row task: once the
+        CTA's next task has staged its inputs (True), or before that task
+        (False). Same bits either way."""
+        _check(lib().ocean_batch_set_deferred_publish(self._h, 1 if defer else 0),
+               "ocean_batch_set_deferred_publish")
+
     def autotune_plan(self) -> list:
-        """Time every (plan, ring slots) combination, keep the fastest; each
-        plan's best median ms (empty when there is nothing to choose)."""
+        """Time every (plan, ring slots, publish) combination, keep the
+        fastest; each plan's best median ms (empty for a batch that runs the
+        per-chunk passes, with nothing to choose)."""
         ms = np.full(max(1, self.plan_count), -1.0, np.float64)
         _check(lib().ocean_batch_autotune_plan(self._h, ms.ctypes.data), "ocean_batch_autotune_plan")
         return [float(m) for m in ms[: self.plan_count] if m >= 0.0]

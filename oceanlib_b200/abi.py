@@ -270,6 +270,8 @@ SIGNATURES = {
     "ocean_batch_plan_count": (C.c_int32, [C.c_void_p]),
     "ocean_batch_set_ring_slots": (C.c_int, [C.c_void_p, C.c_int32]),
     "ocean_batch_ring_slots": (C.c_int32, [C.c_void_p]),
+    "ocean_batch_set_deferred_publish": (C.c_int, [C.c_void_p, C.c_int32]),
+    "ocean_batch_deferred_publish": (C.c_int32, [C.c_void_p]),
     "ocean_batch_autotune_plan": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ocean_frame_static_scratch": (C.c_int, [C.c_uint32, C.c_float, C.c_double, C.c_float,
                                              C.c_float, C.c_void_p, C.c_void_p, C.c_void_p,

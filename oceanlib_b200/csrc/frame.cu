@@ -276,11 +276,42 @@ __device__ __forceinline__ void h0_rows_wait(uint64_t* bar, uint32_t parity, uns
     }
 }
 
+// Release add at GPU scope: every write that happens before it (the CTA's,
+// through the preceding barrier) is visible to an acquirer that sees the sum.
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// The persistent queues' counter adds that a task makes once its inputs are
+// in shared memory (thread 0; pub = {previous task, this task}, either may be
+// null). pub[0] is the CTA's previous task: its writes were all issued before
+// the barrier this task began with, and the time the task spent loading lets
+// them drain, so the release costs little here, where at the top of the loop
+// it stalled the whole CTA. pub[1] is this task itself when it is a column
+// task: it reads its intermediate slot only while staging, so the slot is
+// free for the next ocean's row tasks from here on.
+__device__ __forceinline__ void publish_staged(unsigned* const* pub, int tid)
+{
+    if (pub != nullptr && tid == 0) {
+        if (pub[0] != nullptr) red_release_add(pub[0], 1u);
+        if (pub[1] != nullptr) red_release_add(pub[1], 1u);
+    }
+}
+
 template <class P, int NF, bool FAST>
 __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int group,
                                          float2* __restrict__ inter_slot, float2* smem,
                                          const float2* tws, int tid, uint64_t* h0_bar, uint32_t h0_parity,
-                                         TcEngine<NF>* eng = nullptr, unsigned* error = nullptr)
+                                         TcEngine<NF>* eng = nullptr, unsigned* error = nullptr,
+                                         unsigned* const* pub = nullptr)
 {
     using D = P;
     constexpr int LOG_N = P::LOG_N;
@@ -369,6 +400,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     }
     h0_rows_wait(h0_bar, h0_parity, error);
     __syncthreads();
+    publish_staged(pub, tid);
 
     // Evolve (src/core/evolve.cpp:28-121 and :123-184), one cell at a time.
 #pragma unroll
@@ -430,7 +462,7 @@ template <class P, int NF, bool FAST, bool FOAM, int W, bool CG>
 __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int strip,
                                          const float2* __restrict__ inter_slot, float2* smem,
                                          const float2* tws, int tid, TcEngine<NF>* eng = nullptr,
-                                         unsigned* error = nullptr)
+                                         unsigned* error = nullptr, unsigned* const* pub = nullptr)
 {
     constexpr int N = P::N, G = P::G, SEQ = P::SEQ, SEQ4 = P::SEQ4;
     constexpr int NT = NF * W * G;
@@ -496,6 +528,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
         }
     }
     __syncthreads();
+    publish_staged(pub, tid);
 
     transform_all<P, FAST, NF * W, W>(data, tws, tid, eng, error);
     if constexpr (FSTEP) asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's window copies
@@ -633,20 +666,6 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 
-// Release add at GPU scope: every write that happens before it (the CTA's,
-// through the preceding barrier) is visible to an acquirer that sees the sum.
-__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v)
-{
-    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p)
-{
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
 // Spin until *counter >= target or the error word is set or limit_ns passes.
 // Returns false on timeout / abort.
 __device__ bool wait_at_least(const unsigned* counter, unsigned target, unsigned* error,
@@ -718,7 +737,8 @@ frame_kernel(FrameArgs a, QueueArgs q)
     __shared__ int s_ok;
     // Thread 0's queue state between tasks, kept in shared memory so that it
     // takes no registers in the task code that every thread runs.
-    __shared__ unsigned* s_publish;
+    __shared__ unsigned* s_publish;   // the current task's counter, added after it (row tasks)
+    __shared__ unsigned* s_pub[2];    // publish_staged's pair for the current task
     __shared__ unsigned s_next;
     __shared__ int s_have_next;
     __shared__ uint64_t h0_bar;   // the row tasks' h0 copies; phase k = k-th row task
@@ -751,11 +771,18 @@ frame_kernel(FrameArgs a, QueueArgs q)
         }
     };
 
-    // Thread 0 publishes the previous task with a release add (the barrier
-    // above it orders every thread's writes before it, the pattern grid-wide
-    // barriers use), then takes its next ticket and waits for that task's
-    // inputs; one barrier hands the ticket to the CTA. The publish comes
-    // before the wait: the next task may depend on the one just finished.
+    // Thread 0 takes the next ticket and checks that task's inputs; one
+    // barrier hands the ticket to the CTA. The previous task (a row task: a
+    // column task publishes itself once staged) is published with a release
+    // add (the barrier at the top of the loop orders every thread's writes
+    // before it, the pattern grid-wide barriers use). With q.defer, and the
+    // next task's inputs ready, the next task makes that add once it has
+    // staged them (publish_staged); otherwise it comes here, before the wait,
+    // since the next task may depend on the one just finished. So a CTA never
+    // waits while it holds an unpublished task. Deferring pays with velocity
+    // (64 x 512^2 with foam: 0.995 -> 0.984 ms a frame) and costs without it
+    // (64 x 512^2: 0.608 -> 0.624 ms), where the column tasks wait on the
+    // later adds; the batch defaults by field count and its autotuner times both.
     // Far from the end of the queue the following ticket is drawn one task
     // ahead; near the end tickets are drawn when a CTA is free, since a
     // ticket held by a CTA whose current task still waits would idle others
@@ -772,11 +799,14 @@ frame_kernel(FrameArgs a, QueueArgs q)
     while (true) {
         __syncthreads();  // previous task's writes issued; shared memory free
         if (tid == 0) {
-            if (s_publish != nullptr) red_release_add(s_publish, 1u);
+            unsigned* prev = s_publish;
             const unsigned t = s_have_next ? s_next : atomicAdd(q.ticket, 1u);
             s_have_next = 0;
             int ok = 1;
             unsigned* publish = nullptr;
+            unsigned* self = nullptr;
+            const unsigned* dep = nullptr;
+            unsigned need = 0;
             if (t < total) {
                 if (t + 2u * gridDim.x < total) {
                     s_next = atomicAdd(q.ticket, 1u);
@@ -786,13 +816,20 @@ frame_kernel(FrameArgs a, QueueArgs q)
                 unsigned ocean, idx;
                 decode(t, row, ocean, idx);
                 if (row) {
-                    if (ocean >= static_cast<unsigned>(q.slots))
-                        ok = wait_at_least(q.cols_done + (ocean - q.slots), CT, q.error, q.wait_ns);
+                    if (ocean >= static_cast<unsigned>(q.slots)) dep = q.cols_done + (ocean - q.slots), need = CT;
+                    publish = q.rows_done + ocean;
                 } else {
-                    ok = wait_at_least(q.rows_done + ocean, RT, q.error, q.wait_ns);
+                    dep = q.rows_done + ocean, need = RT;
+                    self = q.cols_done + ocean;
                 }
-                publish = row ? q.rows_done + ocean : q.cols_done + ocean;
             }
+            if (t >= total || !q.defer || (dep != nullptr && ld_acquire(dep) < need)) {
+                if (prev != nullptr) red_release_add(prev, 1u);
+                prev = nullptr;
+                if (dep != nullptr) ok = wait_at_least(dep, need, q.error, q.wait_ns);
+            }
+            s_pub[0] = prev;
+            s_pub[1] = self;
             s_publish = publish;
             s_ticket = t;
             s_ok = ok;
@@ -807,12 +844,12 @@ frame_kernel(FrameArgs a, QueueArgs q)
         const int abs_ocean = a.ocean_base + static_cast<int>(ocean);
         if (row) {
             row_task<P, NF, FAST>(a, abs_ocean, static_cast<int>(idx), a.inter + slot * slot_f2, smem, tws, tid,
-                                  &h0_bar, h0_parity, &eng, q.error);
+                                  &h0_bar, h0_parity, &eng, q.error, s_pub);
             h0_parity ^= 1u;
         } else {
             col_task<P, NF, FAST, FOAM, P::PW, true>(a, abs_ocean, static_cast<int>(idx),
                                                              a.inter + slot * slot_f2, smem, tws, tid,
-                                                             &eng, q.error);
+                                                             &eng, q.error, s_pub);
         }
     }
     if constexpr (TC) eng.release(tid);
@@ -904,16 +941,16 @@ __device__ __forceinline__ void mix_load_twiddles(float2* area, const float2* __
 template <int L, int NF, bool FAST>
 __device__ __noinline__ void mix_run(const MixedGroup& g, bool row, int ocean, int idx, float2* smem,
                                         const float2* tw_area, int tid, uint64_t* h0_bar, uint32_t h0_parity,
-                                        unsigned* error)
+                                        unsigned* error, unsigned* const* pub)
 {
     using P = MixPlan<L>;
     const unsigned slot = static_cast<unsigned>(ocean) % static_cast<unsigned>(g.slots);
     float2* inter = g.a.inter + static_cast<size_t>(slot) * P::N * P::N * NF;
     const float2* tws = tw_area + mix_tw_offset(L);
     if (row) {
-        row_task<P, NF, FAST>(g.a, ocean, idx, inter, smem, tws, tid, h0_bar, h0_parity, nullptr, error);
+        row_task<P, NF, FAST>(g.a, ocean, idx, inter, smem, tws, tid, h0_bar, h0_parity, nullptr, error, pub);
     } else {
-        col_task<P, NF, FAST, false, P::PW, true>(g.a, ocean, idx, inter, smem, tws, tid, nullptr, error);
+        col_task<P, NF, FAST, false, P::PW, true>(g.a, ocean, idx, inter, smem, tws, tid, nullptr, error, pub);
     }
 }
 
@@ -931,6 +968,7 @@ __global__ void __launch_bounds__(64 * NF, 768 / (64 * NF)) mixed_frame_kernel(M
     __shared__ unsigned s_ticket;
     __shared__ int s_ok, s_group, s_row, s_ocean, s_idx;
     __shared__ unsigned* s_publish;
+    __shared__ unsigned* s_pub[2];
     __shared__ unsigned s_next;
     __shared__ int s_have_next;
     __shared__ uint64_t h0_bar;
@@ -965,16 +1003,20 @@ __global__ void __launch_bounds__(64 * NF, 768 / (64 * NF)) mixed_frame_kernel(M
         s_have_next = 1;
     }
     // The persistent kernel's protocol (frame_kernel), with a group lookup:
-    // publish the previous task, take a ticket (one ahead far from the end),
-    // wait for the task's inputs, hand it to the CTA.
+    // take a ticket (one ahead far from the end), check the task's inputs,
+    // publish the previous task here only when they are not ready (before
+    // waiting), else let the task publish it once staged; hand it to the CTA.
     while (true) {
         __syncthreads();
         if (tid == 0) {
-            if (s_publish != nullptr) red_release_add(s_publish, 1u);
+            unsigned* prev = s_publish;
             const unsigned t = s_have_next ? s_next : atomicAdd(m.ticket, 1u);
             s_have_next = 0;
             int ok = 1;
             unsigned* publish = nullptr;
+            unsigned* self = nullptr;
+            const unsigned* dep = nullptr;
+            unsigned need = 0;
             if (t < m.total) {
                 if (t + 2u * gridDim.x < m.total) {
                     s_next = atomicAdd(m.ticket, 1u);
@@ -1002,17 +1044,24 @@ __global__ void __launch_bounds__(64 * NF, 768 / (64 * NF)) mixed_frame_kernel(M
                     }
                 }
                 if (row) {
-                    if (ocean >= static_cast<unsigned>(g.slots))
-                        ok = wait_at_least(g.cols_done + (ocean - g.slots), ct, m.error, m.wait_ns);
+                    if (ocean >= static_cast<unsigned>(g.slots)) dep = g.cols_done + (ocean - g.slots), need = ct;
+                    publish = g.rows_done + ocean;
                 } else {
-                    ok = wait_at_least(g.rows_done + ocean, rt, m.error, m.wait_ns);
+                    dep = g.rows_done + ocean, need = rt;
+                    self = g.cols_done + ocean;
                 }
-                publish = row ? g.rows_done + ocean : g.cols_done + ocean;
                 s_group = gi;
                 s_row = row ? 1 : 0;
                 s_ocean = static_cast<int>(ocean);
                 s_idx = static_cast<int>(idx);
             }
+            if (t >= m.total || !m.defer || (dep != nullptr && ld_acquire(dep) < need)) {
+                if (prev != nullptr) red_release_add(prev, 1u);
+                prev = nullptr;
+                if (dep != nullptr) ok = wait_at_least(dep, need, m.error, m.wait_ns);
+            }
+            s_pub[0] = prev;
+            s_pub[1] = self;
             s_publish = publish;
             s_ticket = t;
             s_ok = ok;
@@ -1022,12 +1071,12 @@ __global__ void __launch_bounds__(64 * NF, 768 / (64 * NF)) mixed_frame_kernel(M
         const MixedGroup& g = s_groups[s_group];
         const bool row = s_row != 0;
         switch (g.log_n) {
-            case 5: mix_run<5, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
-            case 6: mix_run<6, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
-            case 7: mix_run<7, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
-            case 8: mix_run<8, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
-            case 9: mix_run<9, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
-            default: mix_run<10, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error); break;
+            case 5: mix_run<5, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
+            case 6: mix_run<6, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
+            case 7: mix_run<7, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
+            case 8: mix_run<8, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
+            case 9: mix_run<9, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
+            default: mix_run<10, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
         }
         if (row) h0_parity ^= 1u;
     }

@@ -248,6 +248,7 @@ public:
         top_host_ = HostBuf<double>(count_ * kTimeSlots);
         slots_ = static_cast<int>(std::min<uint32_t>(count_, 3));
         max_slots_ = slots_;
+        defer_ = nf_ == 6;
         // The persistent kernel's ring needs `slots_` oceans; the row/column
         // passes one per chunk ocean (all a batch above N = 1024 ever uses).
         const uint32_t inter_oceans =
@@ -690,6 +691,7 @@ private:
         q.count = static_cast<int32_t>(k);
         q.slots = slots_;
         q.wait_ns = 1000000000ull;
+        q.defer = defer_ ? 1 : 0;
         const int grid = frame_grid(foam);
         // A share below 1 leaves SMs to batches of other sizes running
         // concurrently (the ensemble's schedule).
@@ -757,26 +759,43 @@ public:
         slots_ = slots;
     }
 
+    // When the persistent kernel publishes a finished row task: deferred
+    // into the CTA's next task once that task has staged its inputs (true),
+    // or before the next task (false); see QueueArgs::defer. The default is
+    // deferred with velocity (6 fields), not without.
+    bool deferred_publish() const { return defer_; }
+    void set_deferred_publish(bool defer)
+    {
+        check(cudaStreamSynchronize(stream_), "sync");
+        defer_ = defer;
+    }
+
     // The batch's autotuner: times `frames` frames (after two untimed ones)
     // of every task plan with every ring depth (3 and 2 slots, as allocated)
-    // on the batch's own stream, keeps the fastest combination and returns,
-    // plan by plan, the median time in milliseconds of that plan's best ring
-    // depth. Persistent foam state advances with the timed frames (a clear()
-    // resets it). Nothing to choose (one plan, one slot): an empty result.
+    // and both publish timings on the batch's own stream, keeps the fastest
+    // combination and returns, plan by plan, the median time in milliseconds
+    // of that plan's best combination. Persistent foam state advances with
+    // the timed frames (a clear() resets it). Nothing to choose (the per-chunk
+    // passes): an empty result.
     std::vector<double> autotune_plan(int frames = 5)
     {
         std::vector<double> ms;
-        if (!persistent_ || (plan_count() < 2 && max_slots_ <= min_ring_slots())) return ms;
+        if (!persistent_) return ms;
         cudaEvent_t e0, e1;
         check(cudaEventCreate(&e0), "event");
         check(cudaEventCreate(&e1), "event");
         double best = 1e30;
         int best_plan = 0, best_slots = max_slots_;
+        bool best_defer = defer_;
+        const bool defer0 = defer_;
         for (int v = 0; v < plan_count(); ++v) {
             double plan_best = 1e30;
-            for (int sl = max_slots_; sl >= min_ring_slots(); --sl) {
+            for (int c = 0; c < 2 * (max_slots_ - min_ring_slots() + 1); ++c) {
+                const int sl = max_slots_ - c / 2;
+                const bool defer = (c & 1) ? !defer0 : defer0;
                 set_plan(v);
                 set_ring_slots(sl);
+                set_deferred_publish(defer);
                 std::vector<float> t;
                 for (int k = 0; k < frames + 2; ++k) {
                     const double time = 1.0 + k / 60.0;
@@ -795,6 +814,7 @@ public:
                     best = med;
                     best_plan = v;
                     best_slots = sl;
+                    best_defer = defer;
                 }
             }
             ms.push_back(plan_best);
@@ -803,6 +823,7 @@ public:
         cudaEventDestroy(e1);
         set_plan(best_plan);
         set_ring_slots(best_slots);
+        set_deferred_publish(best_defer);
         if (take_error()) throw TimeoutError();
         return ms;
     }
@@ -947,6 +968,7 @@ private:
     bool persistent_ = true;
     int slots_ = 1;      // intermediate ring slots the persistent kernel uses
     int max_slots_ = 1;  // slots the ring buffer holds
+    bool defer_ = false; // QueueArgs::defer of the persistent kernel
     int frame_grid_[2][2] = {{0, 0}, {0, 0}};
     int plan_ = 0;  // the persistent kernel's task plan (frame_plan_count)
     double grid_share_ = 1.0;
@@ -1326,6 +1348,7 @@ public:
         for (auto& b : batches_)
             mixed_ok_ = mixed_ok_ && b->mixable() && b->nf() == batches_[0]->nf() && b->form() == batches_[0]->form();
         if (mixed_ok_) {
+            mix_defer_ = batches_[0]->nf() == 6;
             mix_words_ = DevBuf<unsigned>(2);  // ticket, error word
             check(cudaMemsetAsync(mix_words_.p, 0, 2 * sizeof(unsigned), stream_), "memset");
             for (size_t g = 0; g < batches_.size(); ++g) mix_order_.push_back(g);
@@ -1510,6 +1533,7 @@ private:
         m.ticket = mix_words_.p;
         m.error = mix_words_.p + 1;
         m.wait_ns = 1000000000ull;
+        m.defer = mix_defer_ ? 1 : 0;
         check(cudaMemsetAsync(mix_words_.p, 0, sizeof(unsigned), st), "ticket reset");
         const int grid = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(mix_grid_), first));
         check(launch_mixed_frame(batches_[0]->nf(), batches_[0]->form() == OCEAN_FFT_FAST, m, grid, st),
@@ -1563,7 +1587,9 @@ private:
 
     // Candidates: (1) sizes one after another, each with the whole GPU;
     // (2) concurrent, SM shares by the work estimate; (3) concurrent, shares
-    // by each size's measured stand-alone time. The fastest is kept.
+    // by each size's measured stand-alone time; (4) every size in one mixed
+    // launch, when the sizes allow it. The fastest is kept, the one launch
+    // unless another is more than 3 % faster.
     void autotune()
     {
         const int frames = 5;
@@ -1573,12 +1599,13 @@ private:
             const std::vector<double> ms = b->autotune_plan(frames);
             if (ms.empty()) continue;
             char pb[128];
+            const char* pub = b->deferred_publish() ? "deferred" : "immediate";
             if (ms.size() > 1)
-                std::snprintf(pb, sizeof(pb), "%sN=%u plan %d, %d ring slots (%.3f / %.3f ms)",
-                              plans.empty() ? "" : ", ", b->size(), b->plan(), b->ring_slots(), ms[0], ms[1]);
+                std::snprintf(pb, sizeof(pb), "%sN=%u plan %d, %d ring slots, %s publish (%.3f / %.3f ms)",
+                              plans.empty() ? "" : ", ", b->size(), b->plan(), b->ring_slots(), pub, ms[0], ms[1]);
             else
-                std::snprintf(pb, sizeof(pb), "%sN=%u %d ring slots (%.3f ms)", plans.empty() ? "" : ", ",
-                              b->size(), b->ring_slots(), ms[0]);
+                std::snprintf(pb, sizeof(pb), "%sN=%u %d ring slots, %s publish (%.3f ms)",
+                              plans.empty() ? "" : ", ", b->size(), b->ring_slots(), pub, ms[0]);
             plans += pb;
         }
         std::vector<double> alone(batches_.size());
@@ -1614,10 +1641,24 @@ private:
                     for (size_t g = 0; g < batches_.size(); ++g) batches_[g]->set_ring_slots(kept[g]);
                 }
             }
+            // And with the other publish timing.
+            mix_defer_ = !mix_defer_;
+            const double t3 = time_frames(frames, [&](double t) { update(t, stream_); });
+            if (t3 < t_mixed)
+                t_mixed = t3;
+            else
+                mix_defer_ = !mix_defer_;
             mixed_ = false;
         }
         char buf[256];
-        const bool mixed_wins = t_mixed >= 0.0 && t_mixed <= t_seq && t_mixed <= t_work && t_mixed <= t_meas;
+        // The concurrent schedules depend on how the hardware interleaves the
+        // CTAs of several launches: on 64 ensemble oceans the measured-share
+        // one took 0.858 ms a frame while tuning and 0.962 ms replayed later in
+        // the same process, where the one launch stays within 1 % (0.878 -
+        // 0.884 ms). So the one launch is kept unless another schedule is
+        // more than 3 % faster.
+        const double other = std::min(t_seq, std::min(t_work, t_meas));
+        const bool mixed_wins = t_mixed >= 0.0 && t_mixed <= 1.03 * other;
         if (!mixed_wins && mixed_shallow_) {
             // The shallow rings were for the one launch only.
             for (size_t g = 0; g < batches_.size(); ++g) batches_[g]->set_ring_slots(kept[g]);
@@ -1627,9 +1668,10 @@ private:
             mixed_ = true;
             concurrent_ = false;
             full_grids();
-            std::snprintf(buf, sizeof(buf), "mixed: every size in one persistent launch%s (%.3f ms; sequential %.3f, "
-                          "work-share %.3f, measured-share %.3f)", mixed_shallow_ ? " at 2 ring slots" : "",
-                          t_mixed, t_seq, t_work, t_meas);
+            std::snprintf(buf, sizeof(buf), "mixed: every size in one persistent launch%s, %s publish (%.3f ms; "
+                          "sequential %.3f, work-share %.3f, measured-share %.3f)",
+                          mixed_shallow_ ? " at 2 ring slots" : "", mix_defer_ ? "deferred" : "immediate", t_mixed,
+                          t_seq, t_work, t_meas);
         } else if (t_seq <= t_work && t_seq <= t_meas) {
             concurrent_ = false;
             full_grids();
@@ -1660,6 +1702,7 @@ private:
     bool mixed_ok_ = false;
     bool mixed_ = false;
     bool mixed_shallow_ = false;  // the one launch timed fastest with the shallowest rings
+    bool mix_defer_ = false;      // MixedArgs::defer (default: with velocity)
     int mix_grid_ = 0;
     std::vector<size_t> mix_order_;
     DevBuf<unsigned> mix_words_;
@@ -2088,6 +2131,17 @@ ocean_status ocean_batch_set_ring_slots(ocean_batch* batch, int32_t slots)
 }
 
 int32_t ocean_batch_ring_slots(const ocean_batch* batch) { return batch == nullptr ? 0 : batch->impl.ring_slots(); }
+
+ocean_status ocean_batch_set_deferred_publish(ocean_batch* batch, int32_t defer)
+{
+    if (batch == nullptr) return OCEAN_ERROR_INVALID_ARG;
+    return guarded([&] { batch->impl.set_deferred_publish(defer != 0); });
+}
+
+int32_t ocean_batch_deferred_publish(const ocean_batch* batch)
+{
+    return batch == nullptr ? -1 : (batch->impl.deferred_publish() ? 1 : 0);
+}
 
 ocean_status ocean_batch_autotune_plan(ocean_batch* batch, double* ms)
 {

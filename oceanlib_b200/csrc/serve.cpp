@@ -945,6 +945,7 @@ private:
             q.count = count;
             q.slots = std::min(count, 3);
             q.wait_ns = 1000000000ull;
+            q.defer = k->nf == 6 ? 1 : 0;
             const int grid = static_cast<int>(std::min<uint64_t>(k->grid, uint64_t(count) * k->n));
             check(launch_frame(k->log_n, k->nf, desc_.fft_form, false, a, q, grid, stream_), "frame kernel");
             ++kernels;
@@ -962,6 +963,7 @@ private:
             m.error = error_.p;
             m.wait_ns = 1000000000ull;
             const int nf = oparts[0].k->nf;
+            m.defer = nf == 6 ? 1 : 0;
             const bool fast = desc_.fft_form == OCEAN_FFT_FAST;
             int& grid = mix_grid_[nf == 6 ? 1 : 0];
             if (grid == 0) {

@@ -78,6 +78,11 @@ struct QueueArgs {
     int32_t count;        // oceans in the frame (inter holds `slots` of them)
     int32_t slots;        // intermediate ring slots
     unsigned long long wait_ns;
+    // 1: a row task's counter add waits until the CTA's next task has staged
+    // its inputs (when that task waits on nothing), so its release does not
+    // stall the CTA; 0: the add comes before the next task. Either way a
+    // column task adds its own counter once it has staged its slot.
+    int32_t defer;
 };
 
 // One persistent launch for the whole frame of `q.count` oceans (foam fused
@@ -121,6 +126,7 @@ struct MixedArgs {
     unsigned* ticket;
     unsigned* error;      // sticky: set when a bounded wait gives up
     unsigned long long wait_ns;
+    int32_t defer;        // as QueueArgs::defer, for every group
 };
 bool mixed_size_ok(int log_n);
 uint32_t mixed_tasks(int log_n, int count);

@@ -1,6 +1,7 @@
 """The persistent kernel's task plans (0 default; 1 single-row tasks at
 N = 256 and 512, 64 lanes a sequence with single-row tasks at N = 1024) and
-intermediate ring depths (2 or 3 oceans in flight): every combination gives
+intermediate ring depths (2 or 3 oceans in flight) and both publish timings
+of a finished row task: every combination gives
 the reference's bits, with and without velocity and with persistent foam,
 and the batch autotuner keeps a combination that exists."""
 import hashlib
@@ -41,10 +42,12 @@ def test_every_plan_is_bit_exact(n, velocity):
     batch = ob.OceanBatch(descs)
     assert batch.plan_count == 2
     cells = n * n
-    for plan, slots in ((1, 3), (1, 2), (0, 2), (0, 3)):
+    assert batch.deferred_publish == velocity  # the default: deferred with velocity
+    for plan, slots, defer in ((1, 3, True), (1, 2, False), (0, 2, True), (0, 3, False)):
         batch.set_plan(plan)
         batch.set_ring_slots(slots)
-        assert batch.plan == plan and batch.ring_slots == slots
+        batch.set_deferred_publish(defer)
+        assert batch.plan == plan and batch.ring_slots == slots and batch.deferred_publish == defer
         disp = np.empty((3 * cells, 4), np.float32)
         nrm = np.empty_like(disp)
         vel = np.empty_like(disp) if velocity else None
@@ -90,6 +93,33 @@ def test_batch_autotuner_keeps_an_existing_plan():
     assert batch.plan == int(np.argmin(ms))
     assert batch.ring_slots in (2, 3)
     small = ob.OceanBatch([ob.OceanDesc(size=64, seed=3)])
-    assert small.plan_count == 1 and small.autotune_plan() == []
+    assert small.plan_count == 1 and len(small.autotune_plan()) == 1  # the publish timing is still a choice
     small.close()
+    batch.close()
+
+
+@pytest.mark.parametrize("defer", [False, True])
+def test_publish_timing_many_oceans_many_frames(defer):
+    # 24 oceans of 256^2 with velocity, 3 ring slots: the queue's counters
+    # carry every ocean through the ring eight times a frame; four frames
+    # under each publish timing give the oracle's bits for every ocean.
+    n, count = 256, 24
+    descs = [ob.OceanDesc(size=n, patch_length=150.0 + 7.0 * k, wind_speed=9.0 + 0.5 * k,
+                          wind_direction=0.3 * k, choppiness=1.2, seed=300 + k, compute_velocity=True)
+             for k in range(count)]
+    batch = ob.OceanBatch(descs)
+    batch.set_deferred_publish(defer)
+    cells = n * n
+    disp = np.empty((count * cells, 4), np.float32)
+    nrm = np.empty_like(disp)
+    vel = np.empty_like(disp)
+    for f in range(4):
+        t = 3.0 + 0.75 * f
+        batch.update_host([t], 0.0, disp, nrm, vel)
+        for k in (0, 7, 13, count - 1) if f < 3 else range(count):
+            od, on, ov = O.update(descs[k], t)
+            sl = slice(k * cells, (k + 1) * cells)
+            assert np.array_equal(bits(disp[sl]), bits(od)), (defer, f, k)
+            assert np.array_equal(bits(nrm[sl]), bits(on)), (defer, f, k)
+            assert np.array_equal(bits(vel[sl]), bits(ov)), (defer, f, k)
     batch.close()
