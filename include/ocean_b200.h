@@ -464,7 +464,9 @@ typedef struct ocean_ensemble ocean_ensemble;
  * 4096), or - when every size is 32..1024, all with the same velocity flag,
  * in an FP32 form - one persistent launch whose work queue holds every
  * size's tasks. With autotune != 0 the schedule is chosen by timing each
- * candidate on this GPU at creation; otherwise it is the concurrent one. */
+ * candidate on this GPU at creation (the one launch unless another schedule
+ * is more than 3 % faster: concurrent launches vary from run to run);
+ * otherwise it is the concurrent one. */
 OCEAN_API ocean_ensemble* ocean_ensemble_create(const ocean_desc* oceans, uint32_t count,
                                                 int32_t autotune, ocean_status* out_status);
 OCEAN_API void ocean_ensemble_destroy(ocean_ensemble* ensemble);

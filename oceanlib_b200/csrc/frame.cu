@@ -1362,6 +1362,10 @@ cudaError_t col_dispatch_n(int nf, bool fast, bool foam, const FrameArgs& a, cud
 
 }  // namespace
 
+static_assert(frame_plan_count<8>(false) <= kMaxFramePlans && frame_plan_count<9>(false) <= kMaxFramePlans &&
+                  frame_plan_count<10>(false) <= kMaxFramePlans,
+              "the host sizes its per-plan tables by kMaxFramePlans");
+
 int frame_plan_count(int log_n, int form)
 {
     if (log_n < 4 || log_n > 10) return 0;

@@ -969,7 +969,7 @@ private:
     int slots_ = 1;      // intermediate ring slots the persistent kernel uses
     int max_slots_ = 1;  // slots the ring buffer holds
     bool defer_ = false; // QueueArgs::defer of the persistent kernel
-    int frame_grid_[2][2] = {{0, 0}, {0, 0}};
+    int frame_grid_[kMaxFramePlans][2] = {};  // [plan][foam]: CTAs of one wave
     int plan_ = 0;  // the persistent kernel's task plan (frame_plan_count)
     double grid_share_ = 1.0;
     DevBuf<unsigned> queue_, error_;

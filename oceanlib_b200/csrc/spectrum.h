@@ -96,6 +96,7 @@ cudaError_t launch_frame(int log_n, int nf, int form, bool fuse_foam, const Fram
 int frame_blocks_per_sm(int log_n, int nf, int form, bool fuse_foam, int plan = 0);
 // Task plans the persistent kernel has for a size and form (1 or 2).
 int frame_plan_count(int log_n, int form);
+constexpr int kMaxFramePlans = 2;  // frame_plan_count never exceeds it
 // Bounded waits that nothing completes (tests the timeout paths): on
 // `counter`, which nothing increments, setting *error, and on an mbarrier
 // nothing arrives at, setting *bar_error.
