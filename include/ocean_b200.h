@@ -301,12 +301,12 @@ typedef enum ocean_fft_form {
     OCEAN_FFT_TENSOR = 2 /* four-step DFT on the tensor cores (tcgen05):
                             operands cut into four signed 8-bit digits held
                             as FP16, exact digit products, levels combined
-                            in FP32; N = 512 */
+                            in FP32; N = 64, 128, 256 and 512 */
 } ocean_fft_form;
 
 /* `count` unnormalised inverse DFTs (sign +, as src/core/fft.cpp) of
- * complex sequences of length `size` (a power of two in [16, 1024]; 512 for
- * the tensor form), in the given form. `input` and
+ * complex sequences of length `size` (a power of two in [16, 1024]; 64 to
+ * 512 for the tensor form), in the given form. `input` and
  * `output` are DEVICE arrays of count * size interleaved (re, im) floats;
  * the call waits for the result. For accuracy checks of the forms. */
 OCEAN_API ocean_status ocean_dft_batch(uint32_t size, uint32_t count, int32_t form, const float* input,

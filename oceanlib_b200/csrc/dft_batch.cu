@@ -1,11 +1,13 @@
 // oceanlib-b200: batched 1-D inverse DFTs of device sequences in each form
 // (ocean_dft_batch): the radix-2 Stockham FFT (exact, bit-identical to
-// src/core/fft.cpp), its fast variant, and the tensor-core DFT (tc_dft.cuh).
+// src/core/fft.cpp), its fast variant, and the tensor-core DFT (tc_dft.cuh at
+// N = 512, tc_dft_small.cuh at N = 64, 128 and 256).
 // The frame kernel runs the same code on its rows and columns; this entry
 // point isolates the transform for accuracy checks against FP64.
 #include "ocean_device.cuh"
 #include "spectrum.h"
 #include "tc_dft.cuh"
+#include "tc_dft_small.cuh"
 
 namespace ocean_b200 {
 namespace {
@@ -77,6 +79,65 @@ dft_tc512_kernel(const float2* __restrict__ in, float2* __restrict__ out, int co
     eng.release(tid);
 }
 
+// N = 64, 128, 256: chunks of 6144 / N sequences (384 threads, one CTA per
+// SM for its tensor memory).
+template <int LOG_N>
+using SmallBatchEngine = tc::SmallEngine<LOG_N, (6144 >> LOG_N)>;
+
+template <int LOG_N>
+__host__ __device__ constexpr size_t tc_small_data_bytes()
+{
+    return ((6144 >> LOG_N) * (padded_len(1 << LOG_N) + kSeqPad) * sizeof(float2) + 127) / 128 * 128;
+}
+
+template <int LOG_N>
+__global__ void __launch_bounds__(SmallBatchEngine<LOG_N>::Lay::kThreads)
+dft_tc_small_kernel(const float2* __restrict__ in, float2* __restrict__ out, int count,
+                    const float2* __restrict__ tw, unsigned* error)
+{
+    using Eng = SmallBatchEngine<LOG_N>;
+    constexpr int N = 1 << LOG_N, NT = Eng::Lay::kThreads, S = 6144 >> LOG_N;
+    constexpr int SEQ = padded_len(N) + kSeqPad;
+    static_assert(SEQ * 2 >= Eng::Lay::N1 * Eng::Lay::kZStride, "a sequence's space must hold its staged rows");
+    extern __shared__ float4 smem4[];
+    float2* data = reinterpret_cast<float2*>(smem4);
+    const int tid = threadIdx.x;
+    Eng eng{reinterpret_cast<unsigned char*>(smem4) + tc_small_data_bytes<LOG_N>(), 0};
+    eng.init(tid, NT, tw);
+    for (int base = blockIdx.x * S; base < count; base += gridDim.x * S) {
+        const int k = min(S, count - base);
+        __syncthreads();
+        for (int i = tid; i < k * N; i += NT) {
+            const int s = i >> LOG_N, n = i & (N - 1);
+            data[s * SEQ + pad_idx(n)] = in[static_cast<size_t>(base + s) * N + n];
+        }
+        __syncthreads();
+        eng.dft(data, SEQ, k, tid, error);
+        for (int i = tid; i < k * N; i += NT) {
+            const int s = i >> LOG_N, n = i & (N - 1);
+            out[static_cast<size_t>(base + s) * N + n] = data[s * SEQ + pad_idx(n)];
+        }
+    }
+    eng.release(tid);
+}
+
+template <int LOG_N>
+cudaError_t tc_small_launch(const float2* in, float2* out, int count, const float2* tw, unsigned* error, int sms,
+                            cudaStream_t st)
+{
+    using Eng = SmallBatchEngine<LOG_N>;
+    constexpr int S = 6144 >> LOG_N;
+    constexpr size_t smem = tc_small_data_bytes<LOG_N>() + Eng::Lay::kSmemBytes;
+    static_assert(smem <= 227 * 1024, "one CTA's shared memory");
+    cudaError_t e = cudaFuncSetAttribute(dft_tc_small_kernel<LOG_N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const int chunks = (count + S - 1) / S;
+    dft_tc_small_kernel<LOG_N><<<chunks < sms ? chunks : sms, Eng::Lay::kThreads, smem, st>>>(in, out, count, tw,
+                                                                                              error);
+    return cudaGetLastError();
+}
+
 template <int LOG_N>
 cudaError_t fp32_launch(bool fast, const float2* in, float2* out, int count, const float2* tw, int grid,
                         cudaStream_t st)
@@ -102,6 +163,15 @@ cudaError_t launch_dft_batch(int log_n, int form, const float2* in, float2* out,
                              unsigned* error, int grid, cudaStream_t st)
 {
     if (count <= 0) return cudaSuccess;
+    if (form == 2 && log_n >= 6 && log_n <= 8) {
+        int dev = 0, sms = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        if (log_n == 6) return tc_small_launch<6>(in, out, count, tw, error, sms, st);
+        if (log_n == 7) return tc_small_launch<7>(in, out, count, tw, error, sms, st);
+        return tc_small_launch<8>(in, out, count, tw, error, sms, st);
+    }
     if (form == 2) {
         if (log_n != 9) return cudaErrorInvalidValue;
         const size_t smem = tc_dft_smem_bytes();

@@ -25,6 +25,7 @@
 #include "query_device.cuh"
 #include "spectrum.h"
 #include "tc_dft.cuh"
+#include "tc_dft_small.cuh"
 
 namespace ocean_b200 {
 namespace {
@@ -165,10 +166,27 @@ __host__ __device__ constexpr int foam_window_f2()
     return (1 << LOG_N) * foam_window<W>() / 2;
 }
 
-// The tensor-core engine of a task's 2 NF sequences (one row pair or two
-// columns: 8 without velocity, 12 with): one engine call per transform.
-template <int NF>
-using TcEngine = tc::Engine<2 * NF>;
+// The tensor-core engine of a task's sequences, one engine call per
+// transform: at N = 512 the 2 NF sequences of a row pair or two columns (8
+// without velocity, 12 with); at N = 64, 128 and 256 the ROWS x NF of the
+// plan's rows or columns (16 x threads values in all). Sizes without a
+// tensor-core form name the 512-point engine, which their kernels never use.
+template <int LOG_N>
+__host__ __device__ constexpr bool has_tc_form()
+{
+    return LOG_N >= 6 && LOG_N <= 9;
+}
+template <int LOG_N, int NF>
+struct TcEngineOfT {
+    using type = tc::Engine<2 * NF>;
+};
+template <int LOG_N, int NF>
+    requires(LOG_N >= 6 && LOG_N <= 8)
+struct TcEngineOfT<LOG_N, NF> {
+    using type = tc::SmallEngine<LOG_N, FramePlan<LOG_N, true>::ROWS * NF>;
+};
+template <int LOG_N, int NF>
+using TcEngineOf = typename TcEngineOfT<LOG_N, NF>::type;
 
 // Copy the FP32 twiddle table into shared memory at `tws`.
 template <class P>
@@ -187,11 +205,16 @@ template <class P, bool FAST, int COUNT, int COLW = 0, class Eng = tc::Engine<8>
 __device__ __forceinline__ void transform_all(float2* data, const float2* tws, int tid, Eng* eng,
                                               unsigned* error)
 {
-    if constexpr (P::TC) {
-        static_assert(P::LOG_N == 9, "the tensor-core form is built for N = 512");
+    if constexpr (P::TC && P::LOG_N == 9) {
         static_assert(P::SEQ * 2 >= 16 * tc::kZStride, "a sequence's space must hold its staged stage-3 rows");
         static_assert(COUNT == Eng::Lay::kThreads / 32, "one engine call holds the task's sequences");
         eng->dft512(data, P::SEQ, COUNT, tid, error);
+    } else if constexpr (P::TC) {
+        static_assert(has_tc_form<P::LOG_N>(), "the tensor-core form covers N = 64 to 512");
+        static_assert(P::SEQ * 2 >= Eng::Lay::N1 * Eng::Lay::kZStride,
+                      "a sequence's space must hold its staged stage-3 rows");
+        static_assert(COUNT * P::N == 16 * Eng::Lay::kThreads, "one engine call holds the task's sequences");
+        eng->dft(data, P::SEQ, COUNT, tid, error);
     } else if constexpr (!P::PAIRED) {
         fft_sequence<P::LOG_N, P::G, FAST>(data + (tid / P::G) * P::SEQ, tws, tid % P::G);
     } else {
@@ -310,7 +333,7 @@ template <class P, int NF, bool FAST>
 __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int group,
                                          float2* __restrict__ inter_slot, float2* smem,
                                          const float2* tws, int tid, uint64_t* h0_bar, uint32_t h0_parity,
-                                         TcEngine<NF>* eng = nullptr, unsigned* error = nullptr,
+                                         TcEngineOf<P::LOG_N, NF>* eng = nullptr, unsigned* error = nullptr,
                                          unsigned* const* pub = nullptr)
 {
     using D = P;
@@ -461,7 +484,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
 template <class P, int NF, bool FAST, bool FOAM, int W, bool CG>
 __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int strip,
                                          const float2* __restrict__ inter_slot, float2* smem,
-                                         const float2* tws, int tid, TcEngine<NF>* eng = nullptr,
+                                         const float2* tws, int tid, TcEngineOf<P::LOG_N, NF>* eng = nullptr,
                                          unsigned* error = nullptr, unsigned* const* pub = nullptr)
 {
     constexpr int N = P::N, G = P::G, SEQ = P::SEQ, SEQ4 = P::SEQ4;
@@ -746,9 +769,9 @@ frame_kernel(FrameArgs a, QueueArgs q)
 
     const int tid = threadIdx.x;
     if constexpr (!TC) load_twiddles<P>(tws, a.twiddles, tid, NT);
-    TcEngine<NF> eng{reinterpret_cast<unsigned char*>(smem4) + frame_engine_offset<LOG_N, NF>(), 0};
+    TcEngineOf<LOG_N, NF> eng{reinterpret_cast<unsigned char*>(smem4) + frame_engine_offset<LOG_N, NF>(), 0};
     if constexpr (TC) {
-        static_assert(NT == TcEngine<NF>::Lay::kThreads, "the engine works with the task's threads");
+        static_assert(NT == TcEngineOf<LOG_N, NF>::Lay::kThreads, "the engine works with the task's threads");
         eng.init(tid, NT, a.twiddles);
     }
 
@@ -1256,15 +1279,17 @@ cudaError_t col_launch(const FrameArgs& a, cudaStream_t st)
 template <class P, int NF>
 constexpr size_t frame_smem_bytes()
 {
-    if (P::TC) return frame_engine_offset<P::LOG_N, NF>() + TcEngine<NF>::Lay::kSmemBytes;
+    if (P::TC) return frame_engine_offset<P::LOG_N, NF>() + TcEngineOf<P::LOG_N, NF>::Lay::kSmemBytes;
     return sizeof(float2) * (frame_data_float2<P, NF>() + P::TWF2);
 }
 
 template <int LOG_N, int NF, bool FAST, bool FOAM, bool TC = false, int V = 0>
 struct FrameLaunch {
     using P = PlanOf<LOG_N, V, TC>;
+    using Eng = TcEngineOf<LOG_N, NF>;
     static constexpr int threads() { return P::template threads<NF>(); }
     static constexpr size_t smem() { return frame_smem_bytes<P, NF>(); }
+    static_assert(frame_smem_bytes<P, NF>() <= 227 * 1024, "a task's shared memory fits one CTA");
 
     static cudaError_t prepare()
     {
@@ -1280,7 +1305,7 @@ struct FrameLaunch {
             cudaSuccess)
             return 0;
         // The tensor-core engine's tensor memory bounds its residency.
-        if (TC && n * TcEngine<NF>::Lay::kTmemCols > 512) n = 512 / TcEngine<NF>::Lay::kTmemCols;
+        if (TC && n * Eng::Lay::kTmemCols > 512) n = 512 / Eng::Lay::kTmemCols;
         return n;
     }
 
@@ -1293,14 +1318,14 @@ struct FrameLaunch {
             int n = 0;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<P, NF, FAST, FOAM>, threads(), smem());
             if (e != cudaSuccess) return e;
-            if (n * TcEngine<NF>::Lay::kTmemCols > 512) return cudaErrorInvalidConfiguration;
+            if (n * Eng::Lay::kTmemCols > 512) return cudaErrorInvalidConfiguration;
         }
         frame_kernel<P, NF, FAST, FOAM><<<grid, threads(), smem(), st>>>(a, q);
         return cudaGetLastError();
     }
 };
 
-// form: 0 exact, 1 fast (FMA), 2 tensor cores (N = 512 only).
+// form: 0 exact, 1 fast (FMA), 2 tensor cores (N = 64 to 512).
 template <int LOG_N, int V, typename Fn>
 auto frame_variant_plan(int nf, bool fast, bool foam, Fn&& fn)
 {
@@ -1315,7 +1340,7 @@ auto frame_variant_plan(int nf, bool fast, bool foam, Fn&& fn)
 template <int LOG_N, typename Fn>
 auto frame_variant(int nf, int form, bool foam, int plan, Fn&& fn)
 {
-    if constexpr (LOG_N == 9) {
+    if constexpr (has_tc_form<LOG_N>()) {
         if (form == 2) {
             if (nf == 4) return fn(FrameLaunch<LOG_N, 4, false, false, true>{});
             if (foam) return fn(FrameLaunch<LOG_N, 6, false, true, true>{});
@@ -1375,7 +1400,7 @@ int frame_plan_count(int log_n, int form)
 int frame_blocks_per_sm(int log_n, int nf, int form, bool fuse_foam, int plan)
 {
     if (log_n < 4 || log_n > 10) return 0;
-    if (form == 2 && log_n != 9) return 0;
+    if (form == 2 && (log_n < 6 || log_n > 9)) return 0;
     if (plan < 0 || plan >= frame_plan_count(log_n, form)) return 0;
     return frame_dispatch(log_n, nf, form, fuse_foam, plan, [](auto L) { return decltype(L)::blocks_per_sm(); });
 }
@@ -1384,7 +1409,7 @@ cudaError_t launch_frame(int log_n, int nf, int form, bool fuse_foam, const Fram
                          const QueueArgs& q, int grid, cudaStream_t st, int plan)
 {
     if (log_n < 4 || log_n > 10) return cudaErrorInvalidValue;
-    if (form == 2 && log_n != 9) return cudaErrorInvalidValue;
+    if (form == 2 && (log_n < 6 || log_n > 9)) return cudaErrorInvalidValue;
     if (plan < 0 || plan >= frame_plan_count(log_n, form)) return cudaErrorInvalidValue;
     return frame_dispatch(log_n, nf, form, fuse_foam, plan,
                           [&](auto L) { return decltype(L)::launch(a, q, grid, st); });

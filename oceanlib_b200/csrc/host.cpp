@@ -196,9 +196,10 @@ public:
         }
         form_ = form;
         if (n_ > kMaxPersistentSize) persistent_ = false;
-        // The tensor-core DFT is built for N = 512 and runs in the persistent kernel.
-        if (form_ == OCEAN_FFT_TENSOR && (n_ != 512 || !persistent_))
-            throw std::invalid_argument("the tensor-core form needs N = 512 and the persistent schedule");
+        // The tensor-core DFT is built for N = 64 to 512 and runs in the
+        // persistent kernel.
+        if (form_ == OCEAN_FFT_TENSOR && (n_ < 64 || n_ > 512 || !persistent_))
+            throw std::invalid_argument("the tensor-core form needs N = 64 to 512 and the persistent schedule");
         count_ = count;
         log_n_ = ilog2u(n_);
         nf_ = velocity_ ? 6 : 4;

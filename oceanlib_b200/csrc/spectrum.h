@@ -86,7 +86,7 @@ struct QueueArgs {
 };
 
 // One persistent launch for the whole frame of `q.count` oceans (foam fused
-// when fuse_foam). `form` is an ocean_fft_form (the tensor form: N = 512).
+// when fuse_foam). `form` is an ocean_fft_form (the tensor form: N = 64 to 512).
 // `grid` = CTAs to launch (0 = one wave of resident CTAs).
 // `plan` picks the task plan (0: the default; 1: the alternative of N = 256,
 // 512 and 1024, see frame_plan_count).

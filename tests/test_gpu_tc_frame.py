@@ -54,14 +54,22 @@ def channel_errors(got, ref):
     return errs
 
 
-@pytest.mark.parametrize("case", ["bench_update_512", "foam_patch_512_velocity", "late_time"])
+CASES = {
+    "bench_update_512": lambda: (W.bench_update_patch(512), 100.0),
+    "foam_patch_512_velocity": lambda: (W.foam_patch_512(), 100.0),
+    "late_time": lambda: (W.foam_patch_512(), 1.0e5),  # FP64 phase reduction at large t
+    # the 800 m cascade level (256^2, 15 m/s, depth 30 m, velocity on)
+    "cascade_800m_256": lambda: (W.cascade_3x256()[0], 100.0),
+    "ensemble_128_velocity": lambda: (ob.OceanDesc(size=128, patch_length=140.0, wind_speed=18.0, wind_direction=2.2,
+                                                   choppiness=1.4, seed=42, compute_velocity=True), 100.0),
+    "ensemble_64": lambda: (ob.OceanDesc(size=64, patch_length=60.0, wind_speed=9.0, wind_direction=5.1,
+                                         choppiness=0.8, seed=43), 100.0),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
 def test_tensor_form_frame_against_fp64(case):
-    if case == "bench_update_512":
-        desc, t = W.bench_update_patch(512), 100.0
-    elif case == "foam_patch_512_velocity":
-        desc, t = W.foam_patch_512(), 100.0
-    else:
-        desc, t = W.foam_patch_512(), 1.0e5  # FP64 phase reduction at large t
+    desc, t = CASES[case]()
     ref = O.fp64_frame(desc, t)
     e32 = channel_errors(frame(desc, t, abi.OCEAN_FFT_EXACT), ref)
     etc = channel_errors(frame(desc, t, abi.OCEAN_FFT_TENSOR), ref)
@@ -90,6 +98,28 @@ def test_tensor_form_batch_is_per_ocean_independent():
     assert np.array_equal(normal[1].view(np.uint32), one["normal"].view(np.uint32))
 
 
-def test_tensor_form_needs_n512():
+@pytest.mark.parametrize("n", [64, 128, 256])
+def test_tensor_form_batch_at_small_sizes_is_per_ocean_independent(n):
+    # three oceans with velocity in one batch: the middle one's bits equal a
+    # batch of its own (tasks of one ocean never mix with another's)
+    descs = [ob.OceanDesc(size=n, patch_length=0.9 * n + 20.0, wind_speed=8.0 + s, wind_direction=0.7 * s,
+                          choppiness=1.2, seed=s, compute_velocity=True) for s in (21, 22, 23)]
+    b = ob.OceanBatch(descs, form=abi.OCEAN_FFT_TENSOR)
+    disp = np.empty((3, n, n, 4), np.float32)
+    normal = np.empty_like(disp)
+    velo = np.empty_like(disp)
+    b.update_host([7.5], 0.0, disp, normal, velo)
+    b.close()
+    one = frame(descs[1], 7.5, abi.OCEAN_FFT_TENSOR)
+    assert np.array_equal(disp[1].view(np.uint32), one["displacement"].view(np.uint32))
+    assert np.array_equal(normal[1].view(np.uint32), one["normal"].view(np.uint32))
+    assert np.array_equal(velo[1].view(np.uint32), one["velocity"].view(np.uint32))
+
+
+@pytest.mark.parametrize("n", [16, 32, 1024])
+def test_tensor_form_sizes(n):
+    # N = 64 .. 512 only: below, the four-step factors drop under the
+    # tensor cores' 8-point minimum; at 1024 a task's digits and
+    # accumulators exceed one SM's shared and tensor memory.
     with pytest.raises((ValueError, ob.OceanError)):
-        ob.OceanBatch([W.bench_update_patch(256)], form=abi.OCEAN_FFT_TENSOR)
+        ob.OceanBatch([ob.OceanDesc(size=n, seed=5)], form=abi.OCEAN_FFT_TENSOR)
