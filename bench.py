@@ -435,6 +435,16 @@ def bench_ensemble(torch, frames: int = 30):
         per[name] = timed(True)[0]
     res["schedules_ms_per_frame"] = per
     ens.close()
+    # The same sea states in the tensor-core form (N = 64..512 on the tensor
+    # cores, N = 1024 in the exact form), schedule again by the autotuner.
+    from oceanlib_b200 import abi
+
+    ens = ob.OceanEnsemble(descs, autotune=True, form=abi.OCEAN_FFT_TENSOR)
+    ms_tc, _ = timed(True)
+    res["tensor_core_form"] = {"ms_per_frame": ms_tc, "ocean_updates_per_s": len(descs) * 1000.0 / ms_tc,
+                               "equiv_512sq_updates_per_s": cells / (512 * 512) * 1000.0 / ms_tc,
+                               "schedule": ens.schedule}
+    ens.close()
     return res
 
 

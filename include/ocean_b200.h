@@ -469,6 +469,14 @@ typedef struct ocean_ensemble ocean_ensemble;
  * otherwise it is the concurrent one. */
 OCEAN_API ocean_ensemble* ocean_ensemble_create(const ocean_desc* oceans, uint32_t count,
                                                 int32_t autotune, ocean_status* out_status);
+/* As ocean_ensemble_create, in a given ocean_fft_form instead of the
+ * process-wide one. With OCEAN_FFT_TENSOR the sizes the tensor-core form
+ * covers (64 to 512) run on it and the others (16, 32, 1024) in the exact
+ * FP32 form; ocean_ensemble_describe names them. The tensor-core form runs
+ * the sequential or concurrent schedules (the one-launch schedule is FP32). */
+OCEAN_API ocean_ensemble* ocean_ensemble_create_form(const ocean_desc* oceans, uint32_t count,
+                                                     int32_t autotune, int32_t fft_form,
+                                                     ocean_status* out_status);
 OCEAN_API void ocean_ensemble_destroy(ocean_ensemble* ensemble);
 OCEAN_API uint32_t ocean_ensemble_count(const ocean_ensemble* ensemble);
 /* All oceans to absolute time `time`, asynchronously on `stream` (NULL = the
@@ -735,7 +743,7 @@ OCEAN_API ocean_status ocean_batch_read_profile(ocean_batch* batch, ocean_pass_p
  * bits; the default is 1 with velocity, 0 without.
  * ocean_batch_autotune_plan times a few frames of every (plan, ring slots,
  * publish) combination on the batch's stream (advancing any persistent
- * foam), keeps the fastest and writes each plan's best median milliseconds
+ * foam), keeps the fastest and writes each plan's best milliseconds per frame
  * to `ms` (plan_count entries; may be NULL). */
 OCEAN_API ocean_status ocean_batch_set_plan(ocean_batch* batch, int32_t plan);
 OCEAN_API int32_t ocean_batch_plan(const ocean_batch* batch);

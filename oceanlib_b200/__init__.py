@@ -370,7 +370,7 @@ class OceanBatch:
 
     def autotune_plan(self) -> list:
         """Time every (plan, ring slots, publish) combination, keep the
-        fastest; each plan's best median ms (empty for a batch that runs the
+        fastest; each plan's best ms per frame (empty for a batch that runs the
         per-chunk passes, with nothing to choose)."""
         ms = np.full(max(1, self.plan_count), -1.0, np.float64)
         _check(lib().ocean_batch_autotune_plan(self._h, ms.ctypes.data), "ocean_batch_autotune_plan")
@@ -421,12 +421,17 @@ class OceanBatch:
 
 class OceanEnsemble:
     """Independent sea states of uneven size, advanced together: one stream
-    and one persistent kernel per size, schedule chosen by the autotuner."""
+    and one persistent kernel per size, schedule chosen by the autotuner.
+    `form` (an OCEAN_FFT_* value) overrides the process-wide form; with the
+    tensor-core form, sizes outside 64..512 run the exact FP32 form."""
 
-    def __init__(self, descs: Sequence[OceanDesc], autotune: bool = True):
+    def __init__(self, descs: Sequence[OceanDesc], autotune: bool = True, form: Optional[int] = None):
         arr = (OceanDescC * len(descs))(*[d.to_c() for d in descs])
         st = C.c_int(-1)
-        h = lib().ocean_ensemble_create(arr, len(descs), 1 if autotune else 0, C.byref(st))
+        if form is None:
+            h = lib().ocean_ensemble_create(arr, len(descs), 1 if autotune else 0, C.byref(st))
+        else:
+            h = lib().ocean_ensemble_create_form(arr, len(descs), 1 if autotune else 0, int(form), C.byref(st))
         if not h:
             if st.value == abi.OCEAN_ERROR_INVALID_ARG:
                 raise ValueError(f"invalid ensemble ({status_string(st.value)})")
@@ -486,8 +491,9 @@ class OceanEnsemble:
 
     @property
     def schedule(self) -> str:
-        buf = C.create_string_buffer(512)
-        lib().ocean_ensemble_describe(self._h, buf, 512)
+        n = int(lib().ocean_ensemble_describe(self._h, None, 0))
+        buf = C.create_string_buffer(n + 1)
+        lib().ocean_ensemble_describe(self._h, buf, n + 1)
         return buf.value.decode()
 
 

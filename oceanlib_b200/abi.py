@@ -280,6 +280,8 @@ SIGNATURES = {
     "ocean_check_static_scratch_status": (C.c_int, [C.c_uint32]),
     "ocean_ensemble_create": (C.c_void_p, [C.POINTER(OceanDescC), C.c_uint32, C.c_int32,
                                            C.POINTER(C.c_int)]),
+    "ocean_ensemble_create_form": (C.c_void_p, [C.POINTER(OceanDescC), C.c_uint32, C.c_int32, C.c_int32,
+                                                C.POINTER(C.c_int)]),
     "ocean_ensemble_destroy": (None, [C.c_void_p]),
     "ocean_ensemble_count": (C.c_uint32, [C.c_void_p]),
     "ocean_ensemble_update": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),

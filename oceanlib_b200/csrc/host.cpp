@@ -774,7 +774,7 @@ public:
     // The batch's autotuner: times `frames` frames (after two untimed ones)
     // of every task plan with every ring depth (3 and 2 slots, as allocated)
     // and both publish timings on the batch's own stream, keeps the fastest
-    // combination and returns, plan by plan, the median time in milliseconds
+    // combination and returns, plan by plan, the time per frame in milliseconds
     // of that plan's best combination. Persistent foam state advances with
     // the timed frames (a clear() resets it). Nothing to choose (the per-chunk
     // passes): an empty result.
@@ -797,19 +797,27 @@ public:
                 set_plan(v);
                 set_ring_slots(sl);
                 set_deferred_publish(defer);
-                std::vector<float> t;
-                for (int k = 0; k < frames + 2; ++k) {
-                    const double time = 1.0 + k / 60.0;
+                // Two untimed frames, then the best of three runs of `frames`
+                // frames back to back (the host enqueues ahead of the
+                // device, as in use, so launch latency is not timed).
+                const float dt = foam_on_ ? foam_.fixed_dt : 0.0f;
+                for (int k = 0; k < 2; ++k) {
+                    const double time = 0.5 + k / 60.0;
+                    update(&time, false, dt, stream_);
+                }
+                double med = 1e30;
+                for (int rep = 0; rep < 3; ++rep) {
                     check(cudaEventRecord(e0, stream_), "event");
-                    update(&time, false, foam_on_ ? foam_.fixed_dt : 0.0f, stream_);
+                    for (int k = 0; k < frames; ++k) {
+                        const double time = 1.0 + (rep * frames + k) / 60.0;
+                        update(&time, false, dt, stream_);
+                    }
                     check(cudaEventRecord(e1, stream_), "event");
                     check(cudaEventSynchronize(e1), "event");
                     float m = 0.0f;
                     check(cudaEventElapsedTime(&m, e0, e1), "elapsed");
-                    if (k >= 2) t.push_back(m);
+                    med = std::min(med, static_cast<double>(m) / frames);
                 }
-                std::sort(t.begin(), t.end());
-                const double med = t[t.size() / 2];
                 plan_best = std::min(plan_best, med);
                 if (med < best) {
                     best = med;
@@ -1294,8 +1302,14 @@ private:
 // ---------------------------------------------------------------------------
 class Ensemble {
 public:
-    Ensemble(const ocean_desc* descs, uint32_t count, bool tune)
+    // `form` < 0: the process-wide form (ocean_force_simd_level). With the
+    // tensor-core form, sizes without a tensor-core engine (16, 32, 1024)
+    // run the exact FP32 form; form_note() names them.
+    Ensemble(const ocean_desc* descs, uint32_t count, bool tune, int form = -1)
     {
+        if (form < 0) form = g_form.load();
+        if (form != OCEAN_FFT_EXACT && form != OCEAN_FFT_FAST && form != OCEAN_FFT_TENSOR)
+            throw std::invalid_argument("fft form");
         if (descs == nullptr || count == 0) throw std::invalid_argument("no oceans");
         std::vector<ocean_desc> all(count);
         for (uint32_t i = 0; i < count; ++i) {
@@ -1323,8 +1337,15 @@ public:
                 where_[i] = {static_cast<uint32_t>(g), static_cast<uint32_t>(gd.size())};
                 gd.push_back(all[i]);
             }
-            batches_.push_back(std::make_unique<Batch>(gd.data(), static_cast<uint32_t>(gd.size()),
-                                                       g_form.load(), false, foam, 0));
+            const bool tc_size = gd[0].size >= 64 && gd[0].size <= 512;
+            const int gform = (form == OCEAN_FFT_TENSOR && !tc_size) ? OCEAN_FFT_EXACT : form;
+            if (gform != form) {
+                char nb[48];
+                std::snprintf(nb, sizeof(nb), "%sN=%u", form_note_.empty() ? "" : ", ", gd[0].size);
+                form_note_ += nb;
+            }
+            batches_.push_back(std::make_unique<Batch>(gd.data(), static_cast<uint32_t>(gd.size()), gform, false,
+                                                       foam, 0));
             work_.push_back(static_cast<double>(gd.size()) * gd[0].size * gd[0].size *
                             (gd[0].compute_velocity ? 6.0 : 4.0));
             cudaStream_t s;
@@ -1364,6 +1385,8 @@ public:
             if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "mixed frame occupancy");
             mix_grid_ = per_sm * sms;
         }
+        form_ = form;
+        if (!form_note_.empty()) form_note_ = "exact FP32 form at " + form_note_ + " (no tensor-core engine)";
         apply_shares(work_);
         concurrent_ = true;
         describe_ = "concurrent, SM shares by work estimate";
@@ -1463,7 +1486,11 @@ public:
     cudaStream_t stream() const { return stream_; }
     const Batch& batch_of(uint32_t i) const { return *batches_[where_[i].first]; }
     uint32_t index_of(uint32_t i) const { return where_[i].second; }
-    const std::string& description() const { return describe_; }
+    std::string description() const { return form_note_.empty() ? describe_ : describe_ + "; " + form_note_; }
+    int form() const { return form_; }
+    // Sizes that run the exact FP32 form under the tensor-core form (empty
+    // when every group runs the requested form).
+    const std::string& form_note() const { return form_note_; }
 
 private:
     // Captures one frame under the chosen schedule: the upload of the pinned
@@ -1562,7 +1589,9 @@ private:
         for (auto& b : batches_) b->set_grid_share(1.0);
     }
 
-    // Median time of `frames` frames (after two untimed ones), on stream_.
+    // Time per frame on stream_: two untimed frames, then the best of three
+    // runs of `frames` frames back to back (the host enqueues ahead of the
+    // device, as in use, so launch latency is not timed).
     double time_frames(int frames, const std::function<void(double)>& frame)
     {
         cudaEvent_t a, b;
@@ -1570,20 +1599,19 @@ private:
         check(cudaEventCreate(&b), "event");
         frame(0.5);
         frame(0.6);
-        std::vector<float> ms;
-        for (int k = 0; k < frames; ++k) {
+        double best = 1e30;
+        for (int rep = 0; rep < 3; ++rep) {
             check(cudaEventRecord(a, stream_), "event");
-            frame(1.0 + k / 60.0);
+            for (int k = 0; k < frames; ++k) frame(1.0 + (rep * frames + k) / 60.0);
             check(cudaEventRecord(b, stream_), "event");
             check(cudaEventSynchronize(b), "event");
             float m = 0.0f;
             check(cudaEventElapsedTime(&m, a, b), "elapsed");
-            ms.push_back(m);
+            best = std::min(best, static_cast<double>(m) / frames);
         }
         cudaEventDestroy(a);
         cudaEventDestroy(b);
-        std::sort(ms.begin(), ms.end());
-        return ms[ms.size() / 2];
+        return best;
     }
 
     // Candidates: (1) sizes one after another, each with the whole GPU;
@@ -1594,7 +1622,9 @@ private:
     void autotune()
     {
         const int frames = 5;
-        // Per size: the persistent kernel's task plans, timed alone.
+        // Per size: the persistent kernel's task plans, timed alone on the
+        // whole GPU (the construction left each size its work-share grid).
+        full_grids();
         std::string plans;
         for (auto& b : batches_) {
             const std::vector<double> ms = b->autotune_plan(frames);
@@ -1708,6 +1738,8 @@ private:
     std::vector<size_t> mix_order_;
     DevBuf<unsigned> mix_words_;
     std::string describe_;
+    int form_ = OCEAN_FFT_EXACT;
+    std::string form_note_;
     // graph replay of the frame
     bool use_graph_ = false;
     cudaGraph_t graph_ = nullptr;
@@ -1731,7 +1763,7 @@ struct ocean_sim {
 };
 struct ocean_ensemble {
     ocean_b200::Ensemble impl;
-    ocean_ensemble(const ocean_desc* d, uint32_t n, bool tune) : impl(d, n, tune) {}
+    ocean_ensemble(const ocean_desc* d, uint32_t n, bool tune, int form = -1) : impl(d, n, tune, form) {}
 };
 struct ocean_cascade {
     ocean_b200::Cascade impl;
@@ -2164,6 +2196,15 @@ ocean_ensemble* ocean_ensemble_create(const ocean_desc* oceans, uint32_t count, 
 {
     ocean_ensemble* e = nullptr;
     const ocean_status st = guarded([&] { e = new ocean_ensemble(oceans, count, autotune != 0); });
+    if (out_status != nullptr) *out_status = st;
+    return st == OCEAN_OK ? e : nullptr;
+}
+
+ocean_ensemble* ocean_ensemble_create_form(const ocean_desc* oceans, uint32_t count, int32_t autotune,
+                                           int32_t fft_form, ocean_status* out_status)
+{
+    ocean_ensemble* e = nullptr;
+    const ocean_status st = guarded([&] { e = new ocean_ensemble(oceans, count, autotune != 0, fft_form); });
     if (out_status != nullptr) *out_status = st;
     return st == OCEAN_OK ? e : nullptr;
 }

@@ -159,3 +159,43 @@ def test_sharded_ensemble_holds_this_ranks_share():
         d, n = sh.ensemble.read(local)
         assert np.array_equal(bits(d), bits(od)) and np.array_equal(bits(n), bits(on)), i
     sh.close()
+
+
+def test_tensor_form_ensemble():
+    # Config 4's sizes in the tensor-core form: N = 64..512 run on the tensor
+    # cores, each ocean bit-identical to a tensor-form batch of its own and
+    # within 2e-6 of FP64 per channel; N = 1024, which has no tensor-core
+    # engine, runs the exact FP32 form and matches the oracle's bits.
+    from oceanlib_b200 import abi
+
+    descs = W.ensemble_64(24)
+    sizes = sorted({d.size for d in descs})
+    assert 1024 in sizes and 64 in sizes
+    ens = ob.OceanEnsemble(descs, autotune=True, form=abi.OCEAN_FFT_TENSOR)
+    assert "N=1024" in ens.schedule and "no tensor-core engine" in ens.schedule
+    t = 37.5
+    ens.update(t)
+    ens.synchronize()
+    for n in sizes:
+        i = next(k for k, d in enumerate(descs) if d.size == n)
+        d, nrm = ens.read(i)
+        if n == 1024:
+            od, on, _ = O.update(descs[i], t)
+            assert np.array_equal(bits(d), bits(od)) and np.array_equal(bits(nrm), bits(on))
+            continue
+        alone = ob.OceanBatch([descs[i]], form=abi.OCEAN_FFT_TENSOR)
+        cells = n * n
+        ad = np.empty((cells, 4), np.float32)
+        an = np.empty_like(ad)
+        alone.update_host([t], 0.0, ad, an)
+        alone.close()
+        assert np.array_equal(bits(d), bits(ad)) and np.array_equal(bits(nrm), bits(an)), n
+        if n <= 256:
+            ref = O.fp64_frame(descs[i], t)
+            for name, got in (("displacement", d), ("normal", nrm)):
+                r = ref[name].reshape(cells, 4)
+                for c in range(3):
+                    rms = np.sqrt(np.mean(r[:, c] ** 2))
+                    err = np.abs(got.reshape(cells, 4)[:, c].astype(np.float64) - r[:, c]).max() / rms
+                    assert err <= 2e-6, (n, name, c, err)
+    ens.close()
