@@ -7,10 +7,13 @@
 // chunk of oceans instead, through a field-major intermediate
 // inter[ocean][field][y][x]:
 //
-//   rows      field pair g of row y per task: evolve the row's cells
+//   rows      row y per task: evolve the row's cells once for all NF fields
 //             (src/core/evolve.cpp:28-184; h0(-k) read from the mirrored row
-//             in global memory, which the neighbouring task has just read)
-//             and transform the two sequences.
+//             in global memory, which the neighbouring task has just read),
+//             field pair 0 into shared memory and the other pairs straight
+//             into their rows of the intermediate; transform pair 0, then
+//             each other pair from its row (just written, so read from L2)
+//             back in place.
 //   columns   four columns of one field per task, transformed in place.
 //   finalize  one thread per cell: the NF fields to the RGBA32F outputs
 //             (src/core/evolve.cpp:186-327) and, with persistent foam, the
@@ -37,7 +40,7 @@ struct Large {
     static constexpr int W = 4;                    // columns per column task
     static constexpr int ROW_T = 2 * G;            // threads: two sequences
     static constexpr int COL_T = W * G;            // threads: W sequences
-    static constexpr int ROW_TASKS = 4;            // tasks per row CTA
+    static constexpr int ROW_TASKS = 2;            // rows per row CTA (a row and its mirror)
     // Resident row CTAs per SM the registers are capped for: two at N = 4096
     // (512 threads, 102 KB each; 7% faster than one), three at 2048 (256
     // threads, 51 KB each).
@@ -72,42 +75,46 @@ large_row_kernel(FrameArgs a)
 
 #pragma unroll 1
     for (int k = 0; k < S::ROW_TASKS; ++k) {
-        // Task t: field pair t % NG of row pair slot t / NG, whose two
-        // members (p, N - p), or (0, N/2) for p = 0, are each other's h0(-k)
-        // rows, so consecutive tasks reuse what the L2 just fetched.
-        const int t = blockIdx.x * S::ROW_TASKS + k;
-        const int g = t % NG;
-        const int j = t / NG;
+        // Task t: row slot t, whose two members (p, N - p), or (0, N/2) for
+        // p = 0, are each other's h0(-k) rows, so consecutive tasks reuse
+        // what the L2 just fetched.
+        const int j = blockIdx.x * S::ROW_TASKS + k;
         const int p = j >> 1, r = j & 1;
         const int y = p == 0 ? (r ? N / 2 : 0) : (r ? N - p : p);
         const int my = (N - y) & (N - 1);
         const float kz = __ldg(&kvec[y]);
+        const size_t row = static_cast<size_t>(y) * N;
         __syncthreads();  // the twiddles are complete; the last task's reads are done
+        // Evolve once: pair 0 to shared memory, pairs 1.. to their rows of
+        // the intermediate (coalesced float2 stores, read back below).
         for (int x = tid; x < N; x += NT) {
-            const float2 av = __ldg(&h0[static_cast<size_t>(y) * N + x]);
+            const float2 av = __ldg(&h0[row + x]);
             const float2 bm = __ldg(&h0[static_cast<size_t>(my) * N + ((N - x) & (N - 1))]);
             float2 pv[NF];
-            evolve_cell<NF>(av, bm, __ldg(&geom[static_cast<size_t>(y) * N + x]), __ldg(&kvec[x]), kz, top, pv);
-            float2 u = pv[0], v = pv[1];
-            if (g == 1) {
-                u = pv[2];
-                v = pv[3];
-            }
-            if constexpr (NF == 6) {
-                if (g == 2) {
-                    u = pv[4];
-                    v = pv[5];
+            evolve_cell<NF>(av, bm, __ldg(&geom[row + x]), __ldg(&kvec[x]), kz, top, pv);
+            data[pad_idx(x)] = pv[0];
+            data[SEQ + pad_idx(x)] = pv[1];
+#pragma unroll
+            for (int f = 2; f < NF; ++f) inter[static_cast<size_t>(f) * cells + row + x] = pv[f];
+        }
+#pragma unroll 1
+        for (int g = 0; g < NG; ++g) {
+            if (g > 0) {
+                __syncthreads();  // the last pair's outputs are read out of shared memory
+                // This CTA wrote the pair's row above; the barrier makes its
+                // stores visible, and the loads go to L2.
+                for (int i = tid; i < 2 * N; i += NT) {
+                    const int s = i >> LOG_N, x = i & (N - 1);
+                    data[s * SEQ + pad_idx(x)] = __ldcg(&inter[static_cast<size_t>(2 * g + s) * cells + row + x]);
                 }
             }
-            data[pad_idx(x)] = u;
-            data[SEQ + pad_idx(x)] = v;
-        }
-        __syncthreads();
-        fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);  // ends with a CTA barrier
-        float2* out = inter + static_cast<size_t>(2 * g) * cells + static_cast<size_t>(y) * N;
-        for (int i = tid; i < 2 * N; i += NT) {
-            const int s = i >> LOG_N, x = i & (N - 1);
-            out[static_cast<size_t>(s) * cells + x] = data[s * SEQ + pad_idx(x)];
+            __syncthreads();
+            fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);  // ends with a CTA barrier
+            float2* out = inter + static_cast<size_t>(2 * g) * cells + row;
+            for (int i = tid; i < 2 * N; i += NT) {
+                const int s = i >> LOG_N, x = i & (N - 1);
+                out[static_cast<size_t>(s) * cells + x] = data[s * SEQ + pad_idx(x)];
+            }
         }
     }
 }
@@ -191,8 +198,8 @@ cudaError_t rows_launch(const FrameArgs& a, cudaStream_t st)
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(S::ROW_SMEM));
     if (e != cudaSuccess) return e;
-    static_assert((S::N * (NF / 2)) % S::ROW_TASKS == 0, "row tasks divide evenly among CTAs");
-    const dim3 grid(S::N * (NF / 2) / S::ROW_TASKS, a.chunk);
+    static_assert(S::N % S::ROW_TASKS == 0, "row tasks divide evenly among CTAs");
+    const dim3 grid(S::N / S::ROW_TASKS, a.chunk);
     k<<<grid, S::ROW_T, S::ROW_SMEM, st>>>(a);
     return cudaGetLastError();
 }
