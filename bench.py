@@ -728,6 +728,19 @@ def bench_serving(rate: float = 20000.0, seconds: float = 3.0):
         "capacity_mean_batch_requests": cap["mean_batch_requests"],
     }
     srv.close()
+    # The same sessions and arrivals with every ocean in the tensor-core form.
+    from oceanlib_b200 import abi
+
+    srv = OceanServer(hbm_budget=120e9, form=abi.OCEAN_FFT_TENSOR)
+    sids = [srv.open_session(o, field) for o in oceans]
+    run(1.0, 1)
+    wall, n, st = run(seconds, 2)
+    out["tensor_core_form"] = {"offered_rps": n / seconds, "achieved_rps": st["requests_completed"] / wall,
+                               "latency_p50_ms": st["latency_p50_ms"], "latency_p99_ms": st["latency_p99_ms"],
+                               "update_p99_ms": st["update_p99_ms"], "query_p99_ms": st["query_p99_ms"],
+                               "gpu_busy_fraction": st["gpu_busy_ms"] / (1000.0 * wall),
+                               "failed": st["requests_failed"]}
+    srv.close()
     return out
 
 

@@ -600,7 +600,8 @@ typedef struct ocean_server_desc {
     uint32_t max_batch_requests; /* requests one batch takes at most (default 4096) */
     uint32_t max_batch_points;   /* query points one batch takes at most (default 1 << 20) */
     uint32_t max_query_points;   /* points one query request may carry (default 65536) */
-    int32_t  fft_form;           /* ocean_fft_form of every session's ocean (default exact) */
+    int32_t  fft_form;           /* ocean_fft_form of every session's ocean (default exact;
+                                    the tensor form admits N = 64 to 512) */
     uint32_t reserved;
 } ocean_server_desc;
 

@@ -235,7 +235,8 @@ public:
         if (desc_.max_inflight == 0) desc_.max_inflight = 1;
         if (desc_.max_batch_requests == 0) throw std::invalid_argument("max_batch_requests");
         if (desc_.max_batch_points == 0 || desc_.max_query_points == 0) throw std::invalid_argument("points");
-        if (desc_.fft_form != OCEAN_FFT_EXACT && desc_.fft_form != OCEAN_FFT_FAST)
+        if (desc_.fft_form != OCEAN_FFT_EXACT && desc_.fft_form != OCEAN_FFT_FAST &&
+            desc_.fft_form != OCEAN_FFT_TENSOR)
             throw std::invalid_argument("fft_form");
         check(cudaGetDevice(&device_), "cudaGetDevice");
         check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_), "SM count");
@@ -306,6 +307,8 @@ public:
         validate(od);
         // The dispatcher batches sessions into persistent frame launches.
         if (od.size > kMaxPersistentSize) throw std::invalid_argument("session size above 1024");
+        if (desc_.fft_form == OCEAN_FFT_TENSOR && (od.size < 64 || od.size > 512))
+            throw std::invalid_argument("the tensor-core form needs N = 64 to 512");
         ocean_interaction_desc fd{};
         if (fd_in != nullptr) {
             fd = *fd_in;

@@ -43,11 +43,11 @@ def scripts(count, frames=5, seed=3):
     return out
 
 
-def run_server(oceans, field, picks, sc, order_seed=None, threads=1):
+def run_server(oceans, field, picks, sc, order_seed=None, threads=1, form=abi.OCEAN_FFT_EXACT):
     """Opens `picks` sessions, submits their scripts (interleaved at random
     when order_seed is given, keeping each session's own order), drains, and
     returns {session: (heights list, disp, normal, field)}."""
-    srv = OceanServer()
+    srv = OceanServer(form=form)
     sid = {k: srv.open_session(oceans[k], field) for k in picks}
     heights = {k: [] for k in picks}
     steps = [(k, i) for k in picks for i in range(len(sc[k]))]
@@ -216,3 +216,28 @@ def test_poisson_load_completes_with_batching():
     assert st["mean_batch_requests"] > 1.0
     assert 0.0 < st["latency_p50_ms"] <= st["latency_p99_ms"] <= st["latency_max_ms"]
     assert all(np.isfinite(o).all() for o in outs)
+
+
+def test_tensor_form_sessions_match_tensor_form_batches():
+    # The serving loop in the tensor-core form (config 5's sizes 128, 256 and
+    # 512 all have it): each session's ocean, batched with the others, equals
+    # a tensor-form batch of that ocean alone at the same time, bit for bit;
+    # a size without the form is refused when the session opens.
+    oceans, field = W.serving_sessions(6)
+    sc = scripts(6, frames=3)
+    mix, st = run_server(oceans, field, list(range(6)), sc, order_seed=4, form=abi.OCEAN_FFT_TENSOR)
+    assert st["requests_failed"] == 0 and st["updates_completed"] == 6 * 3
+    for k in range(6):
+        t_last = [item[1] for item in sc[k] if item[0] == "update"][-1]
+        n = oceans[k].size
+        b = ob.OceanBatch([oceans[k]], form=abi.OCEAN_FFT_TENSOR)
+        d = np.empty((n * n, 4), np.float32)
+        nrm = np.empty_like(d)
+        b.update_host([t_last], 0.0, d, nrm)
+        b.close()
+        assert np.array_equal(bits(mix[k][1]), bits(d.reshape(mix[k][1].shape))), n
+        assert np.array_equal(bits(mix[k][2]), bits(nrm.reshape(mix[k][2].shape))), n
+    srv = OceanServer(form=abi.OCEAN_FFT_TENSOR)
+    with pytest.raises((ValueError, ob.OceanError)):
+        srv.open_session(ob.OceanDesc(size=1024, seed=3), field)
+    srv.close()
