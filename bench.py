@@ -324,6 +324,20 @@ def bench_cascade(torch, queries: int = 1_000_000, frames: int = 50):
     torch.cuda.synchronize()
     res["converged_queries_per_s"] = queries / (e1.elapsed_time(e2) / 1000.0)
     cs.close()
+    # The same levels in the tensor-core form.
+    from oceanlib_b200 import abi
+
+    cs = ob.CascadeStack(W.cascade_3x256(), form=abi.OCEAN_FFT_TENSOR)
+    for k in range(3):
+        cs.update(k / 60.0, stream=sh)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for k in range(frames):
+        cs.update(1.0 + k / 60.0, stream=sh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    res["tensor_core_form"] = {"cascade_frames_per_s": frames / (e0.elapsed_time(e1) / 1000.0)}
+    cs.close()
     return res
 
 

@@ -512,6 +512,11 @@ typedef struct ocean_cascade ocean_cascade;
  * equal size advance together in one launch. Evaluates t = 0. */
 OCEAN_API ocean_cascade* ocean_cascade_create(const ocean_desc* levels, uint32_t count,
                                               ocean_status* out_status);
+/* As ocean_cascade_create, in a given ocean_fft_form instead of the
+ * process-wide one (OCEAN_FFT_TENSOR: every level of N = 64 to 512;
+ * other sizes give OCEAN_ERROR_INVALID_ARG). Queries are unchanged. */
+OCEAN_API ocean_cascade* ocean_cascade_create_form(const ocean_desc* levels, uint32_t count,
+                                                   int32_t fft_form, ocean_status* out_status);
 OCEAN_API void ocean_cascade_destroy(ocean_cascade* cascade);
 
 /* Advances every level to absolute time `time` (CascadeStack::update,

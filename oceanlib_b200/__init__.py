@@ -499,12 +499,16 @@ class OceanEnsemble:
 
 class CascadeStack:
     """ocean::CascadeStack (include/ocean/cascade.hpp:45-92): several ocean
-    levels summed at query time, updated together on the GPU."""
+    levels summed at query time, updated together on the GPU. `form` (an
+    OCEAN_FFT_* value) overrides the process-wide form."""
 
-    def __init__(self, levels: Sequence[OceanDesc]):
+    def __init__(self, levels: Sequence[OceanDesc], form: Optional[int] = None):
         arr = (OceanDescC * len(levels))(*[d.to_c() for d in levels])
         st = C.c_int(-1)
-        h = lib().ocean_cascade_create(arr, len(levels), C.byref(st))
+        if form is None:
+            h = lib().ocean_cascade_create(arr, len(levels), C.byref(st))
+        else:
+            h = lib().ocean_cascade_create_form(arr, len(levels), int(form), C.byref(st))
         if not h:
             if st.value == abi.OCEAN_ERROR_INVALID_ARG:
                 raise ValueError(f"invalid cascade ({status_string(st.value)})")

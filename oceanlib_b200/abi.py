@@ -292,6 +292,7 @@ SIGNATURES = {
     "ocean_ensemble_device_buffers": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(DeviceBuffers)]),
     "ocean_ensemble_describe": (C.c_uint64, [C.c_void_p, C.c_char_p, C.c_uint64]),
     "ocean_cascade_create":(C.c_void_p, [C.POINTER(OceanDescC), C.c_uint32, C.POINTER(C.c_int)]),
+    "ocean_cascade_create_form": (C.c_void_p, [C.POINTER(OceanDescC), C.c_uint32, C.c_int32, C.POINTER(C.c_int)]),
     "ocean_cascade_destroy": (None, [C.c_void_p]),
     "ocean_cascade_update": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p]),
     "ocean_cascade_level_count": (C.c_uint32, [C.c_void_p]),

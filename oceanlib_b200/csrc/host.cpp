@@ -1165,9 +1165,14 @@ private:
 // ---------------------------------------------------------------------------
 class Cascade {
 public:
-    Cascade(const ocean_desc* levels, uint32_t count)
+    // `form` < 0: the process-wide form (ocean_force_simd_level). A level's
+    // size must have the form (the tensor-core form: N = 64 to 512).
+    Cascade(const ocean_desc* levels, uint32_t count, int form = -1)
     {
         if (levels == nullptr || count == 0) throw std::invalid_argument("no levels");
+        if (form < 0) form = g_form.load();
+        if (form != OCEAN_FFT_EXACT && form != OCEAN_FFT_FAST && form != OCEAN_FFT_TENSOR)
+            throw std::invalid_argument("fft form");
         if (count > static_cast<uint32_t>(kMaxCascadeLevels)) throw std::invalid_argument("too many levels");
         std::vector<ocean_desc> descs(count);
         for (uint32_t i = 0; i < count; ++i) {
@@ -1195,8 +1200,8 @@ public:
                 where_[i] = {static_cast<uint32_t>(g), static_cast<uint32_t>(gd.size())};
                 gd.push_back(descs[i]);
             }
-            batches_.push_back(std::make_unique<Batch>(gd.data(), static_cast<uint32_t>(gd.size()),
-                                                       g_form.load(), false, foam, 0));
+            batches_.push_back(std::make_unique<Batch>(gd.data(), static_cast<uint32_t>(gd.size()), form, false,
+                                                       foam, 0));
         }
         levels_ = descs;
         // Evaluate t = 0, as a freshly built reference Ocean has.
@@ -1767,7 +1772,7 @@ struct ocean_ensemble {
 };
 struct ocean_cascade {
     ocean_b200::Cascade impl;
-    ocean_cascade(const ocean_desc* levels, uint32_t count) : impl(levels, count) {}
+    ocean_cascade(const ocean_desc* levels, uint32_t count, int form = -1) : impl(levels, count, form) {}
 };
 struct ocean_batch {
     Batch impl;
@@ -2269,6 +2274,15 @@ ocean_cascade* ocean_cascade_create(const ocean_desc* levels, uint32_t count, oc
 {
     ocean_cascade* c = nullptr;
     const ocean_status st = guarded([&] { c = new ocean_cascade(levels, count); });
+    if (out_status != nullptr) *out_status = st;
+    return st == OCEAN_OK ? c : nullptr;
+}
+
+ocean_cascade* ocean_cascade_create_form(const ocean_desc* levels, uint32_t count, int32_t fft_form,
+                                         ocean_status* out_status)
+{
+    ocean_cascade* c = nullptr;
+    const ocean_status st = guarded([&] { c = new ocean_cascade(levels, count, fft_form); });
     if (out_status != nullptr) *out_status = st;
     return st == OCEAN_OK ? c : nullptr;
 }

@@ -119,3 +119,38 @@ def test_cascade_rejects_bad_input():
     st = ob.lib().ocean_cascade_sample_many(cs.handle, None, 4, None, 4, 0.0, 0, None)
     assert st == ob.abi.OCEAN_ERROR_INVALID_ARG
     cs.close()
+
+
+def test_tensor_form_cascade_levels():
+    # Config 3's three 256^2 levels in the tensor-core form: each level equals
+    # a tensor-form batch of that level alone, bit for bit, and stays within
+    # 2e-6 of FP64 per channel; the summed queries run unchanged on them.
+    from oceanlib_b200 import abi
+
+    levels = W.cascade_3x256()
+    t = 41.0
+    cs = ob.CascadeStack(levels, form=abi.OCEAN_FFT_TENSOR)
+    cs.update(t)
+    cs.synchronize()
+    for i, d in enumerate(levels):
+        db = cs.device_buffers(i)
+        n = d.size * d.size
+        host = np.empty((n, 4), np.float32)
+        assert ob.lib().ocean_copy_to_host(host.ctypes.data, db.displacement, host.nbytes) == 0
+        b = ob.OceanBatch([d], form=abi.OCEAN_FFT_TENSOR)
+        bd = np.empty((n, 4), np.float32)
+        bn = np.empty_like(bd)
+        bv = np.empty_like(bd)
+        b.update_host([t], 0.0, bd, bn, bv)
+        b.close()
+        assert np.array_equal(bits(host), bits(bd)), i
+        ref = O.fp64_frame(d, t)["displacement"].reshape(n, 4)
+        for c in range(3):
+            rms = np.sqrt(np.mean(ref[:, c] ** 2))
+            assert np.abs(host[:, c].astype(np.float64) - ref[:, c]).max() / rms <= 2e-6, (i, c)
+    pts = W.cascade_query_points(4096)
+    out = cs.sample_many(pts)
+    assert np.isfinite(out).all()
+    cs.close()
+    with pytest.raises(ValueError):
+        ob.CascadeStack([ob.OceanDesc(size=1024, seed=2)], form=abi.OCEAN_FFT_TENSOR)
