@@ -187,6 +187,24 @@ def test_batch_descriptor_validation_is_host_side():
     assert st.value == abi.OCEAN_ERROR_INVALID_ARG
 
 
+def test_ensemble_and_cascade_forms_are_validated_host_side():
+    # ocean_ensemble_create_form / ocean_cascade_create_form refuse an unknown
+    # form (and empty input) before any device work.
+    lib = ob.lib()
+    descs = (abi.OceanDescC * 2)()
+    for d in descs:
+        lib.ocean_desc_init(C.byref(d))
+    st = C.c_int(-1)
+    assert not lib.ocean_ensemble_create_form(descs, 2, 0, 7, C.byref(st))
+    assert st.value == abi.OCEAN_ERROR_INVALID_ARG
+    assert not lib.ocean_ensemble_create_form(None, 0, 0, abi.OCEAN_FFT_TENSOR, C.byref(st))
+    assert st.value == abi.OCEAN_ERROR_INVALID_ARG
+    assert not lib.ocean_cascade_create_form(descs, 2, 7, C.byref(st))
+    assert st.value == abi.OCEAN_ERROR_INVALID_ARG
+    assert not lib.ocean_cascade_create_form(None, 0, abi.OCEAN_FFT_EXACT, C.byref(st))
+    assert st.value == abi.OCEAN_ERROR_INVALID_ARG
+
+
 def test_reference_header_paths_compile_and_link():
     # include/ocean/ocean.h as C99 (-pedantic -Werror) and include/ocean/*.hpp
     # as C++20, each in a program linked against libocean_b200.so: C and C++
