@@ -31,8 +31,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 # `value` is the plain FP32 form (bit-identical to the reference); the
-# tensor-core form's throughput sits beside it in "tensor_core_form", and the
-# serving loop's request latency in "p99_ms".
+# tensor-core form's throughput sits beside it in "tensor_core_form", the
+# precise form's (FP64 stage blocks: like the tensor form, within 2e-6 of
+# FP64) in "precise_form", and the serving loop's request latency in "p99_ms".
 METRIC = "512^2 ocean updates/s: batched TC-FFT vs plain FP32 @<=2e-6 rel err; p99 ms"
 UNIT = "updates/s"
 N = 512
@@ -60,7 +61,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--schedule", default="persistent", choices=["persistent", "chunked"])
-    ap.add_argument("--form", default="exact", choices=["exact", "fast", "tensor"])
+    ap.add_argument("--form", default="exact", choices=["exact", "fast", "tensor", "precise"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -539,6 +540,9 @@ def bench_plain_update(torch, batch: int = 64, steps: int = 60, cpu_seconds: flo
     tb, out["tensor_core_form"] = run(abi.OCEAN_FFT_TENSOR)
     tb.close()
     out["tensor_core_form"]["vs_plain_fp32"] = out["tensor_core_form"]["value"] / out["fp32"]["value"]
+    pb, out["precise_form"] = run(abi.OCEAN_FFT_PRECISE)
+    pb.close()
+    out["precise_form"]["vs_plain_fp32"] = out["precise_form"]["value"] / out["fp32"]["value"]
     if cpu_seconds > 0:
         import oracle as O
 
@@ -793,7 +797,7 @@ def main():
 
     batch = ob.OceanBatch(descs, foam=W.foam_desc(), chunk=args.chunk,
                           form={"exact": abi.OCEAN_FFT_EXACT, "fast": abi.OCEAN_FFT_FAST,
-                                "tensor": abi.OCEAN_FFT_TENSOR}[args.form],
+                                "tensor": abi.OCEAN_FFT_TENSOR, "precise": abi.OCEAN_FFT_PRECISE}[args.form],
                           schedule=abi.OCEAN_SCHEDULE_CHUNKED if args.schedule == "chunked"
                           else abi.OCEAN_SCHEDULE_PERSISTENT)
     # An explicit stream: the library launches on it and the CUDA events
@@ -885,38 +889,46 @@ def main():
                 "d2h_bytes_per_step": B * CELLS * 3 * 8,
                 "api": "ocean_batch_update_host_rgba16 (RGBA16F packed on the device, foam in the alpha)"}
 
-    # ---- the tensor-core DFT form on the same workload, beside the FP32 form ----
-    tc = None
-    if args.form != "tensor":
-        tcb = ob.OceanBatch(descs, foam=W.foam_desc(), form=abi.OCEAN_FFT_TENSOR)
-        tframe = 0
+    # ---- the tensor-core and precise forms on the same workload, beside the
+    # FP32 form (both within 2e-6 of FP64 on every channel) ----
+    def other_form(form, kernel):
+        ob_ = ob.OceanBatch(descs, foam=W.foam_desc(), form=form)
+        fr = 0
 
-        def tc_step():
-            nonlocal tframe
-            tframe += 1
-            tcb.update([tframe * dt], foam_dt=dt, stream=sh)
+        def step():
+            nonlocal fr
+            fr += 1
+            ob_.update([fr * dt], foam_dt=dt, stream=sh)
 
         for _ in range(max(3, args.warmup)):
-            tc_step()
+            step()
         torch.cuda.synchronize()
-        tc_steps = max(5, args.steps // 3)
-        t_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        steps = max(5, args.steps // 3)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         if world > 1:
             torch.distributed.barrier()
-        tc_launches0 = tcb.launch_count
-        t_ev[0].record(stream)
-        for _ in range(tc_steps):
-            tc_step()
-        t_ev[1].record(stream)
+        launches0 = ob_.launch_count
+        ev[0].record(stream)
+        for _ in range(steps):
+            step()
+        ev[1].record(stream)
         torch.cuda.synchronize()
-        tc_ms = t_ev[0].elapsed_time(t_ev[1])
+        ms = ev[0].elapsed_time(ev[1])
         if world > 1:
-            tc_ms = max_over_ranks(tc_ms, torch.distributed, "cuda")
-        tc = {"value": B * tc_steps * world / (tc_ms / 1000.0), "unit": UNIT,
-              "ms_per_step": tc_ms / tc_steps, "steps": tc_steps,
-              "gpu_launches": int(tcb.launch_count - tc_launches0),
-              "kernel": "frame_kernel, tensor form (tcgen05 four-step DFT, exact FP16 digit-slice GEMMs)"}
-        tcb.close()
+            ms = max_over_ranks(ms, torch.distributed, "cuda")
+        out = {"value": B * steps * world / (ms / 1000.0), "unit": UNIT, "ms_per_step": ms / steps,
+               "steps": steps, "gpu_launches": int(ob_.launch_count - launches0), "kernel": kernel}
+        ob_.close()
+        return out
+
+    tc = None
+    if args.form != "tensor":
+        tc = other_form(abi.OCEAN_FFT_TENSOR,
+                        "frame_kernel, tensor form (tcgen05 four-step DFT, exact FP16 digit-slice GEMMs)")
+    precise = None
+    if args.form != "precise":
+        precise = other_form(abi.OCEAN_FFT_PRECISE,
+                             "frame_kernel, precise form (radix-2 stage blocks in FP64, FP32 between them)")
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -985,6 +997,9 @@ def main():
         if tc is not None:
             tc["vs_plain_fp32"] = tc["value"] / value
             line["tensor_core_form"] = tc
+        if precise is not None:
+            precise["vs_plain_fp32"] = precise["value"] / value
+            line["precise_form"] = precise
         if not args.no_extra and world == 1:
             extra = {}
             plain_cpu = 0.0 if args.no_cpu_baseline else 4.0

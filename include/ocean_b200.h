@@ -162,7 +162,8 @@ OCEAN_API const char* ocean_simd_level(void);
 
 /* include/ocean/ocean.h:262. "scalar" (and "sse2", "avx2", "neon", "exact")
  * select the exact FFT form, whose results are bit-identical to the
- * reference's scalar kernels; "fast" selects the FMA form. Affects handles
+ * reference's scalar kernels; "fast" selects the FMA form and "precise" the
+ * FP64-block form (OCEAN_FFT_PRECISE). Affects handles
  * created after the call. Returns the reference's spelling of the level for
  * the reference names, so "scalar" returns "scalar". */
 OCEAN_API const char* ocean_force_simd_level(const char* name);
@@ -298,10 +299,13 @@ typedef enum ocean_fft_form {
     OCEAN_FFT_EXACT = 0, /* radix-2 Stockham in the reference's operation order,
                             no FMA: bit-identical to the reference           */
     OCEAN_FFT_FAST  = 1, /* same dataflow with fused multiply-adds           */
-    OCEAN_FFT_TENSOR = 2 /* four-step DFT on the tensor cores (tcgen05):
+    OCEAN_FFT_TENSOR = 2, /* four-step DFT on the tensor cores (tcgen05):
                             operands cut into four signed 8-bit digits held
                             as FP16, exact digit products, levels combined
                             in FP32; N = 64, 128, 256 and 512 */
+    OCEAN_FFT_PRECISE = 3 /* the radix-2 dataflow with each register block of
+                            stages computed in FP64 and stored in FP32 once:
+                            within 2e-6 of FP64, every size */
 } ocean_fft_form;
 
 /* `count` unnormalised inverse DFTs (sign +, as src/core/fft.cpp) of

@@ -14,6 +14,7 @@ OCEAN_ERROR_TIMEOUT = 5
 OCEAN_FFT_EXACT = 0
 OCEAN_FFT_FAST = 1
 OCEAN_FFT_TENSOR = 2
+OCEAN_FFT_PRECISE = 3
 
 OCEAN_SCHEDULE_PERSISTENT = 0
 OCEAN_SCHEDULE_CHUNKED = 1

@@ -35,7 +35,8 @@ extern "C" ocean_status ocean_dft_batch(uint32_t size, uint32_t count, int32_t f
     using namespace ocean_b200;
     const bool pow2 = size != 0 && (size & (size - 1)) == 0;
     if (!pow2 || size < 16 || size > 1024 || input == nullptr || output == nullptr) return OCEAN_ERROR_INVALID_ARG;
-    if (form != OCEAN_FFT_EXACT && form != OCEAN_FFT_FAST && form != OCEAN_FFT_TENSOR) return OCEAN_ERROR_INVALID_ARG;
+    if (form != OCEAN_FFT_EXACT && form != OCEAN_FFT_FAST && form != OCEAN_FFT_TENSOR && form != OCEAN_FFT_PRECISE)
+        return OCEAN_ERROR_INVALID_ARG;
     if (form == OCEAN_FFT_TENSOR && (size < 64 || size > 512)) return OCEAN_ERROR_INVALID_ARG;
     if (count == 0) return OCEAN_OK;
     return guarded([&] {

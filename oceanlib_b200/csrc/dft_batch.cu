@@ -1,6 +1,6 @@
 // oceanlib-b200: batched 1-D inverse DFTs of device sequences in each form
 // (ocean_dft_batch): the radix-2 Stockham FFT (exact, bit-identical to
-// src/core/fft.cpp), its fast variant, and the tensor-core DFT (tc_dft.cuh at
+// src/core/fft.cpp), its fast and precise variants, and the tensor-core DFT (tc_dft.cuh at
 // N = 512, tc_dft_small.cuh at N = 64, 128 and 256).
 // The frame kernel runs the same code on its rows and columns; this entry
 // point isolates the transform for accuracy checks against FP64.
@@ -15,7 +15,7 @@ namespace {
 constexpr int kSeqPad = 4;  // float2 between sequences in shared memory
 
 // CTAs take chunks of 8 sequences in turn (several engine calls per CTA).
-template <int LOG_N, bool FAST>
+template <int LOG_N, int AR>
 __global__ void __launch_bounds__(8 * lanes_for(LOG_N))
 dft_fp32_kernel(const float2* __restrict__ in, float2* __restrict__ out, int count,
                 const float2* __restrict__ tw)
@@ -35,7 +35,7 @@ dft_fp32_kernel(const float2* __restrict__ in, float2* __restrict__ out, int cou
             data[s * SEQ + pad_idx(n)] = s < k ? in[static_cast<size_t>(base + s) * N + n] : make_float2(0.0f, 0.0f);
         }
         __syncthreads();
-        fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);
+        fft_sequence<LOG_N, G, AR>(data + (tid / G) * SEQ, tws, tid % G);
         __syncthreads();
         for (int i = tid; i < k * N; i += NT) {
             const int s = i >> LOG_N, n = i & (N - 1);
@@ -139,12 +139,13 @@ cudaError_t tc_small_launch(const float2* in, float2* out, int count, const floa
 }
 
 template <int LOG_N>
-cudaError_t fp32_launch(bool fast, const float2* in, float2* out, int count, const float2* tw, int grid,
+cudaError_t fp32_launch(int ar, const float2* in, float2* out, int count, const float2* tw, int grid,
                         cudaStream_t st)
 {
     constexpr int N = 1 << LOG_N, G = lanes_for(LOG_N);
     const size_t smem = (8 * (padded_len(N) + kSeqPad) + N) * sizeof(float2);
-    auto k = fast ? dft_fp32_kernel<LOG_N, true> : dft_fp32_kernel<LOG_N, false>;
+    auto k = ar == kArFast ? dft_fp32_kernel<LOG_N, kArFast>
+                           : (ar == kArPrecise ? dft_fp32_kernel<LOG_N, kArPrecise> : dft_fp32_kernel<LOG_N, kArExact>);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     k<<<grid, 8 * G, smem, st>>>(in, out, count, tw);
@@ -181,15 +182,15 @@ cudaError_t launch_dft_batch(int log_n, int form, const float2* in, float2* out,
         dft_tc512_kernel<<<grid, BatchEngine::Lay::kThreads, smem, st>>>(in, out, count, tw, error);
         return cudaGetLastError();
     }
-    const bool fast = form == 1;
+    const int ar = arith_of_form(form);
     switch (log_n) {
-        case 4: return fp32_launch<4>(fast, in, out, count, tw, grid, st);
-        case 5: return fp32_launch<5>(fast, in, out, count, tw, grid, st);
-        case 6: return fp32_launch<6>(fast, in, out, count, tw, grid, st);
-        case 7: return fp32_launch<7>(fast, in, out, count, tw, grid, st);
-        case 8: return fp32_launch<8>(fast, in, out, count, tw, grid, st);
-        case 9: return fp32_launch<9>(fast, in, out, count, tw, grid, st);
-        case 10: return fp32_launch<10>(fast, in, out, count, tw, grid, st);
+        case 4: return fp32_launch<4>(ar, in, out, count, tw, grid, st);
+        case 5: return fp32_launch<5>(ar, in, out, count, tw, grid, st);
+        case 6: return fp32_launch<6>(ar, in, out, count, tw, grid, st);
+        case 7: return fp32_launch<7>(ar, in, out, count, tw, grid, st);
+        case 8: return fp32_launch<8>(ar, in, out, count, tw, grid, st);
+        case 9: return fp32_launch<9>(ar, in, out, count, tw, grid, st);
+        case 10: return fp32_launch<10>(ar, in, out, count, tw, grid, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -27,6 +27,8 @@
 #include "tc_dft.cuh"
 #include "tc_dft_small.cuh"
 
+#include <type_traits>
+
 namespace ocean_b200 {
 namespace {
 
@@ -201,7 +203,7 @@ __device__ __forceinline__ void load_twiddles(float2* tws, const float2* __restr
 // (one lane group of G2 per pair, named barrier 1 + pair where a pair spans
 // two warps), or with TC the tensor-core four-step DFT, 8 sequences per
 // engine call (N = 512; its twiddles live in the engine).
-template <class P, bool FAST, int COUNT, int COLW = 0, class Eng = tc::Engine<8>>
+template <class P, int AR, int COUNT, int COLW = 0, class Eng = tc::Engine<8>>
 __device__ __forceinline__ void transform_all(float2* data, const float2* tws, int tid, Eng* eng,
                                               unsigned* error)
 {
@@ -216,14 +218,14 @@ __device__ __forceinline__ void transform_all(float2* data, const float2* tws, i
         static_assert(COUNT * P::N == 16 * Eng::Lay::kThreads, "one engine call holds the task's sequences");
         eng->dft(data, P::SEQ, COUNT, tid, error);
     } else if constexpr (!P::PAIRED) {
-        fft_sequence<P::LOG_N, P::G, FAST>(data + (tid / P::G) * P::SEQ, tws, tid % P::G);
+        fft_sequence<P::LOG_N, P::G, AR>(data + (tid / P::G) * P::SEQ, tws, tid % P::G);
     } else {
         constexpr int G2 = P::G2;
         static_assert(COUNT % 2 == 0, "sequences come in pairs");
         static_assert(G2 <= 32 || (COUNT / 2) < 16, "one named barrier per pair");
         const int pair = tid / G2;
         const int shift = COLW != 0 ? col_pair_shift<COUNT / (COLW != 0 ? COLW : 1), COLW>(pair) : 0;
-        fft_pair<P::LOG_N, G2, FAST>(reinterpret_cast<ulonglong2*>(data) + pair * P::SEQ4 + shift, tws, tid % G2,
+        fft_pair<P::LOG_N, G2, AR>(reinterpret_cast<ulonglong2*>(data) + pair * P::SEQ4 + shift, tws, tid % G2,
                                      1 + pair);
     }
 }
@@ -329,7 +331,7 @@ __device__ __forceinline__ void publish_staged(unsigned* const* pub, int tid)
     }
 }
 
-template <class P, int NF, bool FAST>
+template <class P, int NF, int AR>
 __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int group,
                                          float2* __restrict__ inter_slot, float2* smem,
                                          const float2* tws, int tid, uint64_t* h0_bar, uint32_t h0_parity,
@@ -449,7 +451,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
     }
     __syncthreads();
 
-    transform_all<P, FAST, ROWS * NF>(data, tws, tid, eng, error);
+    transform_all<P, AR, ROWS * NF>(data, tws, tid, eng, error);
     __syncthreads();
 
     // Write the rows cell-major: inter[row][x][f], NF/2 float4 per cell.
@@ -481,7 +483,7 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
 // (column FFTs + finalize + optional foam substep). CG loads read the
 // intermediate from L2: another CTA wrote it during this launch.
 // ---------------------------------------------------------------------------
-template <class P, int NF, bool FAST, bool FOAM, int W, bool CG>
+template <class P, int NF, int AR, bool FOAM, int W, bool CG>
 __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int strip,
                                          const float2* __restrict__ inter_slot, float2* smem,
                                          const float2* tws, int tid, TcEngineOf<P::LOG_N, NF>* eng = nullptr,
@@ -553,7 +555,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
     __syncthreads();
     publish_staged(pub, tid);
 
-    transform_all<P, FAST, NF * W, W>(data, tws, tid, eng, error);
+    transform_all<P, AR, NF * W, W>(data, tws, tid, eng, error);
     if constexpr (FSTEP) asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's window copies
     __syncthreads();
 
@@ -633,7 +635,7 @@ __device__ __forceinline__ void col_task(const FrameArgs& a, int ocean, int stri
 // Per-chunk kernels: grid (groups, oceans in the chunk); ocean o of the chunk
 // uses intermediate slot o.
 // ---------------------------------------------------------------------------
-template <int LOG_N, int NF, bool FAST>
+template <int LOG_N, int NF, int AR>
 __global__ void __launch_bounds__(ChunkPlan<LOG_N>::template threads<NF>())
 row_pass_kernel(FrameArgs a)
 {
@@ -647,11 +649,11 @@ row_pass_kernel(FrameArgs a)
     load_twiddles<P>(tws, a.twiddles, threadIdx.x, NT);
     __syncthreads();  // the twiddles are complete before any transform reads them; the barrier is set up
     const int o = blockIdx.y;
-    row_task<P, NF, FAST>(a, a.ocean_base + o, blockIdx.x, a.inter + static_cast<size_t>(o) * P::N * P::N * NF,
+    row_task<P, NF, AR>(a, a.ocean_base + o, blockIdx.x, a.inter + static_cast<size_t>(o) * P::N * P::N * NF,
                           smem, tws, threadIdx.x, &h0_bar, 0u, nullptr, a.error);
 }
 
-template <int LOG_N, int NF, bool FAST, bool FOAM>
+template <int LOG_N, int NF, int AR, bool FOAM>
 __global__ void __launch_bounds__(NF * Shape<LOG_N>::W * Shape<LOG_N>::G)
 col_pass_kernel(FrameArgs a)
 {
@@ -664,7 +666,7 @@ col_pass_kernel(FrameArgs a)
     load_twiddles<P>(tws, a.twiddles, threadIdx.x, NT);
     __syncthreads();  // the twiddles are complete before any transform reads them
     const int o = blockIdx.y;
-    col_task<P, NF, FAST, FOAM, S::W, false>(a, a.ocean_base + o, blockIdx.x,
+    col_task<P, NF, AR, FOAM, S::W, false>(a, a.ocean_base + o, blockIdx.x,
                                              a.inter + static_cast<size_t>(o) * P::N * P::N * NF, smem, tws,
                                              threadIdx.x);
 }
@@ -739,7 +741,7 @@ __host__ __device__ constexpr size_t frame_engine_offset()
            128 * 128;
 }
 
-template <class P, int NF, bool FAST, bool FOAM>
+template <class P, int NF, int AR, bool FOAM>
 __global__ void __launch_bounds__(P::template threads<NF>(), frame_min_blocks<P, NF>())
 frame_kernel(FrameArgs a, QueueArgs q)
 {
@@ -866,11 +868,11 @@ frame_kernel(FrameArgs a, QueueArgs q)
         const unsigned slot = ocean % static_cast<unsigned>(q.slots);
         const int abs_ocean = a.ocean_base + static_cast<int>(ocean);
         if (row) {
-            row_task<P, NF, FAST>(a, abs_ocean, static_cast<int>(idx), a.inter + slot * slot_f2, smem, tws, tid,
+            row_task<P, NF, AR>(a, abs_ocean, static_cast<int>(idx), a.inter + slot * slot_f2, smem, tws, tid,
                                   &h0_bar, h0_parity, &eng, q.error, s_pub);
             h0_parity ^= 1u;
         } else {
-            col_task<P, NF, FAST, FOAM, P::PW, true>(a, abs_ocean, static_cast<int>(idx),
+            col_task<P, NF, AR, FOAM, P::PW, true>(a, abs_ocean, static_cast<int>(idx),
                                                              a.inter + slot * slot_f2, smem, tws, tid,
                                                              &eng, q.error, s_pub);
         }
@@ -961,7 +963,7 @@ __device__ __forceinline__ void mix_load_twiddles(float2* area, const float2* __
     load_twiddles<MixPlan<L>>(area + mix_tw_offset(L), src, tid, nt);
 }
 
-template <int L, int NF, bool FAST>
+template <int L, int NF, int AR>
 __device__ __noinline__ void mix_run(const MixedGroup& g, bool row, int ocean, int idx, float2* smem,
                                         const float2* tw_area, int tid, uint64_t* h0_bar, uint32_t h0_parity,
                                         unsigned* error, unsigned* const* pub)
@@ -971,13 +973,13 @@ __device__ __noinline__ void mix_run(const MixedGroup& g, bool row, int ocean, i
     float2* inter = g.a.inter + static_cast<size_t>(slot) * P::N * P::N * NF;
     const float2* tws = tw_area + mix_tw_offset(L);
     if (row) {
-        row_task<P, NF, FAST>(g.a, ocean, idx, inter, smem, tws, tid, h0_bar, h0_parity, nullptr, error, pub);
+        row_task<P, NF, AR>(g.a, ocean, idx, inter, smem, tws, tid, h0_bar, h0_parity, nullptr, error, pub);
     } else {
-        col_task<P, NF, FAST, false, P::PW, true>(g.a, ocean, idx, inter, smem, tws, tid, nullptr, error, pub);
+        col_task<P, NF, AR, false, P::PW, true>(g.a, ocean, idx, inter, smem, tws, tid, nullptr, error, pub);
     }
 }
 
-template <int NF, bool FAST>
+template <int NF, int AR>
 __global__ void __launch_bounds__(64 * NF, 768 / (64 * NF)) mixed_frame_kernel(MixedArgs m)
 {
     constexpr int NT = 64 * NF;
@@ -1094,30 +1096,30 @@ __global__ void __launch_bounds__(64 * NF, 768 / (64 * NF)) mixed_frame_kernel(M
         const MixedGroup& g = s_groups[s_group];
         const bool row = s_row != 0;
         switch (g.log_n) {
-            case 5: mix_run<5, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
-            case 6: mix_run<6, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
-            case 7: mix_run<7, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
-            case 8: mix_run<8, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
-            case 9: mix_run<9, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
-            default: mix_run<10, NF, FAST>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
+            case 5: mix_run<5, NF, AR>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
+            case 6: mix_run<6, NF, AR>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
+            case 7: mix_run<7, NF, AR>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
+            case 8: mix_run<8, NF, AR>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
+            case 9: mix_run<9, NF, AR>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
+            default: mix_run<10, NF, AR>(g, row, s_ocean, s_idx, smem, tw_area, tid, &h0_bar, h0_parity, m.error, s_pub); break;
         }
         if (row) h0_parity ^= 1u;
     }
 }
 
-template <int NF, bool FAST>
+template <int NF, int AR>
 struct MixedLaunch {
     static constexpr int threads() { return 64 * NF; }
     static cudaError_t prepare()
     {
-        return cudaFuncSetAttribute(mixed_frame_kernel<NF, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return cudaFuncSetAttribute(mixed_frame_kernel<NF, AR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(mixed_smem_bytes(NF)));
     }
     static int blocks_per_sm()
     {
         if (prepare() != cudaSuccess) return 0;
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mixed_frame_kernel<NF, FAST>, threads(),
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mixed_frame_kernel<NF, AR>, threads(),
                                                           mixed_smem_bytes(NF)) != cudaSuccess)
             return 0;
         return n;
@@ -1126,7 +1128,7 @@ struct MixedLaunch {
     {
         cudaError_t e = prepare();
         if (e != cudaSuccess) return e;
-        mixed_frame_kernel<NF, FAST><<<grid, threads(), mixed_smem_bytes(NF), st>>>(m);
+        mixed_frame_kernel<NF, AR><<<grid, threads(), mixed_smem_bytes(NF), st>>>(m);
         return cudaGetLastError();
     }
 };
@@ -1248,12 +1250,12 @@ constexpr size_t col_smem_bytes()
            (NF * S::W * P::SEQF2 + col_shift_f2_of<P, NF, S::W>() + foam_window_f2<LOG_N, S::W>() + P::TWF2);
 }
 
-template <int LOG_N, int NF, bool FAST>
+template <int LOG_N, int NF, int AR>
 cudaError_t row_launch(const FrameArgs& a, cudaStream_t st)
 {
     using P = ChunkPlan<LOG_N>;
     constexpr size_t smem = row_smem_bytes<LOG_N, NF>();
-    auto k = row_pass_kernel<LOG_N, NF, FAST>;
+    auto k = row_pass_kernel<LOG_N, NF, AR>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -1262,12 +1264,12 @@ cudaError_t row_launch(const FrameArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-template <int LOG_N, int NF, bool FAST, bool FOAM>
+template <int LOG_N, int NF, int AR, bool FOAM>
 cudaError_t col_launch(const FrameArgs& a, cudaStream_t st)
 {
     using S = Shape<LOG_N>;
     constexpr size_t smem = col_smem_bytes<LOG_N, NF>();
-    auto k = col_pass_kernel<LOG_N, NF, FAST, FOAM>;
+    auto k = col_pass_kernel<LOG_N, NF, AR, FOAM>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -1283,7 +1285,7 @@ constexpr size_t frame_smem_bytes()
     return sizeof(float2) * (frame_data_float2<P, NF>() + P::TWF2);
 }
 
-template <int LOG_N, int NF, bool FAST, bool FOAM, bool TC = false, int V = 0>
+template <int LOG_N, int NF, int AR, bool FOAM, bool TC = false, int V = 0>
 struct FrameLaunch {
     using P = PlanOf<LOG_N, V, TC>;
     using Eng = TcEngineOf<LOG_N, NF>;
@@ -1293,7 +1295,7 @@ struct FrameLaunch {
 
     static cudaError_t prepare()
     {
-        return cudaFuncSetAttribute(frame_kernel<P, NF, FAST, FOAM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return cudaFuncSetAttribute(frame_kernel<P, NF, AR, FOAM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem()));
     }
 
@@ -1301,7 +1303,7 @@ struct FrameLaunch {
     {
         if (prepare() != cudaSuccess) return 0;
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<P, NF, FAST, FOAM>, threads(), smem()) !=
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<P, NF, AR, FOAM>, threads(), smem()) !=
             cudaSuccess)
             return 0;
         // The tensor-core engine's tensor memory bounds its residency.
@@ -1316,25 +1318,35 @@ struct FrameLaunch {
         if (TC) {
             // Every resident CTA must obtain its tensor memory without waiting.
             int n = 0;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<P, NF, FAST, FOAM>, threads(), smem());
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, frame_kernel<P, NF, AR, FOAM>, threads(), smem());
             if (e != cudaSuccess) return e;
             if (n * Eng::Lay::kTmemCols > 512) return cudaErrorInvalidConfiguration;
         }
-        frame_kernel<P, NF, FAST, FOAM><<<grid, threads(), smem(), st>>>(a, q);
+        frame_kernel<P, NF, AR, FOAM><<<grid, threads(), smem(), st>>>(a, q);
         return cudaGetLastError();
     }
 };
 
-// form: 0 exact, 1 fast (FMA), 2 tensor cores (N = 64 to 512).
-template <int LOG_N, int V, typename Fn>
-auto frame_variant_plan(int nf, bool fast, bool foam, Fn&& fn)
+// The arithmetic `ar` (kArExact, kArFast, kArPrecise) as a compile-time
+// constant for `fn`.
+template <typename Fn>
+auto with_arith(int ar, Fn&& fn)
 {
-    if (nf == 4) return fast ? fn(FrameLaunch<LOG_N, 4, true, false, false, V>{})
-                             : fn(FrameLaunch<LOG_N, 4, false, false, false, V>{});
-    if (foam) return fast ? fn(FrameLaunch<LOG_N, 6, true, true, false, V>{})
-                          : fn(FrameLaunch<LOG_N, 6, false, true, false, V>{});
-    return fast ? fn(FrameLaunch<LOG_N, 6, true, false, false, V>{})
-                : fn(FrameLaunch<LOG_N, 6, false, false, false, V>{});
+    if (ar == kArFast) return fn(std::integral_constant<int, kArFast>{});
+    if (ar == kArPrecise) return fn(std::integral_constant<int, kArPrecise>{});
+    return fn(std::integral_constant<int, kArExact>{});
+}
+
+// form: an ocean_fft_form (exact, fast, tensor cores at N = 64 to 512, precise).
+template <int LOG_N, int V, typename Fn>
+auto frame_variant_plan(int nf, int ar, bool foam, Fn&& fn)
+{
+    return with_arith(ar, [&](auto A) {
+        constexpr int AR = decltype(A)::value;
+        if (nf == 4) return fn(FrameLaunch<LOG_N, 4, AR, false, false, V>{});
+        if (foam) return fn(FrameLaunch<LOG_N, 6, AR, true, false, V>{});
+        return fn(FrameLaunch<LOG_N, 6, AR, false, false, V>{});
+    });
 }
 
 template <int LOG_N, typename Fn>
@@ -1342,16 +1354,16 @@ auto frame_variant(int nf, int form, bool foam, int plan, Fn&& fn)
 {
     if constexpr (has_tc_form<LOG_N>()) {
         if (form == 2) {
-            if (nf == 4) return fn(FrameLaunch<LOG_N, 4, false, false, true>{});
-            if (foam) return fn(FrameLaunch<LOG_N, 6, false, true, true>{});
-            return fn(FrameLaunch<LOG_N, 6, false, false, true>{});
+            if (nf == 4) return fn(FrameLaunch<LOG_N, 4, kArExact, false, true>{});
+            if (foam) return fn(FrameLaunch<LOG_N, 6, kArExact, true, true>{});
+            return fn(FrameLaunch<LOG_N, 6, kArExact, false, true>{});
         }
     }
-    const bool fast = form == 1;
+    const int ar = arith_of_form(form);
     if constexpr (frame_plan_count<LOG_N>(false) > 1) {
-        if (plan == 1) return frame_variant_plan<LOG_N, 1>(nf, fast, foam, fn);
+        if (plan == 1) return frame_variant_plan<LOG_N, 1>(nf, ar, foam, fn);
     }
-    return frame_variant_plan<LOG_N, 0>(nf, fast, foam, fn);
+    return frame_variant_plan<LOG_N, 0>(nf, ar, foam, fn);
 }
 
 template <typename Fn>
@@ -1369,20 +1381,22 @@ auto frame_dispatch(int log_n, int nf, int form, bool foam, int plan, Fn&& fn)
 }
 
 template <int LOG_N>
-cudaError_t row_dispatch_n(int nf, bool fast, const FrameArgs& a, cudaStream_t st)
+cudaError_t row_dispatch_n(int nf, int ar, const FrameArgs& a, cudaStream_t st)
 {
-    if (nf == 4) return fast ? row_launch<LOG_N, 4, true>(a, st) : row_launch<LOG_N, 4, false>(a, st);
-    return fast ? row_launch<LOG_N, 6, true>(a, st) : row_launch<LOG_N, 6, false>(a, st);
+    return with_arith(ar, [&](auto A) {
+        constexpr int AR = decltype(A)::value;
+        return nf == 4 ? row_launch<LOG_N, 4, AR>(a, st) : row_launch<LOG_N, 6, AR>(a, st);
+    });
 }
 
 template <int LOG_N>
-cudaError_t col_dispatch_n(int nf, bool fast, bool foam, const FrameArgs& a, cudaStream_t st)
+cudaError_t col_dispatch_n(int nf, int ar, bool foam, const FrameArgs& a, cudaStream_t st)
 {
-    if (nf == 4) return fast ? col_launch<LOG_N, 4, true, false>(a, st)
-                             : col_launch<LOG_N, 4, false, false>(a, st);
-    if (foam) return fast ? col_launch<LOG_N, 6, true, true>(a, st)
-                          : col_launch<LOG_N, 6, false, true>(a, st);
-    return fast ? col_launch<LOG_N, 6, true, false>(a, st) : col_launch<LOG_N, 6, false, false>(a, st);
+    return with_arith(ar, [&](auto A) {
+        constexpr int AR = decltype(A)::value;
+        if (nf == 4) return col_launch<LOG_N, 4, AR, false>(a, st);
+        return foam ? col_launch<LOG_N, 6, AR, true>(a, st) : col_launch<LOG_N, 6, AR, false>(a, st);
+    });
 }
 
 }  // namespace
@@ -1425,20 +1439,24 @@ uint32_t mixed_tasks(int log_n, int count)
     return static_cast<uint32_t>(count) * (rt + ct);
 }
 
-int mixed_blocks_per_sm(int nf, bool fast)
+int mixed_blocks_per_sm(int nf, int ar)
 {
-    if (nf == 4) return fast ? MixedLaunch<4, true>::blocks_per_sm() : MixedLaunch<4, false>::blocks_per_sm();
-    return fast ? MixedLaunch<6, true>::blocks_per_sm() : MixedLaunch<6, false>::blocks_per_sm();
+    return with_arith(ar, [&](auto A) {
+        constexpr int AR = decltype(A)::value;
+        return nf == 4 ? MixedLaunch<4, AR>::blocks_per_sm() : MixedLaunch<6, AR>::blocks_per_sm();
+    });
 }
 
-cudaError_t launch_mixed_frame(int nf, bool fast, const MixedArgs& m, int grid, cudaStream_t st)
+cudaError_t launch_mixed_frame(int nf, int ar, const MixedArgs& m, int grid, cudaStream_t st)
 {
     if (m.groups < 1 || m.groups > kMaxMixedGroups) return cudaErrorInvalidValue;
     for (int g = 0; g < m.groups; ++g)
         if (!mixed_size_ok(m.g[g].log_n) || m.g[g].count < 1 || m.g[g].slots < 1)
             return cudaErrorInvalidValue;
-    if (nf == 4) return fast ? MixedLaunch<4, true>::launch(m, grid, st) : MixedLaunch<4, false>::launch(m, grid, st);
-    return fast ? MixedLaunch<6, true>::launch(m, grid, st) : MixedLaunch<6, false>::launch(m, grid, st);
+    return with_arith(ar, [&](auto A) {
+        constexpr int AR = decltype(A)::value;
+        return nf == 4 ? MixedLaunch<4, AR>::launch(m, grid, st) : MixedLaunch<6, AR>::launch(m, grid, st);
+    });
 }
 
 cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned* error, unsigned* bar_error,
@@ -1448,31 +1466,31 @@ cudaError_t launch_wait_probe(const unsigned* counter, unsigned target, unsigned
     return cudaGetLastError();
 }
 
-cudaError_t launch_row_pass(int log_n, int nf, bool fast, const FrameArgs& a, cudaStream_t st)
+cudaError_t launch_row_pass(int log_n, int nf, int ar, const FrameArgs& a, cudaStream_t st)
 {
     switch (log_n) {
-        case 4: return row_dispatch_n<4>(nf, fast, a, st);
-        case 5: return row_dispatch_n<5>(nf, fast, a, st);
-        case 6: return row_dispatch_n<6>(nf, fast, a, st);
-        case 7: return row_dispatch_n<7>(nf, fast, a, st);
-        case 8: return row_dispatch_n<8>(nf, fast, a, st);
-        case 9: return row_dispatch_n<9>(nf, fast, a, st);
-        case 10: return row_dispatch_n<10>(nf, fast, a, st);
+        case 4: return row_dispatch_n<4>(nf, ar, a, st);
+        case 5: return row_dispatch_n<5>(nf, ar, a, st);
+        case 6: return row_dispatch_n<6>(nf, ar, a, st);
+        case 7: return row_dispatch_n<7>(nf, ar, a, st);
+        case 8: return row_dispatch_n<8>(nf, ar, a, st);
+        case 9: return row_dispatch_n<9>(nf, ar, a, st);
+        case 10: return row_dispatch_n<10>(nf, ar, a, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_col_pass(int log_n, int nf, bool fast, bool fuse_foam, const FrameArgs& a,
+cudaError_t launch_col_pass(int log_n, int nf, int ar, bool fuse_foam, const FrameArgs& a,
                             cudaStream_t st)
 {
     switch (log_n) {
-        case 4: return col_dispatch_n<4>(nf, fast, fuse_foam, a, st);
-        case 5: return col_dispatch_n<5>(nf, fast, fuse_foam, a, st);
-        case 6: return col_dispatch_n<6>(nf, fast, fuse_foam, a, st);
-        case 7: return col_dispatch_n<7>(nf, fast, fuse_foam, a, st);
-        case 8: return col_dispatch_n<8>(nf, fast, fuse_foam, a, st);
-        case 9: return col_dispatch_n<9>(nf, fast, fuse_foam, a, st);
-        case 10: return col_dispatch_n<10>(nf, fast, fuse_foam, a, st);
+        case 4: return col_dispatch_n<4>(nf, ar, fuse_foam, a, st);
+        case 5: return col_dispatch_n<5>(nf, ar, fuse_foam, a, st);
+        case 6: return col_dispatch_n<6>(nf, ar, fuse_foam, a, st);
+        case 7: return col_dispatch_n<7>(nf, ar, fuse_foam, a, st);
+        case 8: return col_dispatch_n<8>(nf, ar, fuse_foam, a, st);
+        case 9: return col_dispatch_n<9>(nf, ar, fuse_foam, a, st);
+        case 10: return col_dispatch_n<10>(nf, ar, fuse_foam, a, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -29,6 +29,8 @@
 #include "ocean_device.cuh"
 #include "spectrum.h"
 
+#include <type_traits>
+
 namespace ocean_b200 {
 namespace {
 
@@ -51,7 +53,7 @@ struct Large {
     static_assert(COL_SMEM <= 227 * 1024, "a column CTA fits in shared memory");
 };
 
-template <int LOG_N, int NF, bool FAST>
+template <int LOG_N, int NF, int AR>
 __global__ void __launch_bounds__(Large<LOG_N>::ROW_T, Large<LOG_N>::ROW_BLOCKS)
 large_row_kernel(FrameArgs a)
 {
@@ -109,7 +111,7 @@ large_row_kernel(FrameArgs a)
                 }
             }
             __syncthreads();
-            fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);  // ends with a CTA barrier
+            fft_sequence<LOG_N, G, AR>(data + (tid / G) * SEQ, tws, tid % G);  // ends with a CTA barrier
             float2* out = inter + static_cast<size_t>(2 * g) * cells + row;
             for (int i = tid; i < 2 * N; i += NT) {
                 const int s = i >> LOG_N, x = i & (N - 1);
@@ -119,7 +121,7 @@ large_row_kernel(FrameArgs a)
     }
 }
 
-template <int LOG_N, bool FAST>
+template <int LOG_N, int AR>
 __global__ void __launch_bounds__(Large<LOG_N>::COL_T) large_col_kernel(FrameArgs a, int nf)
 {
     using S = Large<LOG_N>;
@@ -149,7 +151,7 @@ __global__ void __launch_bounds__(Large<LOG_N>::COL_T) large_col_kernel(FrameArg
             data[(2 * h + 1) * SEQ + pad_idx(y)] = make_float2(v.z, v.w);
         }
         __syncthreads();
-        fft_sequence<LOG_N, G, FAST>(data + (tid / G) * SEQ, tws, tid % G);  // ends with a CTA barrier
+        fft_sequence<LOG_N, G, AR>(data + (tid / G) * SEQ, tws, tid % G);  // ends with a CTA barrier
         for (int i = tid; i < N * H; i += NT) {
             const int y = i / H, h = i % H;
             const float2 u = data[(2 * h) * SEQ + pad_idx(y)];
@@ -190,11 +192,11 @@ __global__ void __launch_bounds__(256) large_finalize_kernel(FrameArgs a, int lo
     }
 }
 
-template <int LOG_N, int NF, bool FAST>
+template <int LOG_N, int NF, int AR>
 cudaError_t rows_launch(const FrameArgs& a, cudaStream_t st)
 {
     using S = Large<LOG_N>;
-    auto k = large_row_kernel<LOG_N, NF, FAST>;
+    auto k = large_row_kernel<LOG_N, NF, AR>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(S::ROW_SMEM));
     if (e != cudaSuccess) return e;
@@ -204,11 +206,11 @@ cudaError_t rows_launch(const FrameArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-template <int LOG_N, bool FAST>
+template <int LOG_N, int AR>
 cudaError_t cols_launch(int nf, const FrameArgs& a, cudaStream_t st)
 {
     using S = Large<LOG_N>;
-    auto k = large_col_kernel<LOG_N, FAST>;
+    auto k = large_col_kernel<LOG_N, AR>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(S::COL_SMEM));
     if (e != cudaSuccess) return e;
@@ -218,33 +220,48 @@ cudaError_t cols_launch(int nf, const FrameArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-template <int LOG_N>
-cudaError_t rows_n(int nf, bool fast, const FrameArgs& a, cudaStream_t st)
+// The arithmetic `ar` (kArExact, kArFast, kArPrecise) as a compile-time
+// constant for `fn`.
+template <typename Fn>
+cudaError_t with_arith(int ar, Fn&& fn)
 {
-    if (nf == 4) return fast ? rows_launch<LOG_N, 4, true>(a, st) : rows_launch<LOG_N, 4, false>(a, st);
-    return fast ? rows_launch<LOG_N, 6, true>(a, st) : rows_launch<LOG_N, 6, false>(a, st);
+    if (ar == kArFast) return fn(std::integral_constant<int, kArFast>{});
+    if (ar == kArPrecise) return fn(std::integral_constant<int, kArPrecise>{});
+    return fn(std::integral_constant<int, kArExact>{});
+}
+
+template <int LOG_N>
+cudaError_t rows_n(int nf, int ar, const FrameArgs& a, cudaStream_t st)
+{
+    return with_arith(ar, [&](auto A) {
+        constexpr int AR = decltype(A)::value;
+        return nf == 4 ? rows_launch<LOG_N, 4, AR>(a, st) : rows_launch<LOG_N, 6, AR>(a, st);
+    });
 }
 
 }  // namespace
 
-cudaError_t launch_large_rows(int log_n, int nf, bool fast, const FrameArgs& a, cudaStream_t st)
+cudaError_t launch_large_rows(int log_n, int nf, int ar, const FrameArgs& a, cudaStream_t st)
 {
     if (nf != 4 && nf != 6) return cudaErrorInvalidValue;
     switch (log_n) {
-        case 11: return rows_n<11>(nf, fast, a, st);
-        case 12: return rows_n<12>(nf, fast, a, st);
+        case 11: return rows_n<11>(nf, ar, a, st);
+        case 12: return rows_n<12>(nf, ar, a, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_large_cols(int log_n, int nf, bool fast, const FrameArgs& a, cudaStream_t st)
+cudaError_t launch_large_cols(int log_n, int nf, int ar, const FrameArgs& a, cudaStream_t st)
 {
     if (nf != 4 && nf != 6) return cudaErrorInvalidValue;
-    switch (log_n) {
-        case 11: return fast ? cols_launch<11, true>(nf, a, st) : cols_launch<11, false>(nf, a, st);
-        case 12: return fast ? cols_launch<12, true>(nf, a, st) : cols_launch<12, false>(nf, a, st);
-        default: return cudaErrorInvalidValue;
-    }
+    return with_arith(ar, [&](auto A) {
+        constexpr int AR = decltype(A)::value;
+        switch (log_n) {
+            case 11: return cols_launch<11, AR>(nf, a, st);
+            case 12: return cols_launch<12, AR>(nf, a, st);
+            default: return cudaErrorInvalidValue;
+        }
+    });
 }
 
 cudaError_t launch_large_finalize(int log_n, int nf, bool fuse_foam, const FrameArgs& a, cudaStream_t st)

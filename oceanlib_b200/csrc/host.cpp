@@ -669,12 +669,12 @@ private:
 
     void run_row(const FrameArgs& a, cudaStream_t st)
     {
-        const bool fast = form_ == OCEAN_FFT_FAST;
+        const int ar = arith_of_form(form_);
         if (large()) {
-            timed(0, st, [&] { check(launch_large_rows(log_n_, nf_, fast, a, st), "row pass"); });
+            timed(0, st, [&] { check(launch_large_rows(log_n_, nf_, ar, a, st), "row pass"); });
             return;
         }
-        timed(0, st, [&] { check(launch_row_pass(log_n_, nf_, fast, a, st), "row pass"); });
+        timed(0, st, [&] { check(launch_row_pass(log_n_, nf_, ar, a, st), "row pass"); });
     }
 
     // One persistent launch for oceans [base, base + k) (csrc/frame.cu
@@ -706,13 +706,13 @@ private:
 
     void run_col(const FrameArgs& a, cudaStream_t st, bool foam)
     {
-        const bool fast = form_ == OCEAN_FFT_FAST;
+        const int ar = arith_of_form(form_);
         if (large()) {
-            timed(1, st, [&] { check(launch_large_cols(log_n_, nf_, fast, a, st), "column pass"); });
+            timed(1, st, [&] { check(launch_large_cols(log_n_, nf_, ar, a, st), "column pass"); });
             timed(1, st, [&] { check(launch_large_finalize(log_n_, nf_, foam, a, st), "finalize"); });
             return;
         }
-        timed(1, st, [&] { check(launch_col_pass(log_n_, nf_, fast, foam, a, st), "column pass"); });
+        timed(1, st, [&] { check(launch_col_pass(log_n_, nf_, ar, foam, a, st), "column pass"); });
     }
     static constexpr double kInvTwoPi = 0.159154943091895335769;
 
@@ -1171,7 +1171,8 @@ public:
     {
         if (levels == nullptr || count == 0) throw std::invalid_argument("no levels");
         if (form < 0) form = g_form.load();
-        if (form != OCEAN_FFT_EXACT && form != OCEAN_FFT_FAST && form != OCEAN_FFT_TENSOR)
+        if (form != OCEAN_FFT_EXACT && form != OCEAN_FFT_FAST && form != OCEAN_FFT_TENSOR &&
+            form != OCEAN_FFT_PRECISE)
             throw std::invalid_argument("fft form");
         if (count > static_cast<uint32_t>(kMaxCascadeLevels)) throw std::invalid_argument("too many levels");
         std::vector<ocean_desc> descs(count);
@@ -1313,7 +1314,8 @@ public:
     Ensemble(const ocean_desc* descs, uint32_t count, bool tune, int form = -1)
     {
         if (form < 0) form = g_form.load();
-        if (form != OCEAN_FFT_EXACT && form != OCEAN_FFT_FAST && form != OCEAN_FFT_TENSOR)
+        if (form != OCEAN_FFT_EXACT && form != OCEAN_FFT_FAST && form != OCEAN_FFT_TENSOR &&
+            form != OCEAN_FFT_PRECISE)
             throw std::invalid_argument("fft form");
         if (descs == nullptr || count == 0) throw std::invalid_argument("no oceans");
         std::vector<ocean_desc> all(count);
@@ -1386,7 +1388,7 @@ public:
             check(cudaGetDevice(&dev), "cudaGetDevice");
             check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
             const int per_sm =
-                mixed_blocks_per_sm(batches_[0]->nf(), batches_[0]->form() == OCEAN_FFT_FAST);
+                mixed_blocks_per_sm(batches_[0]->nf(), arith_of_form(batches_[0]->form()));
             if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "mixed frame occupancy");
             mix_grid_ = per_sm * sms;
         }
@@ -1569,7 +1571,7 @@ private:
         m.defer = mix_defer_ ? 1 : 0;
         check(cudaMemsetAsync(mix_words_.p, 0, sizeof(unsigned), st), "ticket reset");
         const int grid = static_cast<int>(std::min<uint64_t>(static_cast<uint64_t>(mix_grid_), first));
-        check(launch_mixed_frame(batches_[0]->nf(), batches_[0]->form() == OCEAN_FFT_FAST, m, grid, st),
+        check(launch_mixed_frame(batches_[0]->nf(), arith_of_form(batches_[0]->form()), m, grid, st),
               "mixed frame kernel");
     }
 
@@ -1938,6 +1940,9 @@ const char* ocean_force_simd_level(const char* name)
             } else if (s == "fast") {
                 ocean_b200::g_level_name = s;
                 ocean_b200::g_form = OCEAN_FFT_FAST;
+            } else if (s == "precise") {
+                ocean_b200::g_level_name = s;
+                ocean_b200::g_form = OCEAN_FFT_PRECISE;
             }
         }
     }
@@ -1999,7 +2004,7 @@ ocean_batch* ocean_batch_create(const ocean_batch_desc* desc, ocean_status* out_
     ocean_status st = OCEAN_OK;
     if (desc == nullptr || desc->struct_size != sizeof(ocean_batch_desc) ||
         (desc->fft_form != OCEAN_FFT_EXACT && desc->fft_form != OCEAN_FFT_FAST &&
-         desc->fft_form != OCEAN_FFT_TENSOR) ||
+         desc->fft_form != OCEAN_FFT_TENSOR && desc->fft_form != OCEAN_FFT_PRECISE) ||
         (desc->schedule != OCEAN_SCHEDULE_PERSISTENT && desc->schedule != OCEAN_SCHEDULE_CHUNKED) ||
         (desc->fft_form == OCEAN_FFT_TENSOR && desc->schedule != OCEAN_SCHEDULE_PERSISTENT)) {
         st = OCEAN_ERROR_INVALID_ARG;

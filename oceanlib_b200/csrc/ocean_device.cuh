@@ -74,24 +74,49 @@ __device__ __forceinline__ int bitrev(int s)
     return o;
 }
 
+// The transforms' arithmetic, a template argument AR of every stage block:
+//   kArExact    the reference's operations in FP32, each multiply and add
+//               rounded (bit-identical to src/core/fft_kernel_scalar.cpp);
+//   kArFast     the same dataflow with fused multiply-adds;
+//   kArPrecise  each stage block's butterflies in FP64 on the values held in
+//               registers, rounded to FP32 once when the block stores them:
+//               three roundings per point and dimension at N = 512 instead
+//               of nine stages of them (within 1.5e-6 of FP64 on every
+//               channel of a 512^2 frame, where the FP32 forms reach 3.5e-6).
+constexpr int kArExact = 0;
+constexpr int kArFast = 1;
+constexpr int kArPrecise = 2;
+
 // Butterfly of the radix-2 Stockham stage (reference:
 // src/core/fft_kernel_scalar.cpp:19-33): a' = a + b, b' = (a - b) * w.
-// EXACT keeps the reference's separate multiplies and adds; FAST fuses.
-template <bool FAST>
+// kArExact keeps the reference's separate multiplies and adds; kArFast fuses.
+template <int AR>
 __device__ __forceinline__ void butterfly(float2& a, float2& b, float2 w)
 {
+    static_assert(AR != kArPrecise, "the precise form works on doubles (butterfly_f64)");
     const float ar = a.x, ai = a.y, br = b.x, bi = b.y;
     a.x = ar + br;
     a.y = ai + bi;
     const float dr = ar - br;
     const float di = ai - bi;
-    if (FAST) {
+    if constexpr (AR == kArFast) {
         b.x = __fmaf_rn(dr, w.x, -(di * w.y));
         b.y = __fmaf_rn(dr, w.y, di * w.x);
     } else {
         b.x = dr * w.x - di * w.y;
         b.y = dr * w.y + di * w.x;
     }
+}
+
+// The same butterfly in FP64 (kArPrecise), the twiddle widened from FP32.
+__device__ __forceinline__ void butterfly_f64(double& ar, double& ai, double& br, double& bi, float2 w)
+{
+    const double wx = w.x, wy = w.y;
+    const double dr = ar - br, di = ai - bi;
+    ar += br;
+    ai += bi;
+    br = fma(dr, wx, -(di * wy));
+    bi = fma(dr, wy, di * wx);
 }
 
 // ---------------------------------------------------------------------------
@@ -123,7 +148,7 @@ __device__ __forceinline__ void group_sync()
     }
 }
 
-template <int LOG_N, int G, int L0, bool FAST>
+template <int LOG_N, int G, int L0, int AR>
 struct StageBlock {
     static constexpr int N = 1 << LOG_N;
     static constexpr int E = N / G;                  // values per lane
@@ -147,17 +172,38 @@ struct StageBlock {
         for (int k = 0; k < C; ++k) {
             const int c = lane + G * k;
             const int P = c >> L0;
+            if constexpr (AR == kArPrecise) {
+                double xr[RR], xi[RR];
 #pragma unroll
-            for (int s = 0; s < r; ++s) {
-                const int half = RR >> (s + 1);
-                const int l = L0 + s;
-                const float2* twl = tw + (N - (N >> l));
+                for (int t = 0; t < RR; ++t) {
+                    xr[t] = v[k][t].x;
+                    xi[t] = v[k][t].y;
+                }
 #pragma unroll
-                for (int S = 0; S < RR; ++S) {
-                    if (S & half) continue;
-                    const int Rk = S & (half - 1);
-                    const float2 wv = twl[(Rk << w) | P];
-                    butterfly<FAST>(v[k][S], v[k][S + half], wv);
+                for (int s = 0; s < r; ++s) {
+                    const int half = RR >> (s + 1);
+                    const float2* twl = tw + (N - (N >> (L0 + s)));
+#pragma unroll
+                    for (int S = 0; S < RR; ++S) {
+                        if (S & half) continue;
+                        butterfly_f64(xr[S], xi[S], xr[S + half], xi[S + half], twl[((S & (half - 1)) << w) | P]);
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < RR; ++t) v[k][t] = make_float2(__double2float_rn(xr[t]), __double2float_rn(xi[t]));
+            } else {
+#pragma unroll
+                for (int s = 0; s < r; ++s) {
+                    const int half = RR >> (s + 1);
+                    const int l = L0 + s;
+                    const float2* twl = tw + (N - (N >> l));
+#pragma unroll
+                    for (int S = 0; S < RR; ++S) {
+                        if (S & half) continue;
+                        const int Rk = S & (half - 1);
+                        const float2 wv = twl[(Rk << w) | P];
+                        butterfly<AR>(v[k][S], v[k][S + half], wv);
+                    }
                 }
             }
         }
@@ -173,15 +219,15 @@ struct StageBlock {
             }
         }
         group_sync<G>();
-        if constexpr (L0 + r < LOG_N) StageBlock<LOG_N, G, L0 + r, FAST>::run(seq, tw, lane);
+        if constexpr (L0 + r < LOG_N) StageBlock<LOG_N, G, L0 + r, AR>::run(seq, tw, lane);
     }
 };
 
 // The complete unnormalised inverse transform of one sequence.
-template <int LOG_N, int G, bool FAST>
+template <int LOG_N, int G, int AR>
 __device__ __forceinline__ void fft_sequence(float2* seq, const float2* tw, int lane)
 {
-    StageBlock<LOG_N, G, 0, FAST>::run(seq, tw, lane);
+    StageBlock<LOG_N, G, 0, AR>::run(seq, tw, lane);
 }
 
 // Lanes per sequence: each lane keeps 16 values (a 4-stage block) where the
@@ -253,15 +299,15 @@ __device__ __forceinline__ void px_unpack(f32x2 v, float& lo, float& hi)
 // multiply into a packed add or subtract that consumes it (one fused
 // multiply-add, rounded once) even with contraction disabled, so the four
 // products are packed multiplies and the two sums that combine them are
-// scalar adds of their halves. FAST fuses as `butterfly<true>` does.
-template <bool FAST>
+// scalar adds of their halves. kArFast fuses as `butterfly<kArFast>` does.
+template <int AR>
 __device__ __forceinline__ void butterfly_pair(f32x2& ar, f32x2& ai, f32x2& br, f32x2& bi, f32x2 wx, f32x2 wy)
 {
     const f32x2 dr = px_sub(ar, br);
     const f32x2 di = px_sub(ai, bi);
     ar = px_add(ar, br);
     ai = px_add(ai, bi);
-    if (FAST) {
+    if constexpr (AR == kArFast) {
         const f32x2 nwy = wy ^ 0x8000000080000000ull;
         br = px_fma(dr, wx, px_mul(di, nwy));
         bi = px_fma(dr, wy, px_mul(di, wx));
@@ -290,7 +336,7 @@ __device__ __forceinline__ void pair_sync(int id)
 
 // StageBlock's r stages on a pair of sequences (same index algebra, lane
 // ownership and twiddles; `tw` is the same float2 table as StageBlock's).
-template <int LOG_N, int G2, int L0, bool FAST>
+template <int LOG_N, int G2, int L0, int AR>
 struct PairBlock {
     static constexpr int N = 1 << LOG_N;
     static constexpr int E = N / G2;
@@ -314,6 +360,47 @@ struct PairBlock {
             }
         }
         pair_sync<G2>(bar_id);
+        if constexpr (AR == kArPrecise) {
+            // The pair's two sequences one after the other, each as doubles
+            // (8 complex values: 32 registers), rounded back into its half
+            // of the packed registers.
+#pragma unroll
+            for (int k = 0; k < C; ++k) {
+                const int c = lane + G2 * k;
+                const int P = c >> L0;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    double xr[RR], xi[RR];
+#pragma unroll
+                    for (int t = 0; t < RR; ++t) {
+                        float r0, r1, i0, i1;
+                        px_unpack(re[k][t], r0, r1);
+                        px_unpack(im[k][t], i0, i1);
+                        xr[t] = h ? r1 : r0;
+                        xi[t] = h ? i1 : i0;
+                    }
+#pragma unroll
+                    for (int s = 0; s < r; ++s) {
+                        const int half = RR >> (s + 1);
+                        const float2* twl = tw + (N - (N >> (L0 + s)));
+#pragma unroll
+                        for (int S = 0; S < RR; ++S) {
+                            if (S & half) continue;
+                            butterfly_f64(xr[S], xi[S], xr[S + half], xi[S + half], twl[((S & (half - 1)) << w) | P]);
+                        }
+                    }
+#pragma unroll
+                    for (int t = 0; t < RR; ++t) {
+                        float r0, r1, i0, i1;
+                        px_unpack(re[k][t], r0, r1);
+                        px_unpack(im[k][t], i0, i1);
+                        const float nr = __double2float_rn(xr[t]), ni = __double2float_rn(xi[t]);
+                        re[k][t] = h ? px_pack(r0, nr) : px_pack(nr, r1);
+                        im[k][t] = h ? px_pack(i0, ni) : px_pack(ni, i1);
+                    }
+                }
+            }
+        } else {
 #pragma unroll
         for (int k = 0; k < C; ++k) {
             const int c = lane + G2 * k;
@@ -331,10 +418,11 @@ struct PairBlock {
                     // f32x2 in registers (a 16-byte (wx, wx, wy, wy) table
                     // entry costs twice the shared-memory wavefronts).
                     const float2 wv = twl[(Rk << w) | P];
-                    butterfly_pair<FAST>(re[k][S], im[k][S], re[k][S + half], im[k][S + half], px_pack(wv.x, wv.x),
-                                         px_pack(wv.y, wv.y));
+                    butterfly_pair<AR>(re[k][S], im[k][S], re[k][S + half], im[k][S + half], px_pack(wv.x, wv.x),
+                                       px_pack(wv.y, wv.y));
                 }
             }
+        }
         }
 #pragma unroll
         for (int k = 0; k < C; ++k) {
@@ -348,15 +436,15 @@ struct PairBlock {
             }
         }
         pair_sync<G2>(bar_id);
-        if constexpr (L0 + r < LOG_N) PairBlock<LOG_N, G2, L0 + r, FAST>::run(seq, tw, lane, bar_id);
+        if constexpr (L0 + r < LOG_N) PairBlock<LOG_N, G2, L0 + r, AR>::run(seq, tw, lane, bar_id);
     }
 };
 
 // The unnormalised inverse transforms of the pair at `seq`.
-template <int LOG_N, int G2, bool FAST>
+template <int LOG_N, int G2, int AR>
 __device__ __forceinline__ void fft_pair(ulonglong2* seq, const float2* tw, int lane, int bar_id)
 {
-    PairBlock<LOG_N, G2, 0, FAST>::run(seq, tw, lane, bar_id);
+    PairBlock<LOG_N, G2, 0, AR>::run(seq, tw, lane, bar_id);
 }
 
 

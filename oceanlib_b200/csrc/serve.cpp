@@ -236,7 +236,7 @@ public:
         if (desc_.max_batch_requests == 0) throw std::invalid_argument("max_batch_requests");
         if (desc_.max_batch_points == 0 || desc_.max_query_points == 0) throw std::invalid_argument("points");
         if (desc_.fft_form != OCEAN_FFT_EXACT && desc_.fft_form != OCEAN_FFT_FAST &&
-            desc_.fft_form != OCEAN_FFT_TENSOR)
+            desc_.fft_form != OCEAN_FFT_TENSOR && desc_.fft_form != OCEAN_FFT_PRECISE)
             throw std::invalid_argument("fft_form");
         check(cudaGetDevice(&device_), "cudaGetDevice");
         check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_), "SM count");
@@ -967,15 +967,15 @@ private:
             m.wait_ns = 1000000000ull;
             const int nf = oparts[0].k->nf;
             m.defer = nf == 6 ? 1 : 0;
-            const bool fast = desc_.fft_form == OCEAN_FFT_FAST;
+            const int ar = arith_of_form(desc_.fft_form);
             int& grid = mix_grid_[nf == 6 ? 1 : 0];
             if (grid == 0) {
-                const int per_sm = mixed_blocks_per_sm(nf, fast);
+                const int per_sm = mixed_blocks_per_sm(nf, ar);
                 if (per_sm <= 0) throw DeviceError(cudaErrorInvalidConfiguration, "mixed frame occupancy");
                 grid = per_sm * sms_;
             }
             check(cudaMemsetAsync(mix_ticket_.p, 0, sizeof(unsigned), stream_), "ticket reset");
-            check(launch_mixed_frame(nf, fast, m, static_cast<int>(std::min<uint64_t>(grid, first)), stream_),
+            check(launch_mixed_frame(nf, ar, m, static_cast<int>(std::min<uint64_t>(grid, first)), stream_),
                   "mixed frame kernel");
             ++kernels;
         }

@@ -85,6 +85,12 @@ struct QueueArgs {
     int32_t defer;
 };
 
+// The transforms' arithmetic of an ocean_fft_form, for the `ar` arguments
+// below: 0 the reference's FP32 operations, 1 fused multiply-adds, 2 FP64
+// within each register stage block (the precise form). The tensor-core form
+// (2) has its own engine and passes through launch_frame's `form`.
+inline int arith_of_form(int form) { return form == 1 ? 1 : (form == 3 ? 2 : 0); }
+
 // One persistent launch for the whole frame of `q.count` oceans (foam fused
 // when fuse_foam). `form` is an ocean_fft_form (the tensor form: N = 64 to 512).
 // `grid` = CTAs to launch (0 = one wave of resident CTAs).
@@ -131,15 +137,15 @@ struct MixedArgs {
 };
 bool mixed_size_ok(int log_n);
 uint32_t mixed_tasks(int log_n, int count);
-int mixed_blocks_per_sm(int nf, bool fast);
-cudaError_t launch_mixed_frame(int nf, bool fast, const MixedArgs& m, int grid, cudaStream_t stream);
+int mixed_blocks_per_sm(int nf, int ar);
+cudaError_t launch_mixed_frame(int nf, int ar, const MixedArgs& m, int grid, cudaStream_t stream);
 
 // Row pass (evolve + row FFTs) and column pass (column FFTs + finalize, with
 // an optional fused foam substep) for `args.chunk` oceans starting at
 // args.ocean_base. log_n in [4, 10]; nf is 4 or 6 complex fields.
-cudaError_t launch_row_pass(int log_n, int nf, bool fast, const FrameArgs& args,
+cudaError_t launch_row_pass(int log_n, int nf, int ar, const FrameArgs& args,
                             cudaStream_t stream);
-cudaError_t launch_col_pass(int log_n, int nf, bool fast, bool fuse_foam,
+cudaError_t launch_col_pass(int log_n, int nf, int ar, bool fuse_foam,
                             const FrameArgs& args, cudaStream_t stream);
 
 // The frame at N = 2048 and 4096 (log_n 11, 12; frame_large.cu), for
@@ -147,8 +153,8 @@ cudaError_t launch_col_pass(int log_n, int nf, bool fast, bool fuse_foam,
 // row FFTs), column FFTs in place, finalize (+ the first foam substep when
 // fuse_foam; nf = 6). The intermediate is field-major: field f of chunk ocean
 // o at args.inter + (o * nf + f) * N * N. args.table must be null.
-cudaError_t launch_large_rows(int log_n, int nf, bool fast, const FrameArgs& args, cudaStream_t stream);
-cudaError_t launch_large_cols(int log_n, int nf, bool fast, const FrameArgs& args, cudaStream_t stream);
+cudaError_t launch_large_rows(int log_n, int nf, int ar, const FrameArgs& args, cudaStream_t stream);
+cudaError_t launch_large_cols(int log_n, int nf, int ar, const FrameArgs& args, cudaStream_t stream);
 cudaError_t launch_large_finalize(int log_n, int nf, bool fuse_foam, const FrameArgs& args,
                                   cudaStream_t stream);
 

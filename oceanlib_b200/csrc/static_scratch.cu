@@ -196,8 +196,8 @@ extern "C" OCEAN_API ocean_status ocean_frame_static_scratch(
     a.ocean_base = 0;
     a.chunk = 1;
     a.error = reinterpret_cast<unsigned*>(scratch + offsetof(Header, status));
-    if (ocean_b200::launch_row_pass(log_n, nf, false, a, st) != cudaSuccess) return OCEAN_ERROR_DEVICE;
-    if (ocean_b200::launch_col_pass(log_n, nf, false, false, a, st) != cudaSuccess)
+    if (ocean_b200::launch_row_pass(log_n, nf, 0, a, st) != cudaSuccess) return OCEAN_ERROR_DEVICE;
+    if (ocean_b200::launch_col_pass(log_n, nf, 0, false, a, st) != cudaSuccess)
         return OCEAN_ERROR_DEVICE;
     return OCEAN_OK;
 }
