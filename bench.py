@@ -460,6 +460,13 @@ def bench_ensemble(torch, frames: int = 30):
                                "equiv_512sq_updates_per_s": cells / (512 * 512) * 1000.0 / ms_tc,
                                "schedule": ens.schedule}
     ens.close()
+    # And in the precise form (every size, FP64 stage blocks), autotuned.
+    ens = ob.OceanEnsemble(descs, autotune=True, form=abi.OCEAN_FFT_PRECISE)
+    ms_pr, _ = timed(True)
+    res["precise_form"] = {"ms_per_frame": ms_pr, "ocean_updates_per_s": len(descs) * 1000.0 / ms_pr,
+                           "equiv_512sq_updates_per_s": cells / (512 * 512) * 1000.0 / ms_pr,
+                           "schedule": ens.schedule}
+    ens.close()
     return res
 
 
