@@ -157,6 +157,7 @@ def test_force_simd_level_semantics():
     assert ob.force_simd_level("SCALAR") == "scalar"
     assert ob.force_simd_level("not-a-real-level") == "scalar"
     assert ob.force_simd_level("fast") == "fast"
+    assert ob.force_simd_level("precise") == "precise"  # the FP64-block form
     assert ob.force_simd_level(None) == "sm_100a"
 
 
