@@ -241,3 +241,23 @@ def test_tensor_form_sessions_match_tensor_form_batches():
     with pytest.raises((ValueError, ob.OceanError)):
         srv.open_session(ob.OceanDesc(size=1024, seed=3), field)
     srv.close()
+
+
+def test_precise_form_sessions_match_precise_form_batches():
+    # The serving loop in the precise form (FP64 stage blocks): each
+    # session's ocean, batched with sessions of other sizes in one launch,
+    # equals a precise-form batch of that ocean alone, bit for bit.
+    oceans, field = W.serving_sessions(6)
+    sc = scripts(6, frames=2)
+    mix, st = run_server(oceans, field, list(range(6)), sc, order_seed=7, form=abi.OCEAN_FFT_PRECISE)
+    assert st["requests_failed"] == 0 and st["updates_completed"] == 6 * 2
+    for k in range(6):
+        t_last = [item[1] for item in sc[k] if item[0] == "update"][-1]
+        n = oceans[k].size
+        b = ob.OceanBatch([oceans[k]], form=abi.OCEAN_FFT_PRECISE)
+        d = np.empty((n * n, 4), np.float32)
+        nrm = np.empty_like(d)
+        b.update_host([t_last], 0.0, d, nrm)
+        b.close()
+        assert np.array_equal(bits(mix[k][1]), bits(d.reshape(mix[k][1].shape))), n
+        assert np.array_equal(bits(mix[k][2]), bits(nrm.reshape(mix[k][2].shape))), n
