@@ -11,11 +11,13 @@
 //   step     - h_new = c1 * (2h - c2 h_old - g dt^2 (G * h)), the (2P+1)^2
 //              convolution accumulated j-outer / i-inner in one float, no FMA,
 //              flushed below 1e-30 (src/core/iwave_step.cpp:7-54). Shared-memory
-//              tile with a P-cell halo; each thread keeps four vertically
-//              adjacent outputs, so every loaded value feeds up to four
-//              accumulators while each accumulator still sees its taps in the
-//              reference order. The taps travel as kernel parameters (constant
-//              bank), so each multiply takes its tap as an operand, no load.
+//              tile with a P-cell halo; each thread keeps R vertically
+//              adjacent outputs (R = 4 for batches of fields, 2 when one
+//              launch has too few tiles to fill the SMs), so every loaded
+//              value feeds up to R accumulators while each accumulator still
+//              sees its taps in the reference order. The taps travel as
+//              kernel parameters (constant bank), so each multiply takes its
+//              tap as an operand, no load.
 // After the substeps, finalize writes (eta, d/dx, d/dz, d/dt)
 // (src/core/iwave_step.cpp:93-124). Compiled with -fmad=false.
 #include "iwave.h"
@@ -27,9 +29,9 @@ namespace {
 constexpr float kFlush = 1.0e-30f;
 constexpr int kTileX = 32;
 constexpr int kTileY = 32;
-constexpr int kRowsPerThread = 4;
 
-template <int P>
+// kRowsPerThread outputs per thread down a column of the 32 x 32 tile.
+template <int P, int kRowsPerThread>
 __global__ void __launch_bounds__(kTileX * (kTileY / kRowsPerThread))
 iwave_step_kernel(const IWaveField* __restrict__ fields, IWaveTaps taps)
 {
@@ -345,13 +347,25 @@ __global__ void combine_kernel(const SurfaceEx* __restrict__ ocean_s, const floa
     out[i] = s;
 }
 
+// Launches with fewer tiles than kFewTiles (a single field up to 512^2, or
+// a few small ones) take two outputs per thread: 16 warps per tile instead
+// of 8, so that the tile loads of twice as many warps are in flight on the
+// SMs the launch reaches. Larger launches fill every SM several times over
+// and keep four outputs per thread (fewer shared-memory loads per tap).
+// Every cell sees the same taps in the same order either way.
+constexpr long kFewTiles = 2 * 148;
+
 template <int P>
 cudaError_t step_launch(const IWaveField* fields, int count, int max_n, const IWaveTaps& taps,
                         cudaStream_t st)
 {
     dim3 grid((max_n + kTileX - 1) / kTileX, (max_n + kTileY - 1) / kTileY, count);
-    dim3 block(kTileX, kTileY / kRowsPerThread);
-    iwave_step_kernel<P><<<grid, block, 0, st>>>(fields, taps);
+    const long tiles = static_cast<long>(grid.x) * grid.y * grid.z;
+    if (tiles < kFewTiles) {
+        iwave_step_kernel<P, 2><<<grid, dim3(kTileX, kTileY / 2), 0, st>>>(fields, taps);
+    } else {
+        iwave_step_kernel<P, 4><<<grid, dim3(kTileX, kTileY / 4), 0, st>>>(fields, taps);
+    }
     return cudaGetLastError();
 }
 
