@@ -407,14 +407,32 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
             return h0 + static_cast<size_t>(row) * N;
         });
     }
-    constexpr int CELLS = ROWS * N;
-    constexpr int ITER = (CELLS + NT - 1) / NT;
+    // HALVES: the paired FP32 plan with two rows, where row jr's Q field
+    // pairs are worked by threads [jr * HT, (jr + 1) * HT): each row's warps
+    // evolve, transform and store their own row and meet on a named barrier
+    // (ids 8 and 9; the pair barriers take 1 + pair) instead of the CTA's, so
+    // neither row waits on the other (the h0 rows both read are in place once
+    // each thread's mbarrier wait returns). Same bits; 64 x 512^2 with velocity
+    // and persistent foam 0.981 -> 0.977 ms a frame.
+    constexpr bool HALVES = PAIRED && !P::TC && ROWS == 2;
+    constexpr int HT = HALVES ? NT / 2 : NT;        // threads per barrier group
+    constexpr int CELLS = HALVES ? N : ROWS * N;    // cells per group
+    constexpr int ITER = (CELLS + HT - 1) / HT;
+    const int hh = HALVES ? tid / HT : 0;
+    const int lt = HALVES ? tid - hh * HT : tid;
+    auto group_bar = [&]() {
+        if constexpr (HALVES) {
+            asm volatile("bar.sync %0, %1;" ::"r"(8 + hh), "r"(HT) : "memory");
+        } else {
+            __syncthreads();
+        }
+    };
     float2 wk_of[ITER];
     float kx_of[ITER], kz_of[ITER];
 #pragma unroll
     for (int it = 0; it < ITER; ++it) {
-        const int cell = tid + it * NT;
-        if (cell < CELLS) {
+        const int cell = hh * N + lt + it * HT;
+        if (lt + it * HT < CELLS) {
             const int jr = cell >> LOG_N;
             const int x = cell & (N - 1);
             const int row = row_of(jr);
@@ -424,14 +442,14 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
         }
     }
     h0_rows_wait(h0_bar, h0_parity, error);
-    __syncthreads();
+    group_bar();
     publish_staged(pub, tid);
 
     // Evolve (src/core/evolve.cpp:28-121 and :123-184), one cell at a time.
 #pragma unroll
     for (int it = 0; it < ITER; ++it) {
-        const int cell = tid + it * NT;
-        if (cell >= CELLS) break;
+        const int cell = hh * N + lt + it * HT;
+        if (lt + it * HT >= CELLS) break;
         const int jr = cell >> LOG_N;
         const int x = cell & (N - 1);
         const float2 av = h0s[jr * N + x];
@@ -449,19 +467,19 @@ __device__ __forceinline__ void row_task(const FrameArgs& a, int ocean, int grou
                 base[q * SEQ4] = make_float4(pv[2 * q].x, pv[2 * q + 1].x, pv[2 * q].y, pv[2 * q + 1].y);
         }
     }
-    __syncthreads();
+    group_bar();
 
     transform_all<P, AR, ROWS * NF>(data, tws, tid, eng, error);
-    __syncthreads();
+    group_bar();
 
     // Write the rows cell-major: inter[row][x][f], NF/2 float4 per cell.
-    // NT is a multiple of Q, so each thread keeps one field pair fp and walks
+    // HT is a multiple of Q, so each thread keeps one field pair fp and walks
     // cells with a constant stride (no division in the loop).
-    constexpr int CSTEP = NT / Q;
+    constexpr int CSTEP = HT / Q;
     float4* inter = reinterpret_cast<float4*>(inter_slot);
-    const int fp = tid % Q;
+    const int fp = lt % Q;
 #pragma unroll 4
-    for (int cell = tid / Q; cell < ROWS * N; cell += CSTEP) {
+    for (int cell = hh * N + lt / Q; cell < (HALVES ? (hh + 1) * N : ROWS * N); cell += CSTEP) {
         const int jr = cell >> LOG_N;
         const int x = cell & (N - 1);
         const int row = row_of(jr);
@@ -761,11 +779,16 @@ frame_kernel(FrameArgs a, QueueArgs q)
     __shared__ unsigned s_ticket;
     __shared__ int s_ok;
     // Thread 0's queue state between tasks, kept in shared memory so that it
-    // takes no registers in the task code that every thread runs.
+    // takes no registers in the task code that every thread runs, except the
+    // ticket drawn one task ahead: its atomic's result lands in a register
+    // that thread 0 reads only at the next task, so the round trip to L2
+    // overlaps the current task instead of holding thread 0 (and with it the
+    // CTA's ticket barrier) until it returns. Same bits; 64 x 512^2 with
+    // velocity and persistent foam 0.999 -> 0.981 ms a frame.
     __shared__ unsigned* s_publish;   // the current task's counter, added after it (row tasks)
     __shared__ unsigned* s_pub[2];    // publish_staged's pair for the current task
-    __shared__ unsigned s_next;
-    __shared__ int s_have_next;
+    unsigned r_next = 0;              // thread 0: the ticket drawn one task ahead
+    int r_have_next = 0;
     __shared__ uint64_t h0_bar;   // the row tasks' h0 copies; phase k = k-th row task
     uint32_t h0_parity = 0;
 
@@ -818,15 +841,15 @@ frame_kernel(FrameArgs a, QueueArgs q)
     if (tid == 0) {
         h0_bar_init(&h0_bar);
         s_publish = nullptr;
-        s_next = atomicAdd(q.ticket, 1u);
-        s_have_next = 1;
+        r_next = atomicAdd(q.ticket, 1u);
+        r_have_next = 1;
     }
     while (true) {
         __syncthreads();  // previous task's writes issued; shared memory free
         if (tid == 0) {
             unsigned* prev = s_publish;
-            const unsigned t = s_have_next ? s_next : atomicAdd(q.ticket, 1u);
-            s_have_next = 0;
+            const unsigned t = r_have_next ? r_next : atomicAdd(q.ticket, 1u);
+            r_have_next = 0;
             int ok = 1;
             unsigned* publish = nullptr;
             unsigned* self = nullptr;
@@ -834,8 +857,8 @@ frame_kernel(FrameArgs a, QueueArgs q)
             unsigned need = 0;
             if (t < total) {
                 if (t + 2u * gridDim.x < total) {
-                    s_next = atomicAdd(q.ticket, 1u);
-                    s_have_next = 1;
+                    r_next = atomicAdd(q.ticket, 1u);
+                    r_have_next = 1;
                 }
                 bool row;
                 unsigned ocean, idx;
@@ -994,8 +1017,8 @@ __global__ void __launch_bounds__(64 * NF, 768 / (64 * NF)) mixed_frame_kernel(M
     __shared__ int s_ok, s_group, s_row, s_ocean, s_idx;
     __shared__ unsigned* s_publish;
     __shared__ unsigned* s_pub[2];
-    __shared__ unsigned s_next;
-    __shared__ int s_have_next;
+    unsigned r_next = 0;              // thread 0: the ticket drawn one task ahead (as frame_kernel)
+    int r_have_next = 0;
     __shared__ uint64_t h0_bar;
     // The group table in shared memory: tasks index it by a runtime group,
     // which on the kernel's parameters would take a copy per thread.
@@ -1024,8 +1047,8 @@ __global__ void __launch_bounds__(64 * NF, 768 / (64 * NF)) mixed_frame_kernel(M
     if (tid == 0) {
         h0_bar_init(&h0_bar);
         s_publish = nullptr;
-        s_next = atomicAdd(m.ticket, 1u);
-        s_have_next = 1;
+        r_next = atomicAdd(m.ticket, 1u);
+        r_have_next = 1;
     }
     // The persistent kernel's protocol (frame_kernel), with a group lookup:
     // take a ticket (one ahead far from the end), check the task's inputs,
@@ -1035,8 +1058,8 @@ __global__ void __launch_bounds__(64 * NF, 768 / (64 * NF)) mixed_frame_kernel(M
         __syncthreads();
         if (tid == 0) {
             unsigned* prev = s_publish;
-            const unsigned t = s_have_next ? s_next : atomicAdd(m.ticket, 1u);
-            s_have_next = 0;
+            const unsigned t = r_have_next ? r_next : atomicAdd(m.ticket, 1u);
+            r_have_next = 0;
             int ok = 1;
             unsigned* publish = nullptr;
             unsigned* self = nullptr;
@@ -1044,8 +1067,8 @@ __global__ void __launch_bounds__(64 * NF, 768 / (64 * NF)) mixed_frame_kernel(M
             unsigned need = 0;
             if (t < m.total) {
                 if (t + 2u * gridDim.x < m.total) {
-                    s_next = atomicAdd(m.ticket, 1u);
-                    s_have_next = 1;
+                    r_next = atomicAdd(m.ticket, 1u);
+                    r_have_next = 1;
                 }
                 int gi = m.groups - 1;
                 while (gi > 0 && t < m.g[gi].first) --gi;
